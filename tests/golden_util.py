@@ -1,0 +1,42 @@
+"""Helpers to turn a reference golden fixture into oracle inputs."""
+import ast
+import glob
+import os
+
+import numpy as np
+
+from oracle.htfeti_oracle import MeshArrays, Options
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+# rho * a hard-coded by the reference, Data.cpp:315-318
+REF_BODY_FORCE = np.array([0.0, 0.0, 98.10 * 2.0])
+
+
+def golden_paths():
+    return sorted(glob.glob(os.path.join(GOLDEN_DIR, "ref_*.npz")))
+
+
+def load(path):
+    g = np.load(path)
+    args = ast.literal_eval(str(g["args"]))
+    return g, args
+
+
+def mesh_from_golden(g, args, clusters=None):
+    """MeshArrays of the reference's own mesh.  Material id 0 gets
+    E * ratio_mat (Data.cpp:47-48); the material id is the IEEE remainder of
+    the subdomain index by 2 (Mesh.cpp:281)."""
+    nsub = int(g["nsub"])
+    E = float(args["young_modulus"])
+    ratio = float(args.get("ratio_mat", "1"))
+    part, mat = g["partition"], g["material"]
+    sub_E = np.array([E * ratio if mat[part == d][0] == 0 else E for d in range(nsub)])
+    nu = float(args.get("poissons_ratio", "0.3"))
+    sub_cluster = np.zeros(nsub, dtype=np.int64) if clusters is None else np.asarray(clusters)
+    return MeshArrays(g["points"], g["elements"], part, sub_cluster, sub_E, np.full(nsub, nu),
+                      g["dirichlet"], g["corner"], REF_BODY_FORCE.copy())
+
+
+def options_from_args(args, **kw):
+    return Options(typeBc=args["typeBc"], preconditioner=args["preconditioner"],
+                   eps_iter=float(args.get("eps_iter", "1e-8")), **kw)
