@@ -1,0 +1,65 @@
+// Device-side data layout of the HTFETI path (shared by the kernels and the
+// host engine).
+//
+// Per subdomain d (n local DOFs, nb of them touched by Bf = the "b set"):
+//   * local DOFs are permuted to [interior (nr) | b set (nb)], the b set
+//     padded with identity rows to nbp = 32*ceil(nb/32);
+//   * K_d is assembled densely (column-major, ld = N = nr + nbp), lower
+//     triangle, and factored in place: the interior columns are eliminated
+//     first, the trailing block then holds S_reg = K_bb - K_bi K_ii^{-1} K_ib;
+//   * F_d = (K_reg^{-1})_bb and the preconditioner block (S_d = S_reg - D_fix
+//     for Dirichlet, K_bb for lumped) are stored as packed lower-triangular
+//     32x32 tiles, tile (I,J) with J<=I at index I(I+1)/2+J, row-major inside
+//     the tile, diagonal tiles stored full;
+//   * b-space vectors (x_b, y_b) are concatenated with per-subdomain offsets
+//     xb_off (multiples of 32).
+#pragma once
+#include <cstdint>
+
+namespace htf {
+
+constexpr int TILE = 32;                  // packed tile edge
+constexpr int TILE_ELEMS = TILE * TILE;
+
+struct SubDev {
+    int n, nr, nb, nbp, nt;               // nt = nbp / 32
+    int N;                                // nr + nbp (dense leading dimension)
+    long long K_off;                      // dense factor (doubles)
+    long long T_off;                      // packed tiles: first tile index (F and S/Kbb share it)
+    long long X_off;                      // nbp x nbp scratch (L_bb^{-1}) during setup
+    int xb_off;                           // offset of the b block in b-space vectors
+    int nfull_off;                        // offset of the N-vector block in full vectors
+    int c;                                // Bc rows of this subdomain
+    int cluster;                          // cluster index
+    int alpha_pos;                        // index of alpha_d in the cluster coarse vector
+    long long V_off;                      // V = [F Bc_b^T, -R_b]: nbp x (c+6), col-major
+    int t_off;                            // offset of V^T x (c+6 values) in the t vector
+    int bcr_off;                          // offset of this subdomain's Bc row ids (c entries)
+    int bce_off;                          // Bc entries (CSR by compressed Bc row): ptr offset
+    long long R_off;                      // R in permuted local order, N x 6 (padded rows 0)
+    int fix[6];                           // fix DOFs (positions in permuted order)
+    double fix_diag[6];                   // original diagonal at the fix DOFs
+};
+
+struct ClusterDev {
+    int nlam_c, ngc;                      // ngc = nlam_c + 6*nsub
+    long long M_off;                      // M = (Ac^{-1}) restricted, ngc x ngc (col-major)
+    int gc_off;                           // offset in the concatenated coarse vectors
+    int gmap_off;                         // gather map: ptr array offset (ngc+1 entries)
+};
+
+// One 32-column step of the batched Cholesky for one subdomain.
+struct StepDesc {
+    int d;      // subdomain
+    int k;      // first column of the step
+    int nb;     // columns in the step (<= 32)
+};
+
+// PCPG state in device memory (one per load case).
+struct PcpgState {
+    double gPz, gPz_prev, wFw, norm0, rho, gamma, rel;
+    int it, done, max_iter, pad;
+    double eps;
+};
+
+}  // namespace htf

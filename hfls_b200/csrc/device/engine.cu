@@ -1,0 +1,1079 @@
+// Engine: GPU setup and PCPG of the HTFETI path.
+//   setup   Cluster::initialization (Cluster.cpp:21-360)
+//   pcpg    Cluster::pcpg + printVTK reconstruction (Cluster.cpp:1363-1458, 1648-1678)
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+
+#include "engine.hpp"
+
+namespace htf {
+
+// kernels (setup_kernels.cu / pcpg_kernels.cu)
+cudaError_t set_gauss_points(cudaStream_t s);
+__global__ void k_assemble(const int *, int, const double *, const int *, const int *, const double *,
+                           const double *, const SubDev *, double *, double *, double, double, double);
+__global__ void k_regularize(SubDev *, int, double *);
+__global__ void k_potrf_diag(const StepDesc *, const SubDev *, double *, int *);
+__global__ void k_trsm_panel(const StepDesc *, const SubDev *, double *);
+__global__ void k_syrk_update(const StepDesc *, const SubDev *, double *);
+__global__ void k_snapshot(const int *, const SubDev *, const double *, double *);
+__global__ void k_trtri_step(int, const int *, const SubDev *, const double *, double *);
+__global__ void k_lauum_tiles(const int *, const SubDev *, const double *, double *);
+__global__ void k_build_V(const SubDev *, const double *, const int *, const int *, const double *,
+                          const double *, double *);
+__global__ void k_build_Fc(const SubDev *, const double *, const int *, const int *, const double *,
+                           const long long *, double *);
+__global__ void k_trsv_fwd(const SubDev *, const double *, double *, long long);
+__global__ void k_trsv_bwd(const SubDev *, const double *, double *, long long);
+__global__ void k_gather_b(int, const int *, const int *, const double *, const double *, double *,
+                           const PcpgState *);
+template <typename T>
+__global__ void k_symv(const SubDev *, const T *, const double *, double *, const PcpgState *);
+__global__ void k_vt(const SubDev *, const double *, const double *, double *, const PcpgState *);
+__global__ void k_gc(int, const int *, const int *, const double *, double *, const PcpgState *);
+__global__ void k_coarse(const ClusterDev *, const double *, const double *, double *, const PcpgState *);
+__global__ void k_correct(const SubDev *, const ClusterDev *, const double *, const int *, const double *,
+                          double *, const PcpgState *);
+__global__ void k_rows(int, const int *, const double *, const double *, const double *, double *,
+                       const double *, double *, const PcpgState *);
+__global__ void k_dot_partial(int, const double *, const double *, double *, const PcpgState *);
+__global__ void k_sum_to(const double *, int, double *, const PcpgState *);
+__global__ void k_gft_partial(const int *, const int *, const int *, const int *, const double *,
+                              const double *, double *, const PcpgState *);
+__global__ void k_gft_final(int, const int *, const double *, const double *, double *, double *,
+                            const PcpgState *);
+__global__ void k_gf_apply(int, const int *, const double *, const double *, const double *, double *,
+                           const double *, double *, const PcpgState *);
+__global__ void k_gf_mult(int, const int *, const double *, const double *, double *);
+__global__ void k_update_lam_g(int, const double *, int, const double *, const double *, double *, double *,
+                               PcpgState *);
+__global__ void k_update_w(int, const double *, int, const double *, double *, PcpgState *);
+__global__ void k_finish_iter(const double *, int, PcpgState *);
+__global__ void k_init_state(const double *, int, PcpgState *, double, int);
+__global__ void k_axpby(int, double, const double *, double, double *);
+
+// ---- glue kernels on full (permuted local) vectors ----------------------
+// t_d = [Bc_b z_b ; -R^T y]  (y full, z full)
+__global__ void k_bc_rt(const SubDev *__restrict__ subs, const int *__restrict__ bce_ptr,
+                        const int *__restrict__ bce_pos, const double *__restrict__ bce_val,
+                        const double *__restrict__ Rbuf, const double *__restrict__ z,
+                        const double *__restrict__ y, double *__restrict__ t) {
+    const SubDev &sd = subs[blockIdx.x];
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nw = blockDim.x / 32;
+    const double *zb = z + sd.nfull_off + sd.nr;
+    for (int q = threadIdx.x; q < sd.c; q += blockDim.x) {
+        double v = 0.0;
+        for (int e = bce_ptr[sd.bce_off + q]; e < bce_ptr[sd.bce_off + q + 1]; ++e) v += bce_val[e] * zb[bce_pos[e]];
+        t[sd.t_off + q] = v;
+    }
+    for (int j = warp; j < 6; j += nw) {
+        const double *R = Rbuf + sd.R_off + (size_t)j * sd.N;
+        const double *yy = y + sd.nfull_off;
+        double s = 0.0;
+        for (int i = lane; i < sd.N; i += 32) s += R[i] * yy[i];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) t[sd.t_off + sd.c + j] = -s;
+    }
+}
+
+// copy the b block of a full vector into b space
+__global__ void k_full_to_b(const SubDev *__restrict__ subs, const double *__restrict__ z, double *__restrict__ xb) {
+    const SubDev &sd = subs[blockIdx.x];
+    for (int i = threadIdx.x; i < sd.nbp; i += blockDim.x) xb[sd.xb_off + i] = (i < sd.nb) ? z[sd.nfull_off + sd.nr + i] : 0.0;
+}
+
+// y_full -= x_b on the b block
+__global__ void k_full_minus_b(const SubDev *__restrict__ subs, const double *__restrict__ xb, double *__restrict__ y) {
+    const SubDev &sd = subs[blockIdx.x];
+    for (int i = threadIdx.x; i < sd.nb; i += blockDim.x) y[sd.nfull_off + sd.nr + i] -= xb[sd.xb_off + i];
+}
+
+// y_full -= Bc^T lambda_c
+__global__ void k_sub_bct(const SubDev *__restrict__ subs, const ClusterDev *__restrict__ cl,
+                          const int *__restrict__ bcr, const int *__restrict__ bce_ptr,
+                          const int *__restrict__ bce_pos, const double *__restrict__ bce_val,
+                          const double *__restrict__ s, double *__restrict__ y) {
+    const SubDev &sd = subs[blockIdx.x];
+    if (threadIdx.x != 0) return;      // few entries; sequential keeps the order fixed
+    const ClusterDev &c = cl[sd.cluster];
+    for (int q = 0; q < sd.c; ++q) {
+        const double lc = s[c.gc_off + bcr[sd.bcr_off + q]];
+        for (int e = bce_ptr[sd.bce_off + q]; e < bce_ptr[sd.bce_off + q + 1]; ++e)
+            y[sd.nfull_off + sd.nr + bce_pos[e]] -= bce_val[e] * lc;
+    }
+}
+
+// u_full += R_d (alpha_c,d - H_d alpha_f,cluster)
+__global__ void k_add_R(const SubDev *__restrict__ subs, const ClusterDev *__restrict__ cl,
+                        const double *__restrict__ Rbuf, const double *__restrict__ Hbuf,
+                        const double *__restrict__ s, const double *__restrict__ alpha_f, double *__restrict__ u) {
+    __shared__ double coef[6];
+    const SubDev &sd = subs[blockIdx.x];
+    const ClusterDev &c = cl[sd.cluster];
+    if (threadIdx.x < 6) {
+        const int j = threadIdx.x;
+        double v = s[c.gc_off + sd.alpha_pos + j];
+        const double *H = Hbuf + 36 * (size_t)blockIdx.x;      // H_d row-major 6x6: H[j*6+k]
+        for (int k = 0; k < 6; ++k) v -= H[j * 6 + k] * alpha_f[6 * sd.cluster + k];
+        coef[j] = v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < sd.N; i += blockDim.x) {
+        double a = u[sd.nfull_off + i];
+        for (int j = 0; j < 6; ++j) a += Rbuf[sd.R_off + (size_t)j * sd.N + i] * coef[j];
+        u[sd.nfull_off + i] = a;
+    }
+}
+
+// e_c = sum_{d in c} H_d^T (R_d^T f_d) = -sum_d H_d^T t_alpha,d ; one thread per (c, k)
+__global__ void k_e_vec(int ncl, const int *__restrict__ cl_sub_ptr, const int *__restrict__ cl_sub,
+                        const SubDev *__restrict__ subs, const double *__restrict__ Hbuf,
+                        const double *__restrict__ t, double *__restrict__ e) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= 6 * ncl) return;
+    const int c = q / 6, k = q % 6;
+    double v = 0.0;
+    for (int p = cl_sub_ptr[c]; p < cl_sub_ptr[c + 1]; ++p) {
+        const int d = cl_sub[p];
+        const SubDev &sd = subs[d];
+        for (int j = 0; j < 6; ++j) v -= Hbuf[36 * (size_t)d + j * 6 + k] * t[sd.t_off + sd.c + j];
+    }
+    e[q] = v;
+}
+
+// a = A x (m x m, col-major), one CTA
+__global__ void k_small_gemv(int m, const double *__restrict__ A, const double *__restrict__ x, double *__restrict__ a) {
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+        double s = 0.0;
+        for (int p = 0; p < m; ++p) s += A[q + (size_t)p * m] * x[p];
+        a[q] = s;
+    }
+}
+
+__global__ void k_to_f32(long long n, const double *__restrict__ a, float *__restrict__ b) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+__global__ void k_copy(long long n, const double *__restrict__ a, double *__restrict__ b, const PcpgState *st) {
+    if (st && st->done) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = a[i];
+}
+
+// ---------------------------------------------------------------------------
+Engine::~Engine() {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    for (auto &b : bufs_) cudaFree(b.p);
+    if (s_) cudaStreamDestroy(s_);
+}
+
+int Engine::check(cudaError_t e, const char *what, std::string &err) {
+    if (e == cudaSuccess) return HTF_OK;
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return (e == cudaErrorMemoryAllocation) ? HTF_ENOMEM : HTF_ECUDA;
+}
+
+template <typename T> T *Engine::alloc(size_t n, std::string &err, int &rc) {
+    if (rc) return nullptr;
+    void *p = nullptr;
+    size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        rc = check(e, "cudaMalloc", err);
+        err += " (" + std::to_string(bytes) + " bytes)";
+        return nullptr;
+    }
+    bufs_.push_back({p, bytes});
+    return static_cast<T *>(p);
+}
+
+#define CK(call)                                                   \
+    do {                                                           \
+        int _rc = check((call), #call, err);                       \
+        if (_rc) return _rc;                                       \
+    } while (0)
+
+static inline int cdiv(long long a, long long b) { return int((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+int Engine::upload_layout(Problem &p, std::string &err) {
+    int rc = HTF_OK;
+    nsub_ = int(p.sub.size());
+    ncl_ = int(p.clu.size());
+    nlam_ = p.n_lam;
+    hs_.assign(nsub_, SubDev());
+    long long K_off = 0, T_off = 0, X_off = 0, V_off = 0, R_off = 0;
+    int xb = 0, nf = 0, t_off = 0, bcr = 0, bce = 0;
+    for (int d = 0; d < nsub_; ++d) {
+        const Subdomain &s = p.sub[d];
+        SubDev &h = hs_[d];
+        h.n = s.n; h.nr = s.nr; h.nb = s.nb;
+        h.nt = (s.nb + TILE - 1) / TILE;
+        h.nbp = h.nt * TILE;
+        h.N = h.nr + h.nbp;
+        h.K_off = K_off; K_off += (long long)h.N * h.N;
+        h.T_off = T_off; T_off += (long long)h.nt * (h.nt + 1) / 2;
+        h.X_off = X_off; X_off += (long long)h.nbp * h.nbp;
+        h.xb_off = xb; xb += h.nbp;
+        h.nfull_off = nf; nf += h.N;
+        h.c = s.c();
+        if (h.c + 6 > 256) {
+            err = "subdomain " + std::to_string(d) + " has " + std::to_string(h.c) +
+                  " Bc rows; at most 250 are supported";
+            return HTF_EINVAL;
+        }
+        h.cluster = s.cluster;
+        h.alpha_pos = p.clu[s.cluster].nlam_c + 6 * s.cl_index;
+        h.V_off = V_off; V_off += (long long)h.nbp * (h.c + 6);
+        h.t_off = t_off; t_off += h.c + 6;
+        h.bcr_off = bcr; bcr += h.c;
+        h.bce_off = bce; bce += h.c + 1;
+        h.R_off = R_off; R_off += (long long)h.N * 6;
+        for (int q = 0; q < 6; ++q) { h.fix[q] = s.perm[s.fix[q]]; h.fix_diag[q] = 0.0; }
+    }
+    nslots_ = xb;
+    nfull_ = nf;
+    ntiles_ = T_off;
+    // clusters
+    hc_.assign(ncl_, ClusterDev());
+    long long M_off = 0;
+    int gc_off = 0;
+    for (int c = 0; c < ncl_; ++c) {
+        hc_[c].nlam_c = p.clu[c].nlam_c;
+        hc_[c].ngc = p.clu[c].ngc();
+        hc_[c].M_off = M_off; M_off += (long long)hc_[c].ngc * hc_[c].ngc;
+        hc_[c].gc_off = gc_off; gc_off += hc_[c].ngc;
+    }
+    ngc_total_ = gc_off;
+    // device allocations
+    d_subs_ = alloc<SubDev>(nsub_, err, rc);
+    d_cl_ = alloc<ClusterDev>(ncl_, err, rc);
+    d_all_subs_ = alloc<int>(nsub_, err, rc);
+    d_K_ = alloc<double>(K_off, err, rc);
+    d_F_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);
+    d_S_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);
+    d_X_ = alloc<double>(X_off, err, rc);
+    d_V_ = alloc<double>(V_off, err, rc);
+    d_R_ = alloc<double>(R_off, err, rc);
+    d_M_ = alloc<double>(M_off, err, rc);
+    d_H_ = alloc<double>(36 * (size_t)nsub_, err, rc);
+    d_status_ = alloc<int>(nsub_, err, rc);
+    if (rc) return rc;
+    // R in permuted order, Bc rows / entries
+    {
+        std::vector<double> R(R_off, 0.0);
+        std::vector<int> bcrows(std::max(bcr, 1)), bptr(std::max(bce, 1));
+        std::vector<int> bpos;
+        std::vector<double> bval;
+        for (int d = 0; d < nsub_; ++d) {
+            const Subdomain &s = p.sub[d];
+            const SubDev &h = hs_[d];
+            for (int j = 0; j < 6; ++j)
+                for (int l = 0; l < s.n; ++l) R[h.R_off + (size_t)j * h.N + s.perm[l]] = s.R[l + (size_t)j * s.n];
+            for (int q = 0; q < h.c; ++q) bcrows[h.bcr_off + q] = s.bc_rows[q];
+            // entries grouped by compressed row
+            std::vector<std::vector<std::pair<int, double>>> rows(h.c);
+            for (size_t e = 0; e < s.bc_row.size(); ++e) {
+                int q = int(std::lower_bound(s.bc_rows.begin(), s.bc_rows.end(), s.bc_row[e]) - s.bc_rows.begin());
+                rows[q].push_back({s.perm[s.bc_col[e]] - s.nr, s.bc_val[e]});
+            }
+            bptr[h.bce_off] = int(bpos.size());
+            for (int q = 0; q < h.c; ++q) {
+                for (auto &pr : rows[q]) { bpos.push_back(pr.first); bval.push_back(pr.second); }
+                bptr[h.bce_off + q + 1] = int(bpos.size());
+            }
+        }
+        d_bcr_ = alloc<int>(bcrows.size(), err, rc);
+        d_bce_ptr_ = alloc<int>(bptr.size(), err, rc);
+        d_bce_pos_ = alloc<int>(std::max<size_t>(bpos.size(), 1), err, rc);
+        d_bce_val_ = alloc<double>(std::max<size_t>(bval.size(), 1), err, rc);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(d_R_, R.data(), R.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_bcr_, bcrows.data(), bcrows.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_bce_ptr_, bptr.data(), bptr.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+        if (!bpos.empty()) {
+            CK(cudaMemcpyAsync(d_bce_pos_, bpos.data(), bpos.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+            CK(cudaMemcpyAsync(d_bce_val_, bval.data(), bval.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+        }
+        CK(cudaStreamSynchronize(s_));
+    }
+    // Bf gather (b slots) and row tables
+    {
+        std::vector<int> sptr(nslots_ + 1, 0), sent;
+        for (int d = 0; d < nsub_; ++d) {
+            const Subdomain &s = p.sub[d];
+            const SubDev &h = hs_[d];
+            for (int i = 0; i < h.nbp; ++i) {
+                int slot = h.xb_off + i;
+                if (i < h.nb)
+                    for (int e = s.bf_ptr[i]; e < s.bf_ptr[i + 1]; ++e)
+                        sent.push_back(2 * s.bf_lam[e] + (s.bf_sign[e] < 0 ? 1 : 0));
+                sptr[slot + 1] = int(sent.size());
+            }
+        }
+        std::vector<int> rslot(2 * (size_t)nlam_, -1);
+        std::vector<double> rsign(2 * (size_t)nlam_, 0.0);
+        for (int r = 0; r < nlam_; ++r)
+            for (int k = 0; k < 2; ++k) {
+                int d = p.rows[r].sub[k];
+                if (d < 0) continue;
+                const Subdomain &s = p.sub[d];
+                int l = int(std::lower_bound(s.l2g.begin(), s.l2g.end(), p.rows[r].dof[k]) - s.l2g.begin());
+                rslot[2 * r + k] = hs_[d].xb_off + (s.perm[l] - s.nr);
+                rsign[2 * r + k] = p.rows[r].sign[k];
+            }
+        d_slot_ptr_ = alloc<int>(sptr.size(), err, rc);
+        d_slot_ent_ = alloc<int>(std::max<size_t>(sent.size(), 1), err, rc);
+        d_rslot_ = alloc<int>(rslot.size(), err, rc);
+        d_rsign_ = alloc<double>(rsign.size(), err, rc);
+        d_weight_ = alloc<double>(nlam_, err, rc);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(d_slot_ptr_, sptr.data(), sptr.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_slot_ent_, sent.data(), sent.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_rslot_, rslot.data(), rslot.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_rsign_, rsign.data(), rsign.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_weight_, p.weight.data(), nlam_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+        CK(cudaStreamSynchronize(s_));
+    }
+    // coarse gather map: gc[q] <- t slots
+    {
+        std::vector<std::vector<int>> lists(ngc_total_);
+        for (int d = 0; d < nsub_; ++d) {
+            const SubDev &h = hs_[d];
+            const ClusterDev &c = hc_[h.cluster];
+            for (int q = 0; q < h.c; ++q) lists[c.gc_off + p.sub[d].bc_rows[q]].push_back(h.t_off + q);
+            for (int j = 0; j < 6; ++j) lists[c.gc_off + h.alpha_pos + j].push_back(h.t_off + h.c + j);
+        }
+        std::vector<int> gptr(ngc_total_ + 1, 0), gidx;
+        for (int q = 0; q < ngc_total_; ++q) {
+            for (int v : lists[q]) gidx.push_back(v);
+            gptr[q + 1] = int(gidx.size());
+        }
+        d_gptr_ = alloc<int>(gptr.size(), err, rc);
+        d_gidx_ = alloc<int>(std::max<size_t>(gidx.size(), 1), err, rc);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(d_gptr_, gptr.data(), gptr.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_gidx_, gidx.data(), gidx.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+    }
+    // vectors
+    const int nrhs = p.nrhs;
+    d_f_ = alloc<double>((size_t)nfull_ * nrhs, err, rc);
+    d_full_ = alloc<double>(nfull_, err, rc);
+    d_full2_ = alloc<double>(nfull_, err, rc);
+    d_lam_ = alloc<double>(nlam_, err, rc);
+    d_g_ = alloc<double>(nlam_, err, rc);
+    d_w_ = alloc<double>(nlam_, err, rc);
+    d_Fw_ = alloc<double>(nlam_, err, rc);
+    d_Pg_ = alloc<double>(nlam_, err, rc);
+    d_z_ = alloc<double>(nlam_, err, rc);
+    d_Pz_ = alloc<double>(nlam_, err, rc);
+    d_d_ = alloc<double>(nlam_, err, rc);
+    d_tmp_ = alloc<double>(nlam_, err, rc);
+    d_xb_ = alloc<double>(nslots_, err, rc);
+    d_yb_ = alloc<double>(nslots_, err, rc);
+    d_t_ = alloc<double>(t_off, err, rc);
+    d_gc_ = alloc<double>(ngc_total_, err, rc);
+    d_s_ = alloc<double>(ngc_total_, err, rc);
+    d_a_ = alloc<double>(6 * (size_t)ncl_, err, rc);
+    d_alpha_ = alloc<double>(6 * (size_t)ncl_, err, rc);
+    npart_ = cdiv(nlam_, 256);
+    d_partial_ = alloc<double>(npart_, err, rc);
+    d_st_ = alloc<PcpgState>(1, err, rc);
+    if (rc) return rc;
+    {
+        std::vector<int> csp(ncl_ + 1, 0), cs;
+        for (int c = 0; c < ncl_; ++c) {
+            for (int d : p.clu[c].subs) cs.push_back(d);
+            csp[c + 1] = int(cs.size());
+        }
+        d_csp_ = alloc<int>(csp.size(), err, rc);
+        d_cs_ = alloc<int>(cs.size(), err, rc);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(d_csp_, csp.data(), csp.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_cs_, cs.data(), cs.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+    }
+    std::vector<int> ids(nsub_);
+    std::iota(ids.begin(), ids.end(), 0);
+    CK(cudaMemcpyAsync(d_all_subs_, ids.data(), nsub_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_cl_, hc_.data(), ncl_ * sizeof(ClusterDev), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemsetAsync(d_status_, 0, nsub_ * sizeof(int), s_));
+    return HTF_OK;
+}
+
+// ---------------------------------------------------------------------------
+int Engine::factorize(Problem &p, std::string &err) {
+    int rc = HTF_OK;
+    const Mesh &m = p.mesh;
+    const int ne = m.n_elems();
+    // element data: coordinates, permuted DOF positions, colours
+    std::vector<double> ec(24 * (size_t)ne);
+    std::vector<int> ep(24 * (size_t)ne);
+    for (int d = 0; d < nsub_; ++d) {
+        const Subdomain &s = p.sub[d];
+        for (int e : s.elems) {
+            const int *q = &m.elems[8 * (size_t)e];
+            for (int a = 0; a < 8; ++a) {
+                for (int c = 0; c < 3; ++c) ec[24 * (size_t)e + 3 * a + c] = m.coords[3 * (size_t)q[a] + c];
+                for (int c = 0; c < 3; ++c) {
+                    int g = 3 * q[a] + c;
+                    int l = int(std::lower_bound(s.l2g.begin(), s.l2g.end(), g) - s.l2g.begin());
+                    ep[24 * (size_t)e + 8 * c + a] = s.perm[l];
+                }
+            }
+        }
+    }
+    // greedy colouring: elements sharing a node get different colours
+    std::vector<uint32_t> mask(m.n_nodes, 0u);
+    std::vector<int> col(ne);
+    int ncol = 0;
+    for (int e = 0; e < ne; ++e) {
+        uint32_t used = 0;
+        for (int a = 0; a < 8; ++a) used |= mask[m.elems[8 * (size_t)e + a]];
+        int c = 0;
+        while (c < 32 && (used >> c & 1u)) ++c;
+        if (c >= 32) { err = "element colouring needs more than 32 colours"; return HTF_EINVAL; }
+        col[e] = c;
+        ncol = std::max(ncol, c + 1);
+        for (int a = 0; a < 8; ++a) mask[m.elems[8 * (size_t)e + a]] |= 1u << c;
+    }
+    std::vector<int> order(ne), cptr(ncol + 1, 0);
+    for (int e = 0; e < ne; ++e) cptr[col[e] + 1]++;
+    for (int c = 0; c < ncol; ++c) cptr[c + 1] += cptr[c];
+    {
+        std::vector<int> pos(cptr.begin(), cptr.end() - 1);
+        for (int e = 0; e < ne; ++e) order[pos[col[e]]++] = e;
+    }
+    double *d_ec = alloc<double>(ec.size(), err, rc);
+    int *d_ep = alloc<int>(ep.size(), err, rc);
+    int *d_es = alloc<int>(ne, err, rc);
+    int *d_order = alloc<int>(ne, err, rc);
+    double *d_E = alloc<double>(nsub_, err, rc);
+    double *d_nu = alloc<double>(nsub_, err, rc);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(d_ec, ec.data(), ec.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_ep, ep.data(), ep.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_es, m.elem_sub.data(), ne * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_order, order.data(), ne * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_E, m.sub_E.data(), nsub_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_nu, m.sub_nu.data(), nsub_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_subs_, hs_.data(), nsub_ * sizeof(SubDev), cudaMemcpyHostToDevice, s_));
+    CK(set_gauss_points(s_));
+    long long Ktot = 0;
+    for (auto &h : hs_) Ktot += (long long)h.N * h.N;
+    CK(cudaMemsetAsync(d_K_, 0, Ktot * sizeof(double), s_));
+    CK(cudaMemsetAsync(d_f_, 0, (size_t)nfull_ * p.nrhs * sizeof(double), s_));
+    for (int c = 0; c < ncol; ++c) {
+        int cnt = cptr[c + 1] - cptr[c];
+        if (cnt == 0) continue;
+        k_assemble<<<cnt, 64, 0, s_>>>(d_order + cptr[c], cnt, d_ec, d_es, d_ep, d_E, d_nu, d_subs_, d_K_, d_f_,
+                                       m.body_force[0], m.body_force[1], m.body_force[2]);
+    }
+    CK(cudaGetLastError());
+    k_regularize<<<nsub_, 128, 0, s_>>>(d_subs_, nsub_, d_K_);
+    CK(cudaGetLastError());
+    const bool dirichlet = opt_.preconditioner != "lumped";
+    int max_nt = 0, max_tiles = 0;
+    for (auto &h : hs_) { max_nt = std::max(max_nt, h.nt); max_tiles = std::max(max_tiles, h.nt * (h.nt + 1) / 2); }
+    if (!dirichlet) {          // lumped: K_bb before any elimination
+        k_snapshot<<<dim3(nsub_, max_tiles), 256, 0, s_>>>(d_all_subs_, d_subs_, d_K_, d_S_);
+        CK(cudaGetLastError());
+    }
+    // step tables
+    std::vector<std::vector<StepDesc>> steps;
+    std::vector<std::vector<int>> snap_after;      // subdomains whose interior ends after step s
+    std::vector<int> snap_first;                   // nr == 0
+    for (int d = 0; d < nsub_; ++d) {
+        const SubDev &h = hs_[d];
+        std::vector<std::pair<int, int>> blocks;
+        for (int k = 0; k < h.nr; k += TILE) blocks.push_back({k, std::min(TILE, h.nr - k)});
+        int interior_steps = int(blocks.size());
+        for (int k = h.nr; k < h.N; k += TILE) blocks.push_back({k, TILE});
+        if (steps.size() < blocks.size()) { steps.resize(blocks.size()); snap_after.resize(blocks.size()); }
+        for (size_t s = 0; s < blocks.size(); ++s) steps[s].push_back({d, blocks[s].first, blocks[s].second});
+        if (interior_steps == 0) snap_first.push_back(d);
+        else snap_after[interior_steps - 1].push_back(d);
+    }
+    std::vector<StepDesc> flat;
+    std::vector<size_t> soff;
+    for (auto &v : steps) { soff.push_back(flat.size()); flat.insert(flat.end(), v.begin(), v.end()); }
+    std::vector<int> snap_flat;
+    std::vector<size_t> snap_off;
+    for (auto &v : snap_after) { snap_off.push_back(snap_flat.size()); snap_flat.insert(snap_flat.end(), v.begin(), v.end()); }
+    size_t snap_first_off = snap_flat.size();
+    snap_flat.insert(snap_flat.end(), snap_first.begin(), snap_first.end());
+    StepDesc *d_steps = alloc<StepDesc>(flat.size(), err, rc);
+    int *d_snap = alloc<int>(std::max<size_t>(snap_flat.size(), 1), err, rc);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(d_steps, flat.data(), flat.size() * sizeof(StepDesc), cudaMemcpyHostToDevice, s_));
+    if (!snap_flat.empty())
+        CK(cudaMemcpyAsync(d_snap, snap_flat.data(), snap_flat.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+    if (dirichlet && !snap_first.empty()) {
+        k_snapshot<<<dim3(int(snap_first.size()), max_tiles), 256, 0, s_>>>(d_snap + snap_first_off, d_subs_, d_K_, d_S_);
+        CK(cudaGetLastError());
+    }
+    for (size_t s = 0; s < steps.size(); ++s) {
+        const int cnt = int(steps[s].size());
+        int max_rows = 0, max_tri = 0;
+        for (auto &st : steps[s]) {
+            const SubDev &h = hs_[st.d];
+            int rows = h.N - st.k - st.nb;
+            max_rows = std::max(max_rows, rows);
+            int nbr = (rows + 63) / 64;
+            max_tri = std::max(max_tri, nbr * (nbr + 1) / 2);
+        }
+        const StepDesc *ds = d_steps + soff[s];
+        k_potrf_diag<<<cnt, 32, 0, s_>>>(ds, d_subs_, d_K_, d_status_);
+        if (max_rows > 0) {
+            k_trsm_panel<<<dim3(cnt, cdiv(max_rows, 128)), 128, 0, s_>>>(ds, d_subs_, d_K_);
+            k_syrk_update<<<dim3(cnt, max_tri), 256, 0, s_>>>(ds, d_subs_, d_K_);
+        }
+        if (dirichlet && !snap_after[s].empty())
+            k_snapshot<<<dim3(int(snap_after[s].size()), max_tiles), 256, 0, s_>>>(d_snap + snap_off[s], d_subs_, d_K_, d_S_);
+        CK(cudaGetLastError());
+    }
+    // X = L_bb^{-1}, F = X^T X
+    for (int i = 0; i < max_nt; ++i)
+        k_trtri_step<<<dim3(nsub_, i + 1), 256, 0, s_>>>(i, d_all_subs_, d_subs_, d_K_, d_X_);
+    CK(cudaGetLastError());
+    k_lauum_tiles<<<dim3(nsub_, max_tiles), 256, 0, s_>>>(d_all_subs_, d_subs_, d_X_, d_F_);
+    CK(cudaGetLastError());
+    int max_cols = 0;
+    for (auto &h : hs_) max_cols = std::max(max_cols, h.c + 6);
+    k_build_V<<<dim3(nsub_, max_cols), 256, 0, s_>>>(d_subs_, d_F_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_R_, d_V_);
+    CK(cudaGetLastError());
+    std::vector<int> status(nsub_);
+    CK(cudaMemcpyAsync(status.data(), d_status_, nsub_ * sizeof(int), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    for (int d = 0; d < nsub_; ++d)
+        if (status[d]) {
+            status_sub = d;
+            err = "K_reg of subdomain " + std::to_string(d) + " is not positive definite (column " +
+                  std::to_string(status[d] - 1) + ")";
+            return HTF_ENOTSPD;
+        }
+    return HTF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// cluster coarse problem (host FP64): M = [Ac^{-1}]_{lambda_c, alpha}
+//   M11 = Fc^{-1} - Z Sr^{-1} Z^T, M12 = Z Sr^{-1}, M22 = H H^T - Sr^{-1}
+//   with Z = Fc^{-1} Gc, Sr = Gc^T Z + H H^T, H = ker(Gc) orthonormal:
+//   the block elimination of the extended saddle-point matrix
+//   [Fc Gc 0; Gc^T 0 H; 0 H^T 0] of Cluster::create_Ac_clust (Cluster.cpp:582-678).
+// ---------------------------------------------------------------------------
+int Engine::coarse(Problem &p, std::string &err) {
+    int rc = HTF_OK;
+    // Fc_d from the device
+    std::vector<long long> fco(nsub_);
+    long long fct = 0;
+    for (int d = 0; d < nsub_; ++d) { fco[d] = fct; fct += (long long)hs_[d].c * hs_[d].c; }
+    long long *d_fco = alloc<long long>(nsub_, err, rc);
+    double *d_Fc = alloc<double>(std::max<long long>(fct, 1), err, rc);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(d_fco, fco.data(), nsub_ * sizeof(long long), cudaMemcpyHostToDevice, s_));
+    k_build_Fc<<<nsub_, 256, 0, s_>>>(d_subs_, d_V_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_fco, d_Fc);
+    CK(cudaGetLastError());
+    std::vector<double> Fc(std::max<long long>(fct, 1));
+    CK(cudaMemcpyAsync(Fc.data(), d_Fc, fct * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    Hd_.assign(nsub_, std::vector<double>(36, 0.0));
+    std::vector<double> Mall;
+    std::vector<std::vector<double>> Ms(ncl_);
+    int fail = 0;
+#pragma omp parallel for schedule(dynamic)
+    for (int ci = 0; ci < ncl_; ++ci) {
+        const Cluster &cl = p.clu[ci];
+        const int nc = cl.nlam_c, ns = int(cl.subs.size()), na = 6 * ns, ng = nc + na;
+        std::vector<double> F(size_t(nc) * nc, 0.0), G(size_t(nc) * na, 0.0), H(size_t(na) * 6, 0.0);
+        for (int k = 0; k < ns; ++k) {
+            const int d = cl.subs[k];
+            const Subdomain &s = p.sub[d];
+            const int c = hs_[d].c;
+            for (int j = 0; j < c; ++j)
+                for (int i = 0; i < c; ++i) F[s.bc_rows[i] + size_t(s.bc_rows[j]) * nc] += Fc[fco[d] + i + (size_t)j * c];
+            for (size_t e = 0; e < s.bc_row.size(); ++e)          // Gc_d = -Bc_d R_d (Cluster.cpp:190-198)
+                for (int j = 0; j < 6; ++j)
+                    G[s.bc_row[e] + size_t(6 * k + j) * nc] -= s.bc_val[e] * s.R[s.bc_col[e] + size_t(j) * s.n];
+            // ker(Gc): alpha_d = R_d^T r for the (unnormalised) rigid modes r of the cluster
+            const int n = s.n;
+            for (int q = 0; q < 6; ++q)
+                for (int j = 0; j < 6; ++j) {
+                    double v = 0.0;
+                    for (int l = 0; l < n / 3; ++l) {
+                        int node = s.l2g[3 * l] / 3;
+                        double x = p.mesh.coords[3 * size_t(node)], y = p.mesh.coords[3 * size_t(node) + 1],
+                               z = p.mesh.coords[3 * size_t(node) + 2];
+                        double g[3] = {0, 0, 0};
+                        switch (q) {
+                            case 0: g[0] = 1; break;
+                            case 1: g[1] = 1; break;
+                            case 2: g[2] = 1; break;
+                            case 3: g[0] = -y; g[1] = x; break;
+                            case 4: g[0] = -z; g[2] = x; break;
+                            default: g[1] = -z; g[2] = y; break;
+                        }
+                        for (int cc = 0; cc < 3; ++cc) v += s.R[3 * l + cc + size_t(j) * n] * g[cc];
+                    }
+                    H[6 * k + j + size_t(q) * na] = v;
+                }
+        }
+        // orthonormalise the columns of H (two passes of Gram-Schmidt)
+        for (int pass = 0; pass < 2; ++pass)
+            for (int q = 0; q < 6; ++q) {
+                double *hq = &H[size_t(q) * na];
+                for (int o = 0; o < q; ++o) {
+                    const double *ho = &H[size_t(o) * na];
+                    double dd = 0.0;
+                    for (int i = 0; i < na; ++i) dd += hq[i] * ho[i];
+                    for (int i = 0; i < na; ++i) hq[i] -= dd * ho[i];
+                }
+                double nn = 0.0;
+                for (int i = 0; i < na; ++i) nn += hq[i] * hq[i];
+                nn = std::sqrt(nn);
+                for (int i = 0; i < na; ++i) hq[i] /= nn;
+            }
+        for (int k = 0; k < ns; ++k)
+            for (int j = 0; j < 6; ++j)
+                for (int q = 0; q < 6; ++q) Hd_[cl.subs[k]][j * 6 + q] = H[6 * k + j + size_t(q) * na];
+        // Cholesky of Fc, Z = Fc^{-1} Gc
+        std::vector<double> L(F);
+        if (!chol_lower(nc, L.data(), nc)) {
+#pragma omp atomic write
+            fail = ci + 1;
+            continue;
+        }
+        std::vector<double> Z(G);
+        chol_solve(nc, L.data(), nc, Z.data(), nc, na);
+        std::vector<double> Sr(size_t(na) * na, 0.0);
+        for (int j = 0; j < na; ++j)
+            for (int i = 0; i < na; ++i) {
+                double v = 0.0;
+                for (int k = 0; k < nc; ++k) v += G[k + size_t(i) * nc] * Z[k + size_t(j) * nc];
+                for (int q = 0; q < 6; ++q) v += H[i + size_t(q) * na] * H[j + size_t(q) * na];
+                Sr[i + size_t(j) * na] = v;
+            }
+        std::vector<double> Ls(Sr);
+        if (!chol_lower(na, Ls.data(), na)) {
+#pragma omp atomic write
+            fail = ci + 1;
+            continue;
+        }
+        std::vector<double> Si(size_t(na) * na, 0.0);
+        for (int i = 0; i < na; ++i) Si[i + size_t(i) * na] = 1.0;
+        chol_solve(na, Ls.data(), na, Si.data(), na, na);
+        std::vector<double> Fi(size_t(nc) * nc, 0.0);
+        for (int i = 0; i < nc; ++i) Fi[i + size_t(i) * nc] = 1.0;
+        chol_solve(nc, L.data(), nc, Fi.data(), nc, nc);
+        std::vector<double> ZS(size_t(nc) * na, 0.0);            // Z Sr^{-1}
+        for (int j = 0; j < na; ++j)
+            for (int k = 0; k < na; ++k) {
+                const double s = Si[k + size_t(j) * na];
+                const double *zk = &Z[size_t(k) * nc];
+                double *o = &ZS[size_t(j) * nc];
+                for (int i = 0; i < nc; ++i) o[i] += zk[i] * s;
+            }
+        std::vector<double> &M = Ms[ci];
+        M.assign(size_t(ng) * ng, 0.0);
+        for (int j = 0; j < nc; ++j) {
+            for (int i = 0; i < nc; ++i) M[i + size_t(j) * ng] = Fi[i + size_t(j) * nc];
+            for (int k = 0; k < na; ++k) {
+                const double zjk = Z[j + size_t(k) * nc];
+                const double *zs = &ZS[size_t(k) * nc];
+                double *o = &M[size_t(j) * ng];
+                for (int i = 0; i < nc; ++i) o[i] -= zs[i] * zjk;
+            }
+        }
+        for (int j = 0; j < na; ++j)
+            for (int i = 0; i < nc; ++i) {
+                M[i + size_t(nc + j) * ng] = ZS[i + size_t(j) * nc];
+                M[(nc + j) + size_t(i) * ng] = ZS[i + size_t(j) * nc];
+            }
+        for (int j = 0; j < na; ++j)
+            for (int i = 0; i < na; ++i) {
+                double v = -Si[i + size_t(j) * na];
+                for (int q = 0; q < 6; ++q) v += H[i + size_t(q) * na] * H[j + size_t(q) * na];
+                M[(nc + i) + size_t(nc + j) * ng] = v;
+            }
+    }
+    if (fail) {
+        err = "cluster coarse matrix of cluster " + std::to_string(fail - 1) + " is not positive definite";
+        return HTF_ENOTSPD;
+    }
+    for (int ci = 0; ci < ncl_; ++ci)
+        CK(cudaMemcpyAsync(d_M_ + hc_[ci].M_off, Ms[ci].data(), Ms[ci].size() * sizeof(double),
+                           cudaMemcpyHostToDevice, s_));
+    std::vector<double> Hflat(36 * (size_t)nsub_);
+    for (int d = 0; d < nsub_; ++d) std::memcpy(&Hflat[36 * (size_t)d], Hd_[d].data(), 36 * sizeof(double));
+    CK(cudaMemcpyAsync(d_H_, Hflat.data(), Hflat.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+    CK(cudaStreamSynchronize(s_));
+    return HTF_OK;
+}
+
+// Gf = Bf Rf, Rf_d = R_d H_d (Cluster.cpp:1332-1352); (Gf^T Gf)^{-1} (1227-1273)
+int Engine::outer_coarse(Problem &p, std::string &err) {
+    int rc = HTF_OK;
+    const int m = 6 * ncl_;
+    std::vector<int> gcl(2 * (size_t)nlam_, -1);
+    std::vector<double> gval(12 * (size_t)nlam_, 0.0);
+    for (int r = 0; r < nlam_; ++r) {
+        for (int k = 0; k < 2; ++k) {
+            int d = p.rows[r].sub[k];
+            if (d < 0) continue;
+            const Subdomain &s = p.sub[d];
+            int l = int(std::lower_bound(s.l2g.begin(), s.l2g.end(), p.rows[r].dof[k]) - s.l2g.begin());
+            double rf[6];
+            for (int q = 0; q < 6; ++q) {
+                double v = 0.0;
+                for (int j = 0; j < 6; ++j) v += s.R[l + size_t(j) * s.n] * Hd_[d][j * 6 + q];
+                rf[q] = p.rows[r].sign[k] * v;
+            }
+            int slot = (k == 1 && gcl[2 * r] == s.cluster) ? 0 : k;
+            gcl[2 * r + slot] = s.cluster;
+            for (int q = 0; q < 6; ++q) gval[6 * (2 * (size_t)r + slot) + q] += rf[q];
+        }
+    }
+    std::vector<double> GtG(size_t(m) * m, 0.0);
+    // per-cluster entry lists for the reduction
+    std::vector<std::vector<int>> crow(ncl_);
+    std::vector<std::vector<double>> cval(ncl_);
+    for (int r = 0; r < nlam_; ++r)
+        for (int k = 0; k < 2; ++k) {
+            int c = gcl[2 * r + k];
+            if (c < 0) continue;
+            crow[c].push_back(r);
+            for (int q = 0; q < 6; ++q) cval[c].push_back(gval[6 * (2 * (size_t)r + k) + q]);
+        }
+    for (int r = 0; r < nlam_; ++r)
+        for (int k1 = 0; k1 < 2; ++k1)
+            for (int k2 = 0; k2 < 2; ++k2) {
+                int c1 = gcl[2 * r + k1], c2 = gcl[2 * r + k2];
+                if (c1 < 0 || c2 < 0) continue;
+                for (int a = 0; a < 6; ++a)
+                    for (int b = 0; b < 6; ++b)
+                        GtG[(6 * c1 + a) + size_t(6 * c2 + b) * m] +=
+                            gval[6 * (2 * (size_t)r + k1) + a] * gval[6 * (2 * (size_t)r + k2) + b];
+            }
+    std::vector<double> L(GtG);
+    if (!chol_lower(m, L.data(), m)) { err = "Gf^T Gf is not positive definite"; return HTF_ENOTSPD; }
+    invGtG_.assign(size_t(m) * m, 0.0);
+    for (int i = 0; i < m; ++i) invGtG_[i + size_t(i) * m] = 1.0;
+    chol_solve(m, L.data(), m, invGtG_.data(), m, m);
+    // chunks
+    const int CH = 4096;
+    std::vector<int> ch_cl, ch_beg, ch_end, clp(ncl_ + 1, 0), rows_all;
+    std::vector<double> vals_all;
+    for (int c = 0; c < ncl_; ++c) {
+        int base = int(rows_all.size());
+        rows_all.insert(rows_all.end(), crow[c].begin(), crow[c].end());
+        vals_all.insert(vals_all.end(), cval[c].begin(), cval[c].end());
+        int n = int(crow[c].size());
+        for (int b = 0; b < std::max(n, 1); b += CH) {
+            ch_cl.push_back(c);
+            ch_beg.push_back(base + b);
+            ch_end.push_back(base + std::min(n, b + CH));
+        }
+        clp[c + 1] = int(ch_cl.size());
+    }
+    nchunks_ = int(ch_cl.size());
+    d_gcl_ = alloc<int>(gcl.size(), err, rc);
+    d_gval_ = alloc<double>(gval.size(), err, rc);
+    d_chunk_cl_ = alloc<int>(nchunks_, err, rc);
+    d_chunk_beg_ = alloc<int>(nchunks_, err, rc);
+    d_chunk_end_ = alloc<int>(nchunks_, err, rc);
+    d_cl_chunk_ptr_ = alloc<int>(ncl_ + 1, err, rc);
+    d_crow_ = alloc<int>(std::max<size_t>(rows_all.size(), 1), err, rc);
+    d_cval_ = alloc<double>(std::max<size_t>(vals_all.size(), 1), err, rc);
+    d_invGtG_ = alloc<double>(invGtG_.size(), err, rc);
+    d_gpart_ = alloc<double>(6 * (size_t)nchunks_, err, rc);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(d_gcl_, gcl.data(), gcl.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_gval_, gval.data(), gval.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_chunk_cl_, ch_cl.data(), nchunks_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_chunk_beg_, ch_beg.data(), nchunks_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_chunk_end_, ch_end.data(), nchunks_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_cl_chunk_ptr_, clp.data(), (ncl_ + 1) * sizeof(int), cudaMemcpyHostToDevice, s_));
+    if (!rows_all.empty()) {
+        CK(cudaMemcpyAsync(d_crow_, rows_all.data(), rows_all.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_cval_, vals_all.data(), vals_all.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+    }
+    CK(cudaMemcpyAsync(d_invGtG_, invGtG_.data(), invGtG_.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+    CK(cudaStreamSynchronize(s_));
+    return HTF_OK;
+}
+
+// ---------------------------------------------------------------------------
+int Engine::setup(Problem &p, std::string &err) {
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
+        err = "no CUDA device";
+        return HTF_ENODEV;
+    }
+    CK(cudaSetDevice(opt_.device));
+    CK(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s_));
+    int rc = upload_layout(p, err);
+    if (!rc) rc = factorize(p, err);
+    if (!rc) rc = coarse(p, err);
+    if (!rc) rc = outer_coarse(p, err);
+    if (!rc) {
+        int max_nbp = 0;
+        for (auto &h : hs_) max_nbp = std::max(max_nbp, h.nbp);
+        symv_smem_ = (1 + 4) * max_nbp * int(sizeof(double));
+        if (symv_smem_ > 48 * 1024) {
+            rc = check(cudaFuncSetAttribute(k_symv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, symv_smem_),
+                       "cudaFuncSetAttribute", err);
+            if (!rc)
+                rc = check(cudaFuncSetAttribute(k_symv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, symv_smem_),
+                           "cudaFuncSetAttribute", err);
+        }
+    }
+    if (!rc && opt_.mixed) {
+        d_F32_ = alloc<float>(ntiles_ * TILE_ELEMS, err, rc);
+        d_S32_ = alloc<float>(ntiles_ * TILE_ELEMS, err, rc);
+        if (!rc) {
+            k_to_f32<<<1184, 256, 0, s_>>>(ntiles_ * TILE_ELEMS, d_F_, d_F32_);
+            k_to_f32<<<1184, 256, 0, s_>>>(ntiles_ * TILE_ELEMS, d_S_, d_S32_);
+            rc = check(cudaGetLastError(), "k_to_f32", err);
+        }
+        mixed_ = true;
+    }
+    if (!rc) rc = check(cudaEventRecord(e1, s_), "cudaEventRecord", err);
+    if (!rc) rc = check(cudaEventSynchronize(e1), "cudaEventSynchronize", err);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    setup_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // algorithmic bytes of one F apply (FP64 or FP32 tiles, V, lambda gather/scatter)
+    double bytes = 0.0;
+    const double sz = mixed_ ? 4.0 : 8.0;
+    for (int d = 0; d < nsub_; ++d) {
+        const Subdomain &s = p.sub[d];
+        const double nb = s.nb;
+        int m_i = s.bf_ptr[s.nb];
+        bytes += sz * nb * (nb + 1) / 2 + 8.0 * nb * (s.c() + 6) + m_i * (8.0 + 4.0) + m_i * 8.0;
+    }
+    fapply_bytes_ = bytes;
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+void Engine::op_F(const double *w, double *Fw, const double *dotv, double *partial, PcpgState *st) {
+    k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, w, nullptr, d_xb_, st);
+    if (mixed_)
+        k_symv<float><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_F32_, d_xb_, d_yb_, st);
+    else
+        k_symv<double><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_F_, d_xb_, d_yb_, st);
+    k_vt<<<nsub_, 256, 0, s_>>>(d_subs_, d_V_, d_xb_, d_t_, st);
+    k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, st);
+    int maxg = 0;
+    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
+    k_coarse<<<dim3(ncl_, cdiv(maxg, 8)), 256, 0, s_>>>(d_cl_, d_M_, d_gc_, d_s_, st);
+    k_correct<<<nsub_, 256, 0, s_>>>(d_subs_, d_cl_, d_V_, d_bcr_, d_s_, d_yb_, st);
+    k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, nullptr, Fw, dotv, partial, st);
+}
+
+void Engine::op_M(const double *x, double *z, PcpgState *st) {
+    if (opt_.preconditioner == "none") {
+        k_copy<<<cdiv(nlam_, 256), 256, 0, s_>>>(nlam_, x, z, st);
+        return;
+    }
+    k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, x, d_weight_, d_xb_, st);
+    if (mixed_)
+        k_symv<float><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_S32_, d_xb_, d_yb_, st);
+    else
+        k_symv<double><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_S_, d_xb_, d_yb_, st);
+    k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, d_weight_, z, nullptr, nullptr, st);
+}
+
+void Engine::op_P(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial,
+                  PcpgState *st) {
+    k_gft_partial<<<nchunks_, 256, 0, s_>>>(d_chunk_cl_, d_chunk_beg_, d_chunk_end_, d_crow_, d_cval_, x, d_gpart_, st);
+    k_gft_final<<<1, 256, 6 * ncl_ * sizeof(double), s_>>>(ncl_, d_cl_chunk_ptr_, d_gpart_, d_invGtG_, d_a_, alpha_out, st);
+    k_gf_apply<<<npart_, 256, 0, s_>>>(nlam_, d_gcl_, d_gval_, x, d_a_, Px, dotv, partial, st);
+}
+
+void Engine::iteration(PcpgState *st) {
+    op_F(d_w_, d_Fw_, d_w_, d_partial_, st);
+    k_update_lam_g<<<std::min(npart_, 1184), 256, 0, s_>>>(nlam_, d_partial_, npart_, d_w_, d_Fw_, d_lam_, d_g_, st);
+    op_P(d_g_, d_Pg_, d_alpha_, nullptr, nullptr, st);
+    op_M(d_Pg_, d_z_, st);
+    op_P(d_z_, d_Pz_, nullptr, d_g_, d_partial_, st);
+    k_update_w<<<std::min(npart_, 1184), 256, 0, s_>>>(nlam_, d_partial_, npart_, d_Pz_, d_w_, st);
+    k_finish_iter<<<1, 256, 0, s_>>>(d_partial_, npart_, st);
+}
+
+int Engine::apply(int op, const double *x, double *y, int nrhs, std::string &err) {
+    for (int k = 0; k < nrhs; ++k) {
+        CK(cudaMemcpyAsync(d_tmp_, x + (size_t)k * nlam_, nlam_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+        if (op == 0) op_F(d_tmp_, d_Fw_, nullptr, nullptr, nullptr);
+        else if (op == 1) op_P(d_tmp_, d_Fw_, nullptr, nullptr, nullptr, nullptr);
+        else op_M(d_tmp_, d_Fw_, nullptr);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(y + (size_t)k * nlam_, d_Fw_, nlam_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    }
+    CK(cudaStreamSynchronize(s_));
+    return HTF_OK;
+}
+
+// one load case: Cluster::pcpg (Cluster.cpp:1363-1458) + printVTK (1648-1678)
+int Engine::solve_one(Problem &p, int rhs, double *u_loc_host, int &iters, double &norm0, double &rel,
+                      double &solve_ms, std::string &err) {
+    const double *f = d_f_ + (size_t)rhs * nfull_;
+    int maxcols = 0;
+    for (auto &h : hs_) maxcols = std::max(maxcols, h.c + 6);
+    int maxg = 0;
+    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
+    auto kplus_full = [&](double *v) {          // v <- K_reg^{-1} v on full vectors
+        k_trsv_fwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, v, 0);
+        k_trsv_bwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, v, 0);
+    };
+    auto coarse_from_full = [&](const double *z, const double *y) {   // s = M [Bc z ; -R^T y]
+        k_bc_rt<<<nsub_, 256, 0, s_>>>(d_subs_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_R_, z, y, d_t_);
+        k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, nullptr);
+        k_coarse<<<dim3(ncl_, cdiv(maxg, 8)), 256, 0, s_>>>(d_cl_, d_M_, d_gc_, d_s_, nullptr);
+    };
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    // x = K_HT^+ f ; d = Bf x  (Cluster.cpp:1385-1387, 967-1040)
+    CK(cudaMemcpyAsync(d_full_, f, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+    kplus_full(d_full_);
+    coarse_from_full(d_full_, f);
+    k_full_to_b<<<nsub_, 256, 0, s_>>>(d_subs_, d_full_, d_yb_);
+    k_correct<<<nsub_, 256, 0, s_>>>(d_subs_, d_cl_, d_V_, d_bcr_, d_s_, d_yb_, nullptr);
+    k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, nullptr, d_d_, nullptr, nullptr, nullptr);
+    // e = Rf^T f ; lambda0 = Gf (GfTGf)^{-1} e  (Cluster.cpp:1390-1394)
+    {
+        k_e_vec<<<cdiv(6 * ncl_, 128), 128, 0, s_>>>(ncl_, d_csp_, d_cs_, d_subs_, d_H_, d_t_, d_gc_);
+        k_small_gemv<<<1, 256, 0, s_>>>(6 * ncl_, d_invGtG_, d_gc_, d_a_);
+        k_gf_mult<<<npart_, 256, 0, s_>>>(nlam_, d_gcl_, d_gval_, d_a_, d_lam_);
+    }
+    CK(cudaEventRecord(e0, s_));
+    // g0 = F lambda0 - d ; Pg ; z = M Pg ; Pz ; gPz  (Cluster.cpp:1398-1412)
+    op_F(d_lam_, d_g_, nullptr, nullptr, nullptr);
+    k_axpby<<<npart_, 256, 0, s_>>>(nlam_, -1.0, d_d_, 1.0, d_g_);
+    op_P(d_g_, d_Pg_, d_alpha_, nullptr, nullptr, nullptr);
+    op_M(d_Pg_, d_z_, nullptr);
+    op_P(d_z_, d_Pz_, nullptr, d_g_, d_partial_, nullptr);
+    k_init_state<<<1, 256, 0, s_>>>(d_partial_, npart_, d_st_, opt_.eps_iter, opt_.max_iter);
+    CK(cudaMemcpyAsync(d_w_, d_Pz_, nlam_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+    CK(cudaGetLastError());
+    // iterations: one captured graph per iteration, host check every few
+    if (!graph_) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        iteration(d_st_);
+        CK(cudaStreamEndCapture(s_, &g));
+        CK(cudaGraphInstantiate(&graph_, g, 0));
+        cudaGraphDestroy(g);
+    }
+    PcpgState hst;
+    const int every = std::max(1, opt_.check_every);
+    for (;;) {
+        for (int k = 0; k < every; ++k) CK(cudaGraphLaunch(graph_, s_));
+        CK(cudaMemcpyAsync(&hst, d_st_, sizeof(PcpgState), cudaMemcpyDeviceToHost, s_));
+        CK(cudaStreamSynchronize(s_));
+        if (hst.done) break;
+    }
+    CK(cudaEventRecord(e1, s_));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    solve_ms = ms;
+    iters = hst.it;
+    norm0 = hst.norm0;
+    rel = hst.rel;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // u = K_HT^+(f - Bf^T lambda) - Rf alpha  (Cluster.cpp:1648-1678)
+    CK(cudaMemcpyAsync(d_full_, f, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+    k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, d_lam_, nullptr, d_xb_, nullptr);
+    k_full_minus_b<<<nsub_, 256, 0, s_>>>(d_subs_, d_xb_, d_full_);                       // y = f - Bf^T lam
+    CK(cudaMemcpyAsync(d_full2_, d_full_, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+    kplus_full(d_full2_);                                                                  // z = K_reg^{-1} y
+    coarse_from_full(d_full2_, d_full_);                                                   // s = M [Bc z; -R^T y]
+    k_sub_bct<<<nsub_, 32, 0, s_>>>(d_subs_, d_cl_, d_bcr_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_s_, d_full_);
+    kplus_full(d_full_);                                                                   // K_reg^{-1}(y - Bc^T lam_c)
+    k_add_R<<<nsub_, 256, 0, s_>>>(d_subs_, d_cl_, d_R_, d_H_, d_s_, d_alpha_, d_full_);
+    CK(cudaGetLastError());
+    if (u_loc_host) CK(cudaMemcpyAsync(u_loc_host, d_full_, nfull_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    if (hst.done == 2) { err = "PCPG breakdown (w'Fw <= 0 or non-finite)"; return HTF_EBREAKDOWN; }
+    return HTF_OK;
+}
+
+int Engine::pcpg(Problem &p, double *u, htf_stats *stats, std::string &err) {
+    const int nrhs = p.nrhs;
+    // nodal loads into the permuted full vectors (lowest subdomain owns a DOF)
+    if (!p.f_nodal.empty()) {
+        const size_t ndof = 3 * (size_t)p.mesh.n_nodes;
+        std::vector<int> owner(ndof, -1);
+        for (int d = 0; d < nsub_; ++d)
+            for (int g : p.sub[d].l2g)
+                if (owner[g] < 0) owner[g] = d;
+        std::vector<double> fh((size_t)nfull_ * nrhs, 0.0);
+        for (int r = 0; r < nrhs; ++r)
+            for (int d = 0; d < nsub_; ++d) {
+                const Subdomain &s = p.sub[d];
+                for (int l = 0; l < s.n; ++l) {
+                    int g = s.l2g[l];
+                    if (owner[g] == d) fh[(size_t)r * nfull_ + hs_[d].nfull_off + s.perm[l]] = p.f_nodal[(size_t)r * ndof + g];
+                }
+            }
+        double *d_tmpf = nullptr;
+        int rc = HTF_OK;
+        d_tmpf = alloc<double>(fh.size(), err, rc);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(d_tmpf, fh.data(), fh.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+        // replicate the assembled body force to every load case, add nodal loads
+        for (int r = 1; r < nrhs; ++r)
+            CK(cudaMemcpyAsync(d_f_ + (size_t)r * nfull_, d_f_, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+        k_axpby<<<cdiv((long long)nfull_ * nrhs, 256), 256, 0, s_>>>(nfull_ * nrhs, 1.0, d_tmpf, 1.0, d_f_);
+        CK(cudaGetLastError());
+        p.f_nodal.clear();          // loads are now in d_f_
+    }
+    std::vector<double> uloc(nfull_);
+    const size_t ndof = 3 * (size_t)p.mesh.n_nodes;
+    double total_ms = 0.0;
+    for (int r = 0; r < nrhs; ++r) {
+        int it = 0;
+        double n0 = 0, rel = 0, ms = 0;
+        int rc = solve_one(p, r, uloc.data(), it, n0, rel, ms, err);
+        total_ms += ms;
+        if (stats && r < 64) { stats->iterations[r] = it; stats->norm_gPz0[r] = n0; stats->final_rel[r] = rel; }
+        if (u) {
+            double *ur = u + (size_t)r * ndof;
+            for (int d = 0; d < nsub_; ++d) {       // last writer wins (Cluster.cpp:1672-1676)
+                const Subdomain &s = p.sub[d];
+                for (int l = 0; l < s.n; ++l) ur[s.l2g[l]] = uloc[hs_[d].nfull_off + s.perm[l]];
+            }
+        }
+        if (rc) return rc;
+        if (it >= opt_.max_iter && rel >= opt_.eps_iter) {
+            if (stats) stats->solve_ms = total_ms;
+            err = "PCPG did not converge within max_iter";
+            return HTF_ENOCONV;
+        }
+    }
+    if (stats) {
+        stats->solve_ms = total_ms;
+        stats->setup_ms = setup_ms;
+        stats->fapply_bytes = fapply_bytes_;
+        stats->n_lambda = nlam_;
+        stats->n_sub = nsub_;
+        stats->n_clusters = ncl_;
+        stats->n_rhs = nrhs;
+        stats->status_sub = status_sub;
+    }
+    return HTF_OK;
+}
+
+}  // namespace htf

@@ -1,0 +1,88 @@
+// Host-side engine of the HTFETI path: owns the device buffers of one
+// problem, runs the GPU setup and the PCPG iterations.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../host/problem.hpp"
+#include "device.cuh"
+
+namespace htf {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+class Engine {
+public:
+    explicit Engine(const Options &o) : opt_(o) {}
+    ~Engine();
+    int setup(Problem &p, std::string &err);
+    int pcpg(Problem &p, double *u, htf_stats *stats, std::string &err);
+    int apply(int op, const double *x, double *y, int nrhs, std::string &err);   // 0=F, 1=P, 2=M
+    double setup_ms = 0.0;
+    int status_sub = -1;
+
+private:
+    template <typename T> T *alloc(size_t n, std::string &err, int &rc);
+    int check(cudaError_t e, const char *what, std::string &err);
+    int upload_layout(Problem &p, std::string &err);
+    int factorize(Problem &p, std::string &err);
+    int coarse(Problem &p, std::string &err);
+    int outer_coarse(Problem &p, std::string &err);
+    // device operators on device vectors (length n_lam)
+    void op_F(const double *w, double *Fw, const double *dotv, double *partial, PcpgState *st);
+    void op_M(const double *x, double *z, PcpgState *st);
+    void op_P(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial,
+              PcpgState *st);
+    void iteration(PcpgState *st);
+    int solve_one(Problem &p, int rhs, double *u_loc_host, int &iters, double &norm0, double &rel,
+                  double &solve_ms, std::string &err);
+
+    Options opt_;
+    cudaStream_t s_ = nullptr;
+    std::vector<DevBuf> bufs_;
+    int nsub_ = 0, ncl_ = 0, nlam_ = 0, nslots_ = 0, nfull_ = 0, ngc_total_ = 0, nt_total_ = 0;
+    long long ntiles_ = 0;
+    std::vector<SubDev> hs_;
+    std::vector<ClusterDev> hc_;
+    SubDev *d_subs_ = nullptr;
+    ClusterDev *d_cl_ = nullptr;
+    int *d_all_subs_ = nullptr;          // 0..nsub-1
+    double *d_K_ = nullptr, *d_F_ = nullptr, *d_S_ = nullptr, *d_X_ = nullptr;
+    float *d_F32_ = nullptr, *d_S32_ = nullptr;
+    double *d_V_ = nullptr, *d_R_ = nullptr, *d_M_ = nullptr, *d_H_ = nullptr;
+    int *d_bcr_ = nullptr, *d_bce_ptr_ = nullptr, *d_bce_pos_ = nullptr;
+    double *d_bce_val_ = nullptr;
+    int *d_slot_ptr_ = nullptr, *d_slot_ent_ = nullptr;
+    int *d_rslot_ = nullptr;
+    double *d_rsign_ = nullptr, *d_weight_ = nullptr;
+    int *d_gptr_ = nullptr, *d_gidx_ = nullptr;
+    int *d_gcl_ = nullptr;
+    double *d_gval_ = nullptr;
+    int *d_chunk_cl_ = nullptr, *d_chunk_beg_ = nullptr, *d_chunk_end_ = nullptr, *d_crow_ = nullptr,
+        *d_cl_chunk_ptr_ = nullptr;
+    double *d_cval_ = nullptr, *d_invGtG_ = nullptr;
+    int nchunks_ = 0;
+    int *d_status_ = nullptr;
+    int *d_csp_ = nullptr, *d_cs_ = nullptr;   // cluster -> subdomain lists
+    // vectors
+    double *d_f_ = nullptr, *d_full_ = nullptr, *d_full2_ = nullptr;
+    double *d_lam_ = nullptr, *d_g_ = nullptr, *d_w_ = nullptr, *d_Fw_ = nullptr, *d_Pg_ = nullptr,
+           *d_z_ = nullptr, *d_Pz_ = nullptr, *d_d_ = nullptr, *d_tmp_ = nullptr;
+    double *d_xb_ = nullptr, *d_yb_ = nullptr, *d_t_ = nullptr, *d_gc_ = nullptr, *d_s_ = nullptr;
+    double *d_a_ = nullptr, *d_alpha_ = nullptr, *d_partial_ = nullptr, *d_gpart_ = nullptr;
+    PcpgState *d_st_ = nullptr;
+    int npart_ = 0;
+    int symv_smem_ = 0;
+    bool mixed_ = false;
+    cudaGraphExec_t graph_ = nullptr;
+    double fapply_ms_ = 0.0, fapply_bytes_ = 0.0;
+    std::vector<std::vector<double>> Hd_;   // per subdomain 6x6 rows of ker(Gc)
+    std::vector<double> invGtG_;
+};
+
+}  // namespace htf

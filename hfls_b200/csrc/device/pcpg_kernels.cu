@@ -1,0 +1,433 @@
+// PCPG kernels of the HTFETI path (sm_100a).  All reductions are
+// deterministic (fixed-order trees, no floating-point atomics), so a solve
+// gives the same bits alone and inside a batch.
+//
+//  F w = Bf K_HT^+ Bf^T w   (Cluster::mult_Ff, Cluster.cpp:1114-1188):
+//    k_gather_b   x_b = Bf_d^T w             signed gather over the b slots
+//    k_symv       y_b = F_d x_b              packed 32x32 lower tiles, one pass
+//    k_vt         t_d = V_d^T x_b            V = [F Bc_b^T, -R_b]
+//    k_gc         gc  = sum_d t_d            per cluster (gather map)
+//    k_coarse     s   = M gc                 M = Ac^{-1} restricted
+//    k_correct    y_b -= V_d s_d
+//    k_rows       Fw  = Bf y                 <= 2 entries per row
+//  Preconditioner (Cluster::Preconditioning, Cluster.cpp:1043-1112):
+//    k_gather_b(weighted) -> k_symv(S_d or K_bb) -> k_rows(weighted)
+//  Projector (Cluster::Projection, Cluster.cpp:1314-1329):
+//    k_gft_partial -> k_gft_final -> k_gf_apply
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "device.cuh"
+
+namespace htf {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// signed gather: x[slot] = sum_e sign_e * (weight[lam_e]) * w[lam_e]
+// ent = 2*lam + (sign < 0)
+// ---------------------------------------------------------------------------
+__global__ void k_gather_b(int nslots, const int *__restrict__ ptr, const int *__restrict__ ent,
+                           const double *__restrict__ w, const double *__restrict__ weight,
+                           double *__restrict__ x, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nslots) return;
+    double v = 0.0;
+    for (int e = ptr[i]; e < ptr[i + 1]; ++e) {
+        const int q = ent[e];
+        const int lam = q >> 1;
+        double a = w[lam];
+        if (weight) a *= weight[lam];
+        v += (q & 1) ? -a : a;
+    }
+    x[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// y_b = A x_b for packed symmetric tiles; one CTA per subdomain, 4 warps,
+// per-warp partial sums in shared memory summed in fixed order.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void reduce_scatter32(double (&p)[32], int lane) {
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const bool upper = lane & s;
+#pragma unroll
+        for (int q = 0; q < s; ++q) {
+            const double send = upper ? p[q] : p[q + s];
+            const double keep = upper ? p[q + s] : p[q];
+            p[q] = keep + __shfl_xor_sync(FULL, send, s);
+        }
+    }
+}
+
+constexpr int SYMV_WARPS = 4;
+
+template <typename T>
+__global__ void __launch_bounds__(SYMV_WARPS * 32) k_symv(const SubDev *__restrict__ subs,
+                                                          const T *__restrict__ tiles,
+                                                          const double *__restrict__ xb,
+                                                          double *__restrict__ yb,
+                                                          const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    extern __shared__ double sm[];
+    const SubDev &sd = subs[blockIdx.x];
+    const int nbp = sd.nbp, nt = sd.nt;
+    double *xs = sm;                       // nbp
+    double *yp = sm + nbp;                 // SYMV_WARPS x nbp
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+    for (int i = threadIdx.x; i < nbp; i += blockDim.x) xs[i] = xb[sd.xb_off + i];
+    for (int i = threadIdx.x; i < SYMV_WARPS * nbp; i += blockDim.x) yp[i] = 0.0;
+    __syncthreads();
+    double *my = yp + warp * nbp;
+    const long long ntiles = (long long)nt * (nt + 1) / 2;
+    const T *base = tiles + sd.T_off * TILE_ELEMS;
+    for (long long t = warp; t < ntiles; t += SYMV_WARPS) {
+        int I = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+        while ((long long)(I + 1) * (I + 2) / 2 <= t) ++I;
+        while ((long long)I * (I + 1) / 2 > t) --I;
+        const int J = (int)(t - (long long)I * (I + 1) / 2);
+        const T *tp = base + t * TILE_ELEMS;
+        double v[32];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) v[r] = (double)tp[r * TILE + lane];    // v[r] = A[r][lane]
+        const double xJ = xs[TILE * J + lane];
+        double p[32];
+        double col = 0.0;
+#pragma unroll
+        for (int r = 0; r < 32; ++r) {
+            p[r] = v[r] * xJ;
+            col += v[r] * xs[TILE * I + r];
+        }
+        reduce_scatter32(p, lane);
+        my[TILE * I + lane] += p[0];                   // row sums -> y_I
+        if (I != J) my[TILE * J + lane] += col;        // column sums -> y_J
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nbp; i += blockDim.x) {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < SYMV_WARPS; ++q) s += yp[q * nbp + i];
+        yb[sd.xb_off + i] = s;
+    }
+}
+
+template __global__ void k_symv<double>(const SubDev *, const double *, const double *, double *,
+                                        const PcpgState *);
+template __global__ void k_symv<float>(const SubDev *, const float *, const double *, double *,
+                                       const PcpgState *);
+
+// t_d = V_d^T x_b  (c+6 values per subdomain)
+__global__ void k_vt(const SubDev *__restrict__ subs, const double *__restrict__ Vbuf,
+                     const double *__restrict__ xb, double *__restrict__ t, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    const SubDev &sd = subs[blockIdx.x];
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nw = blockDim.x / 32;
+    const double *x = xb + sd.xb_off;
+    for (int col = warp; col < sd.c + 6; col += nw) {
+        const double *V = Vbuf + sd.V_off + (size_t)col * sd.nbp;
+        double s = 0.0;
+        for (int i = lane; i < sd.nb; i += 32) s += V[i] * x[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+        if (lane == 0) t[sd.t_off + col] = s;
+    }
+}
+
+// gc[q] = sum of the t entries listed for q (fixed order)
+__global__ void k_gc(int ngc_total, const int *__restrict__ gptr, const int *__restrict__ gidx,
+                     const double *__restrict__ t, double *__restrict__ gc, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ngc_total) return;
+    double s = 0.0;
+    for (int e = gptr[q]; e < gptr[q + 1]; ++e) s += t[gidx[e]];
+    gc[q] = s;
+}
+
+// s = M gc per cluster; one warp per row
+__global__ void k_coarse(const ClusterDev *__restrict__ cl, const double *__restrict__ Mbuf,
+                         const double *__restrict__ gc, double *__restrict__ s, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    const ClusterDev c = cl[blockIdx.x];
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nw = blockDim.x / 32;
+    const int row = blockIdx.y * nw + warp;
+    if (row >= c.ngc) return;
+    const double *M = Mbuf + c.M_off + (size_t)row * c.ngc;     // symmetric: column = row
+    const double *g = gc + c.gc_off;
+    double a = 0.0;
+    for (int p = lane; p < c.ngc; p += 32) a += M[p] * g[p];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(FULL, a, o);
+    if (lane == 0) s[c.gc_off + row] = a;
+}
+
+// y_b -= V_d s_d  with s_d = (s at the Bc rows of d, alpha_d)
+__global__ void k_correct(const SubDev *__restrict__ subs, const ClusterDev *__restrict__ cl,
+                          const double *__restrict__ Vbuf, const int *__restrict__ bcrows,
+                          const double *__restrict__ s, double *__restrict__ yb, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    __shared__ double sd_s[256];
+    const SubDev &sd = subs[blockIdx.x];
+    const ClusterDev &c = cl[sd.cluster];
+    const int nc = sd.c + 6;
+    for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+        const int pos = (q < sd.c) ? bcrows[sd.bcr_off + q] : sd.alpha_pos + (q - sd.c);
+        sd_s[q] = s[c.gc_off + pos];
+    }
+    __syncthreads();
+    const double *V = Vbuf + sd.V_off;
+    double *y = yb + sd.xb_off;
+    for (int i = threadIdx.x; i < sd.nb; i += blockDim.x) {
+        double a = y[i];
+        for (int q = 0; q < nc; ++q) a -= V[i + (size_t)q * sd.nbp] * sd_s[q];
+        y[i] = a;
+    }
+}
+
+// out[r] = wt[r] * sum_k sign_k * y[slot_k]; optional fused dot partial with `dotv`
+__global__ void k_rows(int nlam, const int *__restrict__ rslot, const double *__restrict__ rsign,
+                       const double *__restrict__ yb, const double *__restrict__ weight,
+                       double *__restrict__ out, const double *__restrict__ dotv,
+                       double *__restrict__ partial, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    __shared__ double red[256];
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    double prod = 0.0;
+    if (r < nlam) {
+        double v = 0.0;
+        const int s0 = rslot[2 * r], s1 = rslot[2 * r + 1];
+        if (s0 >= 0) v += rsign[2 * r] * yb[s0];
+        if (s1 >= 0) v += rsign[2 * r + 1] * yb[s1];
+        if (weight) v *= weight[r];
+        out[r] = v;
+        if (dotv) prod = v * dotv[r];
+    }
+    if (!partial) return;
+    red[threadIdx.x] = prod;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+// ---------------------------------------------------------------------------
+// deterministic dot products
+// ---------------------------------------------------------------------------
+__global__ void k_dot_partial(int n, const double *__restrict__ a, const double *__restrict__ b,
+                              double *__restrict__ partial, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+__device__ double block_sum_fixed(const double *partial, int np) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partial[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_sum_to(const double *__restrict__ partial, int np, double *__restrict__ out,
+                         const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    const double s = block_sum_fixed(partial, np);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// ---------------------------------------------------------------------------
+// projector: a = (Gf^T Gf)^{-1} Gf^T x ; Px = x - Gf a
+// Gf stored per cluster as a list of (row, 6 values); per row as up to two
+// (cluster, 6 values) entries.
+// ---------------------------------------------------------------------------
+__global__ void k_gft_partial(const int *__restrict__ chunk_cl, const int *__restrict__ chunk_beg,
+                              const int *__restrict__ chunk_end, const int *__restrict__ crow,
+                              const double *__restrict__ cval, const double *__restrict__ x,
+                              double *__restrict__ partial, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    __shared__ double red[6][256];
+    const int ch = blockIdx.x;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int e = chunk_beg[ch] + threadIdx.x; e < chunk_end[ch]; e += blockDim.x) {
+        const double xv = x[crow[e]];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) s[q] += cval[6 * (size_t)e + q] * xv;
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) red[q][threadIdx.x] = s[q];
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) partial[6 * (size_t)ch + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// one CTA: a = invGtG * (sum of chunk partials per cluster); alpha_out = -a
+__global__ void k_gft_final(int ncl, const int *__restrict__ cl_chunk_ptr, const double *__restrict__ partial,
+                            const double *__restrict__ invGtG, double *__restrict__ a,
+                            double *__restrict__ alpha_out, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    extern __shared__ double gt[];
+    const int m = 6 * ncl;
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+        const int c = q / 6, i = q % 6;
+        double s = 0.0;
+        for (int ch = cl_chunk_ptr[c]; ch < cl_chunk_ptr[c + 1]; ++ch) s += partial[6 * (size_t)ch + i];
+        gt[q] = s;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+        double s = 0.0;
+        for (int p = 0; p < m; ++p) s += invGtG[q + (size_t)p * m] * gt[p];
+        a[q] = s;
+        if (alpha_out) alpha_out[q] = -s;
+    }
+}
+
+__global__ void k_gf_apply(int nlam, const int *__restrict__ gcl, const double *__restrict__ gval,
+                           const double *__restrict__ x, const double *__restrict__ a, double *__restrict__ Px,
+                           const double *__restrict__ dotv, double *__restrict__ partial,
+                           const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    __shared__ double red[256];
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    double prod = 0.0;
+    if (r < nlam) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int c = gcl[2 * r + k];
+            if (c < 0) continue;
+            const double *g = gval + 6 * (size_t)(2 * r + k);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) v += g[q] * a[6 * c + q];
+        }
+        const double pv = x[r] - v;
+        Px[r] = pv;
+        if (dotv) prod = pv * dotv[r];
+    }
+    if (!partial) return;
+    red[threadIdx.x] = prod;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+// lambda = G a  (initial lambda0 = Gf (GfTGf)^{-1} e)
+__global__ void k_gf_mult(int nlam, const int *__restrict__ gcl, const double *__restrict__ gval,
+                          const double *__restrict__ a, double *__restrict__ out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nlam) return;
+    double v = 0.0;
+    for (int k = 0; k < 2; ++k) {
+        const int c = gcl[2 * r + k];
+        if (c < 0) continue;
+        const double *g = gval + 6 * (size_t)(2 * r + k);
+        for (int q = 0; q < 6; ++q) v += g[q] * a[6 * c + q];
+    }
+    out[r] = v;
+}
+
+// ---------------------------------------------------------------------------
+// PCPG scalar / vector updates (Cluster::pcpg, Cluster.cpp:1422-1450)
+// ---------------------------------------------------------------------------
+// after Fw and the partials of w.Fw: rho = -gPz / wFw ; lam += rho w ; g += rho Fw
+__global__ void k_update_lam_g(int n, const double *__restrict__ partial, int np, const double *__restrict__ w,
+                               const double *__restrict__ Fw, double *__restrict__ lam, double *__restrict__ g,
+                               PcpgState *__restrict__ st) {
+    if (st->done) return;
+    __shared__ double rho_s;
+    const double wFw = block_sum_fixed(partial, np);
+    if (threadIdx.x == 0) {
+        double rho = -st->gPz / wFw;
+        if (!(wFw > 0.0) || !isfinite(rho)) rho = 0.0;
+        rho_s = rho;
+        if (blockIdx.x == 0) {
+            st->wFw = wFw;
+            st->rho = rho;
+        }
+    }
+    __syncthreads();
+    const double rho = rho_s;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        lam[i] += rho * w[i];
+        g[i] += rho * Fw[i];
+    }
+}
+
+// after Pz and the partials of g.Pz: gamma, w = Pz + gamma w, convergence test
+__global__ void k_update_w(int n, const double *__restrict__ partial, int np, const double *__restrict__ Pz,
+                           double *__restrict__ w, PcpgState *__restrict__ st) {
+    if (st->done) return;
+    __shared__ double gam_s;
+    const double gPz = block_sum_fixed(partial, np);
+    if (threadIdx.x == 0) gam_s = gPz / st->gPz;
+    __syncthreads();
+    const double gam = gam_s;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) w[i] = Pz[i] + gam * w[i];
+    // st->gPz is committed by k_finish_iter, launched after this kernel
+}
+
+// end of one iteration: commit gPz/gamma, count it, test convergence
+__global__ void k_finish_iter(const double *__restrict__ partial, int np, PcpgState *__restrict__ st) {
+    if (st->done) return;
+    const double gPz = block_sum_fixed(partial, np);
+    if (threadIdx.x == 0) {
+        st->gamma = gPz / st->gPz;
+        st->gPz_prev = st->gPz;
+        st->gPz = gPz;
+        st->it += 1;
+        st->rel = sqrt(gPz) / st->norm0;
+        if (!(st->wFw > 0.0) || !isfinite(gPz)) st->done = 2;          // breakdown
+        else if (sqrt(gPz) < st->eps * st->norm0) st->done = 1;        // converged
+        else if (st->it >= st->max_iter) st->done = 3;                  // max_iter
+    }
+}
+
+// initial state: norm0 = sqrt(g0.Pz0)
+__global__ void k_init_state(const double *__restrict__ partial, int np, PcpgState *__restrict__ st, double eps,
+                             int max_iter) {
+    const double gPz = block_sum_fixed(partial, np);
+    if (threadIdx.x == 0) {
+        st->gPz = gPz;
+        st->gPz_prev = gPz;
+        st->norm0 = sqrt(gPz);
+        st->rel = 1.0;
+        st->it = 0;
+        st->eps = eps;
+        st->max_iter = max_iter;
+        st->wFw = 1.0;
+        st->done = (gPz > 0.0 && isfinite(gPz)) ? ((max_iter <= 0) ? 3 : 0) : (gPz == 0.0 ? 1 : 2);
+    }
+}
+
+// generic: y = a*x + b*y on n entries
+__global__ void k_axpby(int n, double a, const double *__restrict__ x, double b, double *__restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a * x[i] + b * y[i];
+}
+
+}  // namespace htf

@@ -1,0 +1,510 @@
+// Setup kernels of the HTFETI path (FP64, sm_100a).
+//
+//  k_assemble        hex8 element stiffness (2x2x2 Gauss) and body-force
+//                    load, scattered into the dense permuted K_d; elements of
+//                    one colour share no node, so no atomics are needed.
+//                    Restates Data::stf_mtrx_solid45 (Data.cpp:297-490) with
+//                    the standard J^{-T} gradient and Data::feti_numeric
+//                    (Data.cpp:231-273).
+//  k_potrf_diag /    step-synchronous batched right-looking Cholesky: one
+//  k_trsm_panel /    launch per 32-column step covers every subdomain that
+//  k_syrk_update     still has that step (replaces the PARDISO factorisation
+//                    of K_reg, Matrix.cpp:1115-1202).
+//  k_snapshot        copies S_reg - D_fix (Dirichlet) or K_bb (lumped) of the
+//                    trailing block into packed tiles (Matrix.cpp:1708-1871).
+//  k_trtri_step      X = L_bb^{-1}, one launch per 32-row block.
+//  k_lauum_tiles     F = X^T X = (K_reg^{-1})_bb into packed tiles.
+//  k_build_V/Fc      V = [F Bc_b^T, -R_b] and Fc_d = Bc_b F Bc_b^T
+//                    (Cluster.cpp:150-185).
+//  k_trsv_fwd/bwd    batched dense triangular solves with the full factor.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "device.cuh"
+
+namespace htf {
+
+// ---------------------------------------------------------------------------
+// assembly
+// ---------------------------------------------------------------------------
+__constant__ double c_gp[8][3];      // Gauss points (Data.cpp:363-386 order)
+
+// Gauss points +-0.577350269189626 (the reference's literal, Data.cpp:344)
+cudaError_t set_gauss_points(cudaStream_t s) {
+    const double pt = 0.577350269189626;
+    const double gr[8] = {-pt, -pt, -pt, -pt, pt, pt, pt, pt}, gs[8] = {-pt, -pt, pt, pt, -pt, -pt, pt, pt},
+                 gt[8] = {-pt, pt, -pt, pt, -pt, pt, -pt, pt};
+    double gp[8][3];
+    for (int g = 0; g < 8; ++g) { gp[g][0] = gr[g]; gp[g][1] = gs[g]; gp[g][2] = gt[g]; }
+    return cudaMemcpyToSymbolAsync(c_gp, gp, sizeof(gp), 0, cudaMemcpyHostToDevice, s);
+}
+
+__global__ void k_assemble(const int *__restrict__ elist, int count, const double *__restrict__ ecoord,
+                           const int *__restrict__ esub, const int *__restrict__ eperm,
+                           const double *__restrict__ subE, const double *__restrict__ subnu,
+                           const SubDev *__restrict__ subs, double *__restrict__ Kbuf,
+                           double *__restrict__ fbuf, double bfx, double bfy, double bfz) {
+    __shared__ double G[8][8][3];    // dN_a/dx_k at Gauss point g
+    __shared__ double Nw[8][8];      // N_a * detJ
+    __shared__ double W[8];          // detJ
+    __shared__ int P[24];
+    __shared__ double X[8][3];
+    const int e = elist[blockIdx.x];
+    const int t = threadIdx.x;
+    if (t < 24) {
+        X[t / 3][t % 3] = ecoord[24 * (size_t)e + t];
+        P[t] = eperm[24 * (size_t)e + t];
+    }
+    __syncthreads();
+    if (t < 8) {
+        const double r = c_gp[t][0], s = c_gp[t][1], q = c_gp[t][2];
+        const double rn[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+        const double sn[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+        const double tn[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+        double dNr[8], dNs[8], dNt[8], N[8];
+        for (int a = 0; a < 8; ++a) {
+            dNr[a] = 0.125 * rn[a] * (1. + sn[a] * s) * (1. + tn[a] * q);
+            dNs[a] = 0.125 * sn[a] * (1. + rn[a] * r) * (1. + tn[a] * q);
+            dNt[a] = 0.125 * tn[a] * (1. + rn[a] * r) * (1. + sn[a] * s);
+            N[a] = 0.125 * (1. + rn[a] * r) * (1. + sn[a] * s) * (1. + tn[a] * q);
+        }
+        // M[i][j] = d x_i / d r_j
+        double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int a = 0; a < 8; ++a)
+            for (int i = 0; i < 3; ++i) {
+                M[i][0] += dNr[a] * X[a][i];
+                M[i][1] += dNs[a] * X[a][i];
+                M[i][2] += dNt[a] * X[a][i];
+            }
+        const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) -
+                           M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                           M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+        const double id = 1.0 / det;
+        // Mi = M^{-1}: Mi[j][i] = d r_j / d x_i
+        double Mi[3][3];
+        Mi[0][0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) * id;
+        Mi[0][1] = -(M[0][1] * M[2][2] - M[0][2] * M[2][1]) * id;
+        Mi[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) * id;
+        Mi[1][0] = -(M[1][0] * M[2][2] - M[1][2] * M[2][0]) * id;
+        Mi[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) * id;
+        Mi[1][2] = -(M[0][0] * M[1][2] - M[0][2] * M[1][0]) * id;
+        Mi[2][0] = (M[1][0] * M[2][1] - M[1][1] * M[2][0]) * id;
+        Mi[2][1] = -(M[0][0] * M[2][1] - M[0][1] * M[2][0]) * id;
+        Mi[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) * id;
+        for (int a = 0; a < 8; ++a) {
+            for (int i = 0; i < 3; ++i)      // dN/dx_i = sum_j dN/dr_j * dr_j/dx_i
+                G[t][a][i] = dNr[a] * Mi[0][i] + dNs[a] * Mi[1][i] + dNt[a] * Mi[2][i];
+            Nw[t][a] = N[a] * det;
+        }
+        W[t] = det;
+    }
+    __syncthreads();
+    const int d = esub[e];
+    const SubDev sd = subs[d];
+    const double E = subE[d], nu = subnu[d];
+    const double lam = E * nu / ((1. + nu) * (1. - 2. * nu));
+    const double mu = E / (2. * (1. + nu));
+    double *K = Kbuf + sd.K_off;
+    for (int idx = t; idx < 576; idx += blockDim.x) {
+        const int I = idx % 24, J = idx / 24;
+        const int pI = P[I], pJ = P[J];
+        if (pI < pJ) continue;                      // lower triangle in permuted order
+        const int i = I >> 3, a = I & 7, j = J >> 3, b = J & 7;
+        double v = 0.0;
+        for (int g = 0; g < 8; ++g) {
+            double s = lam * G[g][a][i] * G[g][b][j] + mu * G[g][a][j] * G[g][b][i];
+            if (i == j) s += mu * (G[g][a][0] * G[g][b][0] + G[g][a][1] * G[g][b][1] + G[g][a][2] * G[g][b][2]);
+            v += s * W[g];
+        }
+        K[pI + (size_t)pJ * sd.N] += v;
+    }
+    if (t < 24) {
+        const int i = t >> 3, a = t & 7;
+        const double bf = (i == 0) ? bfx : (i == 1) ? bfy : bfz;
+        double v = 0.0;
+        for (int g = 0; g < 8; ++g) v += bf * Nw[g][a];
+        fbuf[sd.nfull_off + P[t]] += v;
+    }
+}
+
+// K_reg = K + D_fix: double the diagonal at the fix DOFs (Matrix.cpp:1029-1057)
+// and put the identity on the padded rows.
+__global__ void k_regularize(SubDev *subs, int nsub, double *Kbuf) {
+    const int d = blockIdx.x;
+    if (d >= nsub) return;
+    SubDev &sd = subs[d];
+    double *K = Kbuf + sd.K_off;
+    if (threadIdx.x < 6) {
+        const int f = sd.fix[threadIdx.x];
+        const double v = K[f + (size_t)f * sd.N];
+        sd.fix_diag[threadIdx.x] = v;
+        K[f + (size_t)f * sd.N] = 2.0 * v;
+    }
+    for (int r = sd.nr + sd.nb + threadIdx.x; r < sd.N; r += blockDim.x) K[r + (size_t)r * sd.N] = 1.0;
+}
+
+// ---------------------------------------------------------------------------
+// batched Cholesky steps
+// ---------------------------------------------------------------------------
+__global__ void k_potrf_diag(const StepDesc *__restrict__ st, const SubDev *__restrict__ subs,
+                             double *__restrict__ Kbuf, int *__restrict__ status) {
+    __shared__ double A[32][33];
+    const StepDesc s = st[blockIdx.x];
+    const SubDev &sd = subs[s.d];
+    double *K = Kbuf + sd.K_off;
+    const int N = sd.N, k = s.k, nb = s.nb, lane = threadIdx.x;
+    for (int c = 0; c < nb; ++c) A[lane][c] = (lane < nb) ? K[(k + lane) + (size_t)(k + c) * N] : 0.0;
+    __syncwarp();
+    for (int j = 0; j < nb; ++j) {
+        if (lane == j) {
+            double dj = A[j][j];
+            if (!(dj > 0.0)) {
+                atomicCAS(&status[s.d], 0, k + j + 1);
+                dj = 1.0;
+            }
+            A[j][j] = sqrt(dj);
+        }
+        __syncwarp();
+        const double dj = A[j][j];
+        if (lane > j && lane < nb) A[lane][j] /= dj;
+        __syncwarp();
+        if (lane > j && lane < nb) {
+            const double lj = A[lane][j];
+            for (int c = j + 1; c <= lane; ++c) A[lane][c] -= lj * A[c][j];
+        }
+        __syncwarp();
+    }
+    if (lane < nb)
+        for (int c = 0; c <= lane; ++c) K[(k + lane) + (size_t)(k + c) * N] = A[lane][c];
+}
+
+__global__ void k_trsm_panel(const StepDesc *__restrict__ st, const SubDev *__restrict__ subs,
+                             double *__restrict__ Kbuf) {
+    __shared__ double L[32][33];
+    const StepDesc s = st[blockIdx.x];
+    const SubDev &sd = subs[s.d];
+    double *K = Kbuf + sd.K_off;
+    const int N = sd.N, k = s.k, nb = s.nb;
+    for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
+        const int r = i % 32, c = i / 32;
+        L[r][c] = (r < nb && c < nb && c <= r) ? K[(k + r) + (size_t)(k + c) * N] : 0.0;
+    }
+    __syncthreads();
+    const int row = k + nb + blockIdx.y * blockDim.x + threadIdx.x;
+    if (row >= N) return;
+    double x[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) x[j] = (j < nb) ? K[row + (size_t)(k + j) * N] : 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        if (j < nb) {
+            double v = x[j];
+#pragma unroll
+            for (int i = 0; i < j; ++i) v -= x[i] * L[j][i];
+            x[j] = v / L[j][j];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+        if (j < nb) K[row + (size_t)(k + j) * N] = x[j];
+}
+
+// C(64x64 block, lower part of the trailing matrix) -= P_i P_j^T, P = panel
+__global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict__ st,
+                                                     const SubDev *__restrict__ subs,
+                                                     double *__restrict__ Kbuf) {
+    __shared__ double Pa[32][64 + 1];
+    __shared__ double Pb[32][64 + 1];
+    const StepDesc s = st[blockIdx.x];
+    const SubDev &sd = subs[s.d];
+    const int N = sd.N, k = s.k, nb = s.nb;
+    const int t0 = k + nb;                  // first trailing row/col
+    const int m = N - t0;
+    const int nbr = (m + 63) / 64;
+    const int tri = blockIdx.y;
+    if (tri >= nbr * (nbr + 1) / 2) return;
+    int bi = (int)((sqrt(8.0 * tri + 1.0) - 1.0) * 0.5);
+    while ((bi + 1) * (bi + 2) / 2 <= tri) ++bi;
+    while (bi * (bi + 1) / 2 > tri) --bi;
+    const int bj = tri - bi * (bi + 1) / 2;
+    const int i0 = t0 + 64 * bi, j0 = t0 + 64 * bj;
+    double *K = Kbuf + sd.K_off;
+    for (int idx = threadIdx.x; idx < 32 * 64; idx += 256) {
+        const int r = idx % 64, kk = idx / 64;
+        const bool ok = kk < nb;
+        Pa[kk][r] = (ok && i0 + r < N) ? K[(i0 + r) + (size_t)(k + kk) * N] : 0.0;
+        Pb[kk][r] = (ok && j0 + r < N) ? K[(j0 + r) + (size_t)(k + kk) * N] : 0.0;
+    }
+    __syncthreads();
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int kk = 0; kk < nb; ++kk) {
+        double av[4], bv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) av[a] = Pa[kk][tx + 16 * a];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) bv[b] = Pb[kk][ty + 16 * b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const int col = j0 + ty + 16 * b;
+        if (col >= N) continue;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int row = i0 + tx + 16 * a;
+            if (row >= N || row < col) continue;
+            K[row + (size_t)col * N] -= acc[a][b];
+        }
+    }
+}
+
+// Copy the trailing nbp x nbp block into packed tiles, minus the fix diagonal.
+__global__ void k_snapshot(const int *__restrict__ dlist, const SubDev *__restrict__ subs,
+                           const double *__restrict__ Kbuf, double *__restrict__ Sbuf) {
+    const SubDev &sd = subs[dlist[blockIdx.x]];
+    const int tile = blockIdx.y;
+    if (tile >= sd.nt * (sd.nt + 1) / 2) return;
+    int I = (int)((sqrt(8.0 * tile + 1.0) - 1.0) * 0.5);
+    while ((I + 1) * (I + 2) / 2 <= tile) ++I;
+    while (I * (I + 1) / 2 > tile) --I;
+    const int J = tile - I * (I + 1) / 2;
+    const double *K = Kbuf + sd.K_off;
+    double *T = Sbuf + (sd.T_off + tile) * TILE_ELEMS;
+    for (int idx = threadIdx.x; idx < TILE_ELEMS; idx += blockDim.x) {
+        const int r = idx / TILE, c = idx % TILE;
+        int gr = sd.nr + TILE * I + r, gc = sd.nr + TILE * J + c;
+        if (gr < gc) { int tmp = gr; gr = gc; gc = tmp; }
+        double v = K[gr + (size_t)gc * sd.N];
+        if (gr == gc)
+            for (int q = 0; q < 6; ++q)
+                if (sd.fix[q] == gr) v -= sd.fix_diag[q];
+        T[idx] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// X = L_bb^{-1}: block row i of X, all block columns j <= i
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_trtri_step(int i, const int *__restrict__ dlist,
+                                                    const SubDev *__restrict__ subs,
+                                                    const double *__restrict__ Kbuf,
+                                                    double *__restrict__ Xbuf) {
+    __shared__ double La[32][33];
+    __shared__ double Xb[32][33];
+    __shared__ double T[32][33];
+    const SubDev &sd = subs[dlist[blockIdx.x]];
+    const int j = blockIdx.y;
+    if (i >= sd.nt || j > i) return;
+    const int N = sd.N, nbp = sd.nbp, base = sd.nr;
+    const double *K = Kbuf + sd.K_off;
+    double *X = Xbuf + sd.X_off;
+    const int tid = threadIdx.x;
+    const int r = tid % 32, c0 = (tid / 32) * 4;
+    double acc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = (i == j && r == c0 + q) ? 1.0 : 0.0;
+    for (int kb = j; kb < i; ++kb) {
+        for (int idx = tid; idx < 1024; idx += 256) {
+            const int rr = idx % 32, cc = idx / 32;
+            La[rr][cc] = K[(base + 32 * i + rr) + (size_t)(base + 32 * kb + cc) * N];
+            Xb[rr][cc] = X[(32 * kb + rr) + (size_t)(32 * j + cc) * nbp];
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int q = 0; q < 32; ++q) {
+            const double l = La[r][q];
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) acc[cc] -= l * Xb[q][c0 + cc];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) T[r][c0 + cc] = acc[cc];
+    for (int idx = tid; idx < 1024; idx += 256) {
+        const int rr = idx % 32, cc = idx / 32;
+        La[rr][cc] = (cc <= rr) ? K[(base + 32 * i + rr) + (size_t)(base + 32 * i + cc) * N] : 0.0;
+    }
+    __syncthreads();
+    if (tid < 32) {                        // forward substitution, one column per thread
+        const int col = tid;
+        for (int rr = 0; rr < 32; ++rr) {
+            double v = T[rr][col];
+            for (int q = 0; q < rr; ++q) v -= La[rr][q] * T[q][col];
+            T[rr][col] = v / La[rr][rr];
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < 1024; idx += 256) {
+        const int rr = idx % 32, cc = idx / 32;
+        X[(32 * i + rr) + (size_t)(32 * j + cc) * nbp] = T[rr][cc];
+    }
+}
+
+// F tile (I,J) = sum_{k >= I} X_kI^T X_kJ  (X lower triangular)
+__global__ void __launch_bounds__(256) k_lauum_tiles(const int *__restrict__ dlist,
+                                                     const SubDev *__restrict__ subs,
+                                                     const double *__restrict__ Xbuf,
+                                                     double *__restrict__ Fbuf) {
+    __shared__ double A[32][33];
+    __shared__ double B[32][33];
+    const SubDev &sd = subs[dlist[blockIdx.x]];
+    const int tile = blockIdx.y;
+    if (tile >= sd.nt * (sd.nt + 1) / 2) return;
+    int I = (int)((sqrt(8.0 * tile + 1.0) - 1.0) * 0.5);
+    while ((I + 1) * (I + 2) / 2 <= tile) ++I;
+    while (I * (I + 1) / 2 > tile) --I;
+    const int J = tile - I * (I + 1) / 2;
+    const double *X = Xbuf + sd.X_off;
+    const int nbp = sd.nbp;
+    const int tid = threadIdx.x, r = tid % 32, c0 = (tid / 32) * 4;
+    double acc[4] = {0, 0, 0, 0};
+    for (int kb = I; kb < sd.nt; ++kb) {
+        for (int idx = tid; idx < 1024; idx += 256) {
+            const int q = idx % 32, cc = idx / 32;
+            A[q][cc] = X[(32 * kb + q) + (size_t)(32 * I + cc) * nbp];
+            B[q][cc] = X[(32 * kb + q) + (size_t)(32 * J + cc) * nbp];
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int q = 0; q < 32; ++q) {
+            const double a = A[q][r];
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) acc[cc] += a * B[q][c0 + cc];
+        }
+        __syncthreads();
+    }
+    double *T = Fbuf + (sd.T_off + tile) * TILE_ELEMS;
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) T[r * TILE + c0 + cc] = acc[cc];
+}
+
+// ---------------------------------------------------------------------------
+// V = [F Bc_b^T, -R_b] and Fc_d = Bc_b V(:, 0:c)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double tile_at(const double *F, const SubDev &sd, int i, int p) {
+    int I = i / TILE, P = p / TILE;
+    if (I >= P) return F[(sd.T_off + (long long)I * (I + 1) / 2 + P) * TILE_ELEMS + (i % TILE) * TILE + (p % TILE)];
+    return F[(sd.T_off + (long long)P * (P + 1) / 2 + I) * TILE_ELEMS + (p % TILE) * TILE + (i % TILE)];
+}
+
+__global__ void k_build_V(const SubDev *__restrict__ subs, const double *__restrict__ Fbuf,
+                          const int *__restrict__ bce_ptr, const int *__restrict__ bce_pos,
+                          const double *__restrict__ bce_val, const double *__restrict__ Rbuf,
+                          double *__restrict__ Vbuf) {
+    const SubDev &sd = subs[blockIdx.x];
+    const int col = blockIdx.y;
+    if (col >= sd.c + 6) return;
+    double *V = Vbuf + sd.V_off + (size_t)col * sd.nbp;
+    if (col < sd.c) {
+        const int e0 = bce_ptr[sd.bce_off + col], e1 = bce_ptr[sd.bce_off + col + 1];
+        for (int i = threadIdx.x; i < sd.nbp; i += blockDim.x) {
+            double v = 0.0;
+            if (i < sd.nb)
+                for (int e = e0; e < e1; ++e) v += bce_val[e] * tile_at(Fbuf, sd, i, bce_pos[e]);
+            V[i] = v;
+        }
+    } else {
+        const double *R = Rbuf + sd.R_off + (size_t)(col - sd.c) * sd.N;
+        for (int i = threadIdx.x; i < sd.nbp; i += blockDim.x) V[i] = (i < sd.nb) ? -R[sd.nr + i] : 0.0;
+    }
+}
+
+__global__ void k_build_Fc(const SubDev *__restrict__ subs, const double *__restrict__ Vbuf,
+                           const int *__restrict__ bce_ptr, const int *__restrict__ bce_pos,
+                           const double *__restrict__ bce_val, const long long *__restrict__ fc_off,
+                           double *__restrict__ Fc) {
+    const SubDev &sd = subs[blockIdx.x];
+    const int c = sd.c;
+    double *out = Fc + fc_off[blockIdx.x];
+    for (int idx = threadIdx.x; idx < c * c; idx += blockDim.x) {
+        const int r = idx % c, q = idx / c;
+        const double *V = Vbuf + sd.V_off + (size_t)q * sd.nbp;
+        double v = 0.0;
+        for (int e = bce_ptr[sd.bce_off + r]; e < bce_ptr[sd.bce_off + r + 1]; ++e) v += bce_val[e] * V[bce_pos[e]];
+        out[idx] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// batched dense triangular solves with the full factor (N x N, lower)
+// v: full vectors (N per subdomain at nfull_off, nrhs columns of length ldv)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_trsv_fwd(const SubDev *__restrict__ subs,
+                                                  const double *__restrict__ Kbuf, double *__restrict__ v,
+                                                  long long ldv) {
+    __shared__ double part[8][32];
+    __shared__ double xs[32];
+    const SubDev &sd = subs[blockIdx.x];
+    const double *L = Kbuf + sd.K_off;
+    double *x = v + sd.nfull_off + (size_t)blockIdx.y * ldv;
+    const int N = sd.N, lane = threadIdx.x % 32, w = threadIdx.x / 32;
+    for (int kb = 0; kb < N; kb += 32) {
+        const int nrow = min(32, N - kb);
+        double acc = 0.0;
+        const int row = kb + lane;
+        if (lane < nrow)
+            for (int c = w; c < kb; c += 8) acc += L[row + (size_t)c * N] * x[c];
+        part[w][lane] = acc;
+        __syncthreads();
+        if (w == 0) {
+            double a = (lane < nrow) ? x[row] : 0.0;
+            for (int q = 0; q < 8; ++q) a -= part[q][lane];
+            for (int q = 0; q < nrow; ++q) {
+                double xq = 0.0;
+                if (lane == q) xq = a / L[row + (size_t)row * N];
+                xq = __shfl_sync(0xffffffffu, xq, q);
+                if (lane == q) xs[q] = xq;
+                if (lane > q && lane < nrow) a -= L[row + (size_t)(kb + q) * N] * xq;
+            }
+            __syncwarp();
+            if (lane < nrow) x[row] = xs[lane];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_trsv_bwd(const SubDev *__restrict__ subs,
+                                                  const double *__restrict__ Kbuf, double *__restrict__ v,
+                                                  long long ldv) {
+    __shared__ double acc_s[32];
+    const SubDev &sd = subs[blockIdx.x];
+    const double *L = Kbuf + sd.K_off;
+    double *x = v + sd.nfull_off + (size_t)blockIdx.y * ldv;
+    const int N = sd.N, lane = threadIdx.x % 32, w = threadIdx.x / 32;
+    const int nblk = (N + 31) / 32;
+    for (int b = nblk - 1; b >= 0; --b) {
+        const int kb = 32 * b, nrow = min(32, N - kb);
+        // acc[r] = x[kb+r] - sum_{c >= kb+nrow} L[c][kb+r] x[c]
+        for (int r = w; r < nrow; r += 8) {
+            const double *col = L + (size_t)(kb + r) * N;
+            double s = 0.0;
+            for (int c = kb + nrow + lane; c < N; c += 32) s += col[c] * x[c];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) acc_s[r] = x[kb + r] - s;
+        }
+        __syncthreads();
+        if (w == 0) {
+            double a = (lane < nrow) ? acc_s[lane] : 0.0;
+            for (int q = nrow - 1; q >= 0; --q) {
+                double xq = 0.0;
+                if (lane == q) xq = a / L[(kb + q) + (size_t)(kb + q) * N];
+                xq = __shfl_sync(0xffffffffu, xq, q);
+                if (lane == q) acc_s[q] = xq;
+                if (lane < q) a -= L[(kb + q) + (size_t)(kb + lane) * N] * xq;
+            }
+            __syncwarp();
+            if (lane < nrow) x[kb + lane] = acc_s[lane];
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace htf

@@ -1,0 +1,112 @@
+// Host-side problem description of the HTFETI path: mesh, per-subdomain
+// DOF maps, the dual layout (Bf, Bc, weights), kernels and fix DOFs, and the
+// small dense coarse objects.  Integer/index work and the O(n) FP64 pieces
+// live here; everything O(n^2) and above runs on the GPU.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "htfeti.h"
+
+namespace htf {
+
+// splitmix64 counter hash -> uniform [0,1)
+uint64_t mix64(uint64_t z);
+double u01(uint64_t seed, uint64_t stream, uint64_t i);
+
+struct Mesh {
+    int n_nodes = 0;
+    std::vector<double> coords;     // 3*n_nodes
+    std::vector<int> elems;         // 8*n_elems
+    std::vector<int> elem_sub;      // n_elems
+    std::vector<int> sub_cluster;   // n_sub
+    std::vector<double> sub_E, sub_nu;
+    std::vector<int> dirichlet;     // reference order
+    std::vector<int> corner;        // sorted
+    double body_force[3] = {0, 0, 0};
+    int n_elems() const { return int(elem_sub.size()); }
+    int n_sub() const { return int(sub_cluster.size()); }
+};
+
+// Mesh::createMesh generalised (Mesh.cpp:69-289).
+int generate_mesh(const htf_mesh_spec &s, Mesh &m, std::string &err);
+int mesh_sizes(const htf_mesh_spec &s, int *nn, int *ne, int *ns, int *nc, int *nd, int *ncr,
+               std::string &err);
+int mesh_traction(const htf_mesh_spec &s, uint64_t seed, int n_rhs, double scale, double *f,
+                  std::string &err);
+
+struct Options {
+    std::string typeBc = "cor";                       // cor | ker | all
+    std::string preconditioner = "Dirichlet_explicit";
+    double eps_iter = 1e-8;
+    int max_iter = 500;
+    bool mixed = false;                               // precision=mixed
+    int device = 0;
+    int check_every = 8;                              // iterations between host convergence checks
+};
+int parse_options(const char *s, Options &o, std::string &err);
+
+// One Bf row: up to two (subdomain, global DOF, sign) entries.
+struct BfRow {
+    int sub[2];
+    int dof[2];
+    double sign[2];
+};
+
+struct Subdomain {
+    int id = 0, cluster = 0, cl_index = 0;   // index inside its cluster
+    std::vector<int> elems;                  // element ids in increasing order
+    std::vector<int> l2g;                    // sorted global DOFs (Data.cpp:111-144)
+    std::vector<int> b;                      // sorted local DOFs touched by Bf (j_col_cmpr)
+    std::vector<int> perm;                   // local DOF -> position in [interior | b] order
+    int n = 0, nb = 0, nr = 0;
+    std::vector<double> R;                   // n x 6, column-major, orthonormal columns
+    std::vector<int> fix;                    // 6 sorted local DOFs (all in b)
+    // Bc entries of this subdomain: cluster row, local DOF, value
+    std::vector<int> bc_row, bc_col;
+    std::vector<double> bc_val;
+    std::vector<int> bc_rows;                // sorted distinct cluster rows (l2g_i_coo of Bc)
+    int c() const { return int(bc_rows.size()); }
+    // Bf entries grouped per b position: CSR
+    std::vector<int> bf_ptr;                 // nb+1
+    std::vector<int> bf_lam;                 // lambda row
+    std::vector<double> bf_sign;
+    std::vector<double> f;                   // assembled load per local DOF, n x nrhs (filled on device)
+};
+
+struct Cluster {
+    std::vector<int> subs;   // global subdomain ids in this cluster
+    int nlam_c = 0;          // Bc rows
+    int ngc() const { return nlam_c + 6 * int(subs.size()); }
+};
+
+struct Problem {
+    Mesh mesh;
+    Options opt;
+    std::vector<Subdomain> sub;
+    std::vector<Cluster> clu;
+    std::vector<BfRow> rows;
+    std::vector<double> weight;
+    int n_lam = 0;
+    int nrhs = 1;
+    std::vector<double> f_nodal;            // 3*n_nodes*nrhs (optional)
+};
+
+// Data::buildMappingStruct + Cluster::create_cluster_constraints +
+// kernels/fix DOFs.  Returns HTF_OK or an error code with err set.
+int build_problem(Problem &p, std::string &err);
+
+// Analytic rigid body modes of the nodes of l2g (column order of
+// Data::create_analytic_ker_K, Data.cpp:61-109), Gram-Schmidt'ed
+// (Matrix.cpp:2450-2472).
+void kernel_of(const Mesh &m, const std::vector<int> &l2g, std::vector<double> &R);
+// Matrix::getNullPivots (Matrix.cpp:835-884) on an n x m column-major matrix.
+std::vector<int> null_pivots(const std::vector<double> &R, int n, int m);
+
+// ---- small dense FP64 helpers (column-major) ----
+bool chol_lower(int n, double *A, int lda);                          // in place
+void chol_solve(int n, const double *L, int lda, double *B, int ldb, int nrhs);
+void sym_eig(int n, std::vector<double> &A, std::vector<double> &w, std::vector<double> &V);
+
+}  // namespace htf

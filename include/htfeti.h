@@ -1,0 +1,154 @@
+/*
+ * htfeti.h - C ABI of the B200 HTFETI (hybrid total FETI) solve path.
+ *
+ * The reference (ostravaTokyo/hfls) exposes its solver only as C++ classes
+ * (Driver, Cluster, Solver, Matrix, Mesh; no FFI).  Every entry point below
+ * replaces one of those class members and says which.  Conventions:
+ *   - return 0 on success, a negative HTF_E* code on failure (never exit());
+ *     htf_last_error() gives a message for the last failing call on a context;
+ *   - caller-owned host buffers, library-owned device memory;
+ *   - one context per host thread; contexts are independent.
+ * Arrays are 0-based.  DOF g = 3*node + component.  Dense matrices are
+ * column-major.
+ */
+#ifndef HTFETI_H
+#define HTFETI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes ------------------------------------------------------- */
+#define HTF_OK 0
+#define HTF_EINVAL -1       /* bad argument or option                          */
+#define HTF_ENOMEM -2       /* device or host allocation failed                */
+#define HTF_ECUDA -3        /* CUDA runtime error (message has the detail)     */
+#define HTF_ENOTSPD -4      /* a regularised K_i or coarse matrix is not SPD   */
+#define HTF_EBREAKDOWN -5   /* PCPG: w'Fw <= 0, NaN or Inf                      */
+#define HTF_ENOCONV -6      /* PCPG: max_iter reached                          */
+#define HTF_ESTATE -7       /* call out of order (e.g. pcpg before setup)      */
+#define HTF_ETIMEDOUT -8    /* a bounded device wait gave up                   */
+#define HTF_ENODEV -9       /* no CUDA device                                  */
+
+/* ---- mesh generation ----------------------------------------------------
+ * Replaces Mesh::createMesh (Mesh.cpp:69-289), generalised to clusters,
+ * non-uniform subdomain slabs, node jitter, per-subdomain materials and the
+ * boundary conditions of the benchmark configurations.                     */
+#define HTF_BC_ROLLERS 0    /* u_x=0 on x=0, u_y=0 on y=0, u_z=0 on z=0 (Mesh.cpp:221-239) */
+#define HTF_BC_CLAMP_X0 1   /* u=0 on the face x=0                                         */
+
+#define HTF_MAT_CONST 0     /* E everywhere                                                 */
+#define HTF_MAT_CHECKER 1   /* E*ratio on even subdomains (Data.cpp:47-48, Mesh.cpp:281)    */
+#define HTF_MAT_LOGUNIFORM 2 /* E_i ~ logU[E_lo, E_hi] per subdomain, seeded                */
+
+typedef struct htf_mesh_spec {
+    int clusters[3];         /* clusters per axis                                   */
+    int subs[3];             /* subdomains per cluster per axis                     */
+    int elems[3];            /* elements per subdomain per axis (uniform slabs)     */
+    const int *widths[3];    /* optional: element count of every subdomain slab
+                                along axis a (clusters[a]*subs[a] entries); NULL =
+                                uniform elems[a]                                    */
+    double jitter;           /* interior nodes moved by U(-jitter*h, jitter*h)      */
+    uint64_t seed;           /* seed of jitter, materials and tractions             */
+    int bc;                  /* HTF_BC_*                                            */
+    int material;            /* HTF_MAT_*                                           */
+    double E, E_hi, nu;      /* CONST: E; CHECKER: E, ratio=E_hi; LOGUNIFORM: [E,E_hi] */
+    double body_force[3];    /* rho*a per unit volume                               */
+} htf_mesh_spec;
+
+/* Sizes of the generated mesh (two-call pattern with htf_mesh_fill). */
+int htf_mesh_sizes(const htf_mesh_spec *spec, int *n_nodes, int *n_elems, int *n_sub,
+                   int *n_clusters, int *n_dirichlet, int *n_corner);
+
+/* Fill caller buffers: coords[3*n_nodes], elems[8*n_elems] (node order of
+ * Mesh.cpp:250-257), elem_sub[n_elems], sub_cluster[n_sub], sub_E[n_sub],
+ * sub_nu[n_sub], dirichlet[n_dirichlet], corner[n_corner] (corner DOFs of
+ * Mesh.cpp:175-208).  Any pointer may be NULL to skip that array.          */
+int htf_mesh_fill(const htf_mesh_spec *spec, double *coords, int *elems, int *elem_sub,
+                  int *sub_cluster, double *sub_E, double *sub_nu, int *dirichlet, int *corner);
+
+/* Seeded N(0,1) nodal forces on the face x=1 for n_rhs load cases, added to
+ * f[3*n_nodes*n_rhs] (column-major: load case k at f + k*3*n_nodes).  The
+ * reference has no traction; it is a configuration load.                   */
+int htf_mesh_traction(const htf_mesh_spec *spec, uint64_t seed, int n_rhs, double scale, double *f);
+
+/* ---- solver context ------------------------------------------------------
+ * Replaces Driver::Driver(map) / Cluster::initialization's options map
+ * (Driver.cpp:14-18, htfeti.cpp:12-57).  `options` is a ';'-separated list
+ * of key=value with the reference's keys (eps_iter, max_iter,
+ * preconditioner = Dirichlet_explicit | Dirichlet_implicit | lumped,
+ * typeBc = cor | ker | all, Ac_extended_by_kerGc) and this build's keys
+ * (precision = fp64 | mixed, device = <cuda ordinal>).                     */
+typedef struct htf_ctx htf_ctx;
+
+int htf_create(const char *options, htf_ctx **ctx);
+int htf_destroy(htf_ctx *ctx);
+const char *htf_last_error(const htf_ctx *ctx);
+
+/* Mesh of one problem.  Replaces the Mesh& argument of
+ * Cluster::initialization (Cluster.cpp:21, 42) and the public Mesh fields
+ * it reads (points, elements, DirichletDOFs, cornerDOFs, Mesh.hpp:72-84).
+ * All arrays are copied.                                                   */
+int htf_set_mesh(htf_ctx *ctx, int n_nodes, const double *coords, int n_elems, const int *elems,
+                 const int *elem_sub, int n_sub, const int *sub_cluster, const double *sub_E,
+                 const double *sub_nu, int n_dirichlet, const int *dirichlet, int n_corner,
+                 const int *corner, const double body_force[3]);
+
+/* Extra nodal forces for n_rhs load cases (f_nodal[3*n_nodes*n_rhs],
+ * column-major), added to the body-force load of every case.  Without this
+ * call there is one load case: the body force.                            */
+int htf_set_loads(htf_ctx *ctx, int n_rhs, const double *f_nodal);
+
+/* Setup.  Replaces Cluster::initialization up to the PCPG call
+ * (Cluster.cpp:21-360): assembly (Data.cpp:25-273), kernels and fix-DOF
+ * regularisation (Matrix.cpp:835-884, 1029-1057), constraints
+ * (Cluster.cpp:682-959), Dirichlet preconditioner (Matrix.cpp:1708-1871),
+ * local and cluster coarse objects (Cluster.cpp:150-352).  On the GPU: hex8
+ * assembly, batched dense Cholesky, explicit F_i = (K_reg^{-1})_bb and S_i. */
+int htf_setup(htf_ctx *ctx);
+
+typedef struct htf_stats {
+    int iterations[64];      /* PCPG iterations per load case (first 64)      */
+    double norm_gPz0[64];
+    double final_rel[64];    /* sqrt(g'Pz)/sqrt(g0'Pz0) at exit               */
+    double setup_ms;         /* device time of htf_setup                      */
+    double solve_ms;         /* device time of the PCPG loops (g0 -> exit)    */
+    double fapply_ms;        /* mean device time of one F apply               */
+    double fapply_bytes;     /* algorithmic bytes of one F apply              */
+    int n_lambda, n_sub, n_clusters, n_rhs;
+    int status_sub;          /* subdomain index of an HTF_ENOTSPD failure     */
+} htf_stats;
+
+/* PCPG for every load case and the displacement field.  Replaces
+ * Cluster::pcpg (Cluster.cpp:1363-1458) and the solution assembly of
+ * Cluster::printVTK (Cluster.cpp:1648-1678): u[3*n_nodes*n_rhs] receives
+ * the displacements (for DOFs shared by several subdomains the highest
+ * subdomain index wins, as in the reference).  u may be NULL.             */
+int htf_pcpg(htf_ctx *ctx, double *u, htf_stats *stats);
+
+/* The dual operators on host vectors of length n_lambda (nrhs columns,
+ * column-major).  Replace Cluster::mult_Ff (Cluster.cpp:1114-1188),
+ * Cluster::Projection (Cluster.cpp:1314-1329) and Cluster::Preconditioning
+ * (Cluster.cpp:1043-1112).                                                */
+int htf_mult_Ff(htf_ctx *ctx, const double *w, double *Fw, int nrhs);
+int htf_projection(htf_ctx *ctx, const double *x, double *Px, int nrhs);
+int htf_preconditioning(htf_ctx *ctx, const double *x, double *Mx, int nrhs);
+
+/* Dual layout for checking: n_lambda, and for every Bf row its entries as
+ * (subdomain, global DOF, sign) with up to two entries per row
+ * (Cluster.cpp:846-924); weights (Cluster.cpp:893-895, 918).  Arrays of
+ * length 2*n_lambda (second entry sub = -1 when the row has one).         */
+int htf_dual_sizes(htf_ctx *ctx, int *n_lambda, int *n_sub, int *n_clusters);
+int htf_dual_layout(htf_ctx *ctx, int *row_sub, int *row_dof, double *row_sign, double *weight);
+
+/* Fix DOFs (6 per subdomain, global DOF ids) chosen for the regularisation
+ * (Matrix.cpp:835-884 restricted to the Bf column set).                   */
+int htf_fix_dofs(htf_ctx *ctx, int *fix_global);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HTFETI_H */

@@ -1,0 +1,106 @@
+"""Host logic of the C ABI (no GPU): exported symbols, the mesh generator
+against the reference's own meshes, the dual layout and the fix DOFs against
+the oracle."""
+import ast
+import os
+import re
+
+import numpy as np
+import pytest
+
+import hfls_b200 as hb
+from oracle.htfeti_oracle import HTFETI, Options, MeshArrays
+from tests.golden_util import golden_paths, load, mesh_from_golden, options_from_args
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_every_declared_symbol():
+    hdr = open(os.path.join(ROOT, "include", "htfeti.h")).read()
+    declared = set(re.findall(r"\b(htf_[a-z_]+)\s*\(", hdr))
+    assert len(declared) >= 15
+    for name in sorted(declared):
+        assert hasattr(hb.lib, name), name
+
+
+def _spec_for_golden(args):
+    g = {k: int(args.get(k, d)) for k, d in (("Nx", 2), ("Ny", 2), ("Nz", 2), ("nx", 5), ("ny", 5), ("nz", 5))}
+    bc = hb.HTF_BC_CLAMP_X0 if args.get("clamp") == "true" else hb.HTF_BC_ROLLERS
+    ratio = float(args.get("ratio_mat", "1"))
+    return hb.mesh_spec(subs=(g["Nx"], g["Ny"], g["Nz"]), elems=(g["nx"], g["ny"], g["nz"]), bc=bc,
+                        material=hb.HTF_MAT_CHECKER, E=float(args["young_modulus"]), E_hi=ratio,
+                        body_force=(0, 0, 98.10 * 2.0))
+
+
+@pytest.mark.parametrize("path", golden_paths(), ids=lambda p: os.path.basename(p)[:-4])
+def test_generator_matches_reference_mesh(path):
+    """Mesh::createMesh (Mesh.cpp:69-289): points bit-exact, connectivity,
+    partition, materials, Dirichlet and corner DOFs identical."""
+    g, args = load(path)
+    m = hb.generate_mesh(_spec_for_golden(args))
+    assert np.array_equal(m.coords, g["points"])
+    assert np.array_equal(m.elems, g["elements"])
+    assert np.array_equal(m.elem_sub, g["partition"])
+    assert np.array_equal(m.dirichlet, g["dirichlet"])
+    assert np.array_equal(m.corner, g["corner"])
+    ref = mesh_from_golden(g, args)
+    assert np.array_equal(m.sub_E, ref.sub_E)
+
+
+def _oracle_mesh(m):
+    return MeshArrays(m.coords, m.elems.astype(np.int64), m.elem_sub.astype(np.int64),
+                      m.sub_cluster.astype(np.int64), m.sub_E, m.sub_nu, m.dirichlet.astype(np.int64),
+                      m.corner.astype(np.int64), m.body_force)
+
+
+CASES = [
+    dict(clusters=(1, 1, 1), subs=(2, 2, 2), elems=(3, 3, 3), bc=hb.HTF_BC_ROLLERS, typeBc="ker"),
+    dict(clusters=(2, 1, 1), subs=(2, 2, 1), elems=(2, 3, 2), bc=hb.HTF_BC_CLAMP_X0, typeBc="cor"),
+    dict(clusters=(1, 2, 2), subs=(2, 1, 2), elems=(3, 2, 2), bc=hb.HTF_BC_CLAMP_X0, typeBc="ker", jitter=0.1),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c['clusters']}x{c['subs']}x{c['elems']}-{c['typeBc']}")
+def test_dual_layout_and_fix_dofs_match_oracle(case):
+    case = dict(case)
+    typeBc = case.pop("typeBc")
+    spec = hb.mesh_spec(material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e4, seed=3, **case)
+    m = hb.generate_mesh(spec)
+    s = hb.Solver({"typeBc": typeBc})
+    s.set_mesh(m)
+    rs, rd, sg, w = s.dual_layout()
+    h = HTFETI(_oracle_mesh(m), Options(typeBc=typeBc, fix_rule="boundary", kerGc="analytic"))
+    assert len(w) == h.n_lam
+    assert np.array_equal(w, h.weight)
+    for r, row in enumerate(h.bf_rows):
+        for k, (d, gdof, sign) in enumerate(row):
+            assert (rs[r, k], rd[r, k], sg[r, k]) == (d, gdof, sign)
+        if len(row) == 1:
+            assert rs[r, 1] == -1
+    fix = s.fix_dofs()
+    for d in range(m.n_sub):
+        assert np.array_equal(fix[d], h.l2g[d][h.fix[d]])
+
+
+def test_generator_jitter_is_interior_and_bounded():
+    spec = hb.mesh_spec(subs=(2, 1, 1), elems=(4, 3, 3), jitter=0.1, seed=11)
+    m = hb.generate_mesh(spec)
+    m0 = hb.generate_mesh(hb.mesh_spec(subs=(2, 1, 1), elems=(4, 3, 3)))
+    d = np.abs(m.coords - m0.coords)
+    h = np.array([1 / 8, 1 / 3, 1 / 3])
+    assert np.all(d <= 0.1 * h + 1e-15)
+    on_boundary = np.any((m0.coords < 1e-12) | (m0.coords > 1 - 1e-12), axis=1)
+    assert np.all(d[on_boundary] == 0)
+    assert np.all(d[~on_boundary] > 0)
+    m2 = hb.generate_mesh(spec)
+    assert np.array_equal(m.coords, m2.coords)
+
+
+def test_options_and_errors():
+    with pytest.raises(hb.HTFError) as e:
+        hb.Solver({"preconditioner": "bogus"})
+    assert e.value.code == -1
+    s = hb.Solver({"typeBc": "all", "eps_iter": "1e-8", "vtkWithinIter": "false"})
+    with pytest.raises(hb.HTFError) as e:
+        s.setup()
+    assert e.value.code == -7
