@@ -12,7 +12,7 @@ import numpy as np
 _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libhtfeti_b200.so")
 if not os.path.exists(LIB_PATH):
-    raise ImportError(f"{LIB_PATH} is missing: build it with `python -m hfls_b200.build`")
+    raise ImportError(f"{LIB_PATH} is missing: build it with `python hfls_b200/build.py`")
 lib = ctypes.CDLL(LIB_PATH)
 
 HTF_BC_ROLLERS, HTF_BC_CLAMP_X0 = 0, 1
@@ -36,7 +36,15 @@ class Stats(ctypes.Structure):
                 ("final_rel", ctypes.c_double * 64), ("setup_ms", ctypes.c_double),
                 ("solve_ms", ctypes.c_double), ("fapply_ms", ctypes.c_double),
                 ("fapply_bytes", ctypes.c_double), ("n_lambda", ctypes.c_int), ("n_sub", ctypes.c_int),
-                ("n_clusters", ctypes.c_int), ("n_rhs", ctypes.c_int), ("status_sub", ctypes.c_int)]
+                ("n_clusters", ctypes.c_int), ("n_rhs", ctypes.c_int), ("status_sub", ctypes.c_int),
+                ("kernel_launches", ctypes.c_longlong)]
+
+
+class ProfileInfo(ctypes.Structure):
+    _fields_ = [("symv_F_ms", ctypes.c_double), ("symv_F_bytes", ctypes.c_double),
+                ("symv_S_ms", ctypes.c_double), ("symv_S_bytes", ctypes.c_double),
+                ("fapply_ms", ctypes.c_double), ("fapply_bytes", ctypes.c_double),
+                ("iteration_ms", ctypes.c_double), ("kernels_per_iteration", ctypes.c_int)]
 
 
 _SIGS = {
@@ -50,6 +58,8 @@ _SIGS = {
     "htf_set_loads": [ctypes.c_void_p, ctypes.c_int, _dp],
     "htf_setup": [ctypes.c_void_p],
     "htf_pcpg": [ctypes.c_void_p, _dp, ctypes.POINTER(Stats)],
+    "htf_solve": [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.POINTER(Stats)],
+    "htf_profile": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ProfileInfo)],
     "htf_mult_Ff": [ctypes.c_void_p, _dp, _dp, ctypes.c_int],
     "htf_projection": [ctypes.c_void_p, _dp, _dp, ctypes.c_int],
     "htf_preconditioning": [ctypes.c_void_p, _dp, _dp, ctypes.c_int],
@@ -198,6 +208,27 @@ class Solver:
         st = Stats()
         self._check(lib.htf_pcpg(self._h, _d(u), ctypes.byref(st)), "htf_pcpg")
         return u, st
+
+    def solve(self, f_nodal=None, u=None, nrhs=None):
+        """New load cases against the resident factors (htf_solve).  f_nodal
+        (n_rhs, 3*n_nodes) is added to the body force; None = body force only."""
+        if f_nodal is None:
+            nrhs = nrhs or 1
+            fp = None
+        else:
+            f_nodal = np.ascontiguousarray(np.atleast_2d(f_nodal), dtype=np.float64)
+            nrhs = f_nodal.shape[0]
+            fp = _d(f_nodal)
+        if u is None:
+            u = np.zeros((nrhs, 3 * self.mesh.n_nodes))
+        st = Stats()
+        self._check(lib.htf_solve(self._h, nrhs, fp, _d(u), ctypes.byref(st)), "htf_solve")
+        return u, st
+
+    def profile(self, reps=20):
+        info = ProfileInfo()
+        self._check(lib.htf_profile(self._h, reps, ctypes.byref(info)), "htf_profile")
+        return info
 
     def n_lambda(self):
         n = ctypes.c_int()

@@ -1,7 +1,7 @@
 """In-tree build of libhtfeti_b200.so (CUDA for sm_100a + C++ host code).
 
-    python -m hfls_b200.build          # incremental
-    python -m hfls_b200.build --clean
+    python hfls_b200/build.py          # incremental (runs without importing the package)
+    python hfls_b200/build.py --clean
 
 CUDA sources are compiled by nvcc with -gencode arch=compute_100a,code=sm_100a;
 host sources by g++ without FMA contraction, so host-side sums match the

@@ -128,7 +128,22 @@ int htf_pcpg(htf_ctx *ctx, double *u, htf_stats *stats) {
     if (!ctx) return HTF_EINVAL;
     if (!ctx->is_setup) return fail(ctx, HTF_ESTATE, "htf_pcpg before htf_setup");
     if (stats) std::memset(stats, 0, sizeof(*stats));
-    return ctx->eng->pcpg(ctx->p, u, stats, ctx->err);
+    const double *fn = ctx->p.f_nodal.empty() ? nullptr : ctx->p.f_nodal.data();
+    return ctx->eng->solve(ctx->p, ctx->p.nrhs, fn, u, stats, ctx->err);
+}
+
+int htf_solve(htf_ctx *ctx, int n_rhs, const double *f_nodal, double *u, htf_stats *stats) {
+    if (!ctx) return HTF_EINVAL;
+    if (!ctx->is_setup) return fail(ctx, HTF_ESTATE, "htf_solve before htf_setup");
+    if (n_rhs < 1) return fail(ctx, HTF_EINVAL, "htf_solve: n_rhs < 1");
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    return ctx->eng->solve(ctx->p, n_rhs, f_nodal, u, stats, ctx->err);
+}
+
+int htf_profile(htf_ctx *ctx, int reps, htf_profile_info *info) {
+    if (!ctx) return HTF_EINVAL;
+    if (!ctx->is_setup) return fail(ctx, HTF_ESTATE, "htf_profile before htf_setup");
+    return ctx->eng->profile(reps, info, ctx->err);
 }
 
 static int apply_op(htf_ctx *ctx, int op, const double *x, double *y, int nrhs) {

@@ -158,6 +158,23 @@ __global__ void k_to_f32(long long n, const double *__restrict__ a, float *__res
         b[i] = (float)a[i];
 }
 
+// f[r][i] = fbody[i] + fn[r][own[i]]
+__global__ void k_build_f(int nfull, int ndof, int nrhs, const double *__restrict__ fbody, const int *__restrict__ own,
+                          const double *__restrict__ fn, double *__restrict__ f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfull) return;
+    const int g = own[i];
+    for (int r = 0; r < nrhs; ++r) f[(size_t)r * nfull + i] = fbody[i] + ((fn && g >= 0) ? fn[(size_t)r * ndof + g] : 0.0);
+}
+
+// u[g] = uloc[win[g]]
+__global__ void k_gather_u(int ndof, const int *__restrict__ win, const double *__restrict__ uloc, double *__restrict__ u) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ndof) return;
+    const int s = win[g];
+    u[g] = (s >= 0) ? uloc[s] : 0.0;
+}
+
 __global__ void k_copy(long long n, const double *__restrict__ a, double *__restrict__ b, const PcpgState *st) {
     if (st && st->done) return;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -820,6 +837,28 @@ int Engine::setup(Problem &p, std::string &err) {
     CK(cudaEventRecord(e0, s_));
     int rc = upload_layout(p, err);
     if (!rc) rc = factorize(p, err);
+    if (!rc) {                    // body-force load, load ownership and the displacement gather map
+        ndof_ = 3 * p.mesh.n_nodes;
+        std::vector<int> own(nfull_, -1), win(ndof_, -1), owner(ndof_, -1);
+        for (int d = 0; d < nsub_; ++d)
+            for (int g : p.sub[d].l2g)
+                if (owner[g] < 0) owner[g] = d;
+        for (int d = 0; d < nsub_; ++d) {
+            const Subdomain &s = p.sub[d];
+            for (int l = 0; l < s.n; ++l) {
+                const int slot = hs_[d].nfull_off + s.perm[l], g = s.l2g[l];
+                if (owner[g] == d) own[slot] = g;
+                win[g] = slot;              // highest subdomain index wins (Cluster.cpp:1672-1676)
+            }
+        }
+        d_fbody_ = alloc<double>(nfull_, err, rc);
+        d_own_ = alloc<int>(nfull_, err, rc);
+        d_win_ = alloc<int>(ndof_, err, rc);
+        if (!rc) rc = check(cudaMemcpyAsync(d_fbody_, d_f_, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_), "copy", err);
+        if (!rc) rc = check(cudaMemcpyAsync(d_own_, own.data(), nfull_ * sizeof(int), cudaMemcpyHostToDevice, s_), "copy", err);
+        if (!rc) rc = check(cudaMemcpyAsync(d_win_, win.data(), ndof_ * sizeof(int), cudaMemcpyHostToDevice, s_), "copy", err);
+        if (!rc) rc = check(cudaStreamSynchronize(s_), "sync", err);
+    }
     if (!rc) rc = coarse(p, err);
     if (!rc) rc = outer_coarse(p, err);
     if (!rc) {
@@ -924,7 +963,7 @@ int Engine::apply(int op, const double *x, double *y, int nrhs, std::string &err
 }
 
 // one load case: Cluster::pcpg (Cluster.cpp:1363-1458) + printVTK (1648-1678)
-int Engine::solve_one(Problem &p, int rhs, double *u_loc_host, int &iters, double &norm0, double &rel,
+int Engine::solve_one(Problem &p, int rhs, double *u_dev, int &iters, double &norm0, double &rel,
                       double &solve_ms, std::string &err) {
     const double *f = d_f_ + (size_t)rhs * nfull_;
     int maxcols = 0;
@@ -972,13 +1011,18 @@ int Engine::solve_one(Problem &p, int rhs, double *u_loc_host, int &iters, doubl
         CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
         iteration(d_st_);
         CK(cudaStreamEndCapture(s_, &g));
+        size_t nn = 0;
+        CK(cudaGraphGetNodes(g, nullptr, &nn));
+        kernels_per_iter_ = int(nn);
         CK(cudaGraphInstantiate(&graph_, g, 0));
         cudaGraphDestroy(g);
     }
     PcpgState hst;
     const int every = std::max(1, opt_.check_every);
+    launches_ += 29 + 12;     // kernels of the start (x, d, lambda0, g0, Pz) and of the reconstruction
     for (;;) {
         for (int k = 0; k < every; ++k) CK(cudaGraphLaunch(graph_, s_));
+        launches_ += (long long)every * kernels_per_iter_;
         CK(cudaMemcpyAsync(&hst, d_st_, sizeof(PcpgState), cudaMemcpyDeviceToHost, s_));
         CK(cudaStreamSynchronize(s_));
         if (hst.done) break;
@@ -1004,65 +1048,47 @@ int Engine::solve_one(Problem &p, int rhs, double *u_loc_host, int &iters, doubl
     kplus_full(d_full_);                                                                   // K_reg^{-1}(y - Bc^T lam_c)
     k_add_R<<<nsub_, 256, 0, s_>>>(d_subs_, d_cl_, d_R_, d_H_, d_s_, d_alpha_, d_full_);
     CK(cudaGetLastError());
-    if (u_loc_host) CK(cudaMemcpyAsync(u_loc_host, d_full_, nfull_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
-    CK(cudaStreamSynchronize(s_));
+    if (u_dev) k_gather_u<<<cdiv(ndof_, 256), 256, 0, s_>>>(ndof_, d_win_, d_full_, u_dev);
+    CK(cudaGetLastError());
     if (hst.done == 2) { err = "PCPG breakdown (w'Fw <= 0 or non-finite)"; return HTF_EBREAKDOWN; }
     return HTF_OK;
 }
 
-int Engine::pcpg(Problem &p, double *u, htf_stats *stats, std::string &err) {
-    const int nrhs = p.nrhs;
-    // nodal loads into the permuted full vectors (lowest subdomain owns a DOF)
-    if (!p.f_nodal.empty()) {
-        const size_t ndof = 3 * (size_t)p.mesh.n_nodes;
-        std::vector<int> owner(ndof, -1);
-        for (int d = 0; d < nsub_; ++d)
-            for (int g : p.sub[d].l2g)
-                if (owner[g] < 0) owner[g] = d;
-        std::vector<double> fh((size_t)nfull_ * nrhs, 0.0);
-        for (int r = 0; r < nrhs; ++r)
-            for (int d = 0; d < nsub_; ++d) {
-                const Subdomain &s = p.sub[d];
-                for (int l = 0; l < s.n; ++l) {
-                    int g = s.l2g[l];
-                    if (owner[g] == d) fh[(size_t)r * nfull_ + hs_[d].nfull_off + s.perm[l]] = p.f_nodal[(size_t)r * ndof + g];
-                }
-            }
-        double *d_tmpf = nullptr;
-        int rc = HTF_OK;
-        d_tmpf = alloc<double>(fh.size(), err, rc);
-        if (rc) return rc;
-        CK(cudaMemcpyAsync(d_tmpf, fh.data(), fh.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
-        // replicate the assembled body force to every load case, add nodal loads
-        for (int r = 1; r < nrhs; ++r)
-            CK(cudaMemcpyAsync(d_f_ + (size_t)r * nfull_, d_f_, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-        k_axpby<<<cdiv((long long)nfull_ * nrhs, 256), 256, 0, s_>>>(nfull_ * nrhs, 1.0, d_tmpf, 1.0, d_f_);
-        CK(cudaGetLastError());
-        p.f_nodal.clear();          // loads are now in d_f_
-    }
-    std::vector<double> uloc(nfull_);
-    const size_t ndof = 3 * (size_t)p.mesh.n_nodes;
+int Engine::ensure_rhs(int nrhs, std::string &err) {
+    if (nrhs <= rhs_cap_) return HTF_OK;
+    int rc = HTF_OK;
+    d_fn_ = alloc<double>((size_t)ndof_ * nrhs, err, rc);
+    d_u_ = alloc<double>((size_t)ndof_ * nrhs, err, rc);
+    d_f_ = alloc<double>((size_t)nfull_ * nrhs, err, rc);
+    if (rc) return rc;
+    rhs_cap_ = nrhs;
+    return HTF_OK;
+}
+
+int Engine::solve(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err) {
+    int rc = ensure_rhs(nrhs, err);
+    if (rc) return rc;
+    launches_ = 1;            // k_build_f
+    if (f_nodal)
+        CK(cudaMemcpyAsync(d_fn_, f_nodal, (size_t)ndof_ * nrhs * sizeof(double), cudaMemcpyHostToDevice, s_));
+    k_build_f<<<cdiv(nfull_, 256), 256, 0, s_>>>(nfull_, ndof_, nrhs, d_fbody_, d_own_, f_nodal ? d_fn_ : nullptr, d_f_);
+    CK(cudaGetLastError());
     double total_ms = 0.0;
     for (int r = 0; r < nrhs; ++r) {
         int it = 0;
         double n0 = 0, rel = 0, ms = 0;
-        int rc = solve_one(p, r, uloc.data(), it, n0, rel, ms, err);
+        rc = solve_one(p, r, d_u_ + (size_t)r * ndof_, it, n0, rel, ms, err);
         total_ms += ms;
         if (stats && r < 64) { stats->iterations[r] = it; stats->norm_gPz0[r] = n0; stats->final_rel[r] = rel; }
-        if (u) {
-            double *ur = u + (size_t)r * ndof;
-            for (int d = 0; d < nsub_; ++d) {       // last writer wins (Cluster.cpp:1672-1676)
-                const Subdomain &s = p.sub[d];
-                for (int l = 0; l < s.n; ++l) ur[s.l2g[l]] = uloc[hs_[d].nfull_off + s.perm[l]];
-            }
-        }
         if (rc) return rc;
-        if (it >= opt_.max_iter && rel >= opt_.eps_iter) {
+        if (it >= opt_.max_iter && !(rel < opt_.eps_iter)) {
             if (stats) stats->solve_ms = total_ms;
             err = "PCPG did not converge within max_iter";
             return HTF_ENOCONV;
         }
     }
+    if (u) CK(cudaMemcpyAsync(u, d_u_, (size_t)ndof_ * nrhs * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
     if (stats) {
         stats->solve_ms = total_ms;
         stats->setup_ms = setup_ms;
@@ -1072,7 +1098,66 @@ int Engine::pcpg(Problem &p, double *u, htf_stats *stats, std::string &err) {
         stats->n_clusters = ncl_;
         stats->n_rhs = nrhs;
         stats->status_sub = status_sub;
+        stats->kernel_launches = launches_;
     }
+    return HTF_OK;
+}
+
+int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
+    if (!info || reps < 1) { err = "bad arguments"; return HTF_EINVAL; }
+    std::memset(info, 0, sizeof(*info));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float ms = 0.f;
+    auto timeit = [&](auto &&fn) -> double {
+        fn();
+        cudaEventRecord(e0, s_);
+        for (int r = 0; r < reps; ++r) fn();
+        cudaEventRecord(e1, s_);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        return double(ms) / reps;
+    };
+    k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, d_lam_, nullptr, d_xb_, nullptr);
+    const double sz = mixed_ ? 4.0 : 8.0;
+    double tri = 0.0, vec = 0.0;
+    for (auto &h : hs_) { tri += sz * double(h.nb) * (h.nb + 1) / 2; vec += 16.0 * h.nb; }
+    info->symv_F_ms = timeit([&] {
+        if (mixed_) k_symv<float><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_F32_, d_xb_, d_yb_, nullptr);
+        else k_symv<double><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_F_, d_xb_, d_yb_, nullptr);
+    });
+    info->symv_F_bytes = tri + vec;
+    info->symv_S_ms = timeit([&] {
+        if (mixed_) k_symv<float><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_S32_, d_xb_, d_yb_, nullptr);
+        else k_symv<double><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_S_, d_xb_, d_yb_, nullptr);
+    });
+    info->symv_S_bytes = tri + vec;
+    info->fapply_ms = timeit([&] { op_F(d_lam_, d_Fw_, nullptr, nullptr, nullptr); });
+    info->fapply_bytes = fapply_bytes_;
+    if (graph_) {
+        // a state with done=1 would skip the work: time with a live state copy
+        PcpgState st{};
+        st.gPz = 1.0; st.norm0 = 1.0; st.eps = 0.0; st.max_iter = 1 << 30; st.wFw = 1.0;
+        PcpgState saved;
+        CK(cudaMemcpyAsync(&saved, d_st_, sizeof(PcpgState), cudaMemcpyDeviceToHost, s_));
+        CK(cudaStreamSynchronize(s_));
+        std::vector<double> lam(nlam_), g(nlam_), w(nlam_);
+        CK(cudaMemcpy(lam.data(), d_lam_, nlam_ * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(g.data(), d_g_, nlam_ * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(w.data(), d_w_, nlam_ * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(d_st_, &st, sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
+        info->iteration_ms = timeit([&] { cudaGraphLaunch(graph_, s_); });
+        CK(cudaMemcpyAsync(d_st_, &saved, sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_lam_, lam.data(), nlam_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_g_, g.data(), nlam_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+        CK(cudaMemcpyAsync(d_w_, w.data(), nlam_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+        CK(cudaStreamSynchronize(s_));
+        info->kernels_per_iteration = kernels_per_iter_;
+    }
+    CK(cudaGetLastError());
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     return HTF_OK;
 }
 

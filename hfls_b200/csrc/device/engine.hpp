@@ -21,7 +21,8 @@ public:
     explicit Engine(const Options &o) : opt_(o) {}
     ~Engine();
     int setup(Problem &p, std::string &err);
-    int pcpg(Problem &p, double *u, htf_stats *stats, std::string &err);
+    int solve(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err);
+    int profile(int reps, htf_profile_info *info, std::string &err);
     int apply(int op, const double *x, double *y, int nrhs, std::string &err);   // 0=F, 1=P, 2=M
     double setup_ms = 0.0;
     int status_sub = -1;
@@ -39,8 +40,9 @@ private:
     void op_P(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial,
               PcpgState *st);
     void iteration(PcpgState *st);
-    int solve_one(Problem &p, int rhs, double *u_loc_host, int &iters, double &norm0, double &rel,
+    int solve_one(Problem &p, int rhs, double *u_dev, int &iters, double &norm0, double &rel,
                   double &solve_ms, std::string &err);
+    int ensure_rhs(int nrhs, std::string &err);
 
     Options opt_;
     cudaStream_t s_ = nullptr;
@@ -69,6 +71,13 @@ private:
     int nchunks_ = 0;
     int *d_status_ = nullptr;
     int *d_csp_ = nullptr, *d_cs_ = nullptr;   // cluster -> subdomain lists
+    double *d_fbody_ = nullptr;                // assembled body-force load (full vectors)
+    int *d_own_ = nullptr;                     // full slot -> global DOF it owns, or -1
+    int *d_win_ = nullptr;                     // global DOF -> full slot of the highest subdomain
+    double *d_fn_ = nullptr, *d_u_ = nullptr;  // nodal loads / displacements (global DOFs x nrhs)
+    int rhs_cap_ = 0, ndof_ = 0;
+    int kernels_per_iter_ = 0;
+    long long launches_ = 0;                   // kernels launched by the current solve call
     // vectors
     double *d_f_ = nullptr, *d_full_ = nullptr, *d_full2_ = nullptr;
     double *d_lam_ = nullptr, *d_g_ = nullptr, *d_w_ = nullptr, *d_Fw_ = nullptr, *d_Pg_ = nullptr,

@@ -88,34 +88,42 @@ std::vector<int> null_pivots(const std::vector<double> &R, int n, int m) {
     return out;
 }
 
+// Right-looking Cholesky, column-contiguous updates.
 bool chol_lower(int n, double *A, int lda) {
-    for (int j = 0; j < n; ++j) {
-        double d = A[j + size_t(j) * lda];
-        for (int k = 0; k < j; ++k) d -= A[j + size_t(k) * lda] * A[j + size_t(k) * lda];
+    for (int k = 0; k < n; ++k) {
+        double *ck = A + size_t(k) * lda;
+        const double d = ck[k];
         if (!(d > 0.0)) return false;
-        d = std::sqrt(d);
-        A[j + size_t(j) * lda] = d;
-        for (int i = j + 1; i < n; ++i) {
-            double s = A[i + size_t(j) * lda];
-            for (int k = 0; k < j; ++k) s -= A[i + size_t(k) * lda] * A[j + size_t(k) * lda];
-            A[i + size_t(j) * lda] = s / d;
+        const double r = std::sqrt(d);
+        ck[k] = r;
+        for (int i = k + 1; i < n; ++i) ck[i] /= r;
+        for (int j = k + 1; j < n; ++j) {
+            const double ljk = ck[j];
+            if (ljk == 0.0) continue;
+            double *cj = A + size_t(j) * lda;
+            for (int i = j; i < n; ++i) cj[i] -= ck[i] * ljk;
         }
     }
     return true;
 }
 
+// L L^T X = B for nrhs columns; forward in axpy form, backward in dot form,
+// both over contiguous columns of L.
 void chol_solve(int n, const double *L, int lda, double *B, int ldb, int nrhs) {
     for (int r = 0; r < nrhs; ++r) {
         double *x = B + size_t(r) * ldb;
-        for (int i = 0; i < n; ++i) {
-            double s = x[i];
-            for (int k = 0; k < i; ++k) s -= L[i + size_t(k) * lda] * x[k];
-            x[i] = s / L[i + size_t(i) * lda];
+        for (int k = 0; k < n; ++k) {
+            const double *ck = L + size_t(k) * lda;
+            const double xk = x[k] / ck[k];
+            x[k] = xk;
+            if (xk != 0.0)
+                for (int i = k + 1; i < n; ++i) x[i] -= ck[i] * xk;
         }
         for (int i = n - 1; i >= 0; --i) {
+            const double *ci = L + size_t(i) * lda;
             double s = x[i];
-            for (int k = i + 1; k < n; ++k) s -= L[k + size_t(i) * lda] * x[k];
-            x[i] = s / L[i + size_t(i) * lda];
+            for (int k = i + 1; k < n; ++k) s -= ci[k] * x[k];
+            x[i] = s / ci[i];
         }
     }
 }

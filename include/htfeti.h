@@ -120,6 +120,7 @@ typedef struct htf_stats {
     double fapply_bytes;     /* algorithmic bytes of one F apply              */
     int n_lambda, n_sub, n_clusters, n_rhs;
     int status_sub;          /* subdomain index of an HTF_ENOTSPD failure     */
+    long long kernel_launches; /* kernels this call launched on the device    */
 } htf_stats;
 
 /* PCPG for every load case and the displacement field.  Replaces
@@ -128,6 +129,27 @@ typedef struct htf_stats {
  * the displacements (for DOFs shared by several subdomains the highest
  * subdomain index wins, as in the reference).  u may be NULL.             */
 int htf_pcpg(htf_ctx *ctx, double *u, htf_stats *stats);
+
+/* Solve n_rhs new load cases with the factors resident on the device.
+ * f_nodal[3*n_nodes*n_rhs] (column-major, may be NULL) is added to the body
+ * force; u[3*n_nodes*n_rhs] receives the displacements as in htf_pcpg.
+ * Host buffers in and out; this is the call a serving loop makes per
+ * request.  Replaces a repeated Cluster::pcpg with a new rhs
+ * (Cluster.cpp:1385-1458) without redoing the setup.                     */
+int htf_solve(htf_ctx *ctx, int n_rhs, const double *f_nodal, double *u, htf_stats *stats);
+
+/* Device timing of the dominant kernels on the library's own stream
+ * (CUDA events, averaged over `reps` launches after one warm-up), with the
+ * algorithmic bytes each launch moves.  No counterpart in the reference
+ * (it only prints clock() totals, Cluster.cpp:378-379, 1451-1452).        */
+typedef struct htf_profile_info {
+    double symv_F_ms, symv_F_bytes;     /* y_b = F_i x_b over all subdomains        */
+    double symv_S_ms, symv_S_bytes;     /* preconditioner block, same layout        */
+    double fapply_ms, fapply_bytes;     /* whole F apply (gather .. scatter)        */
+    double iteration_ms;                /* one captured PCPG iteration              */
+    int kernels_per_iteration;          /* kernel launches in one iteration graph   */
+} htf_profile_info;
+int htf_profile(htf_ctx *ctx, int reps, htf_profile_info *info);
 
 /* The dual operators on host vectors of length n_lambda (nrhs columns,
  * column-major).  Replace Cluster::mult_Ff (Cluster.cpp:1114-1188),
