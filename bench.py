@@ -248,9 +248,10 @@ def main():
     peak, peak_kind = peaks()
     achieved = prof.symv_F_bytes / (prof.symv_F_ms * 1e-3) / 1e9
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tf):
-        traffic = json.load(open(tf)).get("k_symv_fp64_cfg1_bytes_per_launch")
+    tf = os.path.join(ROOT, "profiles", "k_symv_fp64_cfg1.md")
+    if os.path.exists(tf) and args.workload == "full":
+        m = re.search(r"^traffic_bytes_per_launch_scaled:\s*([0-9.eE+]+)", open(tf).read(), re.M)
+        traffic = float(m.group(1)) if m else None
     iterations = int(statistics.median(iters))
     cpu = None if args.no_cpu_baseline else cpu_baseline(iterations, mesh.n_sub)
     ndof = 3 * mesh.n_nodes
