@@ -37,6 +37,7 @@ struct SubDev {
     int bcr_off;                          // offset of this subdomain's Bc row ids (c entries)
     int bce_off;                          // Bc entries (CSR by compressed Bc row): ptr offset
     long long R_off;                      // R in permuted local order, N x 6 (padded rows 0)
+    int u0, u1;                           // SYMV work units of this subdomain [u0, u1)
     int fix[6];                           // fix DOFs (positions in permuted order)
     double fix_diag[6];                   // original diagonal at the fix DOFs
 };
@@ -46,6 +47,17 @@ struct ClusterDev {
     long long M_off;                      // M = (Ac^{-1}) restricted, ngc x ngc (col-major)
     int gc_off;                           // offset in the concatenated coarse vectors
     int gmap_off;                         // gather map: ptr array offset (ngc+1 entries)
+};
+
+// One SYMV work unit: packed tiles [t0, t1) of subdomain d (kind 0), or the
+// V^T x_b product of subdomain d (kind 1).  Units write partial y sums for
+// b rows [0, rows) to scratch at y_off; they are summed in unit order.
+struct SymvUnit {
+    int d, kind;
+    long long t0, t1;
+    long long y_off;
+    int rows;
+    int pad;
 };
 
 // One 32-column step of the batched Cholesky for one subdomain.

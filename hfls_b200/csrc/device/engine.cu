@@ -33,6 +33,14 @@ __global__ void k_gather_b(int, const int *, const int *, const double *, const 
 template <typename T>
 __global__ void k_symv(const SubDev *, const T *, const double *, double *, const PcpgState *);
 __global__ void k_vt(const SubDev *, const double *, const double *, double *, const PcpgState *);
+template <typename T>
+__global__ void k_symv_units(const SymvUnit *, const SubDev *, const T *, const double *, const double *, double *,
+                             double *, const PcpgState *);
+__global__ void k_reduce_correct(const SubDev *, const SymvUnit *, const double *, const ClusterDev *,
+                                 const double *, const int *, const double *, double *, const PcpgState *);
+__global__ void k_gf_apply_fused(int, int, const int *, const double *, const double *, const int *,
+                                 const double *, const double *, double *, double *, double *, const double *,
+                                 double *, const PcpgState *);
 __global__ void k_gc(int, const int *, const int *, const double *, double *, const PcpgState *);
 __global__ void k_coarse(const ClusterDev *, const double *, const double *, double *, const PcpgState *);
 __global__ void k_correct(const SubDev *, const ClusterDev *, const double *, const int *, const double *,
@@ -255,6 +263,31 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     nslots_ = xb;
     nfull_ = nf;
     ntiles_ = T_off;
+    // SYMV work units: ~48 tiles (384 KB in FP64) per unit, sub-contiguous
+    std::vector<SymvUnit> units;
+    long long yoff = 0;
+    const long long UNIT_TILES = 48;
+    for (int d = 0; d < nsub_; ++d) {
+        SubDev &h = hs_[d];
+        const long long nt2 = (long long)h.nt * (h.nt + 1) / 2;
+        h.u0 = int(units.size());
+        for (long long t0 = 0; t0 < nt2; t0 += UNIT_TILES) {
+            const long long t1 = std::min(nt2, t0 + UNIT_TILES);
+            long long I = 0;
+            while ((I + 1) * (I + 2) / 2 <= t1 - 1) ++I;         // tile row of the last tile
+            SymvUnit u{d, 0, t0, t1, yoff, int(TILE * (I + 1)), 0};
+            yoff += u.rows;
+            units.push_back(u);
+        }
+        h.u1 = int(units.size());
+        max_nbp_ = std::max(max_nbp_, h.nbp);
+    }
+    nunits_ = int(units.size());
+    for (int d = 0; d < nsub_; ++d) units.push_back(SymvUnit{d, 1, 0, 0, 0, 0, 0});   // V^T x units
+    d_units_ = alloc<SymvUnit>(units.size(), err, rc);
+    d_ypart_ = alloc<double>(yoff, err, rc);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(d_units_, units.data(), units.size() * sizeof(SymvUnit), cudaMemcpyHostToDevice, s_));
     // clusters
     hc_.assign(ncl_, ClusterDev());
     long long M_off = 0;
@@ -780,7 +813,7 @@ int Engine::outer_coarse(Problem &p, std::string &err) {
     for (int i = 0; i < m; ++i) invGtG_[i + size_t(i) * m] = 1.0;
     chol_solve(m, L.data(), m, invGtG_.data(), m, m);
     // chunks
-    const int CH = 4096;
+    const int CH = 1024;
     std::vector<int> ch_cl, ch_beg, ch_end, clp(ncl_ + 1, 0), rows_all;
     std::vector<double> vals_all;
     for (int c = 0; c < ncl_; ++c) {
@@ -866,6 +899,13 @@ int Engine::setup(Problem &p, std::string &err) {
         for (auto &h : hs_) max_nbp = std::max(max_nbp, h.nbp);
         symv_smem_ = (1 + 4) * max_nbp * int(sizeof(double));
         if (symv_smem_ > 48 * 1024) {
+            rc = check(cudaFuncSetAttribute(k_symv_units<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, symv_smem_),
+                       "cudaFuncSetAttribute", err);
+            if (!rc)
+                rc = check(cudaFuncSetAttribute(k_symv_units<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, symv_smem_),
+                           "cudaFuncSetAttribute", err);
+        }
+        if (!rc && symv_smem_ > 48 * 1024) {
             rc = check(cudaFuncSetAttribute(k_symv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, symv_smem_),
                        "cudaFuncSetAttribute", err);
             if (!rc)
@@ -907,36 +947,35 @@ int Engine::setup(Problem &p, std::string &err) {
 void Engine::op_F(const double *w, double *Fw, const double *dotv, double *partial, PcpgState *st) {
     k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, w, nullptr, d_xb_, st);
     if (mixed_)
-        k_symv<float><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_F32_, d_xb_, d_yb_, st);
+        k_symv_units<float><<<nunits_ + nsub_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F32_, d_V_, d_xb_, d_ypart_, d_t_, st);
     else
-        k_symv<double><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_F_, d_xb_, d_yb_, st);
-    k_vt<<<nsub_, 256, 0, s_>>>(d_subs_, d_V_, d_xb_, d_t_, st);
+        k_symv_units<double><<<nunits_ + nsub_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, st);
     k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, st);
     int maxg = 0;
     for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
     k_coarse<<<dim3(ncl_, cdiv(maxg, 8)), 256, 0, s_>>>(d_cl_, d_M_, d_gc_, d_s_, st);
-    k_correct<<<nsub_, 256, 0, s_>>>(d_subs_, d_cl_, d_V_, d_bcr_, d_s_, d_yb_, st);
+    k_reduce_correct<<<dim3(nsub_, cdiv(max_nbp_, 256)), 256, 0, s_>>>(d_subs_, d_units_, d_ypart_, d_cl_, d_V_, d_bcr_,
+                                                                       d_s_, d_yb_, st);
     k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, nullptr, Fw, dotv, partial, st);
 }
 
 void Engine::op_M(const double *x, double *z, PcpgState *st) {
-    if (opt_.preconditioner == "none") {
-        k_copy<<<cdiv(nlam_, 256), 256, 0, s_>>>(nlam_, x, z, st);
-        return;
-    }
     k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, x, d_weight_, d_xb_, st);
     if (mixed_)
-        k_symv<float><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_S32_, d_xb_, d_yb_, st);
+        k_symv_units<float><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S32_, d_V_, d_xb_, d_ypart_, d_t_, st);
     else
-        k_symv<double><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_S_, d_xb_, d_yb_, st);
+        k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_, st);
+    k_reduce_correct<<<dim3(nsub_, cdiv(max_nbp_, 256)), 256, 0, s_>>>(d_subs_, d_units_, d_ypart_, d_cl_, d_V_, d_bcr_,
+                                                                       nullptr, d_yb_, st);
     k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, d_weight_, z, nullptr, nullptr, st);
 }
 
 void Engine::op_P(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial,
                   PcpgState *st) {
     k_gft_partial<<<nchunks_, 256, 0, s_>>>(d_chunk_cl_, d_chunk_beg_, d_chunk_end_, d_crow_, d_cval_, x, d_gpart_, st);
-    k_gft_final<<<1, 256, 6 * ncl_ * sizeof(double), s_>>>(ncl_, d_cl_chunk_ptr_, d_gpart_, d_invGtG_, d_a_, alpha_out, st);
-    k_gf_apply<<<npart_, 256, 0, s_>>>(nlam_, d_gcl_, d_gval_, x, d_a_, Px, dotv, partial, st);
+    k_gf_apply_fused<<<npart_, 256, 12 * ncl_ * sizeof(double), s_>>>(nlam_, ncl_, d_cl_chunk_ptr_, d_gpart_, d_invGtG_,
+                                                                        d_gcl_, d_gval_, x, d_a_, alpha_out, Px, dotv,
+                                                                        partial, st);
 }
 
 void Engine::iteration(PcpgState *st) {
@@ -1019,7 +1058,7 @@ int Engine::solve_one(Problem &p, int rhs, double *u_dev, int &iters, double &no
     }
     PcpgState hst;
     const int every = std::max(1, opt_.check_every);
-    launches_ += 29 + 12;     // kernels of the start (x, d, lambda0, g0, Pz) and of the reconstruction
+    launches_ += 27 + 12;     // kernels of the start (x, d, lambda0, g0, Pz) and of the reconstruction
     for (;;) {
         for (int k = 0; k < every; ++k) CK(cudaGraphLaunch(graph_, s_));
         launches_ += (long long)every * kernels_per_iter_;
@@ -1124,13 +1163,17 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
     double tri = 0.0, vec = 0.0;
     for (auto &h : hs_) { tri += sz * double(h.nb) * (h.nb + 1) / 2; vec += 16.0 * h.nb; }
     info->symv_F_ms = timeit([&] {
-        if (mixed_) k_symv<float><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_F32_, d_xb_, d_yb_, nullptr);
-        else k_symv<double><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_F_, d_xb_, d_yb_, nullptr);
+        if (mixed_)
+            k_symv_units<float><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F32_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
+        else
+            k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
     });
     info->symv_F_bytes = tri + vec;
     info->symv_S_ms = timeit([&] {
-        if (mixed_) k_symv<float><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_S32_, d_xb_, d_yb_, nullptr);
-        else k_symv<double><<<nsub_, 128, symv_smem_, s_>>>(d_subs_, d_S_, d_xb_, d_yb_, nullptr);
+        if (mixed_)
+            k_symv_units<float><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S32_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
+        else
+            k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
     });
     info->symv_S_bytes = tri + vec;
     info->fapply_ms = timeit([&] { op_F(d_lam_, d_Fw_, nullptr, nullptr, nullptr); });

@@ -78,6 +78,9 @@ private:
     int rhs_cap_ = 0, ndof_ = 0;
     int kernels_per_iter_ = 0;
     long long launches_ = 0;                   // kernels launched by the current solve call
+    SymvUnit *d_units_ = nullptr;              // SYMV work units (+ one V^T x unit per subdomain)
+    double *d_ypart_ = nullptr;                // partial y sums of the units (scratch)
+    int nunits_ = 0, max_nbp_ = 0;
     // vectors
     double *d_f_ = nullptr, *d_full_ = nullptr, *d_full2_ = nullptr;
     double *d_lam_ = nullptr, *d_g_ = nullptr, *d_w_ = nullptr, *d_Fw_ = nullptr, *d_Pg_ = nullptr,

@@ -117,6 +117,111 @@ template __global__ void k_symv<double>(const SubDev *, const double *, const do
 template __global__ void k_symv<float>(const SubDev *, const float *, const double *, double *,
                                        const PcpgState *);
 
+// SYMV over work units (kind 0) and V^T x (kind 1) in one launch; partial y
+// of a unit -> ypart[y_off, y_off+rows), summed later in unit order.
+template <typename T>
+__global__ void __launch_bounds__(SYMV_WARPS * 32) k_symv_units(const SymvUnit *__restrict__ units,
+                                                                const SubDev *__restrict__ subs,
+                                                                const T *__restrict__ tiles,
+                                                                const double *__restrict__ Vbuf,
+                                                                const double *__restrict__ xb,
+                                                                double *__restrict__ ypart,
+                                                                double *__restrict__ t,
+                                                                const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    extern __shared__ double sm[];
+    const SymvUnit u = units[blockIdx.x];
+    const SubDev &sd = subs[u.d];
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+    const double *x = xb + sd.xb_off;
+    if (u.kind == 1) {                      // t_d = V_d^T x_b
+        for (int col = warp; col < sd.c + 6; col += SYMV_WARPS) {
+            const double *V = Vbuf + sd.V_off + (size_t)col * sd.nbp;
+            double a = 0.0;
+            for (int i = lane; i < sd.nb; i += 32) a += V[i] * x[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(FULL, a, o);
+            if (lane == 0) t[sd.t_off + col] = a;
+        }
+        return;
+    }
+    const int rows = u.rows;                // 32 * (last tile row + 1)
+    double *xs = sm;                        // rows
+    double *yp = sm + rows;                 // SYMV_WARPS x rows
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) xs[i] = x[i];
+    for (int i = threadIdx.x; i < SYMV_WARPS * rows; i += blockDim.x) yp[i] = 0.0;
+    __syncthreads();
+    double *my = yp + warp * rows;
+    const T *base = tiles + sd.T_off * TILE_ELEMS;
+    for (long long tt = u.t0 + warp; tt < u.t1; tt += SYMV_WARPS) {
+        int I = (int)((sqrt(8.0 * (double)tt + 1.0) - 1.0) * 0.5);
+        while ((long long)(I + 1) * (I + 2) / 2 <= tt) ++I;
+        while ((long long)I * (I + 1) / 2 > tt) --I;
+        const int J = (int)(tt - (long long)I * (I + 1) / 2);
+        const T *tp = base + tt * TILE_ELEMS;
+        double v[32];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) v[r] = (double)tp[r * TILE + lane];
+        const double xJ = xs[TILE * J + lane];
+        double p[32];
+        double col = 0.0;
+#pragma unroll
+        for (int r = 0; r < 32; ++r) {
+            p[r] = v[r] * xJ;
+            col += v[r] * xs[TILE * I + r];
+        }
+        reduce_scatter32(p, lane);
+        my[TILE * I + lane] += p[0];
+        if (I != J) my[TILE * J + lane] += col;
+    }
+    __syncthreads();
+    double *out = ypart + u.y_off;
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+        double a = 0.0;
+#pragma unroll
+        for (int q = 0; q < SYMV_WARPS; ++q) a += yp[q * rows + i];
+        out[i] = a;
+    }
+}
+
+template __global__ void k_symv_units<double>(const SymvUnit *, const SubDev *, const double *, const double *,
+                                              const double *, double *, double *, const PcpgState *);
+template __global__ void k_symv_units<float>(const SymvUnit *, const SubDev *, const float *, const double *,
+                                             const double *, double *, double *, const PcpgState *);
+
+// y_b = sum of the unit partials (in unit order) [- V_d s_d when s != null];
+// grid (subdomain, chunk of 256 b rows)
+__global__ void k_reduce_correct(const SubDev *__restrict__ subs, const SymvUnit *__restrict__ units,
+                                 const double *__restrict__ ypart, const ClusterDev *__restrict__ cl,
+                                 const double *__restrict__ Vbuf, const int *__restrict__ bcrows,
+                                 const double *__restrict__ s, double *__restrict__ yb,
+                                 const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    __shared__ double sd_s[256];
+    const SubDev &sd = subs[blockIdx.x];
+    const int i = blockIdx.y * blockDim.x + threadIdx.x;
+    const int nc = sd.c + 6;
+    if (s) {
+        const ClusterDev &c = cl[sd.cluster];
+        for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+            const int pos = (q < sd.c) ? bcrows[sd.bcr_off + q] : sd.alpha_pos + (q - sd.c);
+            sd_s[q] = s[c.gc_off + pos];
+        }
+        __syncthreads();
+    }
+    if (blockIdx.y * blockDim.x >= sd.nbp || i >= sd.nbp) return;
+    double a = 0.0;
+    for (int k = sd.u0; k < sd.u1; ++k) {
+        const SymvUnit &u = units[k];
+        if (i < u.rows) a += ypart[u.y_off + i];
+    }
+    if (s && i < sd.nb) {
+        const double *V = Vbuf + sd.V_off + i;
+        for (int q = 0; q < nc; ++q) a -= V[(size_t)q * sd.nbp] * sd_s[q];
+    }
+    yb[sd.xb_off + i] = a;
+}
+
 // t_d = V_d^T x_b  (c+6 values per subdomain)
 __global__ void k_vt(const SubDev *__restrict__ subs, const double *__restrict__ Vbuf,
                      const double *__restrict__ xb, double *__restrict__ t, const PcpgState *__restrict__ st) {
@@ -303,6 +408,65 @@ __global__ void k_gft_final(int ncl, const int *__restrict__ cl_chunk_ptr, const
         a[q] = s;
         if (alpha_out) alpha_out[q] = -s;
     }
+}
+
+// Px = x - Gf a with a = invGtG * (chunk partials summed per cluster)
+// computed by every CTA (the coarse dimension 6*ncl is small); CTA 0 also
+// writes a and -a (alpha) to global memory.
+__global__ void k_gf_apply_fused(int nlam, int ncl, const int *__restrict__ cl_chunk_ptr,
+                                 const double *__restrict__ gpart, const double *__restrict__ invGtG,
+                                 const int *__restrict__ gcl, const double *__restrict__ gval,
+                                 const double *__restrict__ x, double *__restrict__ a_out,
+                                 double *__restrict__ alpha_out, double *__restrict__ Px,
+                                 const double *__restrict__ dotv, double *__restrict__ partial,
+                                 const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    extern __shared__ double sh[];
+    double *gt = sh;                 // 6*ncl
+    double *a = sh + 6 * ncl;        // 6*ncl
+    __shared__ double red[256];
+    const int m = 6 * ncl;
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+        const int c = q / 6, i = q % 6;
+        double s = 0.0;
+        for (int ch = cl_chunk_ptr[c]; ch < cl_chunk_ptr[c + 1]; ++ch) s += gpart[6 * (size_t)ch + i];
+        gt[q] = s;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+        double s = 0.0;
+        for (int p = 0; p < m; ++p) s += invGtG[q + (size_t)p * m] * gt[p];
+        a[q] = s;
+        if (blockIdx.x == 0) {
+            if (a_out) a_out[q] = s;
+            if (alpha_out) alpha_out[q] = -s;
+        }
+    }
+    __syncthreads();
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    double prod = 0.0;
+    if (r < nlam) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int c = gcl[2 * r + k];
+            if (c < 0) continue;
+            const double *g = gval + 6 * (size_t)(2 * r + k);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) v += g[q] * a[6 * c + q];
+        }
+        const double pv = x[r] - v;
+        Px[r] = pv;
+        if (dotv) prod = pv * dotv[r];
+    }
+    if (!partial) return;
+    red[threadIdx.x] = prod;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
 }
 
 __global__ void k_gf_apply(int nlam, const int *__restrict__ gcl, const double *__restrict__ gval,
