@@ -66,7 +66,9 @@ _SIGS = {
     "htf_dual_sizes": [ctypes.c_void_p, _ip, _ip, _ip],
     "htf_dual_layout": [ctypes.c_void_p, _ip, _ip, _dp, _dp],
     "htf_fix_dofs": [ctypes.c_void_p, _ip],
+    "htf_projection_noalloc": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
 }
+HTF_NOALLOC_SCRATCH_DOUBLES = 1048576
 for _name, _args in _SIGS.items():
     _f = getattr(lib, _name)
     _f.argtypes = _args
@@ -253,6 +255,12 @@ class Solver:
         y = np.zeros_like(x)
         self._check(fn(self._h, _d(x), _d(y), x.shape[0]), name)
         return y
+
+    def projection_noalloc(self, x_dev_ptr, px_dev_ptr, stream_ptr=0):
+        """htf_projection_noalloc on device pointers (ints); enqueued on the
+        given CUDA stream, returns without waiting."""
+        self._check(lib.htf_projection_noalloc(self._h, ctypes.c_void_p(x_dev_ptr), ctypes.c_void_p(px_dev_ptr),
+                                               ctypes.c_void_p(stream_ptr)), "htf_projection_noalloc")
 
     def mult_Ff(self, w):
         return self._op(lib.htf_mult_Ff, w, "htf_mult_Ff")

@@ -157,6 +157,19 @@ int htf_mult_Ff(htf_ctx *ctx, const double *w, double *Fw, int nrhs) { return ap
 int htf_projection(htf_ctx *ctx, const double *x, double *Px, int nrhs) { return apply_op(ctx, 1, x, Px, nrhs); }
 int htf_preconditioning(htf_ctx *ctx, const double *x, double *Mx, int nrhs) { return apply_op(ctx, 2, x, Mx, nrhs); }
 
+int htf_projection_noalloc(htf_ctx *ctx, const double *x_dev, double *Px_dev, void *stream) {
+    if (!ctx) return HTF_EINVAL;
+    if (!ctx->is_setup) return fail(ctx, HTF_ESTATE, "htf_projection_noalloc before htf_setup");
+    if (!x_dev || !Px_dev) return fail(ctx, HTF_EINVAL, "htf_projection_noalloc: null vector");
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) return fail(ctx, HTF_ECUDA, "cudaGetDevice failed");
+    if (prev != ctx->eng->device() && cudaSetDevice(ctx->eng->device()) != cudaSuccess)
+        return fail(ctx, HTF_ECUDA, "cudaSetDevice failed");
+    int rc = ctx->eng->project_noalloc(x_dev, Px_dev, static_cast<cudaStream_t>(stream), ctx->err);
+    if (prev != ctx->eng->device()) cudaSetDevice(prev);
+    return rc;
+}
+
 int htf_dual_sizes(htf_ctx *ctx, int *n_lambda, int *n_sub, int *n_clusters) {
     if (!ctx) return HTF_EINVAL;
     if (ctx->p.rows.empty()) {

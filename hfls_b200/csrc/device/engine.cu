@@ -1142,6 +1142,26 @@ int Engine::solve(Problem &p, int nrhs, const double *f_nodal, double *u, htf_st
     return HTF_OK;
 }
 
+// projector with the reduction scratch in the static array of noalloc.cu
+int Engine::project_noalloc(const double *x, double *Px, cudaStream_t stream, std::string &err) {
+    double *scr = nullptr;
+    size_t cap = 0;
+    int rc = noalloc_scratch(&scr, &cap, err);
+    if (rc) return rc;
+    const size_t need = 6 * (size_t)nchunks_ + 6 * (size_t)ncl_;
+    if (need > cap) {
+        err = "htf_projection_noalloc: problem needs " + std::to_string(need) +
+              " doubles of scratch, the static array holds " + std::to_string(cap);
+        return HTF_EINVAL;
+    }
+    k_gft_partial<<<nchunks_, 256, 0, stream>>>(d_chunk_cl_, d_chunk_beg_, d_chunk_end_, d_crow_, d_cval_, x, scr,
+                                                nullptr);
+    k_gf_apply_fused<<<npart_, 256, 12 * ncl_ * sizeof(double), stream>>>(
+        nlam_, ncl_, d_cl_chunk_ptr_, scr, d_invGtG_, d_gcl_, d_gval_, x, scr + 6 * (size_t)nchunks_, nullptr, Px,
+        nullptr, nullptr, nullptr);
+    return check(cudaGetLastError(), "htf_projection_noalloc launch", err);
+}
+
 int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
     if (!info || reps < 1) { err = "bad arguments"; return HTF_EINVAL; }
     std::memset(info, 0, sizeof(*info));

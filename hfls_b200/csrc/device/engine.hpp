@@ -11,6 +11,9 @@
 
 namespace htf {
 
+// static scratch of the allocation-free entry point (noalloc.cu)
+int noalloc_scratch(double **ptr, size_t *cap, std::string &err);
+
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
@@ -23,6 +26,8 @@ public:
     int setup(Problem &p, std::string &err);
     int solve(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err);
     int profile(int reps, htf_profile_info *info, std::string &err);
+    int project_noalloc(const double *x, double *Px, cudaStream_t stream, std::string &err);
+    int device() const { return opt_.device; }
     int apply(int op, const double *x, double *y, int nrhs, std::string &err);   // 0=F, 1=P, 2=M
     double setup_ms = 0.0;
     int status_sub = -1;

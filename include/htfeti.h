@@ -159,6 +159,21 @@ int htf_mult_Ff(htf_ctx *ctx, const double *w, double *Fw, int nrhs);
 int htf_projection(htf_ctx *ctx, const double *x, double *Px, int nrhs);
 int htf_preconditioning(htf_ctx *ctx, const double *x, double *Mx, int nrhs);
 
+/* Projector P x = x - Gf (Gf^T Gf)^{-1} Gf^T x on caller-owned DEVICE
+ * vectors of n_lambda doubles (on the context's device), enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and returning
+ * without waiting.  It allocates nothing: its reduction scratch is a static
+ * device array of HTF_NOALLOC_SCRATCH_DOUBLES doubles (8 MiB, held by every
+ * GPU that loads the library until exit), for callers that cannot allocate
+ * while they project — their own CUDA-graph capture, a fixed device-memory
+ * budget, latency-bound loops.  No counterpart in the reference.  The first
+ * call on a device looks the array up and should come before any stream
+ * capture; all calls share the array, so calls that overlap on the GPU race.
+ * Returns HTF_EINVAL when the problem needs more scratch (6 doubles per 1024
+ * Gf entries plus 6 per cluster) than the array holds.                    */
+#define HTF_NOALLOC_SCRATCH_DOUBLES 1048576
+int htf_projection_noalloc(htf_ctx *ctx, const double *x_dev, double *Px_dev, void *stream);
+
 /* Dual layout for checking: n_lambda, and for every Bf row its entries as
  * (subdomain, global DOF, sign) with up to two entries per row
  * (Cluster.cpp:846-924); weights (Cluster.cpp:893-895, 918).  Arrays of
