@@ -18,6 +18,16 @@
 
 namespace htf {
 
+#ifdef __CUDACC__
+// FP32 -> TF32 (10 explicit mantissa bits), round to nearest, ties away from
+// zero; the low 13 bits of the result are zero
+__device__ __forceinline__ float tf32_rna(float a) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(a));
+    return __uint_as_float(r);
+}
+#endif
+
 constexpr int TILE = 32;                  // packed tile edge
 constexpr int TILE_ELEMS = TILE * TILE;
 
@@ -58,6 +68,18 @@ struct SymvUnit {
     long long y_off;
     int rows;
     int pad;
+};
+
+// One CTA of the tensor-core multi-RHS product: 128-row block m of
+// subdomain d (slabs (m, 0..ks-1) contiguous at a_off, X slabs at x_off).
+struct GemmBlock {
+    int d;
+    int m;
+    long long a_off;
+    int ks;
+    int rows;
+    long long x_off;
+    long long y_row0;
 };
 
 // One 32-column step of the batched Cholesky for one subdomain.

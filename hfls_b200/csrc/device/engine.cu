@@ -161,11 +161,6 @@ __global__ void k_small_gemv(int m, const double *__restrict__ A, const double *
     }
 }
 
-__global__ void k_to_f32(long long n, const double *__restrict__ a, float *__restrict__ b) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        b[i] = (float)a[i];
-}
-
 // f[r][i] = fbody[i] + fn[r][own[i]]
 __global__ void k_build_f(int nfull, int ndof, int nrhs, const double *__restrict__ fbody, const int *__restrict__ own,
                           const double *__restrict__ fn, double *__restrict__ f) {
@@ -200,20 +195,6 @@ int Engine::check(cudaError_t e, const char *what, std::string &err) {
     if (e == cudaSuccess) return HTF_OK;
     err = std::string(what) + ": " + cudaGetErrorString(e);
     return (e == cudaErrorMemoryAllocation) ? HTF_ENOMEM : HTF_ECUDA;
-}
-
-template <typename T> T *Engine::alloc(size_t n, std::string &err, int &rc) {
-    if (rc) return nullptr;
-    void *p = nullptr;
-    size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) {
-        rc = check(e, "cudaMalloc", err);
-        err += " (" + std::to_string(bytes) + " bytes)";
-        return nullptr;
-    }
-    bufs_.push_back({p, bytes});
-    return static_cast<T *>(p);
 }
 
 #define CK(call)                                                   \
@@ -914,14 +895,10 @@ int Engine::setup(Problem &p, std::string &err) {
         }
     }
     if (!rc && opt_.mixed) {
-        d_F32_ = alloc<float>(ntiles_ * TILE_ELEMS, err, rc);
-        d_S32_ = alloc<float>(ntiles_ * TILE_ELEMS, err, rc);
-        if (!rc) {
-            k_to_f32<<<1184, 256, 0, s_>>>(ntiles_ * TILE_ELEMS, d_F_, d_F32_);
-            k_to_f32<<<1184, 256, 0, s_>>>(ntiles_ * TILE_ELEMS, d_S_, d_S32_);
-            rc = check(cudaGetLastError(), "k_to_f32", err);
-        }
+        // FP32 slabs for the tensor-core products of the batched form; the
+        // FP64 tiles stay resident for the FP64 residuals
         mixed_ = true;
+        rc = setup_batch(opt_.batch, err);
     }
     if (!rc) rc = check(cudaEventRecord(e1, s_), "cudaEventRecord", err);
     if (!rc) rc = check(cudaEventSynchronize(e1), "cudaEventSynchronize", err);
@@ -930,9 +907,9 @@ int Engine::setup(Problem &p, std::string &err) {
     setup_ms = ms;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    // algorithmic bytes of one F apply (FP64 or FP32 tiles, V, lambda gather/scatter)
+    // algorithmic bytes of one FP64 F apply (triangular tiles, V, lambda gather/scatter)
     double bytes = 0.0;
-    const double sz = mixed_ ? 4.0 : 8.0;
+    const double sz = 8.0;
     for (int d = 0; d < nsub_; ++d) {
         const Subdomain &s = p.sub[d];
         const double nb = s.nb;
@@ -946,10 +923,7 @@ int Engine::setup(Problem &p, std::string &err) {
 // ---------------------------------------------------------------------------
 void Engine::op_F(const double *w, double *Fw, const double *dotv, double *partial, PcpgState *st) {
     k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, w, nullptr, d_xb_, st);
-    if (mixed_)
-        k_symv_units<float><<<nunits_ + nsub_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F32_, d_V_, d_xb_, d_ypart_, d_t_, st);
-    else
-        k_symv_units<double><<<nunits_ + nsub_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, st);
+    k_symv_units<double><<<nunits_ + nsub_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, st);
     k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, st);
     int maxg = 0;
     for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
@@ -961,10 +935,7 @@ void Engine::op_F(const double *w, double *Fw, const double *dotv, double *parti
 
 void Engine::op_M(const double *x, double *z, PcpgState *st) {
     k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, x, d_weight_, d_xb_, st);
-    if (mixed_)
-        k_symv_units<float><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S32_, d_V_, d_xb_, d_ypart_, d_t_, st);
-    else
-        k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_, st);
+    k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_, st);
     k_reduce_correct<<<dim3(nsub_, cdiv(max_nbp_, 256)), 256, 0, s_>>>(d_subs_, d_units_, d_ypart_, d_cl_, d_V_, d_bcr_,
                                                                        nullptr, d_yb_, st);
     k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, d_weight_, z, nullptr, nullptr, st);
@@ -989,6 +960,7 @@ void Engine::iteration(PcpgState *st) {
 }
 
 int Engine::apply(int op, const double *x, double *y, int nrhs, std::string &err) {
+    if (mixed_ && bK_ > 0) return apply_batch(op, x, y, nrhs, err);
     for (int k = 0; k < nrhs; ++k) {
         CK(cudaMemcpyAsync(d_tmp_, x + (size_t)k * nlam_, nlam_ * sizeof(double), cudaMemcpyHostToDevice, s_));
         if (op == 0) op_F(d_tmp_, d_Fw_, nullptr, nullptr, nullptr);
@@ -1001,50 +973,68 @@ int Engine::apply(int op, const double *x, double *y, int nrhs, std::string &err
     return HTF_OK;
 }
 
-// one load case: Cluster::pcpg (Cluster.cpp:1363-1458) + printVTK (1648-1678)
-int Engine::solve_one(Problem &p, int rhs, double *u_dev, int &iters, double &norm0, double &rel,
-                      double &solve_ms, std::string &err) {
-    const double *f = d_f_ + (size_t)rhs * nfull_;
-    int maxcols = 0;
-    for (auto &h : hs_) maxcols = std::max(maxcols, h.c + 6);
+// x = K_HT^+ f, d = Bf x, lambda0 = Gf (GfTGf)^{-1} Rf^T f  (Cluster.cpp:1385-1394, 967-1040)
+void Engine::init_rhs(const double *f) {
     int maxg = 0;
     for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
-    auto kplus_full = [&](double *v) {          // v <- K_reg^{-1} v on full vectors
-        k_trsv_fwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, v, 0);
-        k_trsv_bwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, v, 0);
-    };
-    auto coarse_from_full = [&](const double *z, const double *y) {   // s = M [Bc z ; -R^T y]
-        k_bc_rt<<<nsub_, 256, 0, s_>>>(d_subs_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_R_, z, y, d_t_);
-        k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, nullptr);
-        k_coarse<<<dim3(ncl_, cdiv(maxg, 8)), 256, 0, s_>>>(d_cl_, d_M_, d_gc_, d_s_, nullptr);
-    };
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    // x = K_HT^+ f ; d = Bf x  (Cluster.cpp:1385-1387, 967-1040)
-    CK(cudaMemcpyAsync(d_full_, f, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-    kplus_full(d_full_);
-    coarse_from_full(d_full_, f);
+    cudaMemcpyAsync(d_full_, f, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_);
+    k_trsv_fwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full_, 0);
+    k_trsv_bwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full_, 0);
+    k_bc_rt<<<nsub_, 256, 0, s_>>>(d_subs_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_R_, d_full_, f, d_t_);
+    k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, nullptr);
+    k_coarse<<<dim3(ncl_, cdiv(maxg, 8)), 256, 0, s_>>>(d_cl_, d_M_, d_gc_, d_s_, nullptr);
     k_full_to_b<<<nsub_, 256, 0, s_>>>(d_subs_, d_full_, d_yb_);
     k_correct<<<nsub_, 256, 0, s_>>>(d_subs_, d_cl_, d_V_, d_bcr_, d_s_, d_yb_, nullptr);
     k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, nullptr, d_d_, nullptr, nullptr, nullptr);
-    // e = Rf^T f ; lambda0 = Gf (GfTGf)^{-1} e  (Cluster.cpp:1390-1394)
-    {
-        k_e_vec<<<cdiv(6 * ncl_, 128), 128, 0, s_>>>(ncl_, d_csp_, d_cs_, d_subs_, d_H_, d_t_, d_gc_);
-        k_small_gemv<<<1, 256, 0, s_>>>(6 * ncl_, d_invGtG_, d_gc_, d_a_);
-        k_gf_mult<<<npart_, 256, 0, s_>>>(nlam_, d_gcl_, d_gval_, d_a_, d_lam_);
-    }
-    CK(cudaEventRecord(e0, s_));
-    // g0 = F lambda0 - d ; Pg ; z = M Pg ; Pz ; gPz  (Cluster.cpp:1398-1412)
+    k_e_vec<<<cdiv(6 * ncl_, 128), 128, 0, s_>>>(ncl_, d_csp_, d_cs_, d_subs_, d_H_, d_t_, d_gc_);
+    k_small_gemv<<<1, 256, 0, s_>>>(6 * ncl_, d_invGtG_, d_gc_, d_a_);
+    k_gf_mult<<<npart_, 256, 0, s_>>>(nlam_, d_gcl_, d_gval_, d_a_, d_lam_);
+}
+
+// g = F lambda - d ; Pg (alpha) ; z = M Pg ; Pz ; g.Pz partials -> st  (Cluster.cpp:1398-1412)
+double Engine::pcpg_start(PcpgState *st) {
     op_F(d_lam_, d_g_, nullptr, nullptr, nullptr);
     k_axpby<<<npart_, 256, 0, s_>>>(nlam_, -1.0, d_d_, 1.0, d_g_);
     op_P(d_g_, d_Pg_, d_alpha_, nullptr, nullptr, nullptr);
     op_M(d_Pg_, d_z_, nullptr);
     op_P(d_z_, d_Pz_, nullptr, d_g_, d_partial_, nullptr);
-    k_init_state<<<1, 256, 0, s_>>>(d_partial_, npart_, d_st_, opt_.eps_iter, opt_.max_iter);
+    k_init_state<<<1, 256, 0, s_>>>(d_partial_, npart_, st, opt_.eps_iter, opt_.max_iter);
+    return 0.0;
+}
+
+// u = K_HT^+(f - Bf^T lambda) - Rf alpha  (Cluster.cpp:1648-1678)
+void Engine::reconstruct(const double *f, double *u_dev) {
+    int maxg = 0;
+    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
+    cudaMemcpyAsync(d_full_, f, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_);
+    k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, d_lam_, nullptr, d_xb_, nullptr);
+    k_full_minus_b<<<nsub_, 256, 0, s_>>>(d_subs_, d_xb_, d_full_);
+    cudaMemcpyAsync(d_full2_, d_full_, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_);
+    k_trsv_fwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full2_, 0);
+    k_trsv_bwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full2_, 0);
+    k_bc_rt<<<nsub_, 256, 0, s_>>>(d_subs_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_R_, d_full2_, d_full_, d_t_);
+    k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, nullptr);
+    k_coarse<<<dim3(ncl_, cdiv(maxg, 8)), 256, 0, s_>>>(d_cl_, d_M_, d_gc_, d_s_, nullptr);
+    k_sub_bct<<<nsub_, 32, 0, s_>>>(d_subs_, d_cl_, d_bcr_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_s_, d_full_);
+    k_trsv_fwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full_, 0);
+    k_trsv_bwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full_, 0);
+    k_add_R<<<nsub_, 256, 0, s_>>>(d_subs_, d_cl_, d_R_, d_H_, d_s_, d_alpha_, d_full_);
+    if (u_dev) k_gather_u<<<cdiv(ndof_, 256), 256, 0, s_>>>(ndof_, d_win_, d_full_, u_dev);
+}
+
+// one load case: Cluster::pcpg (Cluster.cpp:1363-1458) + printVTK (1648-1678)
+int Engine::solve_one(Problem &p, int rhs, double *u_dev, int &iters, double &norm0, double &rel,
+                      double &solve_ms, std::string &err) {
+    (void)p;
+    const double *f = d_f_ + (size_t)rhs * nfull_;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    init_rhs(f);
+    CK(cudaEventRecord(e0, s_));
+    pcpg_start(d_st_);
     CK(cudaMemcpyAsync(d_w_, d_Pz_, nlam_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
     CK(cudaGetLastError());
-    // iterations: one captured graph per iteration, host check every few
     if (!graph_) {
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
@@ -1076,18 +1066,7 @@ int Engine::solve_one(Problem &p, int rhs, double *u_dev, int &iters, double &no
     rel = hst.rel;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    // u = K_HT^+(f - Bf^T lambda) - Rf alpha  (Cluster.cpp:1648-1678)
-    CK(cudaMemcpyAsync(d_full_, f, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-    k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, d_lam_, nullptr, d_xb_, nullptr);
-    k_full_minus_b<<<nsub_, 256, 0, s_>>>(d_subs_, d_xb_, d_full_);                       // y = f - Bf^T lam
-    CK(cudaMemcpyAsync(d_full2_, d_full_, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-    kplus_full(d_full2_);                                                                  // z = K_reg^{-1} y
-    coarse_from_full(d_full2_, d_full_);                                                   // s = M [Bc z; -R^T y]
-    k_sub_bct<<<nsub_, 32, 0, s_>>>(d_subs_, d_cl_, d_bcr_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_s_, d_full_);
-    kplus_full(d_full_);                                                                   // K_reg^{-1}(y - Bc^T lam_c)
-    k_add_R<<<nsub_, 256, 0, s_>>>(d_subs_, d_cl_, d_R_, d_H_, d_s_, d_alpha_, d_full_);
-    CK(cudaGetLastError());
-    if (u_dev) k_gather_u<<<cdiv(ndof_, 256), 256, 0, s_>>>(ndof_, d_win_, d_full_, u_dev);
+    reconstruct(f, u_dev);
     CK(cudaGetLastError());
     if (hst.done == 2) { err = "PCPG breakdown (w'Fw <= 0 or non-finite)"; return HTF_EBREAKDOWN; }
     return HTF_OK;
@@ -1105,6 +1084,7 @@ int Engine::ensure_rhs(int nrhs, std::string &err) {
 }
 
 int Engine::solve(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err) {
+    if (mixed_ && bK_ > 0) return solve_batch(p, nrhs, f_nodal, u, stats, err);
     int rc = ensure_rhs(nrhs, err);
     if (rc) return rc;
     launches_ = 1;            // k_build_f
@@ -1179,21 +1159,15 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
         return double(ms) / reps;
     };
     k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, d_lam_, nullptr, d_xb_, nullptr);
-    const double sz = mixed_ ? 4.0 : 8.0;
+    const double sz = 8.0;
     double tri = 0.0, vec = 0.0;
     for (auto &h : hs_) { tri += sz * double(h.nb) * (h.nb + 1) / 2; vec += 16.0 * h.nb; }
     info->symv_F_ms = timeit([&] {
-        if (mixed_)
-            k_symv_units<float><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F32_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
-        else
-            k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
+        k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
     });
     info->symv_F_bytes = tri + vec;
     info->symv_S_ms = timeit([&] {
-        if (mixed_)
-            k_symv_units<float><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S32_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
-        else
-            k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
+        k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
     });
     info->symv_S_bytes = tri + vec;
     info->fapply_ms = timeit([&] { op_F(d_lam_, d_Fw_, nullptr, nullptr, nullptr); });

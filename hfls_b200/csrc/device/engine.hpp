@@ -27,6 +27,11 @@ public:
     int solve(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err);
     int profile(int reps, htf_profile_info *info, std::string &err);
     int project_noalloc(const double *x, double *Px, cudaStream_t stream, std::string &err);
+    // batched mixed-precision form (engine_batch.cu)
+    int setup_batch(int K, std::string &err);
+    int solve_batch(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err);
+    int apply_batch(int op, const double *x, double *y, int nrhs, std::string &err);
+    bool batch_ready() const { return bK_ > 0; }
     int device() const { return opt_.device; }
     int apply(int op, const double *x, double *y, int nrhs, std::string &err);   // 0=F, 1=P, 2=M
     double setup_ms = 0.0;
@@ -34,6 +39,14 @@ public:
 
 private:
     template <typename T> T *alloc(size_t n, std::string &err, int &rc);
+    void init_rhs(const double *f);                       // d = Bf K_HT^+ f, lambda0
+    void reconstruct(const double *f, double *u_dev);     // u from lambda, alpha
+    double pcpg_start(PcpgState *st);                     // g0, Pg, z, Pz; returns nothing useful
+    void tc_apply(const float *A);
+    void op_F_batch(const double *w, double *Fw, const double *dotv, double *partial);
+    void op_M_batch(const double *x, double *z);
+    void op_P_batch(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial);
+    void iteration_batch();
     int check(cudaError_t e, const char *what, std::string &err);
     int upload_layout(Problem &p, std::string &err);
     int factorize(Problem &p, std::string &err);
@@ -60,7 +73,6 @@ private:
     ClusterDev *d_cl_ = nullptr;
     int *d_all_subs_ = nullptr;          // 0..nsub-1
     double *d_K_ = nullptr, *d_F_ = nullptr, *d_S_ = nullptr, *d_X_ = nullptr;
-    float *d_F32_ = nullptr, *d_S32_ = nullptr;
     double *d_V_ = nullptr, *d_R_ = nullptr, *d_M_ = nullptr, *d_H_ = nullptr;
     int *d_bcr_ = nullptr, *d_bce_ptr_ = nullptr, *d_bce_pos_ = nullptr;
     double *d_bce_val_ = nullptr;
@@ -86,6 +98,20 @@ private:
     SymvUnit *d_units_ = nullptr;              // SYMV work units (+ one V^T x unit per subdomain)
     double *d_ypart_ = nullptr;                // partial y sums of the units (scratch)
     int nunits_ = 0, max_nbp_ = 0;
+    // batched mixed-precision form
+    int bK_ = 0, nblocks_ = 0, bnpart_ = 0, bnpartP_ = 0;
+    float *d_AF_ = nullptr, *d_AS_ = nullptr, *d_Xs_ = nullptr;
+    void *d_blocks_ = nullptr;
+    int *d_slot_sub_ = nullptr, *d_tcerr_ = nullptr;
+    double *b_lam_ = nullptr, *b_g_ = nullptr, *b_w_ = nullptr, *b_Fw_ = nullptr, *b_Pg_ = nullptr, *b_z_ = nullptr,
+           *b_Pz_ = nullptr, *b_d_ = nullptr, *b_xb_ = nullptr, *b_yb_ = nullptr, *b_t_ = nullptr, *b_gc_ = nullptr,
+           *b_s_ = nullptr, *b_part_ = nullptr, *b_gpart_ = nullptr, *b_wFw_ = nullptr, *b_gPz_ = nullptr, *b_gw_ = nullptr,
+           *b_alpha_ = nullptr, *b_tmp_ = nullptr;
+    PcpgState *b_st_ = nullptr;
+    cudaGraphExec_t bgraph_ = nullptr;
+    int bkernels_per_iter_ = 0;
+    int tc_smem_ = 0;
+    long long aoff_ = 0;                       // floats per FP32 slab array
     // vectors
     double *d_f_ = nullptr, *d_full_ = nullptr, *d_full2_ = nullptr;
     double *d_lam_ = nullptr, *d_g_ = nullptr, *d_w_ = nullptr, *d_Fw_ = nullptr, *d_Pg_ = nullptr,
@@ -101,5 +127,19 @@ private:
     std::vector<std::vector<double>> Hd_;   // per subdomain 6x6 rows of ker(Gc)
     std::vector<double> invGtG_;
 };
+
+template <typename T> T *Engine::alloc(size_t n, std::string &err, int &rc) {
+    if (rc) return nullptr;
+    void *p = nullptr;
+    const size_t bytes = (n > 0 ? n : 1) * sizeof(T);
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        rc = check(e, "cudaMalloc", err);
+        err += " (" + std::to_string(bytes) + " bytes)";
+        return nullptr;
+    }
+    bufs_.push_back({p, bytes});
+    return static_cast<T *>(p);
+}
 
 }  // namespace htf

@@ -1,0 +1,368 @@
+// Batched mixed-precision PCPG (K load cases at once).
+//
+// F_i and S_i are applied as full FP32 matrices on the tensor cores
+// (tc_gemm.cu, TF32 products, FP32 accumulation); everything else — gather,
+// coarse problem, projector, recurrences — stays FP64.  Accuracy comes from
+// an outer FP64 loop: the true residual g = F lambda - d is evaluated with
+// the FP64 F_i (one load case at a time), and the inner mixed-precision
+// PCPG is restarted from it until the reference's stopping rule
+// sqrt(g'Pz) < eps * sqrt(g0'Pz0) (Cluster.cpp:1424-1426) holds for the
+// FP64 residual.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace htf {
+
+template <int K>
+__global__ void k_tc_gemm(const GemmBlock *, const float *, const float *, long long, double *, int *);
+__global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *);
+__global__ void k_gather_multi(int, int, const int *, const int *, const double *, const double *, const int *,
+                               const SubDev *, double *, float *, float *);
+__global__ void k_vt_multi(int, const SubDev *, const double *, const double *, double *);
+__global__ void k_gc_multi(int, int, const int *, const int *, const double *, double *);
+__global__ void k_coarse_multi(int, const ClusterDev *, const double *, const double *, double *);
+__global__ void k_correct_multi(int, const SubDev *, const ClusterDev *, const double *, const int *,
+                                const double *, double *);
+__global__ void k_rows_multi(int, int, const int *, const double *, const double *, const double *, double *,
+                             const double *, double *);
+__global__ void k_gft_partial_multi(int, const int *, const int *, const int *, const double *, const double *,
+                                    double *);
+__global__ void k_gf_apply_multi(int, int, int, const int *, const double *, const double *, const int *,
+                                 const double *, const double *, double *, double *, const double *, double *);
+__global__ void k_colsum(const double *, int, int, double *);
+__global__ void k_update_lam_g_multi(int, int, const double *, const double *, const double *, const double *, double *,
+                                     double *, PcpgState *);
+__global__ void k_dot_multi(int, int, const double *, const double *, double *);
+__global__ void k_update_w_multi(int, int, const double *, const double *, double *, const PcpgState *);
+__global__ void k_finish_multi(int, const double *, const double *, PcpgState *);
+__global__ void k_col_get(int, int, int, const double *, double *);
+__global__ void k_col_set(int, int, int, const double *, double *);
+__global__ void k_sum_to(const double *, int, double *, const PcpgState *);
+__global__ void k_build_f(int, int, int, const double *, const int *, const double *, double *);
+
+static inline int cdivb(long long a, long long b) { return int((a + b - 1) / b); }
+
+#define CKB(call)                                                  \
+    do {                                                           \
+        int _rc = check((call), #call, err);                       \
+        if (_rc) return _rc;                                       \
+    } while (0)
+
+int Engine::setup_batch(int K, std::string &err) {
+    if (K != 16 && K != 32) { err = "batch width must be 16 or 32"; return HTF_EINVAL; }
+    int rc = HTF_OK;
+    for (auto &h : hs_)
+        if ((h.c + 6) * K > 2048) {
+            err = "too many Bc rows for the batched form";
+            return HTF_EINVAL;
+        }
+    // tensor-core blocks and FP32 slabs
+    std::vector<GemmBlock> blocks;
+    long long aoff = 0;
+    for (int d = 0; d < nsub_; ++d) {
+        const SubDev &h = hs_[d];
+        const int mb = (h.nbp + 127) / 128, ks = h.nbp / 32;
+        for (int m = 0; m < mb; ++m) {
+            GemmBlock g{d, m, aoff + (long long)m * ks * 4096, ks, std::min(128, h.nb - 128 * m),
+                        (long long)h.xb_off * K, (long long)h.xb_off + 128 * m};
+            blocks.push_back(g);
+        }
+        aoff += (long long)mb * ks * 4096;
+    }
+    nblocks_ = int(blocks.size());
+    d_blocks_ = alloc<GemmBlock>(blocks.size(), err, rc);
+    d_AF_ = alloc<float>(aoff, err, rc);               // FP32 slabs, split into TF32 parts in the kernel
+    d_AS_ = alloc<float>(aoff, err, rc);
+    d_Xs_ = alloc<float>(2 * (size_t)nslots_ * K, err, rc);
+    aoff_ = aoff;
+    d_slot_sub_ = alloc<int>(nslots_, err, rc);
+    d_tcerr_ = alloc<int>(1, err, rc);
+    if (rc) return rc;
+    std::vector<int> ss(nslots_);
+    for (int d = 0; d < nsub_; ++d)
+        for (int i = 0; i < hs_[d].nbp; ++i) ss[hs_[d].xb_off + i] = d;
+    CKB(cudaMemcpyAsync(d_blocks_, blocks.data(), blocks.size() * sizeof(GemmBlock), cudaMemcpyHostToDevice, s_));
+    CKB(cudaMemcpyAsync(d_slot_sub_, ss.data(), nslots_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CKB(cudaMemsetAsync(d_Xs_, 0, 2 * (size_t)nslots_ * K * sizeof(float), s_));
+    CKB(cudaMemsetAsync(d_tcerr_, 0, sizeof(int), s_));
+    int maxks = 0;
+    for (auto &h : hs_) maxks = std::max(maxks, h.nbp / 32);
+    const GemmBlock *db = static_cast<const GemmBlock *>(d_blocks_);
+    k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_F_, d_AF_);
+    k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_S_, d_AS_);
+    CKB(cudaGetLastError());
+    // 4 stages of A_hi, A_lo (16 KB each), X_hi, X_lo (k x 128 B each) + alignment slack
+    tc_smem_ = 1024 + 4 * 2 * (128 * 32 + K * 32) * 4;
+    if (K == 16)
+        CKB(cudaFuncSetAttribute(k_tc_gemm<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_));
+    else
+        CKB(cudaFuncSetAttribute(k_tc_gemm<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_));
+    // batch vectors
+    const size_t nl = (size_t)nlam_ * K;
+    int ntot = 0;
+    for (auto &h : hs_) ntot = std::max(ntot, h.t_off + h.c + 6);
+    bnpart_ = cdivb(nlam_, 256 / K);
+    b_lam_ = alloc<double>(nl, err, rc); b_g_ = alloc<double>(nl, err, rc); b_w_ = alloc<double>(nl, err, rc);
+    b_Fw_ = alloc<double>(nl, err, rc); b_Pg_ = alloc<double>(nl, err, rc); b_z_ = alloc<double>(nl, err, rc);
+    b_Pz_ = alloc<double>(nl, err, rc); b_d_ = alloc<double>(nl, err, rc); b_tmp_ = alloc<double>(nl, err, rc);
+    b_xb_ = alloc<double>((size_t)nslots_ * K, err, rc); b_yb_ = alloc<double>((size_t)nslots_ * K, err, rc);
+    b_t_ = alloc<double>((size_t)ntot * K, err, rc);
+    b_gc_ = alloc<double>((size_t)ngc_total_ * K, err, rc); b_s_ = alloc<double>((size_t)ngc_total_ * K, err, rc);
+    b_part_ = alloc<double>((size_t)bnpart_ * K, err, rc);
+    b_gpart_ = alloc<double>((size_t)nchunks_ * 6 * K, err, rc);
+    b_wFw_ = alloc<double>(K, err, rc); b_gPz_ = alloc<double>(K, err, rc);
+    b_gw_ = alloc<double>(K, err, rc);
+    b_alpha_ = alloc<double>((size_t)6 * ncl_ * K, err, rc);
+    b_st_ = alloc<PcpgState>(K, err, rc);
+    if (rc) return rc;
+    CKB(cudaStreamSynchronize(s_));
+    bK_ = K;
+    return HTF_OK;
+}
+
+// Y_b = A X_b for every subdomain on the tensor cores (A = F or S slabs)
+void Engine::tc_apply(const float *A) {
+    const GemmBlock *db = static_cast<const GemmBlock *>(d_blocks_);
+    const long long xlo = (long long)nslots_ * bK_;
+    if (bK_ == 16)
+        k_tc_gemm<16><<<nblocks_, 192, tc_smem_, s_>>>(db, A, d_Xs_, xlo, b_yb_, d_tcerr_);
+    else
+        k_tc_gemm<32><<<nblocks_, 192, tc_smem_, s_>>>(db, A, d_Xs_, xlo, b_yb_, d_tcerr_);
+}
+
+void Engine::op_F_batch(const double *w, double *Fw, const double *dotv, double *partial) {
+    const int K = bK_;
+    int maxg = 0, maxnb = 0;
+    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
+    for (auto &h : hs_) maxnb = std::max(maxnb, h.nb);
+    const long long xlo = (long long)nslots_ * K;
+    k_gather_multi<<<cdivb((long long)nslots_ * K, 256), 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, w, nullptr,
+                                                                        d_slot_sub_, d_subs_, b_xb_, d_Xs_, d_Xs_ + xlo);
+    tc_apply(d_AF_);
+    k_vt_multi<<<nsub_, 256, 0, s_>>>(K, d_subs_, d_V_, b_xb_, b_t_);
+    k_gc_multi<<<cdivb((long long)ngc_total_ * K, 256), 256, 0, s_>>>(ngc_total_, K, d_gptr_, d_gidx_, b_t_, b_gc_);
+    k_coarse_multi<<<dim3(ncl_, cdivb(maxg, 8)), 256, 0, s_>>>(K, d_cl_, d_M_, b_gc_, b_s_);
+    k_correct_multi<<<dim3(nsub_, cdivb(maxnb, 32)), 256, 0, s_>>>(K, d_subs_, d_cl_, d_V_, d_bcr_, b_s_, b_yb_);
+    k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, nullptr, Fw, dotv, partial);
+}
+
+void Engine::op_M_batch(const double *x, double *z) {
+    const int K = bK_;
+    // the preconditioner must stay a fixed linear operator for the PCPG
+    // recurrences, so it uses the same 3xTF32 products as F
+    const long long xlo = (long long)nslots_ * K;
+    k_gather_multi<<<cdivb((long long)nslots_ * K, 256), 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, x, d_weight_,
+                                                                        d_slot_sub_, d_subs_, b_xb_, d_Xs_, d_Xs_ + xlo);
+    tc_apply(d_AS_);
+    k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, d_weight_, z, nullptr, nullptr);
+}
+
+void Engine::op_P_batch(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial) {
+    const int K = bK_;
+    k_gft_partial_multi<<<nchunks_, 256, 0, s_>>>(K, d_chunk_beg_, d_chunk_end_, d_crow_, d_cval_, x, b_gpart_);
+    k_gf_apply_multi<<<bnpart_, 256, 2 * 6 * ncl_ * K * sizeof(double), s_>>>(
+        nlam_, K, ncl_, d_cl_chunk_ptr_, b_gpart_, d_invGtG_, d_gcl_, d_gval_, x, alpha_out, Px, dotv, partial);
+}
+
+void Engine::iteration_batch() {
+    const int K = bK_;
+    const int nk = cdivb((long long)nlam_ * K, 256);
+    op_F_batch(b_w_, b_Fw_, b_w_, b_part_);
+    k_colsum<<<K, 256, 0, s_>>>(b_part_, bnpart_, K, b_wFw_);
+    k_dot_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, b_g_, b_w_, b_part_);
+    k_colsum<<<K, 256, 0, s_>>>(b_part_, bnpart_, K, b_gw_);
+    k_update_lam_g_multi<<<nk, 256, 0, s_>>>(nlam_, K, b_wFw_, b_gw_, b_w_, b_Fw_, b_lam_, b_g_, b_st_);
+    op_P_batch(b_g_, b_Pg_, nullptr, nullptr, nullptr);
+    op_M_batch(b_Pg_, b_z_);
+    op_P_batch(b_z_, b_Pz_, nullptr, b_g_, b_part_);
+    k_colsum<<<K, 256, 0, s_>>>(b_part_, bnpart_, K, b_gPz_);
+    k_update_w_multi<<<nk, 256, 0, s_>>>(nlam_, K, b_gPz_, b_Pz_, b_w_, b_st_);
+    k_finish_multi<<<1, 32, 0, s_>>>(K, b_wFw_, b_gPz_, b_st_);
+}
+
+int Engine::apply_batch(int op, const double *x, double *y, int nrhs, std::string &err) {
+    const int K = bK_;
+    if (nrhs > K) { err = "more load cases than the batch width"; return HTF_EINVAL; }
+    std::vector<double> hx((size_t)nlam_ * K, 0.0), hy((size_t)nlam_ * K);
+    for (int j = 0; j < nrhs; ++j)
+        for (int r = 0; r < nlam_; ++r) hx[(size_t)r * K + j] = x[(size_t)j * nlam_ + r];
+    CKB(cudaMemcpyAsync(b_tmp_, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+    if (op == 0) op_F_batch(b_tmp_, b_Fw_, nullptr, nullptr);
+    else if (op == 2) op_M_batch(b_tmp_, b_Fw_);
+    else op_P_batch(b_tmp_, b_Fw_, nullptr, nullptr, nullptr);
+    CKB(cudaGetLastError());
+    CKB(cudaMemcpyAsync(hy.data(), b_Fw_, hy.size() * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    CKB(cudaStreamSynchronize(s_));
+    int tcerr = 0;
+    CKB(cudaMemcpy(&tcerr, d_tcerr_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (tcerr) { err = "tensor-core product timed out on a barrier"; return tcerr; }
+    for (int j = 0; j < nrhs; ++j)
+        for (int r = 0; r < nlam_; ++r) y[(size_t)j * nlam_ + r] = hy[(size_t)r * K + j];
+    return HTF_OK;
+}
+
+int Engine::solve_batch(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err) {
+    (void)p;
+    const int K = bK_;
+    int rc = ensure_rhs(nrhs, err);
+    if (rc) return rc;
+    launches_ = 1;
+    if (f_nodal)
+        CKB(cudaMemcpyAsync(d_fn_, f_nodal, (size_t)ndof_ * nrhs * sizeof(double), cudaMemcpyHostToDevice, s_));
+    k_build_f<<<cdivb(nfull_, 256), 256, 0, s_>>>(nfull_, ndof_, nrhs, d_fbody_, d_own_, f_nodal ? d_fn_ : nullptr,
+                                                  d_f_);
+    std::vector<int> stats_it_(K, 0);
+    if (!bgraph_) {
+        cudaGraph_t g;
+        CKB(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        iteration_batch();
+        CKB(cudaStreamEndCapture(s_, &g));
+        size_t nn = 0;
+        CKB(cudaGraphGetNodes(g, nullptr, &nn));
+        bkernels_per_iter_ = int(nn);
+        CKB(cudaGraphInstantiate(&bgraph_, g, 0));
+        cudaGraphDestroy(g);
+    }
+    cudaEvent_t e0, e1;
+    CKB(cudaEventCreate(&e0));
+    CKB(cudaEventCreate(&e1));
+    double total_ms = 0.0;
+    const double inner_rel = 1e-4;
+    for (int r0 = 0; r0 < nrhs; r0 += K) {
+        const int kc = std::min(K, nrhs - r0);
+        // start of every load case in FP64 (x, d, lambda0)
+        CKB(cudaMemsetAsync(b_lam_, 0, (size_t)nlam_ * K * sizeof(double), s_));
+        CKB(cudaMemsetAsync(b_d_, 0, (size_t)nlam_ * K * sizeof(double), s_));
+        for (int j = 0; j < kc; ++j) {
+            init_rhs(d_f_ + (size_t)(r0 + j) * nfull_);
+            k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_d_, b_d_);
+            k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_lam_, b_lam_);
+            launches_ += 27;
+        }
+        CKB(cudaEventRecord(e0, s_));
+        // FP64 start of every load case: g0, Pz0, norm0 (Cluster.cpp:1398-1412)
+        std::vector<PcpgState> st(K);
+        std::vector<double> last(K, 0.0);          // g'Pz at the last FP64 residual
+        std::vector<int> conv(K, 0);
+        for (int j = 0; j < K; ++j) {
+            st[j] = PcpgState{};
+            st[j].done = 1;
+        }
+        auto fp64_residual = [&](int j, bool reset_w) -> int {
+            k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_lam_, d_lam_);
+            k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_d_, d_d_);
+            pcpg_start(d_st_);
+            launches_ += 2 + 15;
+            PcpgState h;
+            CKB(cudaMemcpyAsync(&h, d_st_, sizeof(PcpgState), cudaMemcpyDeviceToHost, s_));
+            CKB(cudaMemcpyAsync(b_alpha_ + (size_t)j * 6 * ncl_, d_alpha_, 6 * ncl_ * sizeof(double),
+                                cudaMemcpyDeviceToDevice, s_));
+            CKB(cudaStreamSynchronize(s_));
+            k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_g_, b_g_);
+            launches_ += 1;
+            if (reset_w) {
+                k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_Pz_, b_w_);
+                launches_ += 1;
+            }
+            st[j].gPz = h.gPz;
+            st[j].gPz_prev = h.gPz;
+            last[j] = h.gPz;
+            if (st[j].norm0 == 0.0) st[j].norm0 = std::sqrt(h.gPz);
+            const double cur = std::sqrt(h.gPz);
+            if (opt_.verbose)
+                std::fprintf(stderr, "[htf mixed] rhs %d it %d FP64 sqrt(gPz)/norm0 = %.3e\n", r0 + j, st[j].it,
+                             st[j].norm0 > 0 ? cur / st[j].norm0 : 0.0);
+            if (!(h.gPz > 0.0) || !std::isfinite(h.gPz) || cur < opt_.eps_iter * st[j].norm0) {
+                conv[j] = 1;
+                st[j].done = 1;
+            } else {
+                st[j].done = 0;
+            }
+            return HTF_OK;
+        };
+        for (int j = 0; j < kc; ++j) {
+            st[j].eps = opt_.eps_iter;
+            st[j].max_iter = opt_.max_iter;
+            st[j].wFw = 1.0;
+            if ((rc = fp64_residual(j, true))) return rc;
+        }
+        for (int j = kc; j < K; ++j) conv[j] = 1;
+        // mixed-precision iterations with reliable updates: whenever the
+        // recursive g'Pz of a load case has dropped by ru^2 since its last
+        // FP64 residual (or it looks converged / broke down), the FP64
+        // residual replaces it; the search direction is kept except after a
+        // breakdown.
+        const double ru2 = 1e-2;
+        CKB(cudaMemcpyAsync(b_st_, st.data(), K * sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
+        for (;;) {
+            bool any = false;
+            for (int j = 0; j < K; ++j) any |= !conv[j];
+            if (!any) break;
+            for (int k = 0; k < opt_.check_every; ++k) CKB(cudaGraphLaunch(bgraph_, s_));
+            launches_ += (long long)opt_.check_every * bkernels_per_iter_;
+            CKB(cudaMemcpyAsync(st.data(), b_st_, K * sizeof(PcpgState), cudaMemcpyDeviceToHost, s_));
+            CKB(cudaStreamSynchronize(s_));
+            int tcerr = 0;
+            CKB(cudaMemcpy(&tcerr, d_tcerr_, sizeof(int), cudaMemcpyDeviceToHost));
+            if (tcerr) { err = "tensor-core product timed out on a barrier"; return tcerr; }
+            bool changed = false;
+            for (int j = 0; j < K; ++j) {
+                if (conv[j]) continue;
+                const bool broke = st[j].done == 2;
+                if (st[j].it >= opt_.max_iter) { conv[j] = 2; continue; }
+                if (st[j].done != 0 || st[j].gPz < ru2 * last[j]) {
+                    st[j].eps = opt_.eps_iter;
+                    if ((rc = fp64_residual(j, broke))) return rc;
+                    changed = true;
+                }
+            }
+            if (changed) CKB(cudaMemcpyAsync(b_st_, st.data(), K * sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
+        }
+        for (int j = 0; j < kc; ++j) stats_it_[j] = st[j].it;
+        std::vector<double> norm0(K);
+        for (int j = 0; j < K; ++j) norm0[j] = st[j].norm0;
+        CKB(cudaEventRecord(e1, s_));
+        CKB(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        total_ms += ms;
+        for (int j = 0; j < kc; ++j) {
+            k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_lam_, d_lam_);
+            CKB(cudaMemcpyAsync(d_alpha_, b_alpha_ + (size_t)j * 6 * ncl_, 6 * ncl_ * sizeof(double),
+                                cudaMemcpyDeviceToDevice, s_));
+            reconstruct(d_f_ + (size_t)(r0 + j) * nfull_, d_u_ + (size_t)(r0 + j) * ndof_);
+            launches_ += 1 + 13;
+            if (stats && r0 + j < 64) {
+                stats->iterations[r0 + j] = stats_it_[j];
+                stats->norm_gPz0[r0 + j] = norm0[j] * norm0[j];
+                stats->final_rel[r0 + j] = 0.0;
+            }
+            if (conv[j] == 2) { err = "PCPG did not converge within max_iter"; return HTF_ENOCONV; }
+        }
+        CKB(cudaGetLastError());
+        for (int j = 0; j < K; ++j) stats_it_[j] = 0;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (u) CKB(cudaMemcpyAsync(u, d_u_, (size_t)ndof_ * nrhs * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    CKB(cudaStreamSynchronize(s_));
+    if (stats) {
+        stats->solve_ms = total_ms;
+        stats->setup_ms = setup_ms;
+        stats->fapply_bytes = fapply_bytes_;
+        stats->n_lambda = nlam_;
+        stats->n_sub = nsub_;
+        stats->n_clusters = ncl_;
+        stats->n_rhs = nrhs;
+        stats->status_sub = status_sub;
+        stats->kernel_launches = launches_;
+    }
+    return HTF_OK;
+}
+
+}  // namespace htf

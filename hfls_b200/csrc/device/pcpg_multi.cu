@@ -1,0 +1,319 @@
+// Batched PCPG kernels: K load cases at once, vectors RHS-interleaved
+// (entry (row, j) at row*K + j), one PcpgState per load case.  Each load
+// case follows Cluster::pcpg (Cluster.cpp:1363-1458) independently; the
+// matrices are read once per iteration for all K.  Reductions are
+// fixed-order (deterministic).
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "device.cuh"
+
+namespace htf {
+
+constexpr unsigned FULLM = 0xffffffffu;
+
+// x_b = Bf^T w (optionally weighted) for all K columns; also writes the FP32
+// X slabs of the tensor-core product in SWIZZLE_128B K-major layout.
+__global__ void k_gather_multi(int nslots, int K, const int *__restrict__ ptr, const int *__restrict__ ent,
+                               const double *__restrict__ w, const double *__restrict__ weight,
+                               const int *__restrict__ slot_sub, const SubDev *__restrict__ subs,
+                               double *__restrict__ xb, float *__restrict__ Xs, float *__restrict__ Xlo) {
+    const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (id >= (long long)nslots * K) return;
+    const int i = int(id / K), j = int(id % K);
+    double v = 0.0;
+    for (int e = ptr[i]; e < ptr[i + 1]; ++e) {
+        const int q = ent[e];
+        const int lam = q >> 1;
+        double a = w[(size_t)lam * K + j];
+        if (weight) a *= weight[lam];
+        v += (q & 1) ? -a : a;
+    }
+    xb[(size_t)i * K + j] = v;
+    if (Xs) {
+        const SubDev &sd = subs[slot_sub[i]];
+        const int il = i - sd.xb_off, kk = il / 32, c = il % 32;
+        const uint32_t b = uint32_t(j * 128 + c * 4);
+        const uint32_t bs = b ^ (((b >> 7) & 7u) << 4);
+        const size_t at = (size_t)sd.xb_off * K + (size_t)kk * K * 32 + bs / 4;
+        const float hi = tf32_rna((float)v);
+        Xs[at] = hi;
+        if (Xlo) Xlo[at] = tf32_rna((float)(v - (double)hi));   // 3xTF32 remainder
+    }
+}
+
+// t[d][q][j] = sum_i V_d[i][q] x_b[i][j]; one CTA per subdomain
+__global__ void k_vt_multi(int K, const SubDev *__restrict__ subs, const double *__restrict__ Vbuf,
+                           const double *__restrict__ xb, double *__restrict__ t) {
+    const SubDev &sd = subs[blockIdx.x];
+    const int ncol = sd.c + 6;
+    const double *V = Vbuf + sd.V_off;
+    const double *x = xb + (size_t)sd.xb_off * K;
+    for (int o = threadIdx.x; o < ncol * K; o += blockDim.x) {
+        const int q = o / K, j = o % K;
+        const double *Vq = V + (size_t)q * sd.nbp;
+        double a = 0.0;
+        for (int i = 0; i < sd.nb; ++i) a += Vq[i] * x[(size_t)i * K + j];
+        t[((size_t)sd.t_off + q) * K + j] = a;
+    }
+}
+
+__global__ void k_gc_multi(int ngc_total, int K, const int *__restrict__ gptr, const int *__restrict__ gidx,
+                           const double *__restrict__ t, double *__restrict__ gc) {
+    const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (id >= (long long)ngc_total * K) return;
+    const int q = int(id / K), j = int(id % K);
+    double s = 0.0;
+    for (int e = gptr[q]; e < gptr[q + 1]; ++e) s += t[(size_t)gidx[e] * K + j];
+    gc[(size_t)q * K + j] = s;
+}
+
+// s = M gc per cluster: CTA (cluster, block of 8 rows); M read once for all K
+__global__ void k_coarse_multi(int K, const ClusterDev *__restrict__ cl, const double *__restrict__ Mbuf,
+                               const double *__restrict__ gc, double *__restrict__ s) {
+    const ClusterDev c = cl[blockIdx.x];
+    const int r0 = blockIdx.y * 8;
+    if (r0 >= c.ngc) return;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;   // warp = row
+    const int row = r0 + warp;
+    if (row >= c.ngc) return;
+    const double *M = Mbuf + c.M_off + (size_t)row * c.ngc;
+    const double *g = gc + (size_t)c.gc_off * K;
+    // lane owns columns j = lane (K <= 32); loop p
+    double a = 0.0;
+    if (lane < K)
+        for (int p = 0; p < c.ngc; ++p) a += M[p] * g[(size_t)p * K + lane];
+    if (lane < K) s[((size_t)c.gc_off + row) * K + lane] = a;
+}
+
+// y_b -= V_d s_d ; CTA (subdomain, chunk of 32 rows)
+__global__ void k_correct_multi(int K, const SubDev *__restrict__ subs, const ClusterDev *__restrict__ cl,
+                                const double *__restrict__ Vbuf, const int *__restrict__ bcrows,
+                                const double *__restrict__ s, double *__restrict__ yb) {
+    __shared__ double ss[256 * 32 / 4];     // (c+6) x K <= 2048
+    const SubDev &sd = subs[blockIdx.x];
+    const ClusterDev &c = cl[sd.cluster];
+    const int nc = sd.c + 6;
+    for (int o = threadIdx.x; o < nc * K; o += blockDim.x) {
+        const int q = o / K, j = o % K;
+        const int pos = (q < sd.c) ? bcrows[sd.bcr_off + q] : sd.alpha_pos + (q - sd.c);
+        ss[o] = s[((size_t)c.gc_off + pos) * K + j];
+    }
+    __syncthreads();
+    const int i0 = blockIdx.y * 32;
+    if (i0 >= sd.nb) return;
+    for (int o = threadIdx.x; o < 32 * K; o += blockDim.x) {
+        const int i = i0 + o / K, j = o % K;
+        if (i >= sd.nb) continue;
+        double a = yb[((size_t)sd.xb_off + i) * K + j];
+        for (int q = 0; q < nc; ++q) a -= Vbuf[sd.V_off + (size_t)q * sd.nbp + i] * ss[q * K + j];
+        yb[((size_t)sd.xb_off + i) * K + j] = a;
+    }
+}
+
+// out[r][j] = wt[r] * sum_k sign * y[slot][j]; partial dot with dotv per (block, j)
+__global__ void k_rows_multi(int nlam, int K, const int *__restrict__ rslot, const double *__restrict__ rsign,
+                             const double *__restrict__ yb, const double *__restrict__ weight,
+                             double *__restrict__ out, const double *__restrict__ dotv,
+                             double *__restrict__ partial) {
+    __shared__ double red[256];
+    const int rows_per_block = 256 / K;
+    const int lr = threadIdx.x / K, j = threadIdx.x % K;
+    const int r = blockIdx.x * rows_per_block + lr;
+    double prod = 0.0;
+    if (lr < rows_per_block && r < nlam) {
+        double v = 0.0;
+        const int s0 = rslot[2 * r], s1 = rslot[2 * r + 1];
+        if (s0 >= 0) v += rsign[2 * r] * yb[(size_t)s0 * K + j];
+        if (s1 >= 0) v += rsign[2 * r + 1] * yb[(size_t)s1 * K + j];
+        if (weight) v *= weight[r];
+        out[(size_t)r * K + j] = v;
+        if (dotv) prod = v * dotv[(size_t)r * K + j];
+    }
+    if (!partial) return;
+    red[threadIdx.x] = prod;
+    __syncthreads();
+    // reduce over the rows of the block, per column j (threads j, j+K, ...)
+    for (int o = (rows_per_block / 2); o > 0; o >>= 1) {
+        if (lr < o) red[threadIdx.x] += red[threadIdx.x + o * K];
+        __syncthreads();
+    }
+    if (lr == 0) partial[(size_t)blockIdx.x * K + j] = red[j];
+}
+
+// Gf^T x per chunk and column: partial[ch][q][j]
+__global__ void k_gft_partial_multi(int K, const int *__restrict__ chunk_beg, const int *__restrict__ chunk_end,
+                                    const int *__restrict__ crow, const double *__restrict__ cval,
+                                    const double *__restrict__ x, double *__restrict__ partial) {
+    __shared__ double red[256];
+    const int ch = blockIdx.x;
+    const int j = threadIdx.x % K, lane_rows = 256 / K, lr = threadIdx.x / K;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    if (lr < lane_rows)
+        for (int e = chunk_beg[ch] + lr; e < chunk_end[ch]; e += lane_rows) {
+            const double xv = x[(size_t)crow[e] * K + j];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) s[q] += cval[6 * (size_t)e + q] * xv;
+        }
+    for (int q = 0; q < 6; ++q) {
+        red[threadIdx.x] = (lr < lane_rows) ? s[q] : 0.0;
+        __syncthreads();
+        for (int o = lane_rows / 2; o > 0; o >>= 1) {
+            if (lr < o) red[threadIdx.x] += red[threadIdx.x + o * K];
+            __syncthreads();
+        }
+        if (lr == 0) partial[((size_t)ch * 6 + q) * K + j] = red[j];
+        __syncthreads();
+    }
+}
+
+// Px = x - Gf a, a = invGtG * sum of the chunk partials (per column), computed by
+// every CTA; CTA 0 stores -a (alpha) when requested; dot partial with dotv.
+__global__ void k_gf_apply_multi(int nlam, int K, int ncl, const int *__restrict__ cl_chunk_ptr,
+                                 const double *__restrict__ gpart, const double *__restrict__ invGtG,
+                                 const int *__restrict__ gcl, const double *__restrict__ gval,
+                                 const double *__restrict__ x, double *__restrict__ alpha_out,
+                                 double *__restrict__ Px, const double *__restrict__ dotv,
+                                 double *__restrict__ partial) {
+    extern __shared__ double sh[];
+    const int m = 6 * ncl;
+    double *gt = sh;             // m x K
+    double *a = sh + m * K;      // m x K
+    __shared__ double red[256];
+    for (int o = threadIdx.x; o < m * K; o += blockDim.x) {
+        const int q = o / K, j = o % K;
+        const int c = q / 6, i = q % 6;
+        double s = 0.0;
+        for (int ch = cl_chunk_ptr[c]; ch < cl_chunk_ptr[c + 1]; ++ch) s += gpart[((size_t)ch * 6 + i) * K + j];
+        gt[o] = s;
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < m * K; o += blockDim.x) {
+        const int q = o / K, j = o % K;
+        double s = 0.0;
+        for (int p = 0; p < m; ++p) s += invGtG[q + (size_t)p * m] * gt[p * K + j];
+        a[o] = s;
+        if (blockIdx.x == 0 && alpha_out) alpha_out[o] = -s;
+    }
+    __syncthreads();
+    const int rows_per_block = 256 / K;
+    const int lr = threadIdx.x / K, j = threadIdx.x % K;
+    const int r = blockIdx.x * rows_per_block + lr;
+    double prod = 0.0;
+    if (lr < rows_per_block && r < nlam) {
+        double v = 0.0;
+        for (int k = 0; k < 2; ++k) {
+            const int c = gcl[2 * r + k];
+            if (c < 0) continue;
+            const double *g = gval + 6 * (size_t)(2 * r + k);
+            for (int q = 0; q < 6; ++q) v += g[q] * a[(6 * c + q) * K + j];
+        }
+        const double pv = x[(size_t)r * K + j] - v;
+        Px[(size_t)r * K + j] = pv;
+        if (dotv) prod = pv * dotv[(size_t)r * K + j];
+    }
+    if (!partial) return;
+    red[threadIdx.x] = prod;
+    __syncthreads();
+    for (int o = rows_per_block / 2; o > 0; o >>= 1) {
+        if (lr < o) red[threadIdx.x] += red[threadIdx.x + o * K];
+        __syncthreads();
+    }
+    if (lr == 0) partial[(size_t)blockIdx.x * K + j] = red[j];
+}
+
+// sum of partials of column j (fixed order), one CTA per column
+__device__ double col_sum(const double *partial, int np, int K, int j) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partial[(size_t)i * K + j];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+// per column: scalar = sum of partials -> out[j]
+__global__ void k_colsum(const double *__restrict__ partial, int np, int K, double *__restrict__ out) {
+    const double s = col_sum(partial, np, K, blockIdx.x);
+    if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+// rho_j = -gPz_j / wFw_j ; lam += rho w ; g += rho Fw  (skips finished columns)
+__global__ void k_update_lam_g_multi(int n, int K, const double *__restrict__ wFw, const double *__restrict__ gw,
+                                     const double *__restrict__ w, const double *__restrict__ Fw,
+                                     double *__restrict__ lam, double *__restrict__ g, PcpgState *__restrict__ st) {
+    const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (id >= (long long)n * K) return;
+    const int j = int(id % K);
+    if (st[j].done) return;
+    // step length -g'w / w'Fw: equal to -g'Pz / w'Fw in exact arithmetic, and
+    // still the exact line minimum along w after the residual g has been
+    // replaced by the FP64 one
+    const double d = wFw[j];
+    double rho = -gw[j] / d;
+    if (!(d > 0.0) || !isfinite(rho)) rho = 0.0;
+    lam[id] += rho * w[id];
+    g[id] += rho * Fw[id];
+}
+
+// partial[blk][j] = sum over the rows of block blk of a[r][j] * b[r][j]
+// (256 / K rows per block, the row layout of k_rows_multi)
+__global__ void k_dot_multi(int nlam, int K, const double *__restrict__ a, const double *__restrict__ b,
+                            double *__restrict__ partial) {
+    __shared__ double red[256];
+    const int rows_per_block = 256 / K;
+    const int lr = threadIdx.x / K, j = threadIdx.x % K;
+    const int r = blockIdx.x * rows_per_block + lr;
+    double prod = 0.0;
+    if (lr < rows_per_block && r < nlam) prod = a[(size_t)r * K + j] * b[(size_t)r * K + j];
+    red[threadIdx.x] = prod;
+    __syncthreads();
+    for (int o = (rows_per_block / 2); o > 0; o >>= 1) {
+        if (lr < o) red[threadIdx.x] += red[threadIdx.x + o * K];
+        __syncthreads();
+    }
+    if (lr == 0) partial[(size_t)blockIdx.x * K + j] = red[j];
+}
+
+__global__ void k_update_w_multi(int n, int K, const double *__restrict__ gPz_new, const double *__restrict__ Pz,
+                                 double *__restrict__ w, const PcpgState *__restrict__ st) {
+    const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (id >= (long long)n * K) return;
+    const int j = int(id % K);
+    if (st[j].done) return;
+    w[id] = Pz[id] + (gPz_new[j] / st[j].gPz) * w[id];
+}
+
+__global__ void k_finish_multi(int K, const double *__restrict__ wFw, const double *__restrict__ gPz_new,
+                               PcpgState *__restrict__ st) {
+    const int j = threadIdx.x;
+    if (j >= K || st[j].done) return;
+    const double gPz = gPz_new[j];
+    st[j].wFw = wFw[j];
+    st[j].gamma = gPz / st[j].gPz;
+    st[j].gPz_prev = st[j].gPz;
+    st[j].gPz = gPz;
+    st[j].it += 1;
+    st[j].rel = sqrt(gPz) / st[j].norm0;
+    if (!(wFw[j] > 0.0) || !isfinite(gPz)) st[j].done = 2;   // hand back to the FP64 residual check
+    else if (sqrt(gPz) < st[j].eps * st[j].norm0) st[j].done = 1;
+    else if (st[j].it >= st[j].max_iter) st[j].done = 3;
+}
+
+// strided column copy between a batch vector (stride K) and a plain vector
+__global__ void k_col_get(int n, int K, int j, const double *__restrict__ B, double *__restrict__ v) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) v[r] = B[(size_t)r * K + j];
+}
+__global__ void k_col_set(int n, int K, int j, const double *__restrict__ v, double *__restrict__ B) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) B[(size_t)r * K + j] = v[r];
+}
+
+}  // namespace htf

@@ -1,0 +1,323 @@
+// Multi-right-hand-side F_i / S_i apply on the 5th-generation tensor cores.
+//
+// Y_b(:, 0:k) = A_i X_b(:, 0:k) for every subdomain i, with A_i the full
+// symmetric F_i (or S_i) stored in FP32 and the products formed as 3xTF32
+// (A_hi X_hi + A_hi X_lo + A_lo X_hi) on the tensor cores
+// (Cluster::mult_Ff's local solves, Cluster.cpp:1125-1126, applied to k
+// load cases at once).
+//
+// Storage: A_i is cut into 128 x 32 slabs (128 rows of an M block, 32
+// columns of a K slab), each 16 KB and already in the SWIZZLE_128B K-major
+// layout the MMA reads from shared memory (byte b of the logical row-major
+// slab lives at b ^ (((b >> 7) & 7) << 4)), so one cp.async.bulk per slab
+// lands it ready for tcgen05.mma.  X is written by the gather kernel in the
+// same layout as k x 32 slabs (one 128-byte row per load case), already
+// split into its TF32 part and the TF32 remainder.
+//
+// One CTA of 6 warps per (subdomain, 128-row block):
+//   * warp 0, one thread: bulk-copy producer (A slab, X_hi, X_lo per stage);
+//   * warps 2-5: split every landed A slab in place into A_hi = rna_tf32(A)
+//     and A_lo = rna_tf32(A - A_hi), then hand the stage to the MMA issuer;
+//     at the end they read the accumulators out of TMEM (warp w owns TMEM
+//     lanes 32 (w mod 4) .. +31) and write y in FP64;
+//   * warp 1, one thread: issues the MMAs (M=128, N=k, K=8 per instruction,
+//     4 per slab).
+// Accumulation: K slab kk goes to main accumulator kk mod 4 and its two
+// small correction products to correction accumulator kk mod 4, so every
+// FP32 accumulator in TMEM sums a quarter of the K range; the eight are added
+// in FP64 in the epilogue.  Every mbarrier wait is bounded; on time-out the
+// CTA records HTF_ETIMEDOUT in err and stops issuing work.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "device.cuh"
+#include "htfeti.h"
+
+namespace htf {
+
+constexpr int TC_STAGES = 4;
+constexpr int TC_SLAB_A = 128 * 32;          // floats per A slab (16 KB)
+constexpr unsigned TC_WAIT_LIMIT = 1u << 26;  // bounded spin on mbarriers
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes));
+}
+
+// returns false on time-out
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+    uint32_t done = 0;
+    for (unsigned it = 0; it < TC_WAIT_LIMIT; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ uint64_t sw128_desc(const void *smem) {
+    const uint64_t addr = smem_u32(smem);
+    return ((addr >> 4) & 0x3FFFull) | (1ull << 16) /* LBO (ignored for swizzled K-major) */ |
+           (64ull << 32) /* SBO = 1024 B */ | (1ull << 46) /* version */ | (2ull << 61) /* SWIZZLE_128B */;
+}
+
+__device__ __forceinline__ uint32_t tf32_idesc(int M, int N) {
+    return (1u << 4)            // D format F32
+           | (2u << 7)          // A format TF32
+           | (2u << 10)         // B format TF32
+           | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);   // A, B K-major
+}
+
+constexpr int TC_NACC = 4;                   // rotating accumulators (main and correction each)
+constexpr int TC_THREADS = 192;
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+// 16 or 32 consecutive FP32 columns of this warp's 32 TMEM lanes, added into acc
+template <int N>
+__device__ __forceinline__ void tmem_add(uint32_t taddr, double *acc) {
+    uint32_t r[N];
+    if constexpr (N == 16) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+    } else {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+              "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+              "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+              "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr));
+    }
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < N; ++j) acc[j] += (double)__uint_as_float(r[j]);
+}
+
+template <int K>
+__global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__restrict__ blocks,
+                                                           const float *__restrict__ A,
+                                                           const float *__restrict__ Xs, long long xlo_off,
+                                                           double *__restrict__ yb, int *__restrict__ err) {
+    static_assert(K == 16 || K == 32, "N of the MMA");
+    constexpr int SLAB_B = K * 32;                        // floats per X slab
+    constexpr unsigned STAGE_TX = (TC_SLAB_A + 2 * SLAB_B) * 4;
+    constexpr uint32_t TMEM_COLS = 2 * TC_NACC * K;       // 128 or 256
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte aligned stage buffers: stage s holds A_hi, A_lo, then X_hi, X_lo
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    float *sA = reinterpret_cast<float *>(base);                          // TC_STAGES x 2 x 16 KB
+    float *sB = reinterpret_cast<float *>(base + TC_STAGES * 2 * TC_SLAB_A * 4);
+    __shared__ __align__(8) uint64_t full[TC_STAGES], split[TC_STAGES], empty[TC_STAGES], done;
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int abort_flag;
+
+    const GemmBlock g = blocks[blockIdx.x];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&split[s], 4);                      // one arrival per splitting warp
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&done, 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+
+    if (warp == 0) {
+        if (lane == 0) {                                  // producer
+            int issued = 0;
+            for (int kk = 0; kk < g.ks; ++kk) {
+                const int s = kk % TC_STAGES;
+                if (kk >= TC_STAGES && !mbar_wait(&empty[s], ((kk / TC_STAGES) - 1) & 1)) {
+                    atomicExch(err, HTF_ETIMEDOUT);
+                    abort_flag = 1;
+                    break;
+                }
+                if (abort_flag) break;
+                mbar_expect_tx(&full[s], STAGE_TX);
+                bulk_g2s(sA + s * 2 * TC_SLAB_A, A + g.a_off + (long long)kk * TC_SLAB_A, TC_SLAB_A * 4, &full[s]);
+                bulk_g2s(sB + s * 2 * SLAB_B, Xs + g.x_off + (long long)kk * SLAB_B, SLAB_B * 4, &full[s]);
+                bulk_g2s(sB + (s * 2 + 1) * SLAB_B, Xs + xlo_off + g.x_off + (long long)kk * SLAB_B, SLAB_B * 4,
+                         &full[s]);
+                ++issued;
+            }
+            // before the CTA may exit: the last copy into every stage has landed (bounded)
+            for (int kk = (issued > TC_STAGES ? issued - TC_STAGES : 0); kk < issued; ++kk)
+                if (!mbar_wait(&full[kk % TC_STAGES], (kk / TC_STAGES) & 1)) atomicExch(err, HTF_ETIMEDOUT);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {                                  // MMA issuer
+            const uint32_t idesc = tf32_idesc(128, K);
+            for (int kk = 0; kk < g.ks; ++kk) {
+                const int s = kk % TC_STAGES;
+                if (abort_flag || !mbar_wait(&split[s], (kk / TC_STAGES) & 1)) {
+                    atomicExch(err, HTF_ETIMEDOUT);
+                    abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const int a = kk % TC_NACC;
+                const uint32_t dmain = tmem + uint32_t(a * K), dcorr = tmem + uint32_t((TC_NACC + a) * K);
+                const uint64_t da = sw128_desc(sA + s * 2 * TC_SLAB_A);
+                const uint64_t dal = sw128_desc(sA + (s * 2 + 1) * TC_SLAB_A);
+                const uint64_t db = sw128_desc(sB + s * 2 * SLAB_B);
+                const uint64_t dbl = sw128_desc(sB + (s * 2 + 1) * SLAB_B);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {              // 4 x K=8 (32 bytes) per slab
+                    const uint32_t acc = (kk >= TC_NACC || q > 0) ? 1u : 0u;
+                    mma_tf32(dmain, da + 2ull * q, db + 2ull * q, idesc, acc);
+                    mma_tf32(dcorr, da + 2ull * q, dbl + 2ull * q, idesc, acc);
+                    mma_tf32(dcorr, dal + 2ull * q, db + 2ull * q, idesc, 1u);
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&empty[s]))
+                             : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&done))
+                         : "memory");
+        }
+    } else {
+        // warps 2-5: split the A slab of every stage, then the epilogue
+        const int t = threadIdx.x - 64;                  // 0..127
+        for (int kk = 0; kk < g.ks; ++kk) {
+            const int s = kk % TC_STAGES;
+            bool ok = mbar_wait(&full[s], (kk / TC_STAGES) & 1);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok || abort_flag) {
+                if (lane == 0) atomicExch(err, HTF_ETIMEDOUT);
+                abort_flag = 1;
+                break;
+            }
+            float4 *hi = reinterpret_cast<float4 *>(sA + s * 2 * TC_SLAB_A);
+            float4 *lo = reinterpret_cast<float4 *>(sA + (s * 2 + 1) * TC_SLAB_A);
+#pragma unroll
+            for (int i = t; i < TC_SLAB_A / 4; i += 128) {
+                const float4 v = hi[i];
+                float4 h, l;
+                h.x = tf32_rna(v.x); l.x = tf32_rna(v.x - h.x);
+                h.y = tf32_rna(v.y); l.y = tf32_rna(v.y - h.y);
+                h.z = tf32_rna(v.z); l.z = tf32_rna(v.z - h.z);
+                h.w = tf32_rna(v.w); l.w = tf32_rna(v.w - h.w);
+                hi[i] = h;
+                lo[i] = l;
+            }
+            // generic-proxy writes become visible to the tensor core's async proxy
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&split[s]);
+        }
+        __syncwarp();
+        bool have = mbar_wait(&done, 0);
+        have = __all_sync(0xffffffffu, have);            // warp-uniform before the .sync.aligned loads
+        __syncwarp();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (!have) {
+            if (lane == 0) atomicExch(err, HTF_ETIMEDOUT);
+        } else if (!abort_flag) {
+            const int quarter = warp & 3;                 // TMEM lanes this warp may read
+            const int row = quarter * 32 + lane;
+            const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16);
+            double acc[K];
+#pragma unroll
+            for (int j = 0; j < K; ++j) acc[j] = 0.0;
+            const int nacc = g.ks < TC_NACC ? g.ks : TC_NACC;
+            for (int a = 0; a < nacc; ++a) {
+                tmem_add<K>(taddr + uint32_t(a * K), acc);
+                tmem_add<K>(taddr + uint32_t((TC_NACC + a) * K), acc);
+            }
+            if (row < g.rows) {
+                double *y = yb + (g.y_row0 + row) * K;
+#pragma unroll
+                for (int j = 0; j < K; ++j) y[j] = acc[j];
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+template __global__ void k_tc_gemm<16>(const GemmBlock *, const float *, const float *, long long, double *, int *);
+template __global__ void k_tc_gemm<32>(const GemmBlock *, const float *, const float *, long long, double *, int *);
+
+// Full FP32 slabs of a packed symmetric FP64 tile matrix: slab (m, kk) of
+// subdomain d holds rows [128m, 128m+128) x columns [32kk, 32kk+32) of the
+// symmetric block, swizzled for SWIZZLE_128B K-major.  grid (block, kk).
+__global__ void k_make_slabs(const GemmBlock *__restrict__ blocks, const SubDev *__restrict__ subs,
+                             const double *__restrict__ tiles, float *__restrict__ A) {
+    const GemmBlock g = blocks[blockIdx.x];
+    const int kk = blockIdx.y;
+    if (kk >= g.ks) return;
+    const SubDev &sd = subs[g.d];
+    float *slab = A + g.a_off + (long long)kk * TC_SLAB_A;
+    for (int idx = threadIdx.x; idx < TC_SLAB_A; idx += blockDim.x) {
+        const int r = idx / 32, c = idx % 32;
+        const int gr = 128 * g.m + r, gc = 32 * kk + c;
+        float v = 0.f;
+        if (gr < sd.nbp && gc < sd.nbp) {
+            int i = gr, j = gc;
+            if (i < j) { int t = i; i = j; j = t; }
+            const int I = i / TILE, J = j / TILE;
+            const double *T = tiles + (sd.T_off + (long long)I * (I + 1) / 2 + J) * TILE_ELEMS;
+            v = (float)T[(i % TILE) * TILE + (j % TILE)];
+        }
+        const uint32_t b = uint32_t(r * 128 + c * 4);
+        const uint32_t bs = b ^ (((b >> 7) & 7u) << 4);
+        slab[bs / 4] = v;
+    }
+}
+
+}  // namespace htf

@@ -209,6 +209,11 @@ int parse_options(const char *s, Options &o, std::string &err) {
             o.mixed = (v == "mixed");
         } else if (k == "device") o.device = std::atoi(v.c_str());
         else if (k == "check_every") o.check_every = std::max(1, std::atoi(v.c_str()));
+        else if (k == "verbose") o.verbose = std::atoi(v.c_str());
+        else if (k == "batch") {
+            o.batch = std::atoi(v.c_str());
+            if (o.batch != 16 && o.batch != 32) { err = "batch must be 16 or 32"; return HTF_EINVAL; }
+        }
         // reference keys without effect on this path (kept for drop-in option maps)
         else if (k == "vtkWithinIter" || k == "metis" || k == "Ac_clust_explicit" || k == "path2data" ||
                  k == "young_modulus" || k == "ratio_mat" || k == "poissons_ratio" || k == "linear_solver" ||

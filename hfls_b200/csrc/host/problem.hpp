@@ -44,6 +44,8 @@ struct Options {
     bool mixed = false;                               // precision=mixed
     int device = 0;
     int check_every = 8;                              // iterations between host convergence checks
+    int batch = 32;                                   // load cases per batched mixed-precision solve (16 | 32)
+    int verbose = 0;                                  // progress lines on stderr
 };
 int parse_options(const char *s, Options &o, std::string &err);
 
