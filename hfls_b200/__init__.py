@@ -44,7 +44,9 @@ class ProfileInfo(ctypes.Structure):
     _fields_ = [("symv_F_ms", ctypes.c_double), ("symv_F_bytes", ctypes.c_double),
                 ("symv_S_ms", ctypes.c_double), ("symv_S_bytes", ctypes.c_double),
                 ("fapply_ms", ctypes.c_double), ("fapply_bytes", ctypes.c_double),
-                ("iteration_ms", ctypes.c_double), ("kernels_per_iteration", ctypes.c_int)]
+                ("iteration_ms", ctypes.c_double), ("kernels_per_iteration", ctypes.c_int),
+                ("batch_width", ctypes.c_int), ("tc_F_ms", ctypes.c_double), ("tc_F_bytes", ctypes.c_double),
+                ("batch_iteration_ms", ctypes.c_double), ("kernels_per_batch_iteration", ctypes.c_int)]
 
 
 _SIGS = {

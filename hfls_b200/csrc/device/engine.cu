@@ -1192,6 +1192,27 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
         CK(cudaStreamSynchronize(s_));
         info->kernels_per_iteration = kernels_per_iter_;
     }
+    if (mixed_ && bK_ > 0) {
+        const int K = bK_;
+        info->batch_width = K;
+        CK(cudaMemsetAsync(b_tmp_, 0, (size_t)nlam_ * K * sizeof(double), s_));
+        profile_batch_gather(b_tmp_);
+        info->tc_F_ms = timeit([&] { tc_apply(d_AF_); });
+        info->tc_F_bytes = 4.0 * aoff_ + 2.0 * 4.0 * nslots_ * K + 8.0 * nslots_ * K;
+        if (bgraph_) {
+            std::vector<PcpgState> st(K), saved(K);
+            for (auto &x : st) {
+                x = PcpgState{};
+                x.gPz = 1.0; x.norm0 = 1.0; x.eps = 0.0; x.max_iter = 1 << 30; x.wFw = 1.0;
+            }
+            CK(cudaMemcpyAsync(saved.data(), b_st_, K * sizeof(PcpgState), cudaMemcpyDeviceToHost, s_));
+            CK(cudaMemcpyAsync(b_st_, st.data(), K * sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
+            info->batch_iteration_ms = timeit([&] { cudaGraphLaunch(bgraph_, s_); });
+            CK(cudaMemcpyAsync(b_st_, saved.data(), K * sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
+            CK(cudaStreamSynchronize(s_));
+            info->kernels_per_batch_iteration = bkernels_per_iter_;
+        }
+    }
     CK(cudaGetLastError());
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

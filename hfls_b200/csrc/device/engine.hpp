@@ -43,6 +43,7 @@ private:
     void reconstruct(const double *f, double *u_dev);     // u from lambda, alpha
     double pcpg_start(PcpgState *st);                     // g0, Pg, z, Pz; returns nothing useful
     void tc_apply(const float *A);
+    void profile_batch_gather(const double *w);
     void op_F_batch(const double *w, double *Fw, const double *dotv, double *partial);
     void op_M_batch(const double *x, double *z);
     void op_P_batch(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial);
@@ -105,7 +106,7 @@ private:
     int *d_slot_sub_ = nullptr, *d_tcerr_ = nullptr;
     double *b_lam_ = nullptr, *b_g_ = nullptr, *b_w_ = nullptr, *b_Fw_ = nullptr, *b_Pg_ = nullptr, *b_z_ = nullptr,
            *b_Pz_ = nullptr, *b_d_ = nullptr, *b_xb_ = nullptr, *b_yb_ = nullptr, *b_t_ = nullptr, *b_gc_ = nullptr,
-           *b_s_ = nullptr, *b_part_ = nullptr, *b_gpart_ = nullptr, *b_wFw_ = nullptr, *b_gPz_ = nullptr, *b_gw_ = nullptr,
+           *b_s_ = nullptr, *b_part_ = nullptr, *b_gpart_ = nullptr, *b_wFw_ = nullptr, *b_gPz_ = nullptr, *b_gw_ = nullptr, *b_gt_ = nullptr, *b_acoef_ = nullptr,
            *b_alpha_ = nullptr, *b_tmp_ = nullptr;
     PcpgState *b_st_ = nullptr;
     cudaGraphExec_t bgraph_ = nullptr;

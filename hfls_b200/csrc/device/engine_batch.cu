@@ -32,8 +32,9 @@ __global__ void k_rows_multi(int, int, const int *, const double *, const double
                              const double *, double *);
 __global__ void k_gft_partial_multi(int, const int *, const int *, const int *, const double *, const double *,
                                     double *);
-__global__ void k_gf_apply_multi(int, int, int, const int *, const double *, const double *, const int *,
-                                 const double *, const double *, double *, double *, const double *, double *);
+__global__ void k_gf_coef_multi(int, int, const int *, const double *, const double *, double *, double *, double *);
+__global__ void k_gf_apply_multi(int, int, const double *, const int *, const double *, const double *, double *,
+                                 const double *, double *);
 __global__ void k_colsum(const double *, int, int, double *);
 __global__ void k_update_lam_g_multi(int, int, const double *, const double *, const double *, const double *, double *,
                                      double *, PcpgState *);
@@ -106,7 +107,8 @@ int Engine::setup_batch(int K, std::string &err) {
     const size_t nl = (size_t)nlam_ * K;
     int ntot = 0;
     for (auto &h : hs_) ntot = std::max(ntot, h.t_off + h.c + 6);
-    bnpart_ = cdivb(nlam_, 256 / K);
+    // row kernels stride over row groups with a fixed grid: few partials per column
+    bnpart_ = std::min(cdivb(nlam_, 256 / K), 1184);
     b_lam_ = alloc<double>(nl, err, rc); b_g_ = alloc<double>(nl, err, rc); b_w_ = alloc<double>(nl, err, rc);
     b_Fw_ = alloc<double>(nl, err, rc); b_Pg_ = alloc<double>(nl, err, rc); b_z_ = alloc<double>(nl, err, rc);
     b_Pz_ = alloc<double>(nl, err, rc); b_d_ = alloc<double>(nl, err, rc); b_tmp_ = alloc<double>(nl, err, rc);
@@ -117,12 +119,21 @@ int Engine::setup_batch(int K, std::string &err) {
     b_gpart_ = alloc<double>((size_t)nchunks_ * 6 * K, err, rc);
     b_wFw_ = alloc<double>(K, err, rc); b_gPz_ = alloc<double>(K, err, rc);
     b_gw_ = alloc<double>(K, err, rc);
+    b_gt_ = alloc<double>((size_t)6 * ncl_ * K, err, rc); b_acoef_ = alloc<double>((size_t)6 * ncl_ * K, err, rc);
     b_alpha_ = alloc<double>((size_t)6 * ncl_ * K, err, rc);
     b_st_ = alloc<PcpgState>(K, err, rc);
     if (rc) return rc;
     CKB(cudaStreamSynchronize(s_));
     bK_ = K;
     return HTF_OK;
+}
+
+// X slabs of a batch vector (for timing the tensor-core product alone)
+void Engine::profile_batch_gather(const double *w) {
+    const long long xlo = (long long)nslots_ * bK_;
+    k_gather_multi<<<cdivb((long long)nslots_ * bK_, 256), 256, 0, s_>>>(nslots_, bK_, d_slot_ptr_, d_slot_ent_, w,
+                                                                          nullptr, d_slot_sub_, d_subs_, b_xb_, d_Xs_,
+                                                                          d_Xs_ + xlo);
 }
 
 // Y_b = A X_b for every subdomain on the tensor cores (A = F or S slabs)
@@ -146,7 +157,7 @@ void Engine::op_F_batch(const double *w, double *Fw, const double *dotv, double 
     tc_apply(d_AF_);
     k_vt_multi<<<nsub_, 256, 0, s_>>>(K, d_subs_, d_V_, b_xb_, b_t_);
     k_gc_multi<<<cdivb((long long)ngc_total_ * K, 256), 256, 0, s_>>>(ngc_total_, K, d_gptr_, d_gidx_, b_t_, b_gc_);
-    k_coarse_multi<<<dim3(ncl_, cdivb(maxg, 8)), 256, 0, s_>>>(K, d_cl_, d_M_, b_gc_, b_s_);
+    k_coarse_multi<<<dim3(ncl_, cdivb(maxg, 64)), 256, 0, s_>>>(K, d_cl_, d_M_, b_gc_, b_s_);
     k_correct_multi<<<dim3(nsub_, cdivb(maxnb, 32)), 256, 0, s_>>>(K, d_subs_, d_cl_, d_V_, d_bcr_, b_s_, b_yb_);
     k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, nullptr, Fw, dotv, partial);
 }
@@ -165,8 +176,8 @@ void Engine::op_M_batch(const double *x, double *z) {
 void Engine::op_P_batch(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial) {
     const int K = bK_;
     k_gft_partial_multi<<<nchunks_, 256, 0, s_>>>(K, d_chunk_beg_, d_chunk_end_, d_crow_, d_cval_, x, b_gpart_);
-    k_gf_apply_multi<<<bnpart_, 256, 2 * 6 * ncl_ * K * sizeof(double), s_>>>(
-        nlam_, K, ncl_, d_cl_chunk_ptr_, b_gpart_, d_invGtG_, d_gcl_, d_gval_, x, alpha_out, Px, dotv, partial);
+    k_gf_coef_multi<<<1, 1024, 0, s_>>>(K, ncl_, d_cl_chunk_ptr_, b_gpart_, d_invGtG_, b_gt_, b_acoef_, alpha_out);
+    k_gf_apply_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, b_acoef_, d_gcl_, d_gval_, x, Px, dotv, partial);
 }
 
 void Engine::iteration_batch() {

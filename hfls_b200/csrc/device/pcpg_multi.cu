@@ -42,19 +42,47 @@ __global__ void k_gather_multi(int nslots, int K, const int *__restrict__ ptr, c
     }
 }
 
-// t[d][q][j] = sum_i V_d[i][q] x_b[i][j]; one CTA per subdomain
+// t[d][q][j] = sum_i V_d[i][q] x_b[i][j]; one CTA per subdomain, 32-row
+// chunks of V and x_b staged in shared memory so each is read once
 __global__ void k_vt_multi(int K, const SubDev *__restrict__ subs, const double *__restrict__ Vbuf,
                            const double *__restrict__ xb, double *__restrict__ t) {
+    __shared__ double Vs[128 * 32];          // ncol x 32, ncol * K <= 2048
+    __shared__ double Xs[32 * 32];           // 32 x K
     const SubDev &sd = subs[blockIdx.x];
     const int ncol = sd.c + 6;
+    const int nout = ncol * K;
     const double *V = Vbuf + sd.V_off;
     const double *x = xb + (size_t)sd.xb_off * K;
-    for (int o = threadIdx.x; o < ncol * K; o += blockDim.x) {
-        const int q = o / K, j = o % K;
-        const double *Vq = V + (size_t)q * sd.nbp;
-        double a = 0.0;
-        for (int i = 0; i < sd.nb; ++i) a += Vq[i] * x[(size_t)i * K + j];
-        t[((size_t)sd.t_off + q) * K + j] = a;
+    double acc[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc[u] = 0.0;
+    for (int i0 = 0; i0 < sd.nb; i0 += 32) {
+        for (int o = threadIdx.x; o < 32 * K; o += blockDim.x) {
+            const int ii = o / K;
+            Xs[o] = (i0 + ii < sd.nb) ? x[(size_t)(i0 + ii) * K + (o % K)] : 0.0;
+        }
+        for (int o = threadIdx.x; o < ncol * 32; o += blockDim.x) {
+            const int q = o / 32, ii = o % 32;
+            Vs[o] = (i0 + ii < sd.nb) ? V[(size_t)q * sd.nbp + i0 + ii] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int o = threadIdx.x + 256 * u;
+            if (o < nout) {
+                const int q = o / K, jj = o % K;
+                double a = acc[u];
+#pragma unroll 8
+                for (int ii = 0; ii < 32; ++ii) a += Vs[q * 32 + ii] * Xs[ii * K + jj];
+                acc[u] = a;
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int o = threadIdx.x + 256 * u;
+        if (o < nout) t[((size_t)sd.t_off + o / K) * K + (o % K)] = acc[u];
     }
 }
 
@@ -68,22 +96,27 @@ __global__ void k_gc_multi(int ngc_total, int K, const int *__restrict__ gptr, c
     gc[(size_t)q * K + j] = s;
 }
 
-// s = M gc per cluster: CTA (cluster, block of 8 rows); M read once for all K
+// s = M gc per cluster: CTA (cluster, block of 64 rows), 8 rows per warp,
+// lane = load case; M read once for all K, gc once per 8 rows
 __global__ void k_coarse_multi(int K, const ClusterDev *__restrict__ cl, const double *__restrict__ Mbuf,
                                const double *__restrict__ gc, double *__restrict__ s) {
     const ClusterDev c = cl[blockIdx.x];
-    const int r0 = blockIdx.y * 8;
-    if (r0 >= c.ngc) return;
-    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;   // warp = row
-    const int row = r0 + warp;
-    if (row >= c.ngc) return;
-    const double *M = Mbuf + c.M_off + (size_t)row * c.ngc;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int row0 = blockIdx.y * 64 + warp * 8;
+    if (row0 >= c.ngc || lane >= K) return;
+    const int nr = min(8, c.ngc - row0);
+    const double *M = Mbuf + c.M_off + (size_t)row0 * c.ngc;     // symmetric: row = column
     const double *g = gc + (size_t)c.gc_off * K;
-    // lane owns columns j = lane (K <= 32); loop p
-    double a = 0.0;
-    if (lane < K)
-        for (int p = 0; p < c.ngc; ++p) a += M[p] * g[(size_t)p * K + lane];
-    if (lane < K) s[((size_t)c.gc_off + row) * K + lane] = a;
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int p = 0; p < c.ngc; ++p) {
+        const double gp = g[(size_t)p * K + lane];
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+            if (r < nr) a[r] += M[(size_t)r * c.ngc + p] * gp;
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+        if (r < nr) s[((size_t)c.gc_off + row0 + r) * K + lane] = a[r];
 }
 
 // y_b -= V_d s_d ; CTA (subdomain, chunk of 32 rows)
@@ -111,34 +144,44 @@ __global__ void k_correct_multi(int K, const SubDev *__restrict__ subs, const Cl
     }
 }
 
-// out[r][j] = wt[r] * sum_k sign * y[slot][j]; partial dot with dotv per (block, j)
-__global__ void k_rows_multi(int nlam, int K, const int *__restrict__ rslot, const double *__restrict__ rsign,
-                             const double *__restrict__ yb, const double *__restrict__ weight,
-                             double *__restrict__ out, const double *__restrict__ dotv,
-                             double *__restrict__ partial) {
+// per-block, per-column tree sum of prod over the block's rows (256 / K rows,
+// threads j, j+K, ...) -> partial[block][j]
+__device__ __forceinline__ void block_col_partial(double prod, int K, double *__restrict__ partial) {
     __shared__ double red[256];
     const int rows_per_block = 256 / K;
     const int lr = threadIdx.x / K, j = threadIdx.x % K;
-    const int r = blockIdx.x * rows_per_block + lr;
-    double prod = 0.0;
-    if (lr < rows_per_block && r < nlam) {
-        double v = 0.0;
-        const int s0 = rslot[2 * r], s1 = rslot[2 * r + 1];
-        if (s0 >= 0) v += rsign[2 * r] * yb[(size_t)s0 * K + j];
-        if (s1 >= 0) v += rsign[2 * r + 1] * yb[(size_t)s1 * K + j];
-        if (weight) v *= weight[r];
-        out[(size_t)r * K + j] = v;
-        if (dotv) prod = v * dotv[(size_t)r * K + j];
-    }
-    if (!partial) return;
     red[threadIdx.x] = prod;
     __syncthreads();
-    // reduce over the rows of the block, per column j (threads j, j+K, ...)
-    for (int o = (rows_per_block / 2); o > 0; o >>= 1) {
+    for (int o = rows_per_block / 2; o > 0; o >>= 1) {
         if (lr < o) red[threadIdx.x] += red[threadIdx.x + o * K];
         __syncthreads();
     }
     if (lr == 0) partial[(size_t)blockIdx.x * K + j] = red[j];
+}
+
+// out[r][j] = wt[r] * sum_k sign * y[slot][j]; partial dot with dotv per
+// (block, j).  Blocks stride over groups of 256 / K rows (fixed assignment,
+// so the partials and their sums are the same on every run).
+__global__ void k_rows_multi(int nlam, int K, const int *__restrict__ rslot, const double *__restrict__ rsign,
+                             const double *__restrict__ yb, const double *__restrict__ weight,
+                             double *__restrict__ out, const double *__restrict__ dotv,
+                             double *__restrict__ partial) {
+    const int rows_per_block = 256 / K;
+    const int lr = threadIdx.x / K, j = threadIdx.x % K;
+    double prod = 0.0;
+    for (int r0 = blockIdx.x * rows_per_block; r0 < nlam; r0 += gridDim.x * rows_per_block) {
+        const int r = r0 + lr;
+        if (lr < rows_per_block && r < nlam) {
+            double v = 0.0;
+            const int s0 = rslot[2 * r], s1 = rslot[2 * r + 1];
+            if (s0 >= 0) v += rsign[2 * r] * yb[(size_t)s0 * K + j];
+            if (s1 >= 0) v += rsign[2 * r + 1] * yb[(size_t)s1 * K + j];
+            if (weight) v *= weight[r];
+            out[(size_t)r * K + j] = v;
+            if (dotv) prod += v * dotv[(size_t)r * K + j];
+        }
+    }
+    if (partial) block_col_partial(prod, K, partial);
 }
 
 // Gf^T x per chunk and column: partial[ch][q][j]
@@ -167,19 +210,12 @@ __global__ void k_gft_partial_multi(int K, const int *__restrict__ chunk_beg, co
     }
 }
 
-// Px = x - Gf a, a = invGtG * sum of the chunk partials (per column), computed by
-// every CTA; CTA 0 stores -a (alpha) when requested; dot partial with dotv.
-__global__ void k_gf_apply_multi(int nlam, int K, int ncl, const int *__restrict__ cl_chunk_ptr,
-                                 const double *__restrict__ gpart, const double *__restrict__ invGtG,
-                                 const int *__restrict__ gcl, const double *__restrict__ gval,
-                                 const double *__restrict__ x, double *__restrict__ alpha_out,
-                                 double *__restrict__ Px, const double *__restrict__ dotv,
-                                 double *__restrict__ partial) {
-    extern __shared__ double sh[];
+// a = (Gf^T Gf)^{-1} Gf^T x per column from the chunk partials; one CTA.
+// gt (m x K) is staged in global scratch; alpha_out = -a when requested.
+__global__ void k_gf_coef_multi(int K, int ncl, const int *__restrict__ cl_chunk_ptr,
+                                const double *__restrict__ gpart, const double *__restrict__ invGtG,
+                                double *__restrict__ gt, double *__restrict__ a, double *__restrict__ alpha_out) {
     const int m = 6 * ncl;
-    double *gt = sh;             // m x K
-    double *a = sh + m * K;      // m x K
-    __shared__ double red[256];
     for (int o = threadIdx.x; o < m * K; o += blockDim.x) {
         const int q = o / K, j = o % K;
         const int c = q / 6, i = q % 6;
@@ -193,33 +229,36 @@ __global__ void k_gf_apply_multi(int nlam, int K, int ncl, const int *__restrict
         double s = 0.0;
         for (int p = 0; p < m; ++p) s += invGtG[q + (size_t)p * m] * gt[p * K + j];
         a[o] = s;
-        if (blockIdx.x == 0 && alpha_out) alpha_out[o] = -s;
+        if (alpha_out) alpha_out[o] = -s;
     }
-    __syncthreads();
+}
+
+// Px = x - Gf a; partial dot with dotv per (block, j); blocks stride over
+// row groups like k_rows_multi
+__global__ void k_gf_apply_multi(int nlam, int K, const double *__restrict__ a, const int *__restrict__ gcl,
+                                 const double *__restrict__ gval, const double *__restrict__ x,
+                                 double *__restrict__ Px, const double *__restrict__ dotv,
+                                 double *__restrict__ partial) {
     const int rows_per_block = 256 / K;
     const int lr = threadIdx.x / K, j = threadIdx.x % K;
-    const int r = blockIdx.x * rows_per_block + lr;
     double prod = 0.0;
-    if (lr < rows_per_block && r < nlam) {
-        double v = 0.0;
-        for (int k = 0; k < 2; ++k) {
-            const int c = gcl[2 * r + k];
-            if (c < 0) continue;
-            const double *g = gval + 6 * (size_t)(2 * r + k);
-            for (int q = 0; q < 6; ++q) v += g[q] * a[(6 * c + q) * K + j];
+    for (int r0 = blockIdx.x * rows_per_block; r0 < nlam; r0 += gridDim.x * rows_per_block) {
+        const int r = r0 + lr;
+        if (lr < rows_per_block && r < nlam) {
+            double v = 0.0;
+            for (int k = 0; k < 2; ++k) {
+                const int c = gcl[2 * r + k];
+                if (c < 0) continue;
+                const double *g = gval + 6 * (size_t)(2 * r + k);
+#pragma unroll
+                for (int q = 0; q < 6; ++q) v += g[q] * a[(6 * c + q) * K + j];
+            }
+            const double pv = x[(size_t)r * K + j] - v;
+            Px[(size_t)r * K + j] = pv;
+            if (dotv) prod += pv * dotv[(size_t)r * K + j];
         }
-        const double pv = x[(size_t)r * K + j] - v;
-        Px[(size_t)r * K + j] = pv;
-        if (dotv) prod = pv * dotv[(size_t)r * K + j];
     }
-    if (!partial) return;
-    red[threadIdx.x] = prod;
-    __syncthreads();
-    for (int o = rows_per_block / 2; o > 0; o >>= 1) {
-        if (lr < o) red[threadIdx.x] += red[threadIdx.x + o * K];
-        __syncthreads();
-    }
-    if (lr == 0) partial[(size_t)blockIdx.x * K + j] = red[j];
+    if (partial) block_col_partial(prod, K, partial);
 }
 
 // sum of partials of column j (fixed order), one CTA per column
@@ -263,22 +302,17 @@ __global__ void k_update_lam_g_multi(int n, int K, const double *__restrict__ wF
 }
 
 // partial[blk][j] = sum over the rows of block blk of a[r][j] * b[r][j]
-// (256 / K rows per block, the row layout of k_rows_multi)
+// (row groups of 256 / K rows, strided like k_rows_multi)
 __global__ void k_dot_multi(int nlam, int K, const double *__restrict__ a, const double *__restrict__ b,
                             double *__restrict__ partial) {
-    __shared__ double red[256];
     const int rows_per_block = 256 / K;
     const int lr = threadIdx.x / K, j = threadIdx.x % K;
-    const int r = blockIdx.x * rows_per_block + lr;
     double prod = 0.0;
-    if (lr < rows_per_block && r < nlam) prod = a[(size_t)r * K + j] * b[(size_t)r * K + j];
-    red[threadIdx.x] = prod;
-    __syncthreads();
-    for (int o = (rows_per_block / 2); o > 0; o >>= 1) {
-        if (lr < o) red[threadIdx.x] += red[threadIdx.x + o * K];
-        __syncthreads();
+    for (int r0 = blockIdx.x * rows_per_block; r0 < nlam; r0 += gridDim.x * rows_per_block) {
+        const int r = r0 + lr;
+        if (lr < rows_per_block && r < nlam) prod += a[(size_t)r * K + j] * b[(size_t)r * K + j];
     }
-    if (lr == 0) partial[(size_t)blockIdx.x * K + j] = red[j];
+    block_col_partial(prod, K, partial);
 }
 
 __global__ void k_update_w_multi(int n, int K, const double *__restrict__ gPz_new, const double *__restrict__ Pz,

@@ -148,6 +148,12 @@ typedef struct htf_profile_info {
     double fapply_ms, fapply_bytes;     /* whole F apply (gather .. scatter)        */
     double iteration_ms;                /* one captured PCPG iteration              */
     int kernels_per_iteration;          /* kernel launches in one iteration graph   */
+    /* batched mixed-precision form (precision=mixed after a solve; else 0)  */
+    int batch_width;                    /* load cases per batch                     */
+    double tc_F_ms, tc_F_bytes;         /* Y_b = F_i X_b for the whole batch on the
+                                           tensor cores: FP32 slabs + X + Y bytes   */
+    double batch_iteration_ms;          /* one captured batched PCPG iteration      */
+    int kernels_per_batch_iteration;
 } htf_profile_info;
 int htf_profile(htf_ctx *ctx, int reps, htf_profile_info *info);
 
