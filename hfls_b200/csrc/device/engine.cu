@@ -1197,7 +1197,7 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
         info->batch_width = K;
         CK(cudaMemsetAsync(b_tmp_, 0, (size_t)nlam_ * K * sizeof(double), s_));
         profile_batch_gather(b_tmp_);
-        info->tc_F_ms = timeit([&] { tc_apply(d_AF_); });
+        info->tc_F_ms = timeit([&] { tc_apply(d_AF_, nullptr); });
         info->tc_F_bytes = 4.0 * aoff_ + 2.0 * 4.0 * nslots_ * K + 8.0 * nslots_ * K;
         if (bgraph_) {
             std::vector<PcpgState> st(K), saved(K);

@@ -42,7 +42,7 @@ private:
     void init_rhs(const double *f);                       // d = Bf K_HT^+ f, lambda0
     void reconstruct(const double *f, double *u_dev);     // u from lambda, alpha
     double pcpg_start(PcpgState *st);                     // g0, Pg, z, Pz; returns nothing useful
-    void tc_apply(const float *A);
+    void tc_apply(const float *A, const double *sc);
     void profile_batch_gather(const double *w);
     void op_F_batch(const double *w, double *Fw, const double *dotv, double *partial);
     void op_M_batch(const double *x, double *z);
@@ -111,7 +111,7 @@ private:
     PcpgState *b_st_ = nullptr;
     cudaGraphExec_t bgraph_ = nullptr;
     int bkernels_per_iter_ = 0;
-    int tc_smem_ = 0;
+    int tc_smem_ = 0, vt_nch_ = 1;
     long long aoff_ = 0;                       // floats per FP32 slab array
     // vectors
     double *d_f_ = nullptr, *d_full_ = nullptr, *d_full2_ = nullptr;

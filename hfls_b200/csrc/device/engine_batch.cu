@@ -19,15 +19,16 @@
 namespace htf {
 
 template <int K>
-__global__ void k_tc_gemm(const GemmBlock *, const float *, const float *, long long, double *, int *);
+__global__ void k_tc_gemm(const GemmBlock *, const float *, const float *, long long, double *, int *,
+                          const SubDev *, const ClusterDev *, const double *, const int *, const double *);
 __global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *);
-__global__ void k_gather_multi(int, int, const int *, const int *, const double *, const double *, const int *,
-                               const SubDev *, double *, float *, float *);
+__global__ void k_gather_multi(int, int, const int *, const int *, const double *, const double *, double *, float *,
+                               float *);
+template <int K>
 __global__ void k_vt_multi(int, const SubDev *, const double *, const double *, double *);
-__global__ void k_gc_multi(int, int, const int *, const int *, const double *, double *);
-__global__ void k_coarse_multi(int, const ClusterDev *, const double *, const double *, double *);
-__global__ void k_correct_multi(int, const SubDev *, const ClusterDev *, const double *, const int *,
-                                const double *, double *);
+__global__ void k_gc_multi(int, int, int, const int *, const int *, const double *, double *);
+template <int K>
+__global__ void k_coarse_multi(const ClusterDev *, const double *, const double *, double *);
 __global__ void k_rows_multi(int, int, const int *, const double *, const double *, const double *, double *,
                              const double *, double *);
 __global__ void k_gft_partial_multi(int, const int *, const int *, const int *, const double *, const double *,
@@ -97,8 +98,8 @@ int Engine::setup_batch(int K, std::string &err) {
     k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_F_, d_AF_);
     k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_S_, d_AS_);
     CKB(cudaGetLastError());
-    // 4 stages of A_hi, A_lo (16 KB each), X_hi, X_lo (k x 128 B each) + alignment slack
-    tc_smem_ = 1024 + 4 * 2 * (128 * 32 + K * 32) * 4;
+    // 5 stages of A_hi, A_lo (16 KB each), X_hi, X_lo (k x 128 B each) + alignment slack
+    tc_smem_ = 1024 + 5 * 2 * (128 * 32 + K * 32) * 4;
     if (K == 16)
         CKB(cudaFuncSetAttribute(k_tc_gemm<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_));
     else
@@ -106,14 +107,18 @@ int Engine::setup_batch(int K, std::string &err) {
     // batch vectors
     const size_t nl = (size_t)nlam_ * K;
     int ntot = 0;
-    for (auto &h : hs_) ntot = std::max(ntot, h.t_off + h.c + 6);
+    vt_nch_ = 1;
+    for (auto &h : hs_) {
+        ntot = std::max(ntot, h.t_off + h.c + 6);
+        vt_nch_ = std::max(vt_nch_, (h.nb + 127) / 128);
+    }
     // row kernels stride over row groups with a fixed grid: few partials per column
     bnpart_ = std::min(cdivb(nlam_, 256 / K), 1184);
     b_lam_ = alloc<double>(nl, err, rc); b_g_ = alloc<double>(nl, err, rc); b_w_ = alloc<double>(nl, err, rc);
     b_Fw_ = alloc<double>(nl, err, rc); b_Pg_ = alloc<double>(nl, err, rc); b_z_ = alloc<double>(nl, err, rc);
     b_Pz_ = alloc<double>(nl, err, rc); b_d_ = alloc<double>(nl, err, rc); b_tmp_ = alloc<double>(nl, err, rc);
     b_xb_ = alloc<double>((size_t)nslots_ * K, err, rc); b_yb_ = alloc<double>((size_t)nslots_ * K, err, rc);
-    b_t_ = alloc<double>((size_t)ntot * K, err, rc);
+    b_t_ = alloc<double>((size_t)ntot * vt_nch_ * K, err, rc);     // V^T x_b partials per 128-row chunk
     b_gc_ = alloc<double>((size_t)ngc_total_ * K, err, rc); b_s_ = alloc<double>((size_t)ngc_total_ * K, err, rc);
     b_part_ = alloc<double>((size_t)bnpart_ * K, err, rc);
     b_gpart_ = alloc<double>((size_t)nchunks_ * 6 * K, err, rc);
@@ -131,34 +136,39 @@ int Engine::setup_batch(int K, std::string &err) {
 // X slabs of a batch vector (for timing the tensor-core product alone)
 void Engine::profile_batch_gather(const double *w) {
     const long long xlo = (long long)nslots_ * bK_;
-    k_gather_multi<<<cdivb((long long)nslots_ * bK_, 256), 256, 0, s_>>>(nslots_, bK_, d_slot_ptr_, d_slot_ent_, w,
-                                                                          nullptr, d_slot_sub_, d_subs_, b_xb_, d_Xs_,
-                                                                          d_Xs_ + xlo);
+    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, bK_, d_slot_ptr_, d_slot_ent_, w, nullptr, b_xb_, d_Xs_,
+                                                 d_Xs_ + xlo);
 }
 
-// Y_b = A X_b for every subdomain on the tensor cores (A = F or S slabs)
-void Engine::tc_apply(const float *A) {
+// Y_b = A X_b for every subdomain on the tensor cores (A = F or S slabs);
+// with sc, also Y_b -= V s (the coarse correction of the F apply)
+void Engine::tc_apply(const float *A, const double *sc) {
     const GemmBlock *db = static_cast<const GemmBlock *>(d_blocks_);
     const long long xlo = (long long)nslots_ * bK_;
     if (bK_ == 16)
-        k_tc_gemm<16><<<nblocks_, 192, tc_smem_, s_>>>(db, A, d_Xs_, xlo, b_yb_, d_tcerr_);
+        k_tc_gemm<16><<<nblocks_, 192, tc_smem_, s_>>>(db, A, d_Xs_, xlo, b_yb_, d_tcerr_, d_subs_, d_cl_, d_V_,
+                                                       d_bcr_, sc);
     else
-        k_tc_gemm<32><<<nblocks_, 192, tc_smem_, s_>>>(db, A, d_Xs_, xlo, b_yb_, d_tcerr_);
+        k_tc_gemm<32><<<nblocks_, 192, tc_smem_, s_>>>(db, A, d_Xs_, xlo, b_yb_, d_tcerr_, d_subs_, d_cl_, d_V_,
+                                                       d_bcr_, sc);
 }
 
 void Engine::op_F_batch(const double *w, double *Fw, const double *dotv, double *partial) {
+    // F w = Bf [F_d x_b - V_d M_c V_d^T x_b]: the coarse solve first, its
+    // correction applied in the tensor-core epilogue
     const int K = bK_;
-    int maxg = 0, maxnb = 0;
+    int maxg = 0;
     for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
-    for (auto &h : hs_) maxnb = std::max(maxnb, h.nb);
     const long long xlo = (long long)nslots_ * K;
-    k_gather_multi<<<cdivb((long long)nslots_ * K, 256), 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, w, nullptr,
-                                                                        d_slot_sub_, d_subs_, b_xb_, d_Xs_, d_Xs_ + xlo);
-    tc_apply(d_AF_);
-    k_vt_multi<<<nsub_, 256, 0, s_>>>(K, d_subs_, d_V_, b_xb_, b_t_);
-    k_gc_multi<<<cdivb((long long)ngc_total_ * K, 256), 256, 0, s_>>>(ngc_total_, K, d_gptr_, d_gidx_, b_t_, b_gc_);
-    k_coarse_multi<<<dim3(ncl_, cdivb(maxg, 64)), 256, 0, s_>>>(K, d_cl_, d_M_, b_gc_, b_s_);
-    k_correct_multi<<<dim3(nsub_, cdivb(maxnb, 32)), 256, 0, s_>>>(K, d_subs_, d_cl_, d_V_, d_bcr_, b_s_, b_yb_);
+    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, w, nullptr, b_xb_, d_Xs_,
+                                                 d_Xs_ + xlo);
+    if (K == 32) k_vt_multi<32><<<dim3(nsub_, vt_nch_), 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
+    else k_vt_multi<16><<<dim3(nsub_, vt_nch_), 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
+    k_gc_multi<<<cdivb((long long)ngc_total_ * K, 256), 256, 0, s_>>>(ngc_total_, K, vt_nch_, d_gptr_, d_gidx_, b_t_,
+                                                                      b_gc_);
+    if (K == 32) k_coarse_multi<32><<<dim3(ncl_, cdivb(maxg, 32)), 128, 0, s_>>>(d_cl_, d_M_, b_gc_, b_s_);
+    else k_coarse_multi<16><<<dim3(ncl_, cdivb(maxg, 32)), 128, 0, s_>>>(d_cl_, d_M_, b_gc_, b_s_);
+    tc_apply(d_AF_, b_s_);
     k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, nullptr, Fw, dotv, partial);
 }
 
@@ -167,9 +177,9 @@ void Engine::op_M_batch(const double *x, double *z) {
     // the preconditioner must stay a fixed linear operator for the PCPG
     // recurrences, so it uses the same 3xTF32 products as F
     const long long xlo = (long long)nslots_ * K;
-    k_gather_multi<<<cdivb((long long)nslots_ * K, 256), 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, x, d_weight_,
-                                                                        d_slot_sub_, d_subs_, b_xb_, d_Xs_, d_Xs_ + xlo);
-    tc_apply(d_AS_);
+    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, x, d_weight_, b_xb_, d_Xs_,
+                                                 d_Xs_ + xlo);
+    tc_apply(d_AS_, nullptr);
     k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, d_weight_, z, nullptr, nullptr);
 }
 

@@ -10,139 +10,185 @@
 
 namespace htf {
 
-constexpr unsigned FULLM = 0xffffffffu;
-
-// x_b = Bf^T w (optionally weighted) for all K columns; also writes the FP32
-// X slabs of the tensor-core product in SWIZZLE_128B K-major layout.
+// x_b = Bf^T w (optionally weighted) for all K columns; also writes the X
+// slabs of the tensor-core product (TF32 part and TF32 remainder) in the
+// SWIZZLE_128B K-major layout.  One CTA per 32 consecutive slots (one K slab
+// of one subdomain: b offsets and padded sizes are multiples of 32); the
+// values go through shared memory so both outputs are written coalesced.
 __global__ void k_gather_multi(int nslots, int K, const int *__restrict__ ptr, const int *__restrict__ ent,
                                const double *__restrict__ w, const double *__restrict__ weight,
-                               const int *__restrict__ slot_sub, const SubDev *__restrict__ subs,
                                double *__restrict__ xb, float *__restrict__ Xs, float *__restrict__ Xlo) {
-    const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (id >= (long long)nslots * K) return;
-    const int i = int(id / K), j = int(id % K);
-    double v = 0.0;
-    for (int e = ptr[i]; e < ptr[i + 1]; ++e) {
-        const int q = ent[e];
-        const int lam = q >> 1;
-        double a = w[(size_t)lam * K + j];
-        if (weight) a *= weight[lam];
-        v += (q & 1) ? -a : a;
+    __shared__ double vs[32 * 33];
+    const int i0 = blockIdx.x * 32;
+    for (int o = threadIdx.x; o < 32 * K; o += blockDim.x) {
+        const int il = o / K, j = o % K, i = i0 + il;
+        double v = 0.0;
+        if (i < nslots)
+            for (int e = ptr[i]; e < ptr[i + 1]; ++e) {
+                const int q = ent[e];
+                const int lam = q >> 1;
+                double a = w[(size_t)lam * K + j];
+                if (weight) a *= weight[lam];
+                v += (q & 1) ? -a : a;
+            }
+        if (i < nslots) xb[(size_t)i * K + j] = v;
+        vs[il * 33 + j] = v;
     }
-    xb[(size_t)i * K + j] = v;
-    if (Xs) {
-        const SubDev &sd = subs[slot_sub[i]];
-        const int il = i - sd.xb_off, kk = il / 32, c = il % 32;
+    if (!Xs) return;
+    __syncthreads();
+    // slab row j (load case) holds the 32 slots of this chunk, 128 bytes
+    for (int o = threadIdx.x; o < 32 * K; o += blockDim.x) {
+        const int j = o / 32, c = o % 32;
+        const double v = vs[c * 33 + j];
         const uint32_t b = uint32_t(j * 128 + c * 4);
         const uint32_t bs = b ^ (((b >> 7) & 7u) << 4);
-        const size_t at = (size_t)sd.xb_off * K + (size_t)kk * K * 32 + bs / 4;
+        const size_t at = (size_t)i0 * K + bs / 4;
         const float hi = tf32_rna((float)v);
         Xs[at] = hi;
         if (Xlo) Xlo[at] = tf32_rna((float)(v - (double)hi));   // 3xTF32 remainder
     }
 }
 
-// t[d][q][j] = sum_i V_d[i][q] x_b[i][j]; one CTA per subdomain, 32-row
-// chunks of V and x_b staged in shared memory so each is read once
-__global__ void k_vt_multi(int K, const SubDev *__restrict__ subs, const double *__restrict__ Vbuf,
-                           const double *__restrict__ xb, double *__restrict__ t) {
-    __shared__ double Vs[128 * 32];          // ncol x 32, ncol * K <= 2048
-    __shared__ double Xs[32 * 32];           // 32 x K
-    const SubDev &sd = subs[blockIdx.x];
+// Partial V_d^T x_b over the 128-row chunk ch of subdomain d:
+// tpart[(t_off + q) * nch + ch][j] = sum_{i in chunk} V_d[i][q] x_b[i][j]
+// (chunks past nb write zeros).  32-row pieces of V (stored i-major in
+// shared memory) and x_b are staged; each thread keeps a QPT x (K/8)
+// register tile (q = its q group, j = jg + 8c).  CTA (subdomain, chunk).
+template <int K>
+__device__ __forceinline__ void vt_chunk(int nch, const SubDev &sd, const double *__restrict__ Vbuf,
+                                         const double *__restrict__ xb, double *__restrict__ tpart) {
+    constexpr int QPT = K == 32 ? 2 : 4, CPT = K / 8, VP = 2048 / K + 1;
+    __shared__ double Vs[32 * VP];           // [ii][q]
+    __shared__ double Xs[32 * K];            // [ii][j]
+    const int ch = blockIdx.y;
     const int ncol = sd.c + 6;
-    const int nout = ncol * K;
+    const int r_end = min(sd.nb, ch * 128 + 128);
     const double *V = Vbuf + sd.V_off;
     const double *x = xb + (size_t)sd.xb_off * K;
-    double acc[8];
+    const int jg = threadIdx.x % 8, qg = threadIdx.x / 8;
+    double acc[QPT][CPT];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) acc[u] = 0.0;
-    for (int i0 = 0; i0 < sd.nb; i0 += 32) {
+    for (int a = 0; a < QPT; ++a)
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[a][c] = 0.0;
+    for (int i0 = ch * 128; i0 < r_end; i0 += 32) {
         for (int o = threadIdx.x; o < 32 * K; o += blockDim.x) {
             const int ii = o / K;
-            Xs[o] = (i0 + ii < sd.nb) ? x[(size_t)(i0 + ii) * K + (o % K)] : 0.0;
+            Xs[o] = (i0 + ii < r_end) ? x[(size_t)(i0 + ii) * K + (o % K)] : 0.0;
         }
         for (int o = threadIdx.x; o < ncol * 32; o += blockDim.x) {
             const int q = o / 32, ii = o % 32;
-            Vs[o] = (i0 + ii < sd.nb) ? V[(size_t)q * sd.nbp + i0 + ii] : 0.0;
+            Vs[ii * VP + q] = (i0 + ii < r_end) ? V[(size_t)q * sd.nbp + i0 + ii] : 0.0;
         }
         __syncthreads();
+#pragma unroll 4
+        for (int ii = 0; ii < 32; ++ii) {
+            double v[QPT], xv[CPT];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int o = threadIdx.x + 256 * u;
-            if (o < nout) {
-                const int q = o / K, jj = o % K;
-                double a = acc[u];
-#pragma unroll 8
-                for (int ii = 0; ii < 32; ++ii) a += Vs[q * 32 + ii] * Xs[ii * K + jj];
-                acc[u] = a;
-            }
+            for (int a = 0; a < QPT; ++a) v[a] = Vs[ii * VP + qg * QPT + a];
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) xv[c] = Xs[ii * K + jg + 8 * c];
+#pragma unroll
+            for (int a = 0; a < QPT; ++a)
+#pragma unroll
+                for (int c = 0; c < CPT; ++c) acc[a][c] += v[a] * xv[c];
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-        const int o = threadIdx.x + 256 * u;
-        if (o < nout) t[((size_t)sd.t_off + o / K) * K + (o % K)] = acc[u];
+    for (int a = 0; a < QPT; ++a) {
+        const int q = qg * QPT + a;
+        if (q < ncol)
+#pragma unroll
+            for (int c = 0; c < CPT; ++c)
+                tpart[(((size_t)sd.t_off + q) * nch + ch) * K + jg + 8 * c] = acc[a][c];
     }
 }
 
-__global__ void k_gc_multi(int ngc_total, int K, const int *__restrict__ gptr, const int *__restrict__ gidx,
-                           const double *__restrict__ t, double *__restrict__ gc) {
+template <int K>
+__global__ void __launch_bounds__(256) k_vt_multi(int nch, const SubDev *__restrict__ subs,
+                                                  const double *__restrict__ Vbuf, const double *__restrict__ xb,
+                                                  double *__restrict__ tpart) {
+    vt_chunk<K>(nch, subs[blockIdx.x], Vbuf, xb, tpart);
+}
+template __global__ void k_vt_multi<16>(int, const SubDev *, const double *, const double *, double *);
+template __global__ void k_vt_multi<32>(int, const SubDev *, const double *, const double *, double *);
+
+// gc[q][j] = sum over the t entries of coarse row q and their row chunks
+__global__ void k_gc_multi(int ngc_total, int K, int nch, const int *__restrict__ gptr, const int *__restrict__ gidx,
+                           const double *__restrict__ tpart, double *__restrict__ gc) {
     const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (id >= (long long)ngc_total * K) return;
     const int q = int(id / K), j = int(id % K);
     double s = 0.0;
-    for (int e = gptr[q]; e < gptr[q + 1]; ++e) s += t[(size_t)gidx[e] * K + j];
+    for (int e = gptr[q]; e < gptr[q + 1]; ++e)
+        for (int ch = 0; ch < nch; ++ch) s += tpart[((size_t)gidx[e] * nch + ch) * K + j];
     gc[(size_t)q * K + j] = s;
 }
 
-// s = M gc per cluster: CTA (cluster, block of 64 rows), 8 rows per warp,
-// lane = load case; M read once for all K, gc once per 8 rows
-__global__ void k_coarse_multi(int K, const ClusterDev *__restrict__ cl, const double *__restrict__ Mbuf,
-                               const double *__restrict__ gc, double *__restrict__ s) {
-    const ClusterDev c = cl[blockIdx.x];
-    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const int row0 = blockIdx.y * 64 + warp * 8;
-    if (row0 >= c.ngc || lane >= K) return;
-    const int nr = min(8, c.ngc - row0);
-    const double *M = Mbuf + c.M_off + (size_t)row0 * c.ngc;     // symmetric: row = column
+// S = M G per cluster (M symmetric ngc x ngc, G = gc ngc x K): CTA
+// (cluster, 32-row block) of 128 threads, 32-column tiles of M and 32-row
+// tiles of G staged in shared memory; each thread keeps a 4-row x (K/16)
+// register tile (rows 4 rg .. 4 rg + 3, columns cg + 16 c).
+template <int K>
+__device__ __forceinline__ void coarse_tile(const ClusterDev &c, const double *__restrict__ Mbuf,
+                                            const double *__restrict__ gc, double *__restrict__ s) {
+    constexpr int CPT = K / 16;
+    __shared__ double Ms[32 * 33];
+    __shared__ double Gs[32 * K];
+    const int row0 = blockIdx.y * 32;
+    const double *M = Mbuf + c.M_off;
     const double *g = gc + (size_t)c.gc_off * K;
-    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int p = 0; p < c.ngc; ++p) {
-        const double gp = g[(size_t)p * K + lane];
+    const int cg = threadIdx.x % 16, rg = threadIdx.x / 16;
+    double acc[4][CPT];
 #pragma unroll
-        for (int r = 0; r < 8; ++r)
-            if (r < nr) a[r] += M[(size_t)r * c.ngc + p] * gp;
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int cc = 0; cc < CPT; ++cc) acc[r][cc] = 0.0;
+    for (int p0 = 0; p0 < c.ngc; p0 += 32) {
+        for (int o = threadIdx.x; o < 32 * 32; o += blockDim.x) {
+            const int r = o / 32, pp = o % 32;
+            Ms[r * 33 + pp] =
+                (row0 + r < c.ngc && p0 + pp < c.ngc) ? M[(size_t)(row0 + r) * c.ngc + p0 + pp] : 0.0;
+        }
+        for (int o = threadIdx.x; o < 32 * K; o += blockDim.x) {
+            const int pp = o / K;
+            Gs[o] = (p0 + pp < c.ngc) ? g[(size_t)(p0 + pp) * K + (o % K)] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int pp = 0; pp < 32; ++pp) {
+            double m[4], gv[CPT];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) m[r] = Ms[(4 * rg + r) * 33 + pp];
+#pragma unroll
+            for (int cc = 0; cc < CPT; ++cc) gv[cc] = Gs[pp * K + cg + 16 * cc];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int cc = 0; cc < CPT; ++cc) acc[r][cc] += m[r] * gv[cc];
+        }
+        __syncthreads();
     }
 #pragma unroll
-    for (int r = 0; r < 8; ++r)
-        if (r < nr) s[((size_t)c.gc_off + row0 + r) * K + lane] = a[r];
+    for (int r = 0; r < 4; ++r) {
+        const int row = row0 + 4 * rg + r;
+        if (row < c.ngc)
+#pragma unroll
+            for (int cc = 0; cc < CPT; ++cc) s[((size_t)c.gc_off + row) * K + cg + 16 * cc] = acc[r][cc];
+    }
 }
 
-// y_b -= V_d s_d ; CTA (subdomain, chunk of 32 rows)
-__global__ void k_correct_multi(int K, const SubDev *__restrict__ subs, const ClusterDev *__restrict__ cl,
-                                const double *__restrict__ Vbuf, const int *__restrict__ bcrows,
-                                const double *__restrict__ s, double *__restrict__ yb) {
-    __shared__ double ss[256 * 32 / 4];     // (c+6) x K <= 2048
-    const SubDev &sd = subs[blockIdx.x];
-    const ClusterDev &c = cl[sd.cluster];
-    const int nc = sd.c + 6;
-    for (int o = threadIdx.x; o < nc * K; o += blockDim.x) {
-        const int q = o / K, j = o % K;
-        const int pos = (q < sd.c) ? bcrows[sd.bcr_off + q] : sd.alpha_pos + (q - sd.c);
-        ss[o] = s[((size_t)c.gc_off + pos) * K + j];
-    }
-    __syncthreads();
-    const int i0 = blockIdx.y * 32;
-    if (i0 >= sd.nb) return;
-    for (int o = threadIdx.x; o < 32 * K; o += blockDim.x) {
-        const int i = i0 + o / K, j = o % K;
-        if (i >= sd.nb) continue;
-        double a = yb[((size_t)sd.xb_off + i) * K + j];
-        for (int q = 0; q < nc; ++q) a -= Vbuf[sd.V_off + (size_t)q * sd.nbp + i] * ss[q * K + j];
-        yb[((size_t)sd.xb_off + i) * K + j] = a;
-    }
+template <int K>
+__global__ void __launch_bounds__(128) k_coarse_multi(const ClusterDev *__restrict__ cl,
+                                                      const double *__restrict__ Mbuf, const double *__restrict__ gc,
+                                                      double *__restrict__ s) {
+    const ClusterDev c = cl[blockIdx.x];
+    if (blockIdx.y * 32 >= c.ngc) return;
+    coarse_tile<K>(c, Mbuf, gc, s);
 }
+template __global__ void k_coarse_multi<16>(const ClusterDev *, const double *, const double *, double *);
+template __global__ void k_coarse_multi<32>(const ClusterDev *, const double *, const double *, double *);
 
 // per-block, per-column tree sum of prod over the block's rows (256 / K rows,
 // threads j, j+K, ...) -> partial[block][j]

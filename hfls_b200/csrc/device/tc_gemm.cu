@@ -35,7 +35,7 @@
 
 namespace htf {
 
-constexpr int TC_STAGES = 4;
+constexpr int TC_STAGES = 5;
 constexpr int TC_SLAB_A = 128 * 32;          // floats per A slab (16 KB)
 constexpr unsigned TC_WAIT_LIMIT = 1u << 26;  // bounded spin on mbarriers
 
@@ -129,11 +129,19 @@ __device__ __forceinline__ void tmem_add(uint32_t taddr, double *acc) {
     for (int j = 0; j < N; ++j) acc[j] += (double)__uint_as_float(r[j]);
 }
 
+// With scoarse != nullptr the epilogue also applies the coarse correction of the
+// F apply, y_b -= V_d s_d (V_d = [F_d Bc_d^T, -R_d] FP64, s_d the cluster
+// coarse solution at the subdomain's Bc rows and alpha slot).
 template <int K>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__restrict__ blocks,
                                                            const float *__restrict__ A,
                                                            const float *__restrict__ Xs, long long xlo_off,
-                                                           double *__restrict__ yb, int *__restrict__ err) {
+                                                           double *__restrict__ yb, int *__restrict__ err,
+                                                           const SubDev *__restrict__ subs,
+                                                           const ClusterDev *__restrict__ cl,
+                                                           const double *__restrict__ V,
+                                                           const int *__restrict__ bcrows,
+                                                           const double *__restrict__ scoarse) {
     static_assert(K == 16 || K == 32, "N of the MMA");
     constexpr int SLAB_B = K * 32;                        // floats per X slab
     constexpr unsigned STAGE_TX = (TC_SLAB_A + 2 * SLAB_B) * 4;
@@ -261,25 +269,46 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__re
         have = __all_sync(0xffffffffu, have);            // warp-uniform before the .sync.aligned loads
         __syncwarp();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int quarter = warp & 3;                     // TMEM lanes this warp may read
+        const int row = quarter * 32 + lane;
+        double acc[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) acc[j] = 0.0;
         if (!have) {
             if (lane == 0) atomicExch(err, HTF_ETIMEDOUT);
         } else if (!abort_flag) {
-            const int quarter = warp & 3;                 // TMEM lanes this warp may read
-            const int row = quarter * 32 + lane;
             const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16);
-            double acc[K];
-#pragma unroll
-            for (int j = 0; j < K; ++j) acc[j] = 0.0;
             const int nacc = g.ks < TC_NACC ? g.ks : TC_NACC;
             for (int a = 0; a < nacc; ++a) {
                 tmem_add<K>(taddr + uint32_t(a * K), acc);
                 tmem_add<K>(taddr + uint32_t((TC_NACC + a) * K), acc);
             }
-            if (row < g.rows) {
-                double *y = yb + (g.y_row0 + row) * K;
-#pragma unroll
-                for (int j = 0; j < K; ++j) y[j] = acc[j];
+        }
+        if (scoarse) {
+            // s_d staged in the (now idle) stage buffers by the four epilogue warps
+            const SubDev &sd = subs[g.d];
+            const int gc_off = cl[sd.cluster].gc_off;
+            const int nc = sd.c + 6;
+            double *ss = reinterpret_cast<double *>(base);
+            for (int o = threadIdx.x - 64; o < nc * K; o += 128) {
+                const int q = o / K, j = o % K;
+                const int pos = q < sd.c ? bcrows[sd.bcr_off + q] : sd.alpha_pos + (q - sd.c);
+                ss[o] = scoarse[((size_t)gc_off + pos) * K + j];
             }
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (row < g.rows) {
+                const double *Vr = V + sd.V_off + 128 * g.m + row;
+                for (int q = 0; q < nc; ++q) {
+                    const double vq = Vr[(size_t)q * sd.nbp];
+#pragma unroll
+                    for (int j = 0; j < K; ++j) acc[j] -= vq * ss[q * K + j];
+                }
+            }
+        }
+        if (have && !abort_flag && row < g.rows) {
+            double *y = yb + (g.y_row0 + row) * K;
+#pragma unroll
+            for (int j = 0; j < K; ++j) y[j] = acc[j];
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -290,8 +319,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__re
     }
 }
 
-template __global__ void k_tc_gemm<16>(const GemmBlock *, const float *, const float *, long long, double *, int *);
-template __global__ void k_tc_gemm<32>(const GemmBlock *, const float *, const float *, long long, double *, int *);
+template __global__ void k_tc_gemm<16>(const GemmBlock *, const float *, const float *, long long, double *, int *,
+                                       const SubDev *, const ClusterDev *, const double *, const int *,
+                                       const double *);
+template __global__ void k_tc_gemm<32>(const GemmBlock *, const float *, const float *, long long, double *, int *,
+                                       const SubDev *, const ClusterDev *, const double *, const int *,
+                                       const double *);
 
 // Full FP32 slabs of a packed symmetric FP64 tile matrix: slab (m, kk) of
 // subdomain d holds rows [128m, 128m+128) x columns [32kk, 32kk+32) of the
