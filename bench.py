@@ -10,6 +10,12 @@ factors and F_i / S_i resident on the device):
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
+Alongside it (same mesh, body force (0, 0, -1), 32 seeded N(0,1) traction
+load cases): the batched mixed-precision form (F_i / S_i FP32 on the tensor
+cores, FP64 residual replacement) against the FP64 form on the same load
+cases, with the displacement error against an FP64 solve at eps 1e-10
+("mixed" in the JSON line; --no-mixed skips it).
+
 Under torchrun (N > 1) every rank solves its own replica of the workload on
 its own GPU (the solve has no cross-GPU exchange on one node here), timing
 is the max over ranks.  --impl reference times the reference CPU solver
@@ -39,6 +45,9 @@ SPEC = dict(clusters=(2, 2, 2), subs=(4, 4, 4), elems=(8, 8, 8), jitter=0.1, see
 WORKLOAD_ITERATIONS = 638   # PCPG iterations of the workload at 1e-8 (measured by the GPU arm)
 OPTS = {"typeBc": "cor", "preconditioner": "Dirichlet_explicit", "eps_iter": "1e-8", "max_iter": "5000"}
 REF_SAMPLE = dict(Nx=2, Ny=1, Nz=1, nx=8, ny=8, nz=8)     # subdomains of the workload's size, one cluster
+MIXED_RHS = 32
+MIXED_WORKLOAD = ("same cube, body force (0,0,-1) + 32 seeded N(0,1) tractions on x=1, solved as one batch of 32: "
+                  "F_i/S_i FP32 slabs, 3xTF32 tcgen05 products, FP64 coarse/projector/residual replacement, eps 1e-8")
 
 
 def peaks():
@@ -196,6 +205,61 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def run_mixed(hb, local, dist):
+    """Batched mixed-precision solve of MIXED_RHS load cases vs the FP64 form
+    on four of them (time per load case; displacement error against FP64 at
+    eps 1e-10).  Times are CUDA-event solve times, max over ranks."""
+    spec_kw = dict(SPEC, body_force=(0.0, 0.0, -1.0))
+    spec = hb.mesh_spec(material=hb.HTF_MAT_LOGUNIFORM, bc=hb.HTF_BC_CLAMP_X0, **spec_kw)
+    mesh = hb.generate_mesh(spec)
+    f = hb.traction(spec, seed=3, n_rhs=MIXED_RHS)
+    pick = [0, MIXED_RHS // 3, 2 * MIXED_RHS // 3, MIXED_RHS - 1]
+    s = hb.Solver(dict(OPTS, device=str(local), precision="mixed", batch="32"))
+    s.set_mesh(mesh)
+    s.setup()
+    u = np.zeros((MIXED_RHS, 3 * mesh.n_nodes))
+    s.solve(f, u=u)                                     # warm-up (graph capture, caches)
+    barrier(dist)
+    t = time.perf_counter()
+    _, st = s.solve(f, u=u)
+    wall = time.perf_counter() - t
+    mixed_ms = max_over_ranks(dist, st.solve_ms)
+    wall = max_over_ranks(dist, wall)
+    its = list(st.iterations[:MIXED_RHS])
+    prof = s.profile(reps=10)
+    del s
+    s64 = hb.Solver(dict(OPTS, device=str(local)))
+    s64.set_mesh(mesh)
+    s64.setup()
+    u64, st64 = s64.solve(f[pick])
+    fp64_ms = max_over_ranks(dist, st64.solve_ms) / len(pick)
+    its64 = list(st64.iterations[:len(pick)])
+    del s64
+    sref = hb.Solver(dict(OPTS, device=str(local), eps_iter="1e-10", max_iter="10000"))
+    sref.set_mesh(mesh)
+    sref.setup()
+    uref, _ = sref.solve(f[pick])
+    del sref
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    peak, peak_kind = peaks()
+    tc_gbs = prof.tc_F_bytes / (prof.tc_F_ms * 1e-3) / 1e9
+    return {
+        "workload": MIXED_WORKLOAD, "load_cases": MIXED_RHS, "batch": 32,
+        "solve_s_per_load_case": mixed_ms / 1e3 / MIXED_RHS,
+        "fp64_solve_s_per_load_case": fp64_ms / 1e3,
+        "speedup_vs_fp64": fp64_ms / (mixed_ms / MIXED_RHS),
+        "e2e_s_per_load_case": wall / MIXED_RHS,
+        "iterations_median": int(statistics.median(its)), "iterations_max": int(max(its)),
+        "fp64_iterations": its64,
+        "u_rel_err_max": max(rel(u[k], uref[i]) for i, k in enumerate(pick)),
+        "fp64_u_rel_err_max": max(rel(u64[i], uref[i]) for i in range(len(pick))),
+        "u_err_reference": "FP64 GPU solve at eps 1e-10 of load cases %s" % pick,
+        "batch_iteration_ms": prof.batch_iteration_ms,
+        "tc_F": {"kernel": "k_tc_gemm<32> (F_i FP32 slabs x 32 load cases)", "ms": prof.tc_F_ms,
+                 "bytes": prof.tc_F_bytes, "gbs": tc_gbs, "frac": tc_gbs / peak, "peak_kind": peak_kind},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -203,6 +267,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision multi-load-case measurement")
     ap.add_argument("--workload", default="full", choices=["full", "small"],
                     help="small: one cluster of 2x4x4 subdomains of 8^3 (F_i + S_i 0.3 GB > L2), "
                          "for ncu captures only")
@@ -243,7 +308,12 @@ def main():
     ms = max_over_ranks(dist, statistics.mean(solve_ms))
     e2e = max_over_ranks(dist, statistics.mean(e2e_s))
     prof = s.profile(reps=20)
+    del s
+    # every rank solves its mixed-precision replica too (collective max inside)
+    mixed = None if args.no_mixed or args.workload != "full" else run_mixed(hb, local, dist)
     if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
         return 0
     peak, peak_kind = peaks()
     achieved = prof.symv_F_bytes / (prof.symv_F_ms * 1e-3) / 1e9
@@ -274,6 +344,7 @@ def main():
                      "launch_ms": prof.symv_F_ms},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
+        "mixed": mixed,
     }
     print(json.dumps(line))
     if dist is not None:
