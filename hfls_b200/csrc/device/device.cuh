@@ -26,6 +26,9 @@ __device__ __forceinline__ float tf32_rna(float a) {
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(a));
     return __uint_as_float(r);
 }
+// the TF32 value a tensor-core product uses for an FP32 operand (low 13
+// mantissa bits dropped)
+__device__ __forceinline__ float tf32_trunc(float a) { return __uint_as_float(__float_as_uint(a) & 0xFFFFE000u); }
 #endif
 
 constexpr int TILE = 32;                  // packed tile edge

@@ -16,16 +16,19 @@
 //
 // One CTA of 6 warps per (subdomain, 128-row block):
 //   * warp 0, one thread: bulk-copy producer (A slab, X_hi, X_lo per stage);
-//   * warps 2-5: split every landed A slab in place into A_hi = rna_tf32(A)
-//     and A_lo = rna_tf32(A - A_hi), then hand the stage to the MMA issuer;
+//   * warps 2-5: form A_lo = rna_tf32(A - trunc_tf32(A)) of every landed A
+//     slab (the MMA reads the FP32 slab itself as A_hi: a TF32 operand's
+//     low 13 mantissa bits do not take part in the product), then hand the
+//     stage to the MMA issuer;
 //     at the end they read the accumulators out of TMEM (warp w owns TMEM
 //     lanes 32 (w mod 4) .. +31) and write y in FP64;
 //   * warp 1, one thread: issues the MMAs (M=128, N=k, K=8 per instruction,
 //     4 per slab).
-// Accumulation: K slab kk goes to main accumulator kk mod 4 and its two
-// small correction products to correction accumulator kk mod 4, so every
-// FP32 accumulator in TMEM sums a quarter of the K range; the eight are added
-// in FP64 in the epilogue.  Every mbarrier wait is bounded; on time-out the
+// Products per K step of 8: A_hi [X_hi | X_lo] as one N = 2k MMA (A_hi read
+// from shared memory once) and A_lo X_hi.  Accumulation: K slab kk goes to
+// accumulator group kk mod 4 (hi-hi, hi-lo and lo-hi columns), so every FP32
+// accumulator in TMEM sums a quarter of the K range; the groups are added in
+// FP64 in the epilogue.  Every mbarrier wait is bounded; on time-out the
 // CTA records HTF_ETIMEDOUT in err and stops issuing work.
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -145,9 +148,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__re
     static_assert(K == 16 || K == 32, "N of the MMA");
     constexpr int SLAB_B = K * 32;                        // floats per X slab
     constexpr unsigned STAGE_TX = (TC_SLAB_A + 2 * SLAB_B) * 4;
-    constexpr uint32_t TMEM_COLS = 2 * TC_NACC * K;       // 128 or 256
+    constexpr int GW = 3 * K;                              // TMEM columns per accumulator group
+    constexpr uint32_t TMEM_COLS = K == 32 ? 512 : 256;   // power of two >= TC_NACC * GW
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // 1024-byte aligned stage buffers: stage s holds A_hi, A_lo, then X_hi, X_lo
+    // 1024-byte aligned stage buffers: stage s holds A (FP32), A_lo, then X_hi, X_lo
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     float *sA = reinterpret_cast<float *>(base);                          // TC_STAGES x 2 x 16 KB
@@ -204,7 +208,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__re
         }
     } else if (warp == 1) {
         if (lane == 0) {                                  // MMA issuer
-            const uint32_t idesc = tf32_idesc(128, K);
+            const uint32_t idesc = tf32_idesc(128, K), idesc2 = tf32_idesc(128, 2 * K);
             for (int kk = 0; kk < g.ks; ++kk) {
                 const int s = kk % TC_STAGES;
                 if (abort_flag || !mbar_wait(&split[s], (kk / TC_STAGES) & 1)) {
@@ -213,18 +217,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__re
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const int a = kk % TC_NACC;
-                const uint32_t dmain = tmem + uint32_t(a * K), dcorr = tmem + uint32_t((TC_NACC + a) * K);
+                const uint32_t d = tmem + uint32_t((kk % TC_NACC) * GW);   // [hi-hi | hi-lo | lo-hi]
                 const uint64_t da = sw128_desc(sA + s * 2 * TC_SLAB_A);
                 const uint64_t dal = sw128_desc(sA + (s * 2 + 1) * TC_SLAB_A);
-                const uint64_t db = sw128_desc(sB + s * 2 * SLAB_B);
-                const uint64_t dbl = sw128_desc(sB + (s * 2 + 1) * SLAB_B);
+                const uint64_t db = sw128_desc(sB + s * 2 * SLAB_B);      // X_hi, X_lo: 2k rows
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {              // 4 x K=8 (32 bytes) per slab
                     const uint32_t acc = (kk >= TC_NACC || q > 0) ? 1u : 0u;
-                    mma_tf32(dmain, da + 2ull * q, db + 2ull * q, idesc, acc);
-                    mma_tf32(dcorr, da + 2ull * q, dbl + 2ull * q, idesc, acc);
-                    mma_tf32(dcorr, dal + 2ull * q, db + 2ull * q, idesc, 1u);
+                    mma_tf32(d, da + 2ull * q, db + 2ull * q, idesc2, acc);
+                    mma_tf32(d + 2 * K, dal + 2ull * q, db + 2ull * q, idesc, acc);
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&empty[s]))
@@ -246,17 +247,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__re
                 abort_flag = 1;
                 break;
             }
-            float4 *hi = reinterpret_cast<float4 *>(sA + s * 2 * TC_SLAB_A);
+            const float4 *a4 = reinterpret_cast<const float4 *>(sA + s * 2 * TC_SLAB_A);
             float4 *lo = reinterpret_cast<float4 *>(sA + (s * 2 + 1) * TC_SLAB_A);
 #pragma unroll
             for (int i = t; i < TC_SLAB_A / 4; i += 128) {
-                const float4 v = hi[i];
-                float4 h, l;
-                h.x = tf32_rna(v.x); l.x = tf32_rna(v.x - h.x);
-                h.y = tf32_rna(v.y); l.y = tf32_rna(v.y - h.y);
-                h.z = tf32_rna(v.z); l.z = tf32_rna(v.z - h.z);
-                h.w = tf32_rna(v.w); l.w = tf32_rna(v.w - h.w);
-                hi[i] = h;
+                const float4 v = a4[i];
+                float4 l;
+                l.x = tf32_rna(v.x - tf32_trunc(v.x));
+                l.y = tf32_rna(v.y - tf32_trunc(v.y));
+                l.z = tf32_rna(v.z - tf32_trunc(v.z));
+                l.w = tf32_rna(v.w - tf32_trunc(v.w));
                 lo[i] = l;
             }
             // generic-proxy writes become visible to the tensor core's async proxy
@@ -280,8 +280,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__re
             const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16);
             const int nacc = g.ks < TC_NACC ? g.ks : TC_NACC;
             for (int a = 0; a < nacc; ++a) {
-                tmem_add<K>(taddr + uint32_t(a * K), acc);
-                tmem_add<K>(taddr + uint32_t((TC_NACC + a) * K), acc);
+                tmem_add<K>(taddr + uint32_t(a * GW), acc);
+                tmem_add<K>(taddr + uint32_t(a * GW + K), acc);
+                tmem_add<K>(taddr + uint32_t(a * GW + 2 * K), acc);
             }
         }
         if (scoarse) {
