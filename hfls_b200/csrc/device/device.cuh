@@ -32,6 +32,7 @@ __device__ __forceinline__ float tf32_trunc(float a) { return __uint_as_float(__
 #endif
 
 constexpr int TILE = 32;                  // packed tile edge
+constexpr int TC_STAGES = 2;              // pipeline stages of the tensor-core product (2 CTAs per SM)
 constexpr int TILE_ELEMS = TILE * TILE;
 
 struct SubDev {

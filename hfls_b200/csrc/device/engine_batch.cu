@@ -98,8 +98,8 @@ int Engine::setup_batch(int K, std::string &err) {
     k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_F_, d_AF_);
     k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_S_, d_AS_);
     CKB(cudaGetLastError());
-    // 5 stages of A_hi, A_lo (16 KB each), X_hi, X_lo (k x 128 B each) + alignment slack
-    tc_smem_ = 1024 + 5 * 2 * (128 * 32 + K * 32) * 4;
+    // TC_STAGES stages of A, A_lo (16 KB each), X_hi, X_lo (k x 128 B each) + alignment slack
+    tc_smem_ = 1024 + TC_STAGES * 2 * (128 * 32 + K * 32) * 4;
     if (K == 16)
         CKB(cudaFuncSetAttribute(k_tc_gemm<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_));
     else

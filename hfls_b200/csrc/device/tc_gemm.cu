@@ -26,8 +26,8 @@
 //     4 per slab).
 // Products per K step of 8: A_hi [X_hi | X_lo] as one N = 2k MMA (A_hi read
 // from shared memory once) and A_lo X_hi.  Accumulation: K slab kk goes to
-// accumulator group kk mod 4 (hi-hi, hi-lo and lo-hi columns), so every FP32
-// accumulator in TMEM sums a quarter of the K range; the groups are added in
+// accumulator group kk mod 2 (hi-hi, hi-lo and lo-hi columns), so every FP32
+// accumulator in TMEM sums half of the K range; the groups are added in
 // FP64 in the epilogue.  Every mbarrier wait is bounded; on time-out the
 // CTA records HTF_ETIMEDOUT in err and stops issuing work.
 #include <cuda_runtime.h>
@@ -38,7 +38,6 @@
 
 namespace htf {
 
-constexpr int TC_STAGES = 5;
 constexpr int TC_SLAB_A = 128 * 32;          // floats per A slab (16 KB)
 constexpr unsigned TC_WAIT_LIMIT = 1u << 26;  // bounded spin on mbarriers
 
@@ -90,7 +89,7 @@ __device__ __forceinline__ uint32_t tf32_idesc(int M, int N) {
            | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);   // A, B K-major
 }
 
-constexpr int TC_NACC = 4;                   // rotating accumulators (main and correction each)
+constexpr int TC_NACC = 2;                   // rotating accumulator groups
 constexpr int TC_THREADS = 192;
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
@@ -136,7 +135,7 @@ __device__ __forceinline__ void tmem_add(uint32_t taddr, double *acc) {
 // F apply, y_b -= V_d s_d (V_d = [F_d Bc_d^T, -R_d] FP64, s_d the cluster
 // coarse solution at the subdomain's Bc rows and alpha slot).
 template <int K>
-__global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__restrict__ blocks,
+__global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__restrict__ blocks,
                                                            const float *__restrict__ A,
                                                            const float *__restrict__ Xs, long long xlo_off,
                                                            double *__restrict__ yb, int *__restrict__ err,
@@ -149,7 +148,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__re
     constexpr int SLAB_B = K * 32;                        // floats per X slab
     constexpr unsigned STAGE_TX = (TC_SLAB_A + 2 * SLAB_B) * 4;
     constexpr int GW = 3 * K;                              // TMEM columns per accumulator group
-    constexpr uint32_t TMEM_COLS = K == 32 ? 512 : 256;   // power of two >= TC_NACC * GW
+    constexpr uint32_t TMEM_COLS = K == 32 ? 256 : 128;   // power of two >= TC_NACC * GW
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte aligned stage buffers: stage s holds A (FP32), A_lo, then X_hi, X_lo
     unsigned char *base = reinterpret_cast<unsigned char *>(
