@@ -33,7 +33,8 @@ __global__ void k_rows_multi(int, int, const int *, const double *, const double
                              const double *, double *);
 __global__ void k_gft_partial_multi(int, const int *, const int *, const int *, const double *, const double *,
                                     double *);
-__global__ void k_gf_coef_multi(int, int, const int *, const double *, const double *, double *, double *, double *);
+__global__ void k_gt_sum_multi(int, const int *, const double *, double *);
+__global__ void k_gf_coef_multi(int, int, const double *, const double *, double *, double *);
 __global__ void k_gf_apply_multi(int, int, const double *, const int *, const double *, const double *, double *,
                                  const double *, double *);
 __global__ void k_colsum(const double *, int, int, double *);
@@ -177,7 +178,7 @@ void Engine::op_M_batch(const double *x, double *z) {
     // the preconditioner must stay a fixed linear operator for the PCPG
     // recurrences, so it uses the same 3xTF32 products as F
     const long long xlo = (long long)nslots_ * K;
-    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, x, d_weight_, b_xb_, d_Xs_,
+    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, x, d_weight_, nullptr, d_Xs_,
                                                  d_Xs_ + xlo);
     tc_apply(d_AS_, nullptr);
     k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, d_weight_, z, nullptr, nullptr);
@@ -186,7 +187,8 @@ void Engine::op_M_batch(const double *x, double *z) {
 void Engine::op_P_batch(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial) {
     const int K = bK_;
     k_gft_partial_multi<<<nchunks_, 256, 0, s_>>>(K, d_chunk_beg_, d_chunk_end_, d_crow_, d_cval_, x, b_gpart_);
-    k_gf_coef_multi<<<1, 1024, 0, s_>>>(K, ncl_, d_cl_chunk_ptr_, b_gpart_, d_invGtG_, b_gt_, b_acoef_, alpha_out);
+    k_gt_sum_multi<<<ncl_, 6 * K, 0, s_>>>(K, d_cl_chunk_ptr_, b_gpart_, b_gt_);
+    k_gf_coef_multi<<<1, 1024, 0, s_>>>(K, ncl_, d_invGtG_, b_gt_, b_acoef_, alpha_out);
     k_gf_apply_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, b_acoef_, d_gcl_, d_gval_, x, Px, dotv, partial);
 }
 

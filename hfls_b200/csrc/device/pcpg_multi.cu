@@ -10,7 +10,8 @@
 
 namespace htf {
 
-// x_b = Bf^T w (optionally weighted) for all K columns; also writes the X
+// x_b = Bf^T w (optionally weighted; x_b itself only when xb != nullptr) for
+// all K columns; also writes the X
 // slabs of the tensor-core product (TF32 part and TF32 remainder) in the
 // SWIZZLE_128B K-major layout.  One CTA per 32 consecutive slots (one K slab
 // of one subdomain: b offsets and padded sizes are multiples of 32); the
@@ -31,7 +32,7 @@ __global__ void k_gather_multi(int nslots, int K, const int *__restrict__ ptr, c
                 if (weight) a *= weight[lam];
                 v += (q & 1) ? -a : a;
             }
-        if (i < nslots) xb[(size_t)i * K + j] = v;
+        if (xb && i < nslots) xb[(size_t)i * K + j] = v;
         vs[il * 33 + j] = v;
     }
     if (!Xs) return;
@@ -58,6 +59,7 @@ template <int K>
 __device__ __forceinline__ void vt_chunk(int nch, const SubDev &sd, const double *__restrict__ Vbuf,
                                          const double *__restrict__ xb, double *__restrict__ tpart) {
     constexpr int QPT = K == 32 ? 2 : 4, CPT = K / 8, VP = 2048 / K + 1;
+    constexpr int UX = 32 * K / 256, UV = 2048 / K * 32 / 256;   // staged values per thread
     __shared__ double Vs[32 * VP];           // [ii][q]
     __shared__ double Xs[32 * K];            // [ii][j]
     const int ch = blockIdx.y;
@@ -71,16 +73,30 @@ __device__ __forceinline__ void vt_chunk(int nch, const SubDev &sd, const double
     for (int a = 0; a < QPT; ++a)
 #pragma unroll
         for (int c = 0; c < CPT; ++c) acc[a][c] = 0.0;
-    for (int i0 = ch * 128; i0 < r_end; i0 += 32) {
-        for (int o = threadIdx.x; o < 32 * K; o += blockDim.x) {
-            const int ii = o / K;
-            Xs[o] = (i0 + ii < r_end) ? x[(size_t)(i0 + ii) * K + (o % K)] : 0.0;
+    double xr[UX], vr[UV];
+    auto fetch = [&](int i0) {
+#pragma unroll
+        for (int u = 0; u < UX; ++u) {
+            const int o = threadIdx.x + 256 * u, ii = o / K;
+            xr[u] = (i0 + ii < r_end) ? x[(size_t)(i0 + ii) * K + (o % K)] : 0.0;
         }
-        for (int o = threadIdx.x; o < ncol * 32; o += blockDim.x) {
-            const int q = o / 32, ii = o % 32;
-            Vs[ii * VP + q] = (i0 + ii < r_end) ? V[(size_t)q * sd.nbp + i0 + ii] : 0.0;
+#pragma unroll
+        for (int u = 0; u < UV; ++u) {
+            const int o = threadIdx.x + 256 * u, q = o / 32, ii = o % 32;
+            vr[u] = (q < ncol && i0 + ii < r_end) ? V[(size_t)q * sd.nbp + i0 + ii] : 0.0;
+        }
+    };
+    if (ch * 128 < r_end) fetch(ch * 128);
+    for (int i0 = ch * 128; i0 < r_end; i0 += 32) {
+#pragma unroll
+        for (int u = 0; u < UX; ++u) Xs[threadIdx.x + 256 * u] = xr[u];
+#pragma unroll
+        for (int u = 0; u < UV; ++u) {
+            const int o = threadIdx.x + 256 * u;
+            Vs[(o % 32) * VP + o / 32] = vr[u];
         }
         __syncthreads();
+        if (i0 + 32 < r_end) fetch(i0 + 32);        // next piece in flight during the FMAs
 #pragma unroll 4
         for (int ii = 0; ii < 32; ++ii) {
             double v[QPT], xv[CPT];
@@ -133,7 +149,7 @@ __global__ void k_gc_multi(int ngc_total, int K, int nch, const int *__restrict_
 template <int K>
 __device__ __forceinline__ void coarse_tile(const ClusterDev &c, const double *__restrict__ Mbuf,
                                             const double *__restrict__ gc, double *__restrict__ s) {
-    constexpr int CPT = K / 16;
+    constexpr int CPT = K / 16, UG = 32 * K / 128;
     __shared__ double Ms[32 * 33];
     __shared__ double Gs[32 * K];
     const int row0 = blockIdx.y * 32;
@@ -145,17 +161,30 @@ __device__ __forceinline__ void coarse_tile(const ClusterDev &c, const double *_
     for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int cc = 0; cc < CPT; ++cc) acc[r][cc] = 0.0;
+    double mr[8], gr[UG];
+    auto fetch = [&](int p0) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int o = threadIdx.x + 128 * u, r = o / 32, pp = o % 32;
+            mr[u] = (row0 + r < c.ngc && p0 + pp < c.ngc) ? M[(size_t)(row0 + r) * c.ngc + p0 + pp] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < UG; ++u) {
+            const int o = threadIdx.x + 128 * u, pp = o / K;
+            gr[u] = (p0 + pp < c.ngc) ? g[(size_t)(p0 + pp) * K + (o % K)] : 0.0;
+        }
+    };
+    fetch(0);
     for (int p0 = 0; p0 < c.ngc; p0 += 32) {
-        for (int o = threadIdx.x; o < 32 * 32; o += blockDim.x) {
-            const int r = o / 32, pp = o % 32;
-            Ms[r * 33 + pp] =
-                (row0 + r < c.ngc && p0 + pp < c.ngc) ? M[(size_t)(row0 + r) * c.ngc + p0 + pp] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int o = threadIdx.x + 128 * u;
+            Ms[(o / 32) * 33 + o % 32] = mr[u];
         }
-        for (int o = threadIdx.x; o < 32 * K; o += blockDim.x) {
-            const int pp = o / K;
-            Gs[o] = (p0 + pp < c.ngc) ? g[(size_t)(p0 + pp) * K + (o % K)] : 0.0;
-        }
+#pragma unroll
+        for (int u = 0; u < UG; ++u) Gs[threadIdx.x + 128 * u] = gr[u];
         __syncthreads();
+        if (p0 + 32 < c.ngc) fetch(p0 + 32);          // next tile in flight during the FMAs
 #pragma unroll 4
         for (int pp = 0; pp < 32; ++pp) {
             double m[4], gv[CPT];
@@ -230,46 +259,73 @@ __global__ void k_rows_multi(int nlam, int K, const int *__restrict__ rslot, con
     if (partial) block_col_partial(prod, K, partial);
 }
 
-// Gf^T x per chunk and column: partial[ch][q][j]
-__global__ void k_gft_partial_multi(int K, const int *__restrict__ chunk_beg, const int *__restrict__ chunk_end,
-                                    const int *__restrict__ crow, const double *__restrict__ cval,
-                                    const double *__restrict__ x, double *__restrict__ partial) {
-    __shared__ double red[256];
+// Gf^T x per chunk and column: partial[ch][q][j].  Thread (lr, j) walks
+// every (256/K)-th entry of the chunk, four entries per step so the row-index
+// and x loads of consecutive entries are in flight together; the 6 sums are
+// then reduced over lr in one pass through shared memory.
+__global__ void __launch_bounds__(256) k_gft_partial_multi(int K, const int *__restrict__ chunk_beg,
+                                                           const int *__restrict__ chunk_end,
+                                                           const int *__restrict__ crow,
+                                                           const double *__restrict__ cval,
+                                                           const double *__restrict__ x,
+                                                           double *__restrict__ partial) {
+    __shared__ double red[6 * 256];
     const int ch = blockIdx.x;
-    const int j = threadIdx.x % K, lane_rows = 256 / K, lr = threadIdx.x / K;
+    const int j = threadIdx.x % K, nl = 256 / K, lr = threadIdx.x / K;
+    const int beg = chunk_beg[ch], end = chunk_end[ch];
     double s[6] = {0, 0, 0, 0, 0, 0};
-    if (lr < lane_rows)
-        for (int e = chunk_beg[ch] + lr; e < chunk_end[ch]; e += lane_rows) {
-            const double xv = x[(size_t)crow[e] * K + j];
+    int e = beg + lr;
+    for (; e + 3 * nl < end; e += 4 * nl) {
+        int r[4];
+        double xv[4];
 #pragma unroll
-            for (int q = 0; q < 6; ++q) s[q] += cval[6 * (size_t)e + q] * xv;
+        for (int u = 0; u < 4; ++u) r[u] = crow[e + u * nl];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) xv[u] = x[(size_t)r[u] * K + j];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const double *cv = cval + 6 * (size_t)(e + u * nl);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) s[q] += cv[q] * xv[u];
         }
-    for (int q = 0; q < 6; ++q) {
-        red[threadIdx.x] = (lr < lane_rows) ? s[q] : 0.0;
+    }
+    for (; e < end; e += nl) {
+        const double xv = x[(size_t)crow[e] * K + j];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) s[q] += cval[6 * (size_t)e + q] * xv;
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) red[q * 256 + threadIdx.x] = s[q];
+    __syncthreads();
+    for (int o = nl / 2; o > 0; o >>= 1) {
+        if (lr < o)
+#pragma unroll
+            for (int q = 0; q < 6; ++q) red[q * 256 + threadIdx.x] += red[q * 256 + threadIdx.x + o * K];
         __syncthreads();
-        for (int o = lane_rows / 2; o > 0; o >>= 1) {
-            if (lr < o) red[threadIdx.x] += red[threadIdx.x + o * K];
-            __syncthreads();
-        }
-        if (lr == 0) partial[((size_t)ch * 6 + q) * K + j] = red[j];
-        __syncthreads();
+    }
+    if (lr == 0)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) partial[((size_t)ch * 6 + q) * K + j] = red[q * 256 + j];
+}
+
+// gt[c][i][j] = sum of the chunk partials of cluster c (fixed order); CTA per
+// cluster, thread (i, j)
+__global__ void k_gt_sum_multi(int K, const int *__restrict__ cl_chunk_ptr, const double *__restrict__ gpart,
+                               double *__restrict__ gt) {
+    const int c = blockIdx.x;
+    for (int o = threadIdx.x; o < 6 * K; o += blockDim.x) {
+        const int i = o / K, j = o % K;
+        double s = 0.0;
+        for (int chk = cl_chunk_ptr[c]; chk < cl_chunk_ptr[c + 1]; ++chk) s += gpart[((size_t)chk * 6 + i) * K + j];
+        gt[((size_t)c * 6 + i) * K + j] = s;
     }
 }
 
-// a = (Gf^T Gf)^{-1} Gf^T x per column from the chunk partials; one CTA.
-// gt (m x K) is staged in global scratch; alpha_out = -a when requested.
-__global__ void k_gf_coef_multi(int K, int ncl, const int *__restrict__ cl_chunk_ptr,
-                                const double *__restrict__ gpart, const double *__restrict__ invGtG,
-                                double *__restrict__ gt, double *__restrict__ a, double *__restrict__ alpha_out) {
+// a = (Gf^T Gf)^{-1} gt per column (gt = Gf^T x from k_gt_sum_multi); one
+// CTA; alpha_out = -a when requested.
+__global__ void k_gf_coef_multi(int K, int ncl, const double *__restrict__ invGtG, const double *__restrict__ gt,
+                                double *__restrict__ a, double *__restrict__ alpha_out) {
     const int m = 6 * ncl;
-    for (int o = threadIdx.x; o < m * K; o += blockDim.x) {
-        const int q = o / K, j = o % K;
-        const int c = q / 6, i = q % 6;
-        double s = 0.0;
-        for (int ch = cl_chunk_ptr[c]; ch < cl_chunk_ptr[c + 1]; ++ch) s += gpart[((size_t)ch * 6 + i) * K + j];
-        gt[o] = s;
-    }
-    __syncthreads();
     for (int o = threadIdx.x; o < m * K; o += blockDim.x) {
         const int q = o / K, j = o % K;
         double s = 0.0;
