@@ -19,6 +19,9 @@ HTF_BC_ROLLERS, HTF_BC_CLAMP_X0 = 0, 1
 HTF_MAT_CONST, HTF_MAT_CHECKER, HTF_MAT_LOGUNIFORM = 0, 1, 2
 ERRORS = {0: "HTF_OK", -1: "HTF_EINVAL", -2: "HTF_ENOMEM", -3: "HTF_ECUDA", -4: "HTF_ENOTSPD",
           -5: "HTF_EBREAKDOWN", -6: "HTF_ENOCONV", -7: "HTF_ESTATE", -8: "HTF_ETIMEDOUT", -9: "HTF_ENODEV"}
+for _c, _n in ERRORS.items():
+    globals()[_n] = _c
+
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -49,6 +52,15 @@ class ProfileInfo(ctypes.Structure):
                 ("batch_iteration_ms", ctypes.c_double), ("kernels_per_batch_iteration", ctypes.c_int)]
 
 
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("rc", ctypes.c_int), ("n_rhs", ctypes.c_int),
+                ("iterations_max", ctypes.c_int), ("t_submit_ms", ctypes.c_double), ("t_admit_ms", ctypes.c_double),
+                ("t_start_ms", ctypes.c_double), ("t_done_ms", ctypes.c_double), ("setup_ms", ctypes.c_double),
+                ("solve_ms", ctypes.c_double), ("bytes", ctypes.c_double), ("bytes_estimate", ctypes.c_double)]
+
+
+HTF_REQ_QUEUED, HTF_REQ_SETUP, HTF_REQ_RUNNING, HTF_REQ_DONE, HTF_REQ_FAILED = range(5)
+
 _SIGS = {
     "htf_mesh_sizes": [ctypes.POINTER(MeshSpec)] + [_ip] * 6,
     "htf_mesh_fill": [ctypes.POINTER(MeshSpec), _dp, _ip, _ip, _ip, _dp, _dp, _ip, _ip],
@@ -69,6 +81,12 @@ _SIGS = {
     "htf_dual_layout": [ctypes.c_void_p, _ip, _ip, _dp, _dp],
     "htf_fix_dofs": [ctypes.c_void_p, _ip],
     "htf_projection_noalloc": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    "htf_server_create": [ctypes.c_char_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "htf_server_destroy": [ctypes.c_void_p],
+    "htf_server_submit": [ctypes.c_void_p, ctypes.POINTER(MeshSpec), ctypes.c_int, _dp, _dp,
+                          ctypes.POINTER(ctypes.c_longlong)],
+    "htf_server_wait": [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.POINTER(RequestInfo)],
+    "htf_server_info": [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(RequestInfo)],
 }
 HTF_NOALLOC_SCRATCH_DOUBLES = 1048576
 for _name, _args in _SIGS.items():
@@ -77,6 +95,8 @@ for _name, _args in _SIGS.items():
     _f.restype = ctypes.c_int
 lib.htf_last_error.argtypes = [ctypes.c_void_p]
 lib.htf_last_error.restype = ctypes.c_char_p
+lib.htf_server_error.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
+lib.htf_server_error.restype = ctypes.c_char_p
 
 
 class HTFError(RuntimeError):
@@ -272,3 +292,62 @@ class Solver:
 
     def preconditioning(self, x):
         return self._op(lib.htf_preconditioning, x, "htf_preconditioning")
+
+
+class Server:
+    """Continuous-batching solve server (htf_server_*): requests of different
+    meshes and load cases are admitted by device footprint and advance
+    together in the batched mixed-precision form.
+
+    submit() copies the loads and returns a ticket; the displacements land in
+    an array owned by this object, returned by wait(ticket)."""
+
+    def __init__(self, options=None, hbm_budget_bytes=0.0, max_live=8):
+        opts = ";".join(f"{k}={v}" for k, v in (options or {}).items())
+        h = ctypes.c_void_p()
+        rc = lib.htf_server_create(opts.encode(), float(hbm_budget_bytes), int(max_live), ctypes.byref(h))
+        if rc:
+            raise HTFError(rc, "htf_server_create")
+        self._h = h
+        self._out = {}
+
+    def submit(self, spec, f_nodal=None, n_rhs=None):
+        if f_nodal is not None:
+            f = np.ascontiguousarray(np.atleast_2d(f_nodal), dtype=np.float64)
+            n_rhs = f.shape[0]
+        else:
+            f, n_rhs = None, n_rhs or 1
+        n = [ctypes.c_int() for _ in range(6)]
+        lib.htf_mesh_sizes(ctypes.byref(spec), *[ctypes.byref(v) for v in n])
+        u = np.zeros((n_rhs, 3 * n[0].value))
+        t = ctypes.c_longlong()
+        rc = lib.htf_server_submit(self._h, ctypes.byref(spec), n_rhs, _d(f) if f is not None else None, _d(u),
+                                   ctypes.byref(t))
+        if rc:
+            raise HTFError(rc, "htf_server_submit: " + lib.htf_server_error(self._h, 0).decode())
+        self._out[t.value] = (u, spec)          # keep u (written by the server) and the spec alive
+        return t.value
+
+    def info(self, ticket):
+        i = RequestInfo()
+        rc = lib.htf_server_info(self._h, ticket, ctypes.byref(i))
+        if rc:
+            raise HTFError(rc, "htf_server_info")
+        return i
+
+    def wait(self, ticket, timeout_ms=-1.0):
+        """Displacements (n_rhs, 3*n_nodes) and the RequestInfo; raises on a failed request."""
+        i = RequestInfo()
+        rc = lib.htf_server_wait(self._h, ticket, float(timeout_ms), ctypes.byref(i))
+        if rc:
+            raise HTFError(rc, "request %d: %s" % (ticket, lib.htf_server_error(self._h, ticket).decode()))
+        return self._out[ticket][0], i
+
+    def close(self):
+        """Lets every submitted request finish, then stops the server."""
+        if getattr(self, "_h", None):
+            lib.htf_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

@@ -23,7 +23,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 CU_SOURCES = ["device/setup_kernels.cu", "device/pcpg_kernels.cu", "device/engine.cu", "device/noalloc.cu",
               "device/tc_gemm.cu", "device/pcpg_multi.cu", "device/engine_batch.cu"]
-CPP_SOURCES = ["host/mesh.cpp", "host/problem.cpp", "capi.cpp"]
+CPP_SOURCES = ["host/mesh.cpp", "host/problem.cpp", "capi.cpp", "server.cpp"]
 HEADERS = ["device/device.cuh", "device/engine.hpp", "host/problem.hpp"]
 
 INC = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]

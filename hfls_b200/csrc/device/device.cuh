@@ -76,14 +76,31 @@ struct SymvUnit {
 
 // One CTA of the tensor-core multi-RHS product: 128-row block m of
 // subdomain d (slabs (m, 0..ks-1) contiguous at a_off, X slabs at x_off).
+// `set` names the TcSet (problem) the block belongs to: one launch can cover
+// the blocks of several problems.
 struct GemmBlock {
-    int d;
-    int m;
-    long long a_off;
-    int ks;
-    int rows;
-    long long x_off;
-    long long y_row0;
+    int d;                                // subdomain within its problem
+    int m;                                // 128-row block index
+    long long a_off;                      // first slab (floats) in the set's A arrays
+    int ks;                               // K slabs (32 columns each)
+    int rows;                             // valid rows of the block
+    long long x_off;                      // first X slab (floats)
+    long long y_row0;                     // first output row (b-space slot)
+    int set;
+    int pad;
+};
+
+// Operands of the tensor-core products of one problem.
+struct TcSet {
+    const float *AF, *AS;                 // FP32 slabs of F_i and S_i
+    const float *Xs;                      // X_hi slabs; X_lo slabs at Xs + xlo
+    long long xlo;
+    double *yb;                           // b-space output, RHS-interleaved
+    const SubDev *subs;
+    const ClusterDev *cl;
+    const double *V;                      // coarse-correction columns
+    const int *bcr;                       // Bc row ids per subdomain
+    const double *sc;                     // coarse solution of the F product
 };
 
 // One 32-column step of the batched Cholesky for one subdomain.

@@ -186,9 +186,20 @@ __global__ void k_copy(long long n, const double *__restrict__ a, double *__rest
 
 // ---------------------------------------------------------------------------
 Engine::~Engine() {
+    if (own_s_) cudaStreamSynchronize(own_s_);
+    if (s_ && s_ != own_s_) cudaStreamSynchronize(s_);
     if (graph_) cudaGraphExecDestroy(graph_);
+    if (bgraph_) cudaGraphExecDestroy(bgraph_);
+    if (run_e0_) cudaEventDestroy(run_e0_);
+    if (run_e1_) cudaEventDestroy(run_e1_);
     for (auto &b : bufs_) cudaFree(b.p);
-    if (s_) cudaStreamDestroy(s_);
+    if (own_s_) cudaStreamDestroy(own_s_);
+}
+
+size_t Engine::device_bytes() const {
+    size_t t = 0;
+    for (auto &b : bufs_) t += b.bytes;
+    return t;
 }
 
 int Engine::check(cudaError_t e, const char *what, std::string &err) {
@@ -844,7 +855,8 @@ int Engine::setup(Problem &p, std::string &err) {
         return HTF_ENODEV;
     }
     CK(cudaSetDevice(opt_.device));
-    CK(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&own_s_, cudaStreamNonBlocking));
+    s_ = own_s_;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1196,9 +1208,13 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
         const int K = bK_;
         info->batch_width = K;
         CK(cudaMemsetAsync(b_tmp_, 0, (size_t)nlam_ * K * sizeof(double), s_));
+        CK(cudaMemsetAsync(b_s_, 0, (size_t)ngc_total_ * K * sizeof(double), s_));
         profile_batch_gather(b_tmp_);
-        info->tc_F_ms = timeit([&] { tc_apply(d_AF_, nullptr); });
-        info->tc_F_bytes = 4.0 * aoff_ + 2.0 * 4.0 * nslots_ * K + 8.0 * nslots_ * K;
+        info->tc_F_ms = timeit([&] { tc_apply(0); });
+        // FP32 slabs, X_hi + X_lo, Y, and the V columns of the epilogue's correction
+        double vbytes = 0.0;
+        for (auto &h : hs_) vbytes += 8.0 * h.nbp * (h.c + 6);
+        info->tc_F_bytes = 4.0 * aoff_ + 2.0 * 4.0 * nslots_ * K + 8.0 * nslots_ * K + vbytes;
         if (bgraph_) {
             std::vector<PcpgState> st(K), saved(K);
             for (auto &x : st) {

@@ -14,6 +14,20 @@ namespace htf {
 // static scratch of the allocation-free entry point (noalloc.cu)
 int noalloc_scratch(double **ptr, size_t *cap, std::string &err);
 
+// tensor-core product over blocks of one or more problems (engine_batch.cu)
+int tc_launch(int K, const GemmBlock *blocks, int nblocks, const TcSet *sets, int which, int smem, int *err,
+              cudaStream_t s);
+int tc_smem_bytes(int K);
+
+// host-side state of one chunk of load cases in the batched form
+struct BatchRun {
+    int r0 = 0, kc = 0;
+    std::vector<PcpgState> st;
+    std::vector<double> last;      // g'Pz at the last FP64 residual
+    std::vector<double> rel;       // last FP64 sqrt(g'Pz)/norm0
+    std::vector<int> conv;         // 0 running, 1 converged, 2 max_iter
+};
+
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
@@ -32,6 +46,25 @@ public:
     int solve_batch(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err);
     int apply_batch(int op, const double *x, double *y, int nrhs, std::string &err);
     bool batch_ready() const { return bK_ > 0; }
+    // steps of a batched solve, for callers that interleave several problems
+    int batch_loads(int nrhs, const double *f_nodal, std::string &err);
+    int batch_begin(int r0, int kc, std::string &err);
+    int batch_check(bool &all_done, std::string &err);
+    int batch_finish(htf_stats *stats, double &ms, std::string &err);
+    int batch_graph(std::string &err);
+    void iter_a();                                  // before the F product
+    void iter_b();                                  // between the F and S products
+    void iter_c();                                  // after the S product
+    TcSet tc_set() const;
+    const std::vector<GemmBlock> &tc_blocks() const { return hblocks_; }
+    int batch_width() const { return bK_; }
+    int *tc_err() const { return d_tcerr_; }
+    int n_dof() const { return ndof_; }
+    const double *u_dev() const { return d_u_; }
+    size_t device_bytes() const;
+    // stream of every later launch (the engine's own one by default)
+    void set_stream(cudaStream_t s) { s_ = s ? s : own_s_; }
+    cudaStream_t stream() const { return s_; }
     int device() const { return opt_.device; }
     int apply(int op, const double *x, double *y, int nrhs, std::string &err);   // 0=F, 1=P, 2=M
     double setup_ms = 0.0;
@@ -42,7 +75,12 @@ private:
     void init_rhs(const double *f);                       // d = Bf K_HT^+ f, lambda0
     void reconstruct(const double *f, double *u_dev);     // u from lambda, alpha
     double pcpg_start(PcpgState *st);                     // g0, Pg, z, Pz; returns nothing useful
-    void tc_apply(const float *A, const double *sc);
+    void tc_apply(int which);
+    void f_pre(const double *w);
+    void f_post(double *Fw, const double *dotv, double *partial);
+    void m_pre(const double *x);
+    void m_post(double *z);
+    int fp64_residual(int j, bool reset_w, std::string &err);
     void profile_batch_gather(const double *w);
     void op_F_batch(const double *w, double *Fw, const double *dotv, double *partial);
     void op_M_batch(const double *x, double *z);
@@ -64,7 +102,7 @@ private:
     int ensure_rhs(int nrhs, std::string &err);
 
     Options opt_;
-    cudaStream_t s_ = nullptr;
+    cudaStream_t s_ = nullptr, own_s_ = nullptr;
     std::vector<DevBuf> bufs_;
     int nsub_ = 0, ncl_ = 0, nlam_ = 0, nslots_ = 0, nfull_ = 0, ngc_total_ = 0, nt_total_ = 0;
     long long ntiles_ = 0;
@@ -103,6 +141,10 @@ private:
     int bK_ = 0, nblocks_ = 0, bnpart_ = 0, bnpartP_ = 0;
     float *d_AF_ = nullptr, *d_AS_ = nullptr, *d_Xs_ = nullptr;
     void *d_blocks_ = nullptr;
+    TcSet *d_tcset_ = nullptr;
+    std::vector<GemmBlock> hblocks_;
+    BatchRun run_;
+    cudaEvent_t run_e0_ = nullptr, run_e1_ = nullptr;
     int *d_slot_sub_ = nullptr, *d_tcerr_ = nullptr;
     double *b_lam_ = nullptr, *b_g_ = nullptr, *b_w_ = nullptr, *b_Fw_ = nullptr, *b_Pg_ = nullptr, *b_z_ = nullptr,
            *b_Pz_ = nullptr, *b_d_ = nullptr, *b_xb_ = nullptr, *b_yb_ = nullptr, *b_t_ = nullptr, *b_gc_ = nullptr,

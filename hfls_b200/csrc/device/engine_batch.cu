@@ -1,13 +1,19 @@
 // Batched mixed-precision PCPG (K load cases at once).
 //
 // F_i and S_i are applied as full FP32 matrices on the tensor cores
-// (tc_gemm.cu, TF32 products, FP32 accumulation); everything else — gather,
-// coarse problem, projector, recurrences — stays FP64.  Accuracy comes from
-// an outer FP64 loop: the true residual g = F lambda - d is evaluated with
-// the FP64 F_i (one load case at a time), and the inner mixed-precision
-// PCPG is restarted from it until the reference's stopping rule
-// sqrt(g'Pz) < eps * sqrt(g0'Pz0) (Cluster.cpp:1424-1426) holds for the
-// FP64 residual.
+// (tc_gemm.cu, 3xTF32 products, FP32 accumulation in TMEM); gather, coarse
+// problem, projector and recurrences stay FP64.  Each load case follows
+// Cluster::pcpg (Cluster.cpp:1363-1458) with reliable updates: its residual
+// is replaced by the FP64 one g = F lambda - d (FP64 F_i, one load case at a
+// time) whenever its recursive g'Pz has dropped 100x or it looks converged,
+// and convergence is declared only on the FP64 residual with the reference's
+// rule sqrt(g'Pz) < eps * sqrt(g0'Pz0) (Cluster.cpp:1424-1426).
+//
+// A solve is batch_loads -> per chunk of K load cases batch_begin, then
+// {check_every iterations; batch_check} until done, batch_finish.  One
+// iteration is iter_a | F product | iter_b | S product | iter_c, so a
+// server can run the phases of several problems around one tensor-core
+// launch over all their blocks.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -19,8 +25,7 @@
 namespace htf {
 
 template <int K>
-__global__ void k_tc_gemm(const GemmBlock *, const float *, const float *, long long, double *, int *,
-                          const SubDev *, const ClusterDev *, const double *, const int *, const double *);
+__global__ void k_tc_gemm(const GemmBlock *, const TcSet *, int, int *);
 __global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *);
 __global__ void k_gather_multi(int, int, const int *, const int *, const double *, const double *, double *, float *,
                                float *);
@@ -72,7 +77,7 @@ int Engine::setup_batch(int K, std::string &err) {
         const int mb = (h.nbp + 127) / 128, ks = h.nbp / 32;
         for (int m = 0; m < mb; ++m) {
             GemmBlock g{d, m, aoff + (long long)m * ks * 4096, ks, std::min(128, h.nb - 128 * m),
-                        (long long)h.xb_off * K, (long long)h.xb_off + 128 * m};
+                        (long long)h.xb_off * K, (long long)h.xb_off + 128 * m, 0, 0};
             blocks.push_back(g);
         }
         aoff += (long long)mb * ks * 4096;
@@ -85,6 +90,8 @@ int Engine::setup_batch(int K, std::string &err) {
     aoff_ = aoff;
     d_slot_sub_ = alloc<int>(nslots_, err, rc);
     d_tcerr_ = alloc<int>(1, err, rc);
+    d_tcset_ = alloc<TcSet>(1, err, rc);
+    hblocks_ = blocks;
     if (rc) return rc;
     std::vector<int> ss(nslots_);
     for (int d = 0; d < nsub_; ++d)
@@ -100,7 +107,7 @@ int Engine::setup_batch(int K, std::string &err) {
     k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_S_, d_AS_);
     CKB(cudaGetLastError());
     // TC_STAGES stages of A, A_lo (16 KB each), X_hi, X_lo (k x 128 B each) + alignment slack
-    tc_smem_ = 1024 + TC_STAGES * 2 * (128 * 32 + K * 32) * 4;
+    tc_smem_ = tc_smem_bytes(K);
     if (K == 16)
         CKB(cudaFuncSetAttribute(k_tc_gemm<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_));
     else
@@ -129,9 +136,15 @@ int Engine::setup_batch(int K, std::string &err) {
     b_alpha_ = alloc<double>((size_t)6 * ncl_ * K, err, rc);
     b_st_ = alloc<PcpgState>(K, err, rc);
     if (rc) return rc;
-    CKB(cudaStreamSynchronize(s_));
     bK_ = K;
+    const TcSet ts = tc_set();
+    CKB(cudaMemcpyAsync(d_tcset_, &ts, sizeof(TcSet), cudaMemcpyHostToDevice, s_));
+    CKB(cudaStreamSynchronize(s_));
     return HTF_OK;
+}
+
+TcSet Engine::tc_set() const {
+    return TcSet{d_AF_, d_AS_, d_Xs_, (long long)nslots_ * bK_, b_yb_, d_subs_, d_cl_, d_V_, d_bcr_, b_s_};
 }
 
 // X slabs of a batch vector (for timing the tensor-core product alone)
@@ -141,22 +154,25 @@ void Engine::profile_batch_gather(const double *w) {
                                                  d_Xs_ + xlo);
 }
 
-// Y_b = A X_b for every subdomain on the tensor cores (A = F or S slabs);
-// with sc, also Y_b -= V s (the coarse correction of the F apply)
-void Engine::tc_apply(const float *A, const double *sc) {
-    const GemmBlock *db = static_cast<const GemmBlock *>(d_blocks_);
-    const long long xlo = (long long)nslots_ * bK_;
-    if (bK_ == 16)
-        k_tc_gemm<16><<<nblocks_, 192, tc_smem_, s_>>>(db, A, d_Xs_, xlo, b_yb_, d_tcerr_, d_subs_, d_cl_, d_V_,
-                                                       d_bcr_, sc);
-    else
-        k_tc_gemm<32><<<nblocks_, 192, tc_smem_, s_>>>(db, A, d_Xs_, xlo, b_yb_, d_tcerr_, d_subs_, d_cl_, d_V_,
-                                                       d_bcr_, sc);
+// one tensor-core launch over the given blocks / operand sets (which: 0 = F
+// with coarse correction, 1 = S)
+int tc_launch(int K, const GemmBlock *blocks, int nblocks, const TcSet *sets, int which, int smem, int *err,
+              cudaStream_t s) {
+    if (nblocks <= 0) return 0;
+    if (K == 16) k_tc_gemm<16><<<nblocks, 192, smem, s>>>(blocks, sets, which, err);
+    else k_tc_gemm<32><<<nblocks, 192, smem, s>>>(blocks, sets, which, err);
+    return 0;
 }
 
-void Engine::op_F_batch(const double *w, double *Fw, const double *dotv, double *partial) {
-    // F w = Bf [F_d x_b - V_d M_c V_d^T x_b]: the coarse solve first, its
-    // correction applied in the tensor-core epilogue
+int tc_smem_bytes(int K) { return 1024 + TC_STAGES * 2 * (128 * 32 + K * 32) * 4; }
+
+void Engine::tc_apply(int which) {
+    tc_launch(bK_, static_cast<const GemmBlock *>(d_blocks_), nblocks_, d_tcset_, which, tc_smem_, d_tcerr_, s_);
+}
+
+// F w = Bf [F_d x_b - V_d M_c V_d^T x_b]: the coarse solve before the
+// tensor-core product, whose epilogue applies the correction
+void Engine::f_pre(const double *w) {
     const int K = bK_;
     int maxg = 0;
     for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
@@ -169,19 +185,34 @@ void Engine::op_F_batch(const double *w, double *Fw, const double *dotv, double 
                                                                       b_gc_);
     if (K == 32) k_coarse_multi<32><<<dim3(ncl_, cdivb(maxg, 32)), 128, 0, s_>>>(d_cl_, d_M_, b_gc_, b_s_);
     else k_coarse_multi<16><<<dim3(ncl_, cdivb(maxg, 32)), 128, 0, s_>>>(d_cl_, d_M_, b_gc_, b_s_);
-    tc_apply(d_AF_, b_s_);
-    k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, nullptr, Fw, dotv, partial);
+}
+
+void Engine::f_post(double *Fw, const double *dotv, double *partial) {
+    k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, bK_, d_rslot_, d_rsign_, b_yb_, nullptr, Fw, dotv, partial);
+}
+
+// the preconditioner must stay a fixed linear operator for the PCPG
+// recurrences, so it uses the same 3xTF32 products as F
+void Engine::m_pre(const double *x) {
+    const long long xlo = (long long)nslots_ * bK_;
+    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, bK_, d_slot_ptr_, d_slot_ent_, x, d_weight_, nullptr, d_Xs_,
+                                                 d_Xs_ + xlo);
+}
+
+void Engine::m_post(double *z) {
+    k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, bK_, d_rslot_, d_rsign_, b_yb_, d_weight_, z, nullptr, nullptr);
+}
+
+void Engine::op_F_batch(const double *w, double *Fw, const double *dotv, double *partial) {
+    f_pre(w);
+    tc_apply(0);
+    f_post(Fw, dotv, partial);
 }
 
 void Engine::op_M_batch(const double *x, double *z) {
-    const int K = bK_;
-    // the preconditioner must stay a fixed linear operator for the PCPG
-    // recurrences, so it uses the same 3xTF32 products as F
-    const long long xlo = (long long)nslots_ * K;
-    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, x, d_weight_, nullptr, d_Xs_,
-                                                 d_Xs_ + xlo);
-    tc_apply(d_AS_, nullptr);
-    k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, d_weight_, z, nullptr, nullptr);
+    m_pre(x);
+    tc_apply(1);
+    m_post(z);
 }
 
 void Engine::op_P_batch(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial) {
@@ -192,20 +223,37 @@ void Engine::op_P_batch(const double *x, double *Px, double *alpha_out, const do
     k_gf_apply_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, b_acoef_, d_gcl_, d_gval_, x, Px, dotv, partial);
 }
 
-void Engine::iteration_batch() {
+// one batched iteration = iter_a | F product | iter_b | S product | iter_c
+void Engine::iter_a() { f_pre(b_w_); }
+
+void Engine::iter_b() {
     const int K = bK_;
     const int nk = cdivb((long long)nlam_ * K, 256);
-    op_F_batch(b_w_, b_Fw_, b_w_, b_part_);
+    f_post(b_Fw_, b_w_, b_part_);
     k_colsum<<<K, 256, 0, s_>>>(b_part_, bnpart_, K, b_wFw_);
     k_dot_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, b_g_, b_w_, b_part_);
     k_colsum<<<K, 256, 0, s_>>>(b_part_, bnpart_, K, b_gw_);
     k_update_lam_g_multi<<<nk, 256, 0, s_>>>(nlam_, K, b_wFw_, b_gw_, b_w_, b_Fw_, b_lam_, b_g_, b_st_);
     op_P_batch(b_g_, b_Pg_, nullptr, nullptr, nullptr);
-    op_M_batch(b_Pg_, b_z_);
+    m_pre(b_Pg_);
+}
+
+void Engine::iter_c() {
+    const int K = bK_;
+    const int nk = cdivb((long long)nlam_ * K, 256);
+    m_post(b_z_);
     op_P_batch(b_z_, b_Pz_, nullptr, b_g_, b_part_);
     k_colsum<<<K, 256, 0, s_>>>(b_part_, bnpart_, K, b_gPz_);
     k_update_w_multi<<<nk, 256, 0, s_>>>(nlam_, K, b_gPz_, b_Pz_, b_w_, b_st_);
     k_finish_multi<<<1, 32, 0, s_>>>(K, b_wFw_, b_gPz_, b_st_);
+}
+
+void Engine::iteration_batch() {
+    iter_a();
+    tc_apply(0);
+    iter_b();
+    tc_apply(1);
+    iter_c();
 }
 
 int Engine::apply_batch(int op, const double *x, double *y, int nrhs, std::string &err) {
@@ -229,149 +277,184 @@ int Engine::apply_batch(int op, const double *x, double *y, int nrhs, std::strin
     return HTF_OK;
 }
 
-int Engine::solve_batch(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err) {
-    (void)p;
-    const int K = bK_;
+// ---------------------------------------------------------------------------
+// load cases of a solve: f for nrhs columns on the device
+int Engine::batch_loads(int nrhs, const double *f_nodal, std::string &err) {
     int rc = ensure_rhs(nrhs, err);
     if (rc) return rc;
-    launches_ = 1;
     if (f_nodal)
         CKB(cudaMemcpyAsync(d_fn_, f_nodal, (size_t)ndof_ * nrhs * sizeof(double), cudaMemcpyHostToDevice, s_));
     k_build_f<<<cdivb(nfull_, 256), 256, 0, s_>>>(nfull_, ndof_, nrhs, d_fbody_, d_own_, f_nodal ? d_fn_ : nullptr,
                                                   d_f_);
-    std::vector<int> stats_it_(K, 0);
-    if (!bgraph_) {
-        cudaGraph_t g;
-        CKB(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-        iteration_batch();
-        CKB(cudaStreamEndCapture(s_, &g));
-        size_t nn = 0;
-        CKB(cudaGraphGetNodes(g, nullptr, &nn));
-        bkernels_per_iter_ = int(nn);
-        CKB(cudaGraphInstantiate(&bgraph_, g, 0));
-        cudaGraphDestroy(g);
+    CKB(cudaGetLastError());
+    return HTF_OK;
+}
+
+// FP64 residual of load case j of the running chunk (Cluster.cpp:1398-1412
+// from the current lambda): g, Pz, g'Pz; replaces the batch residual column,
+// and the search direction too when reset_w
+int Engine::fp64_residual(int j, bool reset_w, std::string &err) {
+    BatchRun &r = run_;
+    const int K = bK_;
+    k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_lam_, d_lam_);
+    k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_d_, d_d_);
+    pcpg_start(d_st_);
+    launches_ += 2 + 15;
+    PcpgState h;
+    CKB(cudaMemcpyAsync(&h, d_st_, sizeof(PcpgState), cudaMemcpyDeviceToHost, s_));
+    CKB(cudaMemcpyAsync(b_alpha_ + (size_t)j * 6 * ncl_, d_alpha_, 6 * ncl_ * sizeof(double),
+                        cudaMemcpyDeviceToDevice, s_));
+    CKB(cudaStreamSynchronize(s_));
+    k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_g_, b_g_);
+    launches_ += 1;
+    if (reset_w) {
+        k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_Pz_, b_w_);
+        launches_ += 1;
     }
-    cudaEvent_t e0, e1;
-    CKB(cudaEventCreate(&e0));
-    CKB(cudaEventCreate(&e1));
+    PcpgState &st = r.st[j];
+    st.gPz = h.gPz;
+    st.gPz_prev = h.gPz;
+    r.last[j] = h.gPz;
+    if (st.norm0 == 0.0) st.norm0 = std::sqrt(h.gPz);
+    const double cur = std::sqrt(h.gPz);
+    r.rel[j] = st.norm0 > 0 ? cur / st.norm0 : 0.0;
+    if (opt_.verbose)
+        std::fprintf(stderr, "[htf mixed] rhs %d it %d FP64 sqrt(gPz)/norm0 = %.3e\n", r.r0 + j, st.it, r.rel[j]);
+    if (!(h.gPz > 0.0) || !std::isfinite(h.gPz) || cur < opt_.eps_iter * st.norm0) {
+        r.conv[j] = 1;
+        st.done = 1;
+    } else {
+        st.done = 0;
+    }
+    return HTF_OK;
+}
+
+int Engine::batch_begin(int r0, int kc, std::string &err) {
+    const int K = bK_;
+    if (kc < 1 || kc > K) { err = "bad load-case chunk"; return HTF_EINVAL; }
+    if (!run_e0_) {
+        CKB(cudaEventCreate(&run_e0_));
+        CKB(cudaEventCreate(&run_e1_));
+    }
+    BatchRun &r = run_;
+    r.r0 = r0;
+    r.kc = kc;
+    r.st.assign(K, PcpgState{});
+    r.last.assign(K, 0.0);
+    r.rel.assign(K, 0.0);
+    r.conv.assign(K, 0);
+    CKB(cudaMemsetAsync(b_lam_, 0, (size_t)nlam_ * K * sizeof(double), s_));
+    CKB(cudaMemsetAsync(b_d_, 0, (size_t)nlam_ * K * sizeof(double), s_));
+    CKB(cudaMemsetAsync(d_tcerr_, 0, sizeof(int), s_));
+    for (int j = 0; j < kc; ++j) {
+        init_rhs(d_f_ + (size_t)(r0 + j) * nfull_);
+        k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_d_, b_d_);
+        k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_lam_, b_lam_);
+        launches_ += 27;
+    }
+    CKB(cudaEventRecord(run_e0_, s_));
+    for (int j = 0; j < K; ++j) r.st[j].done = 1;
+    int rc;
+    for (int j = 0; j < kc; ++j) {
+        r.st[j].eps = opt_.eps_iter;
+        r.st[j].max_iter = opt_.max_iter;
+        r.st[j].wFw = 1.0;
+        if ((rc = fp64_residual(j, true, err))) return rc;
+    }
+    for (int j = kc; j < K; ++j) r.conv[j] = 1;
+    CKB(cudaMemcpyAsync(b_st_, r.st.data(), K * sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
+    return HTF_OK;
+}
+
+// after some iterations: FP64 residuals where due; all_done when every load
+// case has converged (or hit max_iter)
+int Engine::batch_check(bool &all_done, std::string &err) {
+    BatchRun &r = run_;
+    const int K = bK_;
+    const double ru2 = 1e-2;
+    CKB(cudaMemcpyAsync(r.st.data(), b_st_, K * sizeof(PcpgState), cudaMemcpyDeviceToHost, s_));
+    CKB(cudaStreamSynchronize(s_));
+    int tcerr = 0;
+    CKB(cudaMemcpy(&tcerr, d_tcerr_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (tcerr) { err = "tensor-core product timed out on a barrier"; return tcerr; }
+    bool changed = false;
+    int rc;
+    for (int j = 0; j < K; ++j) {
+        if (r.conv[j]) continue;
+        const bool broke = r.st[j].done == 2;
+        if (r.st[j].it >= opt_.max_iter) { r.conv[j] = 2; continue; }
+        if (r.st[j].done != 0 || r.st[j].gPz < ru2 * r.last[j]) {
+            r.st[j].eps = opt_.eps_iter;
+            if ((rc = fp64_residual(j, broke, err))) return rc;
+            changed = true;
+        }
+    }
+    if (changed) CKB(cudaMemcpyAsync(b_st_, r.st.data(), K * sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
+    all_done = true;
+    for (int j = 0; j < K; ++j) all_done &= r.conv[j] != 0;
+    return HTF_OK;
+}
+
+// displacements of the chunk's load cases into d_u_; per-load-case stats
+int Engine::batch_finish(htf_stats *stats, double &ms, std::string &err) {
+    BatchRun &r = run_;
+    const int K = bK_;
+    CKB(cudaEventRecord(run_e1_, s_));
+    CKB(cudaEventSynchronize(run_e1_));
+    float fms = 0.f;
+    cudaEventElapsedTime(&fms, run_e0_, run_e1_);
+    ms = fms;
+    for (int j = 0; j < r.kc; ++j) {
+        k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_lam_, d_lam_);
+        CKB(cudaMemcpyAsync(d_alpha_, b_alpha_ + (size_t)j * 6 * ncl_, 6 * ncl_ * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s_));
+        reconstruct(d_f_ + (size_t)(r.r0 + j) * nfull_, d_u_ + (size_t)(r.r0 + j) * ndof_);
+        launches_ += 1 + 13;
+        if (stats && r.r0 + j < 64) {
+            stats->iterations[r.r0 + j] = r.st[j].it;
+            stats->norm_gPz0[r.r0 + j] = r.st[j].norm0 * r.st[j].norm0;
+            stats->final_rel[r.r0 + j] = r.rel[j];
+        }
+    }
+    CKB(cudaGetLastError());
+    for (int j = 0; j < r.kc; ++j)
+        if (r.conv[j] == 2) { err = "PCPG did not converge within max_iter"; return HTF_ENOCONV; }
+    return HTF_OK;
+}
+
+int Engine::batch_graph(std::string &err) {
+    if (bgraph_) return HTF_OK;
+    cudaGraph_t g;
+    CKB(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+    iteration_batch();
+    CKB(cudaStreamEndCapture(s_, &g));
+    size_t nn = 0;
+    CKB(cudaGraphGetNodes(g, nullptr, &nn));
+    bkernels_per_iter_ = int(nn);
+    CKB(cudaGraphInstantiate(&bgraph_, g, 0));
+    cudaGraphDestroy(g);
+    return HTF_OK;
+}
+
+int Engine::solve_batch(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err) {
+    (void)p;
+    const int K = bK_;
+    launches_ = 1;
+    int rc = batch_loads(nrhs, f_nodal, err);
+    if (!rc) rc = batch_graph(err);
+    if (rc) return rc;
     double total_ms = 0.0;
-    const double inner_rel = 1e-4;
     for (int r0 = 0; r0 < nrhs; r0 += K) {
-        const int kc = std::min(K, nrhs - r0);
-        // start of every load case in FP64 (x, d, lambda0)
-        CKB(cudaMemsetAsync(b_lam_, 0, (size_t)nlam_ * K * sizeof(double), s_));
-        CKB(cudaMemsetAsync(b_d_, 0, (size_t)nlam_ * K * sizeof(double), s_));
-        for (int j = 0; j < kc; ++j) {
-            init_rhs(d_f_ + (size_t)(r0 + j) * nfull_);
-            k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_d_, b_d_);
-            k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_lam_, b_lam_);
-            launches_ += 27;
-        }
-        CKB(cudaEventRecord(e0, s_));
-        // FP64 start of every load case: g0, Pz0, norm0 (Cluster.cpp:1398-1412)
-        std::vector<PcpgState> st(K);
-        std::vector<double> last(K, 0.0);          // g'Pz at the last FP64 residual
-        std::vector<int> conv(K, 0);
-        for (int j = 0; j < K; ++j) {
-            st[j] = PcpgState{};
-            st[j].done = 1;
-        }
-        auto fp64_residual = [&](int j, bool reset_w) -> int {
-            k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_lam_, d_lam_);
-            k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_d_, d_d_);
-            pcpg_start(d_st_);
-            launches_ += 2 + 15;
-            PcpgState h;
-            CKB(cudaMemcpyAsync(&h, d_st_, sizeof(PcpgState), cudaMemcpyDeviceToHost, s_));
-            CKB(cudaMemcpyAsync(b_alpha_ + (size_t)j * 6 * ncl_, d_alpha_, 6 * ncl_ * sizeof(double),
-                                cudaMemcpyDeviceToDevice, s_));
-            CKB(cudaStreamSynchronize(s_));
-            k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_g_, b_g_);
-            launches_ += 1;
-            if (reset_w) {
-                k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_Pz_, b_w_);
-                launches_ += 1;
-            }
-            st[j].gPz = h.gPz;
-            st[j].gPz_prev = h.gPz;
-            last[j] = h.gPz;
-            if (st[j].norm0 == 0.0) st[j].norm0 = std::sqrt(h.gPz);
-            const double cur = std::sqrt(h.gPz);
-            if (opt_.verbose)
-                std::fprintf(stderr, "[htf mixed] rhs %d it %d FP64 sqrt(gPz)/norm0 = %.3e\n", r0 + j, st[j].it,
-                             st[j].norm0 > 0 ? cur / st[j].norm0 : 0.0);
-            if (!(h.gPz > 0.0) || !std::isfinite(h.gPz) || cur < opt_.eps_iter * st[j].norm0) {
-                conv[j] = 1;
-                st[j].done = 1;
-            } else {
-                st[j].done = 0;
-            }
-            return HTF_OK;
-        };
-        for (int j = 0; j < kc; ++j) {
-            st[j].eps = opt_.eps_iter;
-            st[j].max_iter = opt_.max_iter;
-            st[j].wFw = 1.0;
-            if ((rc = fp64_residual(j, true))) return rc;
-        }
-        for (int j = kc; j < K; ++j) conv[j] = 1;
-        // mixed-precision iterations with reliable updates: whenever the
-        // recursive g'Pz of a load case has dropped by ru^2 since its last
-        // FP64 residual (or it looks converged / broke down), the FP64
-        // residual replaces it; the search direction is kept except after a
-        // breakdown.
-        const double ru2 = 1e-2;
-        CKB(cudaMemcpyAsync(b_st_, st.data(), K * sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
-        for (;;) {
-            bool any = false;
-            for (int j = 0; j < K; ++j) any |= !conv[j];
-            if (!any) break;
+        if ((rc = batch_begin(r0, std::min(K, nrhs - r0), err))) return rc;
+        for (bool done = false; !done;) {
             for (int k = 0; k < opt_.check_every; ++k) CKB(cudaGraphLaunch(bgraph_, s_));
             launches_ += (long long)opt_.check_every * bkernels_per_iter_;
-            CKB(cudaMemcpyAsync(st.data(), b_st_, K * sizeof(PcpgState), cudaMemcpyDeviceToHost, s_));
-            CKB(cudaStreamSynchronize(s_));
-            int tcerr = 0;
-            CKB(cudaMemcpy(&tcerr, d_tcerr_, sizeof(int), cudaMemcpyDeviceToHost));
-            if (tcerr) { err = "tensor-core product timed out on a barrier"; return tcerr; }
-            bool changed = false;
-            for (int j = 0; j < K; ++j) {
-                if (conv[j]) continue;
-                const bool broke = st[j].done == 2;
-                if (st[j].it >= opt_.max_iter) { conv[j] = 2; continue; }
-                if (st[j].done != 0 || st[j].gPz < ru2 * last[j]) {
-                    st[j].eps = opt_.eps_iter;
-                    if ((rc = fp64_residual(j, broke))) return rc;
-                    changed = true;
-                }
-            }
-            if (changed) CKB(cudaMemcpyAsync(b_st_, st.data(), K * sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
+            if ((rc = batch_check(done, err))) return rc;
         }
-        for (int j = 0; j < kc; ++j) stats_it_[j] = st[j].it;
-        std::vector<double> norm0(K);
-        for (int j = 0; j < K; ++j) norm0[j] = st[j].norm0;
-        CKB(cudaEventRecord(e1, s_));
-        CKB(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
+        double ms = 0.0;
+        if ((rc = batch_finish(stats, ms, err))) return rc;
         total_ms += ms;
-        for (int j = 0; j < kc; ++j) {
-            k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_lam_, d_lam_);
-            CKB(cudaMemcpyAsync(d_alpha_, b_alpha_ + (size_t)j * 6 * ncl_, 6 * ncl_ * sizeof(double),
-                                cudaMemcpyDeviceToDevice, s_));
-            reconstruct(d_f_ + (size_t)(r0 + j) * nfull_, d_u_ + (size_t)(r0 + j) * ndof_);
-            launches_ += 1 + 13;
-            if (stats && r0 + j < 64) {
-                stats->iterations[r0 + j] = stats_it_[j];
-                stats->norm_gPz0[r0 + j] = norm0[j] * norm0[j];
-                stats->final_rel[r0 + j] = 0.0;
-            }
-            if (conv[j] == 2) { err = "PCPG did not converge within max_iter"; return HTF_ENOCONV; }
-        }
-        CKB(cudaGetLastError());
-        for (int j = 0; j < K; ++j) stats_it_[j] = 0;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (u) CKB(cudaMemcpyAsync(u, d_u_, (size_t)ndof_ * nrhs * sizeof(double), cudaMemcpyDeviceToHost, s_));
     CKB(cudaStreamSynchronize(s_));
     if (stats) {

@@ -131,19 +131,14 @@ __device__ __forceinline__ void tmem_add(uint32_t taddr, double *acc) {
     for (int j = 0; j < N; ++j) acc[j] += (double)__uint_as_float(r[j]);
 }
 
-// With scoarse != nullptr the epilogue also applies the coarse correction of the
-// F apply, y_b -= V_d s_d (V_d = [F_d Bc_d^T, -R_d] FP64, s_d the cluster
-// coarse solution at the subdomain's Bc rows and alpha slot).
+// which = 0: F product (A = the set's F slabs) with the coarse correction
+// y_b -= V_d s_d in the epilogue (V_d = [F_d Bc_d^T, -R_d] FP64, s_d the
+// cluster coarse solution at the subdomain's Bc rows and alpha slot);
+// which = 1: S product (A = the set's S slabs), no correction.
 template <int K>
 __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__restrict__ blocks,
-                                                           const float *__restrict__ A,
-                                                           const float *__restrict__ Xs, long long xlo_off,
-                                                           double *__restrict__ yb, int *__restrict__ err,
-                                                           const SubDev *__restrict__ subs,
-                                                           const ClusterDev *__restrict__ cl,
-                                                           const double *__restrict__ V,
-                                                           const int *__restrict__ bcrows,
-                                                           const double *__restrict__ scoarse) {
+                                                           const TcSet *__restrict__ sets, int which,
+                                                           int *__restrict__ err) {
     static_assert(K == 16 || K == 32, "N of the MMA");
     constexpr int SLAB_B = K * 32;                        // floats per X slab
     constexpr unsigned STAGE_TX = (TC_SLAB_A + 2 * SLAB_B) * 4;
@@ -160,6 +155,12 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
     __shared__ volatile int abort_flag;
 
     const GemmBlock g = blocks[blockIdx.x];
+    const TcSet &ts = sets[g.set];
+    const float *__restrict__ A = which == 0 ? ts.AF : ts.AS;
+    const float *__restrict__ Xs = ts.Xs;
+    const long long xlo_off = ts.xlo;
+    double *__restrict__ yb = ts.yb;
+    const double *__restrict__ scoarse = which == 0 ? ts.sc : nullptr;
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
 
     if (threadIdx.x == 0) {
@@ -286,18 +287,18 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
         }
         if (scoarse) {
             // s_d staged in the (now idle) stage buffers by the four epilogue warps
-            const SubDev &sd = subs[g.d];
-            const int gc_off = cl[sd.cluster].gc_off;
+            const SubDev &sd = ts.subs[g.d];
+            const int gc_off = ts.cl[sd.cluster].gc_off;
             const int nc = sd.c + 6;
             double *ss = reinterpret_cast<double *>(base);
             for (int o = threadIdx.x - 64; o < nc * K; o += 128) {
                 const int q = o / K, j = o % K;
-                const int pos = q < sd.c ? bcrows[sd.bcr_off + q] : sd.alpha_pos + (q - sd.c);
+                const int pos = q < sd.c ? ts.bcr[sd.bcr_off + q] : sd.alpha_pos + (q - sd.c);
                 ss[o] = scoarse[((size_t)gc_off + pos) * K + j];
             }
             asm volatile("bar.sync 1, 128;" ::: "memory");
             if (row < g.rows) {
-                const double *Vr = V + sd.V_off + 128 * g.m + row;
+                const double *Vr = ts.V + sd.V_off + 128 * g.m + row;
                 for (int q = 0; q < nc; ++q) {
                     const double vq = Vr[(size_t)q * sd.nbp];
 #pragma unroll
@@ -319,12 +320,8 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
     }
 }
 
-template __global__ void k_tc_gemm<16>(const GemmBlock *, const float *, const float *, long long, double *, int *,
-                                       const SubDev *, const ClusterDev *, const double *, const int *,
-                                       const double *);
-template __global__ void k_tc_gemm<32>(const GemmBlock *, const float *, const float *, long long, double *, int *,
-                                       const SubDev *, const ClusterDev *, const double *, const int *,
-                                       const double *);
+template __global__ void k_tc_gemm<16>(const GemmBlock *, const TcSet *, int, int *);
+template __global__ void k_tc_gemm<32>(const GemmBlock *, const TcSet *, int, int *);
 
 // Full FP32 slabs of a packed symmetric FP64 tile matrix: slab (m, kk) of
 // subdomain d holds rows [128m, 128m+128) x columns [32kk, 32kk+32) of the

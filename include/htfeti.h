@@ -191,6 +191,49 @@ int htf_dual_layout(htf_ctx *ctx, int *row_sub, int *row_dof, double *row_sign, 
  * (Matrix.cpp:835-884 restricted to the Bf column set).                   */
 int htf_fix_dofs(htf_ctx *ctx, int *fix_global);
 
+/* ---- Continuous-batching solve server (no counterpart in the reference,
+ * which solves one problem per process, htfeti.cpp:8-21).  Requests — a
+ * mesh spec and 1..batch load cases — are admitted in arrival order while
+ * the estimated device footprint of their factors, F_i / S_i and vectors fits
+ * the HBM budget and fewer than max_live are set up or running; their setup
+ * overlaps the iterations of running requests; all running requests advance
+ * together in the batched mixed-precision form (options as for htf_create,
+ * precision forced to mixed), their F and S products in one tensor-core
+ * launch.  A request's result does not depend on the others in the mix.
+ * htf_server_destroy lets every submitted request finish first.            */
+typedef struct htf_server htf_server;
+
+#define HTF_REQ_QUEUED 0
+#define HTF_REQ_SETUP 1
+#define HTF_REQ_RUNNING 2
+#define HTF_REQ_DONE 3
+#define HTF_REQ_FAILED 4
+
+typedef struct htf_request_info {
+    int status;                         /* HTF_REQ_*                                */
+    int rc;                             /* HTF_OK or the failed request's code      */
+    int n_rhs, iterations_max;
+    double t_submit_ms, t_admit_ms;     /* wall times since the server was created  */
+    double t_start_ms, t_done_ms;       /* joined the iterations / finished         */
+    double setup_ms, solve_ms;          /* device time of setup and of the solve    */
+    double bytes;                       /* device bytes held by the request         */
+    double bytes_estimate;              /* the footprint estimate it was admitted on */
+} htf_request_info;
+
+/* hbm_budget_bytes <= 0: 85 % of the device's free memory; max_live <= 0: 8 */
+int htf_server_create(const char *options, double hbm_budget_bytes, int max_live, htf_server **srv);
+int htf_server_destroy(htf_server *srv);
+/* f_nodal: 3*n_nodes*n_rhs nodal loads (copied; NULL = body force only);
+ * u: caller-owned 3*n_nodes*n_rhs displacements, written at completion    */
+int htf_server_submit(htf_server *srv, const htf_mesh_spec *spec, int n_rhs, const double *f_nodal, double *u,
+                      long long *ticket);
+/* timeout_ms < 0 waits for completion; HTF_ETIMEDOUT if still running;
+ * returns the request's own code once it has finished                     */
+int htf_server_wait(htf_server *srv, long long ticket, double timeout_ms, htf_request_info *info);
+int htf_server_info(htf_server *srv, long long ticket, htf_request_info *info);
+/* message of a failed request (ticket > 0) or of the last failed submit   */
+const char *htf_server_error(htf_server *srv, long long ticket);
+
 #ifdef __cplusplus
 }
 #endif
