@@ -265,6 +265,14 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
             if (lane == 0) mbar_arrive(&split[s]);
         }
         __syncwarp();
+        if (scoarse) {                                   // warm L2 with this row's V entries while the last MMAs run
+            const SubDev &sd = ts.subs[g.d];
+            const int prow = (warp & 3) * 32 + lane;
+            if (prow < g.rows) {
+                const double *Vr = ts.V + sd.V_off + 128 * g.m + prow;
+                for (int q = 0; q < sd.c + 6; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(Vr + (size_t)q * sd.nbp));
+            }
+        }
         bool have = mbar_wait(&done, 0);
         have = __all_sync(0xffffffffu, have);            // warp-uniform before the .sync.aligned loads
         __syncwarp();
@@ -298,18 +306,37 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
             }
             asm volatile("bar.sync 1, 128;" ::: "memory");
             if (row < g.rows) {
+                // V entries in groups of 8 independent loads
                 const double *Vr = ts.V + sd.V_off + 128 * g.m + row;
-                for (int q = 0; q < nc; ++q) {
+                int q = 0;
+                for (; q + 8 <= nc; q += 8) {
+                    double v[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) v[u] = Vr[(size_t)(q + u) * sd.nbp];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+#pragma unroll
+                        for (int j = 0; j < K; ++j) acc[j] -= v[u] * ss[(q + u) * K + j];
+                }
+                for (; q < nc; ++q) {
                     const double vq = Vr[(size_t)q * sd.nbp];
 #pragma unroll
                     for (int j = 0; j < K; ++j) acc[j] -= vq * ss[q * K + j];
                 }
             }
+            asm volatile("bar.sync 1, 128;" ::: "memory");   // ss is overwritten below
         }
-        if (have && !abort_flag && row < g.rows) {
-            double *y = yb + (g.y_row0 + row) * K;
+        if (have && !abort_flag) {
+            // each warp's 32 output rows are contiguous in yb: transpose them
+            // through shared memory (row stride K+1 doubles) and store coalesced
+            double *st = reinterpret_cast<double *>(base) + quarter * 32 * (K + 1);
 #pragma unroll
-            for (int j = 0; j < K; ++j) y[j] = acc[j];
+            for (int j = 0; j < K; ++j) st[lane * (K + 1) + j] = acc[j];
+            __syncwarp();
+            const int r0 = quarter * 32;
+            const int nrow = min(32, g.rows - r0);
+            double *y = yb + (g.y_row0 + r0) * K;
+            for (int e = lane; e < nrow * K; e += 32) y[e] = st[(e / K) * (K + 1) + (e % K)];
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
