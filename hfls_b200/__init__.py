@@ -49,7 +49,8 @@ class ProfileInfo(ctypes.Structure):
                 ("fapply_ms", ctypes.c_double), ("fapply_bytes", ctypes.c_double),
                 ("iteration_ms", ctypes.c_double), ("kernels_per_iteration", ctypes.c_int),
                 ("batch_width", ctypes.c_int), ("tc_F_ms", ctypes.c_double), ("tc_F_bytes", ctypes.c_double),
-                ("batch_iteration_ms", ctypes.c_double), ("kernels_per_batch_iteration", ctypes.c_int)]
+                ("batch_iteration_ms", ctypes.c_double), ("kernels_per_batch_iteration", ctypes.c_int),
+                ("setup_phase_ms", ctypes.c_double * 8)]
 
 
 class RequestInfo(ctypes.Structure):

@@ -1,4 +1,5 @@
 // C ABI of the HTFETI path (declared in include/htfeti.h).
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -114,10 +115,12 @@ int htf_setup(htf_ctx *ctx) {
     if (!ctx) return HTF_EINVAL;
     if (!ctx->has_mesh) return fail(ctx, HTF_ESTATE, "htf_setup before htf_set_mesh");
     if (ctx->is_setup) return fail(ctx, HTF_ESTATE, "htf_setup called twice");
+    const auto t0 = std::chrono::steady_clock::now();
     int rc = htf::build_problem(ctx->p, ctx->err);
     if (rc) return rc;
     ctx->eng.reset(new (std::nothrow) htf::Engine(ctx->p.opt));
     if (!ctx->eng) return fail(ctx, HTF_ENOMEM, "engine allocation failed");
+    ctx->eng->phase_ms[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     rc = ctx->eng->setup(ctx->p, ctx->err);
     if (rc) return rc;
     ctx->is_setup = true;

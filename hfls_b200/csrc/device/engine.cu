@@ -2,6 +2,7 @@
 //   setup   Cluster::initialization (Cluster.cpp:21-360)
 //   pcpg    Cluster::pcpg + printVTK reconstruction (Cluster.cpp:1363-1458, 1648-1678)
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -854,6 +855,12 @@ int Engine::setup(Problem &p, std::string &err) {
         err = "no CUDA device";
         return HTF_ENODEV;
     }
+    auto clk = std::chrono::steady_clock::now();
+    auto lap = [&](int i) {
+        const auto now = std::chrono::steady_clock::now();
+        phase_ms[i] = std::chrono::duration<double, std::milli>(now - clk).count();
+        clk = now;
+    };
     CK(cudaSetDevice(opt_.device));
     CK(cudaStreamCreateWithFlags(&own_s_, cudaStreamNonBlocking));
     s_ = own_s_;
@@ -861,8 +868,13 @@ int Engine::setup(Problem &p, std::string &err) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     CK(cudaEventRecord(e0, s_));
+    CK(cudaStreamSynchronize(s_));
+    lap(1);
     int rc = upload_layout(p, err);
+    if (!rc) rc = check(cudaStreamSynchronize(s_), "sync", err);
+    lap(2);
     if (!rc) rc = factorize(p, err);
+    lap(3);
     if (!rc) {                    // body-force load, load ownership and the displacement gather map
         ndof_ = 3 * p.mesh.n_nodes;
         std::vector<int> own(nfull_, -1), win(ndof_, -1), owner(ndof_, -1);
@@ -885,8 +897,11 @@ int Engine::setup(Problem &p, std::string &err) {
         if (!rc) rc = check(cudaMemcpyAsync(d_win_, win.data(), ndof_ * sizeof(int), cudaMemcpyHostToDevice, s_), "copy", err);
         if (!rc) rc = check(cudaStreamSynchronize(s_), "sync", err);
     }
+    lap(4);
     if (!rc) rc = coarse(p, err);
+    lap(5);
     if (!rc) rc = outer_coarse(p, err);
+    lap(6);
     if (!rc) {
         int max_nbp = 0;
         for (auto &h : hs_) max_nbp = std::max(max_nbp, h.nbp);
@@ -914,6 +929,7 @@ int Engine::setup(Problem &p, std::string &err) {
     }
     if (!rc) rc = check(cudaEventRecord(e1, s_), "cudaEventRecord", err);
     if (!rc) rc = check(cudaEventSynchronize(e1), "cudaEventSynchronize", err);
+    lap(7);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     setup_ms = ms;
@@ -985,17 +1001,23 @@ int Engine::apply(int op, const double *x, double *y, int nrhs, std::string &err
     return HTF_OK;
 }
 
-// x = K_HT^+ f, d = Bf x, lambda0 = Gf (GfTGf)^{-1} Rf^T f  (Cluster.cpp:1385-1394, 967-1040)
-void Engine::init_rhs(const double *f) {
+// x = K_HT^+ f, d = Bf x, lambda0 = Gf (GfTGf)^{-1} Rf^T f  (Cluster.cpp:1385-1394, 967-1040);
+// with x_solved the triangular solves K_reg^{-1} f were done already (for
+// several load cases at once) and x_solved holds them
+void Engine::init_rhs(const double *f, const double *x_solved) {
     int maxg = 0;
     for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
-    cudaMemcpyAsync(d_full_, f, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_);
-    k_trsv_fwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full_, 0);
-    k_trsv_bwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full_, 0);
-    k_bc_rt<<<nsub_, 256, 0, s_>>>(d_subs_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_R_, d_full_, f, d_t_);
+    const double *x = x_solved;
+    if (!x) {
+        cudaMemcpyAsync(d_full_, f, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_);
+        k_trsv_fwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full_, 0);
+        k_trsv_bwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full_, 0);
+        x = d_full_;
+    }
+    k_bc_rt<<<nsub_, 256, 0, s_>>>(d_subs_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_R_, x, f, d_t_);
     k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, nullptr);
     k_coarse<<<dim3(ncl_, cdiv(maxg, 8)), 256, 0, s_>>>(d_cl_, d_M_, d_gc_, d_s_, nullptr);
-    k_full_to_b<<<nsub_, 256, 0, s_>>>(d_subs_, d_full_, d_yb_);
+    k_full_to_b<<<nsub_, 256, 0, s_>>>(d_subs_, x, d_yb_);
     k_correct<<<nsub_, 256, 0, s_>>>(d_subs_, d_cl_, d_V_, d_bcr_, d_s_, d_yb_, nullptr);
     k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, nullptr, d_d_, nullptr, nullptr, nullptr);
     k_e_vec<<<cdiv(6 * ncl_, 128), 128, 0, s_>>>(ncl_, d_csp_, d_cs_, d_subs_, d_H_, d_t_, d_gc_);
@@ -1157,6 +1179,7 @@ int Engine::project_noalloc(const double *x, double *Px, cudaStream_t stream, st
 int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
     if (!info || reps < 1) { err = "bad arguments"; return HTF_EINVAL; }
     std::memset(info, 0, sizeof(*info));
+    for (int i = 0; i < 8; ++i) info->setup_phase_ms[i] = phase_ms[i];
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));

@@ -68,11 +68,13 @@ public:
     int device() const { return opt_.device; }
     int apply(int op, const double *x, double *y, int nrhs, std::string &err);   // 0=F, 1=P, 2=M
     double setup_ms = 0.0;
+    double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // see htf_profile_info::setup_phase_ms
     int status_sub = -1;
 
 private:
     template <typename T> T *alloc(size_t n, std::string &err, int &rc);
-    void init_rhs(const double *f);                       // d = Bf K_HT^+ f, lambda0
+    void init_rhs(const double *f, const double *x_solved = nullptr);   // d = Bf K_HT^+ f, lambda0
+    void trsm_multi(double *v, int nrhs);                 // v_j = K_reg^{-1} v_j, nrhs <= 32 columns of nfull
     void reconstruct(const double *f, double *u_dev);     // u from lambda, alpha
     double pcpg_start(PcpgState *st);                     // g0, Pg, z, Pz; returns nothing useful
     void tc_apply(int which);
@@ -150,6 +152,8 @@ private:
            *b_Pz_ = nullptr, *b_d_ = nullptr, *b_xb_ = nullptr, *b_yb_ = nullptr, *b_t_ = nullptr, *b_gc_ = nullptr,
            *b_s_ = nullptr, *b_part_ = nullptr, *b_gpart_ = nullptr, *b_wFw_ = nullptr, *b_gPz_ = nullptr, *b_gw_ = nullptr, *b_gt_ = nullptr, *b_acoef_ = nullptr,
            *b_alpha_ = nullptr, *b_tmp_ = nullptr;
+    double *b_fullA_ = nullptr, *b_fullB_ = nullptr;   // full vectors of the batch (nfull x K)
+    double *b_srec_ = nullptr;                         // coarse solutions of the reconstruction (ngc x K)
     PcpgState *b_st_ = nullptr;
     cudaGraphExec_t bgraph_ = nullptr;
     int bkernels_per_iter_ = 0;

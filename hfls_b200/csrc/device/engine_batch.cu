@@ -52,6 +52,20 @@ __global__ void k_col_get(int, int, int, const double *, double *);
 __global__ void k_col_set(int, int, int, const double *, double *);
 __global__ void k_sum_to(const double *, int, double *, const PcpgState *);
 __global__ void k_build_f(int, int, int, const double *, const int *, const double *, double *);
+__global__ void k_trsm_fwd_multi(const SubDev *, const double *, double *, long long, int);
+__global__ void k_trsm_bwd_multi(const SubDev *, const double *, double *, long long, int);
+__global__ void k_gather_b(int, const int *, const int *, const double *, const double *, double *,
+                           const PcpgState *);
+__global__ void k_full_minus_b(const SubDev *, const double *, double *);
+__global__ void k_bc_rt(const SubDev *, const int *, const int *, const double *, const double *, const double *,
+                        const double *, double *);
+__global__ void k_gc(int, const int *, const int *, const double *, double *, const PcpgState *);
+__global__ void k_coarse(const ClusterDev *, const double *, const double *, double *, const PcpgState *);
+__global__ void k_sub_bct(const SubDev *, const ClusterDev *, const int *, const int *, const int *, const double *,
+                          const double *, double *);
+__global__ void k_add_R(const SubDev *, const ClusterDev *, const double *, const double *, const double *,
+                        const double *, double *);
+__global__ void k_gather_u(int, const int *, const double *, double *);
 
 static inline int cdivb(long long a, long long b) { return int((a + b - 1) / b); }
 
@@ -135,6 +149,9 @@ int Engine::setup_batch(int K, std::string &err) {
     b_gt_ = alloc<double>((size_t)6 * ncl_ * K, err, rc); b_acoef_ = alloc<double>((size_t)6 * ncl_ * K, err, rc);
     b_alpha_ = alloc<double>((size_t)6 * ncl_ * K, err, rc);
     b_st_ = alloc<PcpgState>(K, err, rc);
+    b_fullA_ = alloc<double>((size_t)nfull_ * K, err, rc);
+    b_fullB_ = alloc<double>((size_t)nfull_ * K, err, rc);
+    b_srec_ = alloc<double>((size_t)ngc_total_ * K, err, rc);
     if (rc) return rc;
     bK_ = K;
     const TcSet ts = tc_set();
@@ -346,11 +363,16 @@ int Engine::batch_begin(int r0, int kc, std::string &err) {
     CKB(cudaMemsetAsync(b_lam_, 0, (size_t)nlam_ * K * sizeof(double), s_));
     CKB(cudaMemsetAsync(b_d_, 0, (size_t)nlam_ * K * sizeof(double), s_));
     CKB(cudaMemsetAsync(d_tcerr_, 0, sizeof(int), s_));
+    // K_reg^{-1} f for the whole chunk: the factor is read once
+    CKB(cudaMemcpyAsync(b_fullB_, d_f_ + (size_t)r0 * nfull_, (size_t)kc * nfull_ * sizeof(double),
+                        cudaMemcpyDeviceToDevice, s_));
+    trsm_multi(b_fullB_, kc);
+    launches_ += 2;
     for (int j = 0; j < kc; ++j) {
-        init_rhs(d_f_ + (size_t)(r0 + j) * nfull_);
+        init_rhs(d_f_ + (size_t)(r0 + j) * nfull_, b_fullB_ + (size_t)j * nfull_);
         k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_d_, b_d_);
         k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_lam_, b_lam_);
-        launches_ += 27;
+        launches_ += 25;
     }
     CKB(cudaEventRecord(run_e0_, s_));
     for (int j = 0; j < K; ++j) r.st[j].done = 1;
@@ -404,12 +426,41 @@ int Engine::batch_finish(htf_stats *stats, double &ms, std::string &err) {
     float fms = 0.f;
     cudaEventElapsedTime(&fms, run_e0_, run_e1_);
     ms = fms;
-    for (int j = 0; j < r.kc; ++j) {
+    // u_j = K_HT^+(f_j - Bf^T lambda_j) - Rf alpha_j (Cluster.cpp:1648-1678) for the whole
+    // chunk, with the two K_reg^{-1} solves of every load case done at once
+    const int kc = r.kc;
+    int maxg = 0;
+    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
+    CKB(cudaMemcpyAsync(b_fullA_, d_f_ + (size_t)r.r0 * nfull_, (size_t)kc * nfull_ * sizeof(double),
+                        cudaMemcpyDeviceToDevice, s_));
+    for (int j = 0; j < kc; ++j) {
+        double *fa = b_fullA_ + (size_t)j * nfull_;
         k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_lam_, d_lam_);
-        CKB(cudaMemcpyAsync(d_alpha_, b_alpha_ + (size_t)j * 6 * ncl_, 6 * ncl_ * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s_));
-        reconstruct(d_f_ + (size_t)(r.r0 + j) * nfull_, d_u_ + (size_t)(r.r0 + j) * ndof_);
-        launches_ += 1 + 13;
+        k_gather_b<<<cdivb(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, d_lam_, nullptr, d_xb_,
+                                                        nullptr);
+        k_full_minus_b<<<nsub_, 256, 0, s_>>>(d_subs_, d_xb_, fa);
+    }
+    CKB(cudaMemcpyAsync(b_fullB_, b_fullA_, (size_t)kc * nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+    trsm_multi(b_fullB_, kc);
+    for (int j = 0; j < kc; ++j) {
+        double *fa = b_fullA_ + (size_t)j * nfull_;
+        k_bc_rt<<<nsub_, 256, 0, s_>>>(d_subs_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_R_, b_fullB_ + (size_t)j * nfull_,
+                                       fa, d_t_);
+        k_gc<<<cdivb(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, nullptr);
+        k_coarse<<<dim3(ncl_, cdivb(maxg, 8)), 256, 0, s_>>>(d_cl_, d_M_, d_gc_, b_srec_ + (size_t)j * ngc_total_,
+                                                            nullptr);
+        k_sub_bct<<<nsub_, 32, 0, s_>>>(d_subs_, d_cl_, d_bcr_, d_bce_ptr_, d_bce_pos_, d_bce_val_,
+                                        b_srec_ + (size_t)j * ngc_total_, fa);
+    }
+    trsm_multi(b_fullA_, kc);
+    for (int j = 0; j < kc; ++j) {
+        double *fa = b_fullA_ + (size_t)j * nfull_;
+        k_add_R<<<nsub_, 256, 0, s_>>>(d_subs_, d_cl_, d_R_, d_H_, b_srec_ + (size_t)j * ngc_total_,
+                                       b_alpha_ + (size_t)j * 6 * ncl_, fa);
+        k_gather_u<<<cdivb(ndof_, 256), 256, 0, s_>>>(ndof_, d_win_, fa, d_u_ + (size_t)(r.r0 + j) * ndof_);
+    }
+    launches_ += 4 + 9 * kc;
+    for (int j = 0; j < kc; ++j) {
         if (stats && r.r0 + j < 64) {
             stats->iterations[r.r0 + j] = r.st[j].it;
             stats->norm_gPz0[r.r0 + j] = r.st[j].norm0 * r.st[j].norm0;
@@ -420,6 +471,11 @@ int Engine::batch_finish(htf_stats *stats, double &ms, std::string &err) {
     for (int j = 0; j < r.kc; ++j)
         if (r.conv[j] == 2) { err = "PCPG did not converge within max_iter"; return HTF_ENOCONV; }
     return HTF_OK;
+}
+
+void Engine::trsm_multi(double *v, int nrhs) {
+    k_trsm_fwd_multi<<<nsub_, 256, 0, s_>>>(d_subs_, d_K_, v, nfull_, nrhs);
+    k_trsm_bwd_multi<<<nsub_, 256, 0, s_>>>(d_subs_, d_K_, v, nfull_, nrhs);
 }
 
 int Engine::batch_graph(std::string &err) {

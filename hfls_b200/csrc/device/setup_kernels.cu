@@ -508,3 +508,165 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(const SubDev *__restrict__ sub
 }
 
 }  // namespace htf
+
+namespace htf {
+
+// ---------------------------------------------------------------------------
+// batched dense triangular solves with the full factor for up to 32
+// right-hand sides at once (the load cases of a batch): the factor is read
+// once per call instead of once per load case.  Column j of subdomain d lives
+// at v + nfull_off + j*ldv.  One CTA of 8 warps per subdomain; warp w owns
+// columns 4w..4w+3, lane = row inside the current 32-row block.  The next
+// 32x32 chunk of L and of X is loaded into registers while the current one
+// is multiplied out of shared memory.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict__ subs,
+                                                        const double *__restrict__ Kbuf, double *__restrict__ v,
+                                                        long long ldv, int nrhs) {
+    __shared__ double Ls[32][33];
+    __shared__ double Xs[32][33];
+    __shared__ double rinv[32];
+    const SubDev &sd = subs[blockIdx.x];
+    const double *L = Kbuf + sd.K_off;
+    double *x = v + sd.nfull_off;
+    const int N = sd.N, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nblk = (N + 31) / 32;
+    for (int b = 0; b < nblk; ++b) {
+        const int kb = 32 * b, nrow = min(32, N - kb);
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        double lr[4], xr[4];
+        // chunk cb: L rows kb.., columns 32cb.. (all < kb <= N); X rows 32cb..
+        auto load = [&](int cb) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int c = w + 8 * i;
+                lr[i] = (lane < nrow) ? L[(kb + lane) + (size_t)(32 * cb + c) * N] : 0.0;
+                xr[i] = (c < nrhs) ? x[(32 * cb + lane) + (size_t)c * ldv] : 0.0;
+            }
+        };
+        if (b > 0) load(0);
+        for (int cb = 0; cb < b; ++cb) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                Ls[lane][w + 8 * i] = lr[i];
+                Xs[lane][w + 8 * i] = xr[i];
+            }
+            __syncthreads();
+            if (cb + 1 < b) load(cb + 1);
+#pragma unroll 8
+            for (int c = 0; c < 32; ++c) {
+                const double l = Ls[lane][c];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] += l * Xs[c][4 * w + q];
+            }
+            __syncthreads();
+        }
+        // diagonal block: forward substitution, one shuffle per row
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int c = w + 8 * i;
+            Ls[lane][c] = (lane < nrow && c <= lane) ? L[(kb + lane) + (size_t)(kb + c) * N] : 0.0;
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) rinv[lane] = (lane < nrow) ? 1.0 / Ls[lane][lane] : 0.0;
+        __syncthreads();
+        double a[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = 4 * w + q;
+            a[q] = (lane < nrow && j < nrhs) ? x[(kb + lane) + (size_t)j * ldv] - acc[q] : 0.0;
+        }
+        for (int p = 0; p < nrow; ++p) {
+            const double rp = rinv[p], lp = Ls[lane][p];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double y = __shfl_sync(0xffffffffu, a[q] * rp, p);
+                if (lane == p) a[q] = y;
+                else if (lane > p) a[q] -= lp * y;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = 4 * w + q;
+            if (lane < nrow && j < nrhs) x[(kb + lane) + (size_t)j * ldv] = a[q];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_trsm_bwd_multi(const SubDev *__restrict__ subs,
+                                                        const double *__restrict__ Kbuf, double *__restrict__ v,
+                                                        long long ldv, int nrhs) {
+    __shared__ double Ls[32][33];
+    __shared__ double Xs[32][33];
+    __shared__ double rinv[32];
+    const SubDev &sd = subs[blockIdx.x];
+    const double *L = Kbuf + sd.K_off;
+    double *x = v + sd.nfull_off;
+    const int N = sd.N, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nblk = (N + 31) / 32;
+    for (int b = nblk - 1; b >= 0; --b) {
+        const int kb = 32 * b, nrow = min(32, N - kb);
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        double lr[4], xr[4];
+        // chunk cb > b: rows c = 32cb + lane of L's columns kb.. (L^T), X rows c
+        auto load = [&](int cb) {
+            const int c = 32 * cb + lane;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int r = w + 8 * i;
+                lr[i] = (c < N && r < nrow) ? L[c + (size_t)(kb + r) * N] : 0.0;
+                xr[i] = (c < N && r < nrhs) ? x[c + (size_t)r * ldv] : 0.0;
+            }
+        };
+        if (b + 1 < nblk) load(b + 1);
+        for (int cb = b + 1; cb < nblk; ++cb) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                Ls[lane][w + 8 * i] = lr[i];          // Ls[c][r] = L[32cb + c][kb + r]
+                Xs[lane][w + 8 * i] = xr[i];
+            }
+            __syncthreads();
+            if (cb + 1 < nblk) load(cb + 1);
+#pragma unroll 8
+            for (int c = 0; c < 32; ++c) {
+                const double l = Ls[c][lane];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] += l * Xs[c][4 * w + q];
+            }
+            __syncthreads();
+        }
+        // diagonal block: Ls[p][r] = L[kb + p][kb + r], r <= p; back substitution with L^T
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int r = w + 8 * i;
+            Ls[lane][r] = (lane < nrow && r <= lane) ? L[(kb + lane) + (size_t)(kb + r) * N] : 0.0;
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) rinv[lane] = (lane < nrow) ? 1.0 / Ls[lane][lane] : 0.0;
+        __syncthreads();
+        double a[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = 4 * w + q;
+            a[q] = (lane < nrow && j < nrhs) ? x[(kb + lane) + (size_t)j * ldv] - acc[q] : 0.0;
+        }
+        for (int p = nrow - 1; p >= 0; --p) {
+            const double rp = rinv[p], lp = Ls[p][lane];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double y = __shfl_sync(0xffffffffu, a[q] * rp, p);
+                if (lane == p) a[q] = y;
+                else if (lane < p) a[q] -= lp * y;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = 4 * w + q;
+            if (lane < nrow && j < nrhs) x[(kb + lane) + (size_t)j * ldv] = a[q];
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace htf

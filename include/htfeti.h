@@ -154,6 +154,12 @@ typedef struct htf_profile_info {
                                            tensor cores: FP32 slabs + X + Y bytes   */
     double batch_iteration_ms;          /* one captured batched PCPG iteration      */
     int kernels_per_batch_iteration;
+    /* host wall time of the phases of htf_setup (ms): 0 problem build (maps,
+     * Bf/Bc, kernels, fix DOFs), 1 device context and stream, 2 layout upload
+     * and allocation, 3 assembly + factorisation + F_i/S_i, 4 load and
+     * displacement maps, 5 cluster coarse problems, 6 outer coarse problem,
+     * 7 FP32 slabs of the batched form                                       */
+    double setup_phase_ms[8];
 } htf_profile_info;
 int htf_profile(htf_ctx *ctx, int reps, htf_profile_info *info);
 
