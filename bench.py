@@ -48,6 +48,13 @@ REF_SAMPLE = dict(Nx=2, Ny=1, Nz=1, nx=8, ny=8, nz=8)     # subdomains of the wo
 MIXED_RHS = 32
 MIXED_WORKLOAD = ("same cube, body force (0,0,-1) + 32 seeded N(0,1) tractions on x=1, solved as one batch of 32: "
                   "F_i/S_i FP32 slabs, 3xTF32 tcgen05 products, FP64 coarse/projector/residual replacement, eps 1e-8")
+SERVE_REQUESTS = 16          # requests of the seeded stream that one bench run serves
+SERVE_RATE = 1.0             # Poisson arrivals per second
+SERVE_WORKLOAD = ("seeded Poisson stream (rate %.1f/s): cube meshes of c^3 clusters, (c s)^3 subdomains of e^3 hex8, "
+                  "c in 1..4, s in 2..5, e in 4..10, 1..16 load cases (body force + N(0,1) traction on x=1), "
+                  "E logU[1,1e4] per subdomain, nu U[0.2,0.4] per request, clamp x=0, jitter 0.1h, eps 1e-8; "
+                  "served by htf_server (mixed precision, batch 16) vs the plain FP64 per-request path "
+                  "(set up and solve one request after another, FIFO on the same arrivals)" % SERVE_RATE)
 
 
 def peaks():
@@ -260,6 +267,93 @@ def run_mixed(hb, local, dist):
     }
 
 
+def serve_stream(hb, n, seed=4):
+    """The first n requests of the seeded serving stream: (arrival s, spec, load cases, seed)."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    for i in range(n):
+        t += float(rng.exponential(1.0 / SERVE_RATE))
+        c, s, e = int(rng.integers(1, 5)), int(rng.integers(2, 6)), int(rng.integers(4, 11))
+        k, nu = int(rng.integers(1, 17)), float(rng.uniform(0.2, 0.4))
+        spec = hb.mesh_spec(clusters=(c, c, c), subs=(s, s, s), elems=(e, e, e), jitter=0.1, seed=1000 + i,
+                            material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e4, nu=nu, bc=hb.HTF_BC_CLAMP_X0,
+                            body_force=(0.0, 0.0, -1.0))
+        out.append((t, spec, k, 2000 + i, (c, s, e)))
+    return out
+
+
+def pct(v, q):
+    return float(np.percentile(np.asarray(v), q)) if len(v) else None
+
+
+def run_serving(hb, local, n_req):
+    """Continuous-batching server on a bounded prefix of the serving stream,
+    then the plain FP64 per-request path on the same requests."""
+    import torch
+    free, _ = torch.cuda.mem_get_info(local)
+    budget = 0.85 * free
+    stream = serve_stream(hb, n_req)
+    loads = []
+    for (_, spec, k, fseed, dims) in stream:
+        c, s, e = dims
+        lower = 8.0 * 9.0 * ((c * s) * (e + 1) ** 2) ** 3      # dense factors alone
+        loads.append(hb.traction(spec, seed=fseed, n_rhs=k) if lower <= budget else None)
+    opts = dict(OPTS, device=str(local), precision="mixed", batch="16", max_iter="3000")
+    srv = hb.Server(opts, hbm_budget_bytes=budget, max_live=8)
+    tickets = []
+    t0 = time.perf_counter()
+    for (ta, spec, k, _, _), f in zip(stream, loads):
+        dt = t0 + ta - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        tickets.append(srv.submit(spec, f, n_rhs=k))
+    served = []
+    for i, t in enumerate(tickets):
+        try:
+            u, info = srv.wait(t)
+            served.append((i, u.copy(), info.t_submit_ms, info.t_done_ms, info.iterations_max))
+        except hb.HTFError as e:
+            served.append((i, None, None, None, e.code, str(e)[:200]))
+    srv.close()
+    ok = [x for x in served if x[1] is not None]
+    lat = [x[3] - x[2] for x in ok]
+    cases = sum(stream[x[0]][2] for x in ok)
+    makespan = (max(x[3] for x in ok) - min(x[2] for x in ok)) / 1e3 if ok else None
+    # plain FP64 per-request path: service time of each served request, FIFO on the same arrivals
+    service, err = [], 0.0
+    for (i, u, _, _, _) in ok:
+        ta, spec, k, _, _ = stream[i]
+        t = time.perf_counter()
+        s = hb.Solver(dict(OPTS, device=str(local), max_iter="5000"))
+        s.set_mesh(hb.generate_mesh(spec))
+        s.setup()
+        u64, _ = s.solve(loads[i])
+        del s
+        service.append(time.perf_counter() - t)
+        err = max(err, max(float(np.linalg.norm(u[j] - u64[j]) / np.linalg.norm(u64[j])) for j in range(k)))
+    fin, lat64 = 0.0, []
+    for (i, *_), sv in zip(ok, service):
+        ta = stream[i][0]
+        fin = max(fin, ta) + sv
+        lat64.append(1e3 * (fin - ta))
+    first = stream[ok[0][0]][0] if ok else 0.0
+    return {
+        "workload": SERVE_WORKLOAD, "requests": n_req, "served": len(ok),
+        "rejected_oversize": sum(1 for x in served if x[1] is None and x[4] == hb.HTF_ENOMEM),
+        "failed_other": sum(1 for x in served if x[1] is None and x[4] != hb.HTF_ENOMEM),
+        "load_cases": cases, "budget_gb": budget / 1e9,
+        "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "mean_ms": float(np.mean(lat)) if lat else None,
+        "solves_per_s": cases / makespan if makespan else None,
+        "requests_per_s": len(ok) / makespan if makespan else None,
+        "fp64_per_request": {"p50_ms": pct(lat64, 50), "p99_ms": pct(lat64, 99),
+                             "solves_per_s": cases / (fin - first) if ok else None,
+                             "service_s": [round(x, 3) for x in service]},
+        "u_rel_err_max_vs_fp64": err,
+        "sizes": [dict(c=x[4][0], s=x[4][1], e=x[4][2], load_cases=x[2]) for x in stream],
+        "errors": [x[5] for x in served if x[1] is None],
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -268,6 +362,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision multi-load-case measurement")
+    ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS,
+                    help="requests of the seeded serving stream to serve (0 skips the serving measurement)")
     ap.add_argument("--workload", default="full", choices=["full", "small"],
                     help="small: one cluster of 2x4x4 subdomains of 8^3 (F_i + S_i 0.3 GB > L2), "
                          "for ncu captures only")
@@ -311,6 +407,10 @@ def main():
     del s
     # every rank solves its mixed-precision replica too (collective max inside)
     mixed = None if args.no_mixed or args.workload != "full" else run_mixed(hb, local, dist)
+    serving = None
+    if args.serve_requests > 0 and args.workload == "full":
+        barrier(dist)
+        serving = run_serving(hb, local, args.serve_requests)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -345,6 +445,7 @@ def main():
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "mixed": mixed,
+        "serving": serving,
     }
     print(json.dumps(line))
     if dist is not None:

@@ -203,15 +203,16 @@ size_t Engine::device_bytes() const {
     return t;
 }
 
-int Engine::check(cudaError_t e, const char *what, std::string &err) {
+int Engine::check(cudaError_t e, const char *what, std::string &err, const char *file, int line) {
     if (e == cudaSuccess) return HTF_OK;
     err = std::string(what) + ": " + cudaGetErrorString(e);
+    if (file) err += " (" + std::string(file) + ":" + std::to_string(line) + ")";
     return (e == cudaErrorMemoryAllocation) ? HTF_ENOMEM : HTF_ECUDA;
 }
 
 #define CK(call)                                                   \
     do {                                                           \
-        int _rc = check((call), #call, err);                       \
+        int _rc = check((call), #call, err, "engine.cu", __LINE__); \
         if (_rc) return _rc;                                       \
     } while (0)
 
@@ -601,161 +602,6 @@ int Engine::factorize(Problem &p, std::string &err) {
     return HTF_OK;
 }
 
-// ---------------------------------------------------------------------------
-// cluster coarse problem (host FP64): M = [Ac^{-1}]_{lambda_c, alpha}
-//   M11 = Fc^{-1} - Z Sr^{-1} Z^T, M12 = Z Sr^{-1}, M22 = H H^T - Sr^{-1}
-//   with Z = Fc^{-1} Gc, Sr = Gc^T Z + H H^T, H = ker(Gc) orthonormal:
-//   the block elimination of the extended saddle-point matrix
-//   [Fc Gc 0; Gc^T 0 H; 0 H^T 0] of Cluster::create_Ac_clust (Cluster.cpp:582-678).
-// ---------------------------------------------------------------------------
-int Engine::coarse(Problem &p, std::string &err) {
-    int rc = HTF_OK;
-    // Fc_d from the device
-    std::vector<long long> fco(nsub_);
-    long long fct = 0;
-    for (int d = 0; d < nsub_; ++d) { fco[d] = fct; fct += (long long)hs_[d].c * hs_[d].c; }
-    long long *d_fco = alloc<long long>(nsub_, err, rc);
-    double *d_Fc = alloc<double>(std::max<long long>(fct, 1), err, rc);
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(d_fco, fco.data(), nsub_ * sizeof(long long), cudaMemcpyHostToDevice, s_));
-    k_build_Fc<<<nsub_, 256, 0, s_>>>(d_subs_, d_V_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_fco, d_Fc);
-    CK(cudaGetLastError());
-    std::vector<double> Fc(std::max<long long>(fct, 1));
-    CK(cudaMemcpyAsync(Fc.data(), d_Fc, fct * sizeof(double), cudaMemcpyDeviceToHost, s_));
-    CK(cudaStreamSynchronize(s_));
-    Hd_.assign(nsub_, std::vector<double>(36, 0.0));
-    std::vector<double> Mall;
-    std::vector<std::vector<double>> Ms(ncl_);
-    int fail = 0;
-#pragma omp parallel for schedule(dynamic)
-    for (int ci = 0; ci < ncl_; ++ci) {
-        const Cluster &cl = p.clu[ci];
-        const int nc = cl.nlam_c, ns = int(cl.subs.size()), na = 6 * ns, ng = nc + na;
-        std::vector<double> F(size_t(nc) * nc, 0.0), G(size_t(nc) * na, 0.0), H(size_t(na) * 6, 0.0);
-        for (int k = 0; k < ns; ++k) {
-            const int d = cl.subs[k];
-            const Subdomain &s = p.sub[d];
-            const int c = hs_[d].c;
-            for (int j = 0; j < c; ++j)
-                for (int i = 0; i < c; ++i) F[s.bc_rows[i] + size_t(s.bc_rows[j]) * nc] += Fc[fco[d] + i + (size_t)j * c];
-            for (size_t e = 0; e < s.bc_row.size(); ++e)          // Gc_d = -Bc_d R_d (Cluster.cpp:190-198)
-                for (int j = 0; j < 6; ++j)
-                    G[s.bc_row[e] + size_t(6 * k + j) * nc] -= s.bc_val[e] * s.R[s.bc_col[e] + size_t(j) * s.n];
-            // ker(Gc): alpha_d = R_d^T r for the (unnormalised) rigid modes r of the cluster
-            const int n = s.n;
-            for (int q = 0; q < 6; ++q)
-                for (int j = 0; j < 6; ++j) {
-                    double v = 0.0;
-                    for (int l = 0; l < n / 3; ++l) {
-                        int node = s.l2g[3 * l] / 3;
-                        double x = p.mesh.coords[3 * size_t(node)], y = p.mesh.coords[3 * size_t(node) + 1],
-                               z = p.mesh.coords[3 * size_t(node) + 2];
-                        double g[3] = {0, 0, 0};
-                        switch (q) {
-                            case 0: g[0] = 1; break;
-                            case 1: g[1] = 1; break;
-                            case 2: g[2] = 1; break;
-                            case 3: g[0] = -y; g[1] = x; break;
-                            case 4: g[0] = -z; g[2] = x; break;
-                            default: g[1] = -z; g[2] = y; break;
-                        }
-                        for (int cc = 0; cc < 3; ++cc) v += s.R[3 * l + cc + size_t(j) * n] * g[cc];
-                    }
-                    H[6 * k + j + size_t(q) * na] = v;
-                }
-        }
-        // orthonormalise the columns of H (two passes of Gram-Schmidt)
-        for (int pass = 0; pass < 2; ++pass)
-            for (int q = 0; q < 6; ++q) {
-                double *hq = &H[size_t(q) * na];
-                for (int o = 0; o < q; ++o) {
-                    const double *ho = &H[size_t(o) * na];
-                    double dd = 0.0;
-                    for (int i = 0; i < na; ++i) dd += hq[i] * ho[i];
-                    for (int i = 0; i < na; ++i) hq[i] -= dd * ho[i];
-                }
-                double nn = 0.0;
-                for (int i = 0; i < na; ++i) nn += hq[i] * hq[i];
-                nn = std::sqrt(nn);
-                for (int i = 0; i < na; ++i) hq[i] /= nn;
-            }
-        for (int k = 0; k < ns; ++k)
-            for (int j = 0; j < 6; ++j)
-                for (int q = 0; q < 6; ++q) Hd_[cl.subs[k]][j * 6 + q] = H[6 * k + j + size_t(q) * na];
-        // Cholesky of Fc, Z = Fc^{-1} Gc
-        std::vector<double> L(F);
-        if (!chol_lower(nc, L.data(), nc)) {
-#pragma omp atomic write
-            fail = ci + 1;
-            continue;
-        }
-        std::vector<double> Z(G);
-        chol_solve(nc, L.data(), nc, Z.data(), nc, na);
-        std::vector<double> Sr(size_t(na) * na, 0.0);
-        for (int j = 0; j < na; ++j)
-            for (int i = 0; i < na; ++i) {
-                double v = 0.0;
-                for (int k = 0; k < nc; ++k) v += G[k + size_t(i) * nc] * Z[k + size_t(j) * nc];
-                for (int q = 0; q < 6; ++q) v += H[i + size_t(q) * na] * H[j + size_t(q) * na];
-                Sr[i + size_t(j) * na] = v;
-            }
-        std::vector<double> Ls(Sr);
-        if (!chol_lower(na, Ls.data(), na)) {
-#pragma omp atomic write
-            fail = ci + 1;
-            continue;
-        }
-        std::vector<double> Si(size_t(na) * na, 0.0);
-        for (int i = 0; i < na; ++i) Si[i + size_t(i) * na] = 1.0;
-        chol_solve(na, Ls.data(), na, Si.data(), na, na);
-        std::vector<double> Fi(size_t(nc) * nc, 0.0);
-        for (int i = 0; i < nc; ++i) Fi[i + size_t(i) * nc] = 1.0;
-        chol_solve(nc, L.data(), nc, Fi.data(), nc, nc);
-        std::vector<double> ZS(size_t(nc) * na, 0.0);            // Z Sr^{-1}
-        for (int j = 0; j < na; ++j)
-            for (int k = 0; k < na; ++k) {
-                const double s = Si[k + size_t(j) * na];
-                const double *zk = &Z[size_t(k) * nc];
-                double *o = &ZS[size_t(j) * nc];
-                for (int i = 0; i < nc; ++i) o[i] += zk[i] * s;
-            }
-        std::vector<double> &M = Ms[ci];
-        M.assign(size_t(ng) * ng, 0.0);
-        for (int j = 0; j < nc; ++j) {
-            for (int i = 0; i < nc; ++i) M[i + size_t(j) * ng] = Fi[i + size_t(j) * nc];
-            for (int k = 0; k < na; ++k) {
-                const double zjk = Z[j + size_t(k) * nc];
-                const double *zs = &ZS[size_t(k) * nc];
-                double *o = &M[size_t(j) * ng];
-                for (int i = 0; i < nc; ++i) o[i] -= zs[i] * zjk;
-            }
-        }
-        for (int j = 0; j < na; ++j)
-            for (int i = 0; i < nc; ++i) {
-                M[i + size_t(nc + j) * ng] = ZS[i + size_t(j) * nc];
-                M[(nc + j) + size_t(i) * ng] = ZS[i + size_t(j) * nc];
-            }
-        for (int j = 0; j < na; ++j)
-            for (int i = 0; i < na; ++i) {
-                double v = -Si[i + size_t(j) * na];
-                for (int q = 0; q < 6; ++q) v += H[i + size_t(q) * na] * H[j + size_t(q) * na];
-                M[(nc + i) + size_t(nc + j) * ng] = v;
-            }
-    }
-    if (fail) {
-        err = "cluster coarse matrix of cluster " + std::to_string(fail - 1) + " is not positive definite";
-        return HTF_ENOTSPD;
-    }
-    for (int ci = 0; ci < ncl_; ++ci)
-        CK(cudaMemcpyAsync(d_M_ + hc_[ci].M_off, Ms[ci].data(), Ms[ci].size() * sizeof(double),
-                           cudaMemcpyHostToDevice, s_));
-    std::vector<double> Hflat(36 * (size_t)nsub_);
-    for (int d = 0; d < nsub_; ++d) std::memcpy(&Hflat[36 * (size_t)d], Hd_[d].data(), 36 * sizeof(double));
-    CK(cudaMemcpyAsync(d_H_, Hflat.data(), Hflat.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
-    CK(cudaStreamSynchronize(s_));
-    return HTF_OK;
-}
-
 // Gf = Bf Rf, Rf_d = R_d H_d (Cluster.cpp:1332-1352); (Gf^T Gf)^{-1} (1227-1273)
 int Engine::outer_coarse(Problem &p, std::string &err) {
     int rc = HTF_OK;
@@ -855,6 +701,7 @@ int Engine::setup(Problem &p, std::string &err) {
         err = "no CUDA device";
         return HTF_ENODEV;
     }
+    cudaGetLastError();           // an error left by an earlier, unrelated call is not this setup's
     auto clk = std::chrono::steady_clock::now();
     auto lap = [&](int i) {
         const auto now = std::chrono::steady_clock::now();
@@ -931,7 +778,7 @@ int Engine::setup(Problem &p, std::string &err) {
     if (!rc) rc = check(cudaEventSynchronize(e1), "cudaEventSynchronize", err);
     lap(7);
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
+    if (!rc) cudaEventElapsedTime(&ms, e0, e1);
     setup_ms = ms;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -988,6 +835,7 @@ void Engine::iteration(PcpgState *st) {
 }
 
 int Engine::apply(int op, const double *x, double *y, int nrhs, std::string &err) {
+    cudaGetLastError();
     if (mixed_ && bK_ > 0) return apply_batch(op, x, y, nrhs, err);
     for (int k = 0; k < nrhs; ++k) {
         CK(cudaMemcpyAsync(d_tmp_, x + (size_t)k * nlam_, nlam_ * sizeof(double), cudaMemcpyHostToDevice, s_));
@@ -1118,6 +966,7 @@ int Engine::ensure_rhs(int nrhs, std::string &err) {
 }
 
 int Engine::solve(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err) {
+    cudaGetLastError();           // an error left by an earlier, unrelated call is not this solve's
     if (mixed_ && bK_ > 0) return solve_batch(p, nrhs, f_nodal, u, stats, err);
     int rc = ensure_rhs(nrhs, err);
     if (rc) return rc;

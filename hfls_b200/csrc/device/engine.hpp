@@ -88,7 +88,7 @@ private:
     void op_M_batch(const double *x, double *z);
     void op_P_batch(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial);
     void iteration_batch();
-    int check(cudaError_t e, const char *what, std::string &err);
+    int check(cudaError_t e, const char *what, std::string &err, const char *file = nullptr, int line = 0);
     int upload_layout(Problem &p, std::string &err);
     int factorize(Problem &p, std::string &err);
     int coarse(Problem &p, std::string &err);

@@ -52,8 +52,8 @@ __global__ void k_col_get(int, int, int, const double *, double *);
 __global__ void k_col_set(int, int, int, const double *, double *);
 __global__ void k_sum_to(const double *, int, double *, const PcpgState *);
 __global__ void k_build_f(int, int, int, const double *, const int *, const double *, double *);
-__global__ void k_trsm_fwd_multi(const SubDev *, const double *, double *, long long, int);
-__global__ void k_trsm_bwd_multi(const SubDev *, const double *, double *, long long, int);
+__global__ void k_trsm_fwd_multi(const SubDev *, const double *, double *, long long, int, const int *);
+__global__ void k_trsm_bwd_multi(const SubDev *, const double *, double *, long long, int, const int *);
 __global__ void k_gather_b(int, const int *, const int *, const double *, const double *, double *,
                            const PcpgState *);
 __global__ void k_full_minus_b(const SubDev *, const double *, double *);
@@ -71,7 +71,7 @@ static inline int cdivb(long long a, long long b) { return int((a + b - 1) / b);
 
 #define CKB(call)                                                  \
     do {                                                           \
-        int _rc = check((call), #call, err);                       \
+        int _rc = check((call), #call, err, "engine_batch.cu", __LINE__); \
         if (_rc) return _rc;                                       \
     } while (0)
 
@@ -474,8 +474,8 @@ int Engine::batch_finish(htf_stats *stats, double &ms, std::string &err) {
 }
 
 void Engine::trsm_multi(double *v, int nrhs) {
-    k_trsm_fwd_multi<<<nsub_, 256, 0, s_>>>(d_subs_, d_K_, v, nfull_, nrhs);
-    k_trsm_bwd_multi<<<nsub_, 256, 0, s_>>>(d_subs_, d_K_, v, nfull_, nrhs);
+    k_trsm_fwd_multi<<<nsub_, 256, 0, s_>>>(d_subs_, d_K_, v, nfull_, nrhs, nullptr);
+    k_trsm_bwd_multi<<<nsub_, 256, 0, s_>>>(d_subs_, d_K_, v, nfull_, nrhs, nullptr);
 }
 
 int Engine::batch_graph(std::string &err) {

@@ -515,20 +515,26 @@ namespace htf {
 // batched dense triangular solves with the full factor for up to 32
 // right-hand sides at once (the load cases of a batch): the factor is read
 // once per call instead of once per load case.  Column j of subdomain d lives
-// at v + nfull_off + j*ldv.  One CTA of 8 warps per subdomain; warp w owns
-// columns 4w..4w+3, lane = row inside the current 32-row block.  The next
-// 32x32 chunk of L and of X is loaded into registers while the current one
-// is multiplied out of shared memory.
+// at v + nfull_off + j*ld (ld = ldv, or N when ldv <= 0).  One CTA of 8 warps
+// per (subdomain, chunk of 32 columns = blockIdx.y); warp w owns columns
+// 4w..4w+3 of the chunk, lane = row inside the current 32-row block.  The
+// chunk has nrhs columns, or min(32, ncols[d] - 32*blockIdx.y) when ncols is
+// given.  The next 32x32 block of L and of X is loaded into registers while
+// the current one is multiplied out of shared memory.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict__ subs,
                                                         const double *__restrict__ Kbuf, double *__restrict__ v,
-                                                        long long ldv, int nrhs) {
+                                                        long long ldv, int nrhs, const int *__restrict__ ncols) {
     __shared__ double Ls[32][33];
     __shared__ double Xs[32][33];
     __shared__ double rinv[32];
     const SubDev &sd = subs[blockIdx.x];
+    const long long ld = ldv > 0 ? ldv : sd.N;
+    const int c0 = 32 * blockIdx.y;
+    if (ncols) nrhs = min(32, ncols[blockIdx.x] - c0);
+    if (nrhs <= 0) return;
     const double *L = Kbuf + sd.K_off;
-    double *x = v + sd.nfull_off;
+    double *x = v + sd.nfull_off + (size_t)c0 * ld;
     const int N = sd.N, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nblk = (N + 31) / 32;
     for (int b = 0; b < nblk; ++b) {
@@ -541,7 +547,7 @@ __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict
             for (int i = 0; i < 4; ++i) {
                 const int c = w + 8 * i;
                 lr[i] = (lane < nrow) ? L[(kb + lane) + (size_t)(32 * cb + c) * N] : 0.0;
-                xr[i] = (c < nrhs) ? x[(32 * cb + lane) + (size_t)c * ldv] : 0.0;
+                xr[i] = (c < nrhs) ? x[(32 * cb + lane) + (size_t)c * ld] : 0.0;
             }
         };
         if (b > 0) load(0);
@@ -574,7 +580,7 @@ __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int j = 4 * w + q;
-            a[q] = (lane < nrow && j < nrhs) ? x[(kb + lane) + (size_t)j * ldv] - acc[q] : 0.0;
+            a[q] = (lane < nrow && j < nrhs) ? x[(kb + lane) + (size_t)j * ld] - acc[q] : 0.0;
         }
         for (int p = 0; p < nrow; ++p) {
             const double rp = rinv[p], lp = Ls[lane][p];
@@ -588,7 +594,7 @@ __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int j = 4 * w + q;
-            if (lane < nrow && j < nrhs) x[(kb + lane) + (size_t)j * ldv] = a[q];
+            if (lane < nrow && j < nrhs) x[(kb + lane) + (size_t)j * ld] = a[q];
         }
         __syncthreads();
     }
@@ -596,13 +602,17 @@ __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict
 
 __global__ void __launch_bounds__(256) k_trsm_bwd_multi(const SubDev *__restrict__ subs,
                                                         const double *__restrict__ Kbuf, double *__restrict__ v,
-                                                        long long ldv, int nrhs) {
+                                                        long long ldv, int nrhs, const int *__restrict__ ncols) {
     __shared__ double Ls[32][33];
     __shared__ double Xs[32][33];
     __shared__ double rinv[32];
     const SubDev &sd = subs[blockIdx.x];
+    const long long ld = ldv > 0 ? ldv : sd.N;
+    const int c0 = 32 * blockIdx.y;
+    if (ncols) nrhs = min(32, ncols[blockIdx.x] - c0);
+    if (nrhs <= 0) return;
     const double *L = Kbuf + sd.K_off;
-    double *x = v + sd.nfull_off;
+    double *x = v + sd.nfull_off + (size_t)c0 * ld;
     const int N = sd.N, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nblk = (N + 31) / 32;
     for (int b = nblk - 1; b >= 0; --b) {
@@ -616,7 +626,7 @@ __global__ void __launch_bounds__(256) k_trsm_bwd_multi(const SubDev *__restrict
             for (int i = 0; i < 4; ++i) {
                 const int r = w + 8 * i;
                 lr[i] = (c < N && r < nrow) ? L[c + (size_t)(kb + r) * N] : 0.0;
-                xr[i] = (c < N && r < nrhs) ? x[c + (size_t)r * ldv] : 0.0;
+                xr[i] = (c < N && r < nrhs) ? x[c + (size_t)r * ld] : 0.0;
             }
         };
         if (b + 1 < nblk) load(b + 1);
@@ -649,7 +659,7 @@ __global__ void __launch_bounds__(256) k_trsm_bwd_multi(const SubDev *__restrict
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int j = 4 * w + q;
-            a[q] = (lane < nrow && j < nrhs) ? x[(kb + lane) + (size_t)j * ldv] - acc[q] : 0.0;
+            a[q] = (lane < nrow && j < nrhs) ? x[(kb + lane) + (size_t)j * ld] - acc[q] : 0.0;
         }
         for (int p = nrow - 1; p >= 0; --p) {
             const double rp = rinv[p], lp = Ls[p][lane];
@@ -663,7 +673,7 @@ __global__ void __launch_bounds__(256) k_trsm_bwd_multi(const SubDev *__restrict
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int j = 4 * w + q;
-            if (lane < nrow && j < nrhs) x[(kb + lane) + (size_t)j * ldv] = a[q];
+            if (lane < nrow && j < nrhs) x[(kb + lane) + (size_t)j * ld] = a[q];
         }
         __syncthreads();
     }

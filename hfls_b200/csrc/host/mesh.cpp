@@ -70,6 +70,19 @@ int mesh_sizes(const htf_mesh_spec &s, int *nn, int *ne, int *ns, int *nc, int *
     return HTF_OK;
 }
 
+double dense_factor_bytes(const htf_mesh_spec &s) {
+    Axes ax;
+    std::string err;
+    if (make_axes(s, ax, err)) return 0.0;
+    double sum[3] = {0.0, 0.0, 0.0};          // sum of (w+1)^2 over the slabs of each axis
+    for (int a = 0; a < 3; ++a)
+        for (int k = 0; k < ax.NS[a]; ++k) {
+            const double w = ax.bound[a][k + 1] - ax.bound[a][k] + 1;
+            sum[a] += w * w;
+        }
+    return 8.0 * 9.0 * sum[0] * sum[1] * sum[2];
+}
+
 int generate_mesh(const htf_mesh_spec &s, Mesh &m, std::string &err) {
     Axes ax;
     int rc = make_axes(s, ax, err);

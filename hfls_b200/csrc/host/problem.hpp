@@ -31,6 +31,9 @@ struct Mesh {
 
 // Mesh::createMesh generalised (Mesh.cpp:69-289).
 int generate_mesh(const htf_mesh_spec &s, Mesh &m, std::string &err);
+// sum over subdomains of 8 n_d^2 (n_d = 3 x nodes of subdomain d): the dense
+// factors alone, a lower bound of the device footprint of a spec's problem
+double dense_factor_bytes(const htf_mesh_spec &s);
 int mesh_sizes(const htf_mesh_spec &s, int *nn, int *ne, int *ns, int *nc, int *nd, int *ncr,
                std::string &err);
 int mesh_traction(const htf_mesh_spec &s, uint64_t seed, int n_rhs, double scale, double *f,

@@ -163,7 +163,9 @@ int Server::submit(const htf_mesh_spec &spec, int nrhs, const double *f, double 
             r->spec.widths[a] = r->widths[a].data();
         }
     r->nrhs = nrhs;
-    if (f) r->f.assign(f, f + (size_t)3 * nn * nrhs);
+    // the dense factors alone exceed the budget: fail at once, before any host work
+    const double lower = dense_factor_bytes(r->spec);
+    if (f && lower <= budget_) r->f.assign(f, f + (size_t)3 * nn * nrhs);
     r->u_out = u;
     r->info.status = HTF_REQ_QUEUED;
     r->info.n_rhs = nrhs;
@@ -172,6 +174,17 @@ int Server::submit(const htf_mesh_spec &spec, int nrhs, const double *f, double 
     r->id = next_id_++;
     r->info.t_submit_ms = now_ms();
     *ticket = r->id;
+    if (lower > budget_) {
+        r->info.bytes_estimate = lower;
+        r->info.rc = HTF_ENOMEM;
+        r->info.status = HTF_REQ_FAILED;
+        r->info.t_done_ms = r->info.t_submit_ms;
+        r->err = "request needs more than " + std::to_string(size_t(lower) >> 20) +
+                 " MiB for its dense factors, more than the server budget";
+        all_[r->id] = std::move(r);
+        cv_.notify_all();
+        return HTF_OK;
+    }
     ++outstanding_;
     queue_.push_back(r.get());
     all_[r->id] = std::move(r);

@@ -109,3 +109,19 @@ def test_multiple_load_cases():
         ref = o.pcpg(rhs_index=k, eps_iter=1e-10)
         assert abs(st.iterations[k] - ref["iterations"]) <= 2
         assert rel(u[k], ref["u"]) < 1e-8
+
+
+def test_failed_setup_leaves_the_library_usable():
+    """A setup that runs out of device memory (one subdomain of 60^3
+    elements: a 3.7 TB dense factor) fails with HTF_ENOMEM and leaves no CUDA
+    error behind: the next problem sets up and solves."""
+    big = hb.Solver({"typeBc": "cor"})
+    big.set_mesh(hb.generate_mesh(hb.mesh_spec(subs=(1, 1, 1), elems=(60, 60, 60))))
+    with pytest.raises(hb.HTFError) as e:
+        big.setup()
+    assert e.value.code == hb.HTF_ENOMEM
+    big.close()
+    spec, opts = SMALL[0]
+    m, s, o = make(spec, opts)
+    u, st = s.pcpg()
+    assert rel(u[0], o.pcpg()["u"]) < 1e-6
