@@ -347,9 +347,9 @@ int Engine::coarse(Problem &p, std::string &err) {
     for (int c = 0; c < ncl_; ++c) {
         const int nc = p.clu[c].nlam_c, na = 6 * int(p.clu[c].subs.size());
         mF[c] = SubDev{};
-        mF[c].N = nc; mF[c].K_off = oF[c]; mF[c].nfull_off = int(oW[c]);
+        mF[c].N = nc; mF[c].K_off = oF[c]; mF[c].K_bset = -1; mF[c].nfull_off = int(oW[c]);
         mS[c] = SubDev{};
-        mS[c].N = na; mS[c].K_off = oS[c]; mS[c].nfull_off = int(oS[c]);
+        mS[c].N = na; mS[c].K_off = oS[c]; mS[c].K_bset = -1; mS[c].nfull_off = int(oS[c]);
         colsW[c] = nc > 0 ? na + nc : 0;
         colsS[c] = na;
         cp.push_back(CopyDesc{nc, na, 0, nc, nc, dG + oG[c], dW + oW[c], 1.0});                 // W = [Gc | I]

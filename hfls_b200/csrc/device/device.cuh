@@ -4,9 +4,13 @@
 // Per subdomain d (n local DOFs, nb of them touched by Bf = the "b set"):
 //   * local DOFs are permuted to [interior (nr) | b set (nb)], the b set
 //     padded with identity rows to nbp = 32*ceil(nb/32);
-//   * K_d is assembled densely (column-major, ld = N = nr + nbp), lower
-//     triangle, and factored in place: the interior columns are eliminated
-//     first, the trailing block then holds S_reg = K_bb - K_bi K_ii^{-1} K_ib;
+//   * K_d (lower triangle) is stored as column panels, one per 32-column
+//     step of the factorisation: interior steps start at 0, 32, ..; b-set
+//     steps at nr, nr+32, ..; the panel of the step starting at column cb
+//     holds rows [cb, N) of its columns, column-major with ld = N - cb
+//     (kidx below).  It is assembled and factored in place: the interior
+//     columns are eliminated first, the trailing block then holds
+//     S_reg = K_bb - K_bi K_ii^{-1} K_ib;
 //   * F_d = (K_reg^{-1})_bb and the preconditioner block (S_d = S_reg - D_fix
 //     for Dirichlet, K_bb for lumped) are stored as packed lower-triangular
 //     32x32 tiles, tile (I,J) with J<=I at index I(I+1)/2+J, row-major inside
@@ -37,8 +41,10 @@ constexpr int TILE_ELEMS = TILE * TILE;
 
 struct SubDev {
     int n, nr, nb, nbp, nt;               // nt = nbp / 32
-    int N;                                // nr + nbp (dense leading dimension)
-    long long K_off;                      // dense factor (doubles)
+    int N;                                // nr + nbp (order of the factor)
+    long long K_off;                      // factor panels (doubles)
+    long long K_bset;                     // offset of the first b-set panel from K_off;
+                                          // < 0: plain column-major N x N (ld = N)
     long long T_off;                      // packed tiles: first tile index (F and S/Kbb share it)
     long long X_off;                      // nbp x nbp scratch (L_bb^{-1}) during setup
     int xb_off;                           // offset of the b block in b-space vectors
@@ -62,6 +68,45 @@ struct ClusterDev {
     int gc_off;                           // offset in the concatenated coarse vectors
     int gmap_off;                         // gather map: ptr array offset (ngc+1 entries)
 };
+
+#ifdef __CUDACC__
+#define HTF_HD __host__ __device__ __forceinline__
+#else
+#define HTF_HD inline
+#endif
+
+// doubles of the factor panels of a subdomain with nr interior DOFs and
+// nbp padded b-set DOFs, and the offset of its first b-set panel
+HTF_HD long long kpanel_interior(int nr, int N) {
+    const long long nI = (nr + 31) / 32;
+    if (nI == 0) return 0;
+    const long long last = nI - 1, wl = nr - 32 * last;
+    return 32 * last * N - 512 * last * (last - 1) + wl * (N - 32 * last);
+}
+HTF_HD long long kpanel_doubles(int nr, int nbp) {
+    const long long nt = nbp / 32;
+    return kpanel_interior(nr, nr + nbp) + 512 * nt * (nt + 1);
+}
+
+// Address of factor entry (r, c), r >= c, of subdomain s
+HTF_HD long long kcol(const SubDev &s, int c) {     // address of (0, c) if it were stored: add r
+    if (s.K_bset < 0) return s.K_off + (long long)c * s.N;     // plain column-major N x N
+    long long base;
+    int cb;
+    if (c < s.nr) {
+        const long long b = c >> 5;
+        cb = int(b << 5);
+        base = 32 * b * s.N - 512 * b * (b - 1);
+    } else {
+        const long long j = (c - s.nr) >> 5;
+        cb = s.nr + int(j << 5);
+        base = s.K_bset + 32 * j * s.nbp - 512 * j * (j - 1);
+    }
+    return s.K_off + base + (long long)(c - cb) * (s.N - cb) - cb;
+}
+HTF_HD long long kidx(const SubDev &s, int r, int c) { return kcol(s, c) + r; }
+// leading dimension of the panel of the step starting at column k
+HTF_HD long long kld(const SubDev &s, int k) { return s.K_bset < 0 ? s.N : s.N - k; }
 
 // One SYMV work unit: packed tiles [t0, t1) of subdomain d (kind 0), or the
 // V^T x_b product of subdomain d (kind 1).  Units write partial y sums for

@@ -226,6 +226,9 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     nlam_ = p.n_lam;
     hs_.assign(nsub_, SubDev());
     long long K_off = 0, T_off = 0, X_off = 0, V_off = 0, R_off = 0;
+    const long long XWAVE = 1LL << 29;           // 4 GiB
+    xwave_.assign(1, 0);
+    xwave_max_ = 0;
     int xb = 0, nf = 0, t_off = 0, bcr = 0, bce = 0;
     for (int d = 0; d < nsub_; ++d) {
         const Subdomain &s = p.sub[d];
@@ -234,9 +237,17 @@ int Engine::upload_layout(Problem &p, std::string &err) {
         h.nt = (s.nb + TILE - 1) / TILE;
         h.nbp = h.nt * TILE;
         h.N = h.nr + h.nbp;
-        h.K_off = K_off; K_off += (long long)h.N * h.N;
+        h.K_off = K_off; K_off += kpanel_doubles(h.nr, h.nbp);
+        h.K_bset = kpanel_interior(h.nr, h.N);
         h.T_off = T_off; T_off += (long long)h.nt * (h.nt + 1) / 2;
-        h.X_off = X_off; X_off += (long long)h.nbp * h.nbp;
+        // L_bb^{-1} scratch of the F_i set-up, in waves of subdomains of at most XWAVE doubles
+        const long long xs = (long long)h.nbp * h.nbp;
+        if (X_off > 0 && X_off + xs > XWAVE) {
+            xwave_.push_back(d);
+            X_off = 0;
+        }
+        h.X_off = X_off; X_off += xs;
+        xwave_max_ = std::max(xwave_max_, X_off);
         h.xb_off = xb; xb += h.nbp;
         h.nfull_off = nf; nf += h.N;
         h.c = s.c();
@@ -254,6 +265,7 @@ int Engine::upload_layout(Problem &p, std::string &err) {
         h.R_off = R_off; R_off += (long long)h.N * 6;
         for (int q = 0; q < 6; ++q) { h.fix[q] = s.perm[s.fix[q]]; h.fix_diag[q] = 0.0; }
     }
+    xwave_.push_back(nsub_);
     nslots_ = xb;
     nfull_ = nf;
     ntiles_ = T_off;
@@ -300,7 +312,6 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     d_K_ = alloc<double>(K_off, err, rc);
     d_F_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);
     d_S_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);
-    d_X_ = alloc<double>(X_off, err, rc);
     d_V_ = alloc<double>(V_off, err, rc);
     d_R_ = alloc<double>(R_off, err, rc);
     d_M_ = alloc<double>(M_off, err, rc);
@@ -456,6 +467,7 @@ int Engine::factorize(Problem &p, std::string &err) {
     // element data: coordinates, permuted DOF positions, colours
     std::vector<double> ec(24 * (size_t)ne);
     std::vector<int> ep(24 * (size_t)ne);
+#pragma omp parallel for schedule(dynamic, 4)
     for (int d = 0; d < nsub_; ++d) {
         const Subdomain &s = p.sub[d];
         for (int e : s.elems) {
@@ -507,7 +519,7 @@ int Engine::factorize(Problem &p, std::string &err) {
     CK(cudaMemcpyAsync(d_subs_, hs_.data(), nsub_ * sizeof(SubDev), cudaMemcpyHostToDevice, s_));
     CK(set_gauss_points(s_));
     long long Ktot = 0;
-    for (auto &h : hs_) Ktot += (long long)h.N * h.N;
+    for (auto &h : hs_) Ktot += kpanel_doubles(h.nr, h.nbp);
     CK(cudaMemsetAsync(d_K_, 0, Ktot * sizeof(double), s_));
     CK(cudaMemsetAsync(d_f_, 0, (size_t)nfull_ * p.nrhs * sizeof(double), s_));
     for (int c = 0; c < ncol; ++c) {
@@ -579,12 +591,27 @@ int Engine::factorize(Problem &p, std::string &err) {
             k_snapshot<<<dim3(int(snap_after[s].size()), max_tiles), 256, 0, s_>>>(d_snap + snap_off[s], d_subs_, d_K_, d_S_);
         CK(cudaGetLastError());
     }
-    // X = L_bb^{-1}, F = X^T X
-    for (int i = 0; i < max_nt; ++i)
-        k_trtri_step<<<dim3(nsub_, i + 1), 256, 0, s_>>>(i, d_all_subs_, d_subs_, d_K_, d_X_);
-    CK(cudaGetLastError());
-    k_lauum_tiles<<<dim3(nsub_, max_tiles), 256, 0, s_>>>(d_all_subs_, d_subs_, d_X_, d_F_);
-    CK(cudaGetLastError());
+    // X = L_bb^{-1}, F = X^T X, in waves of subdomains sharing one scratch buffer
+    {
+        double *X = nullptr;
+        CK(cudaMalloc(&X, std::max<long long>(xwave_max_, 1) * sizeof(double)));
+        for (size_t w = 0; w + 1 < xwave_.size(); ++w) {
+            const int a = xwave_[w], b = xwave_[w + 1];
+            int wnt = 0, wtiles = 0;
+            for (int d = a; d < b; ++d) {
+                wnt = std::max(wnt, hs_[d].nt);
+                wtiles = std::max(wtiles, hs_[d].nt * (hs_[d].nt + 1) / 2);
+            }
+            for (int i = 0; i < wnt; ++i)
+                k_trtri_step<<<dim3(b - a, i + 1), 256, 0, s_>>>(i, d_all_subs_ + a, d_subs_, d_K_, X);
+            k_lauum_tiles<<<dim3(b - a, wtiles), 256, 0, s_>>>(d_all_subs_ + a, d_subs_, X, d_F_);
+        }
+        const cudaError_t le = cudaGetLastError();
+        const cudaError_t se = cudaStreamSynchronize(s_);
+        cudaFree(X);
+        CK(le);
+        CK(se);
+    }
     int max_cols = 0;
     for (auto &h : hs_) max_cols = std::max(max_cols, h.c + 6);
     k_build_V<<<dim3(nsub_, max_cols), 256, 0, s_>>>(d_subs_, d_F_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_R_, d_V_);

@@ -113,7 +113,9 @@ private:
     SubDev *d_subs_ = nullptr;
     ClusterDev *d_cl_ = nullptr;
     int *d_all_subs_ = nullptr;          // 0..nsub-1
-    double *d_K_ = nullptr, *d_F_ = nullptr, *d_S_ = nullptr, *d_X_ = nullptr;
+    double *d_K_ = nullptr, *d_F_ = nullptr, *d_S_ = nullptr;
+    std::vector<int> xwave_;             // subdomain boundaries of the L_bb^{-1} scratch waves
+    long long xwave_max_ = 0;            // doubles of the largest wave
     double *d_V_ = nullptr, *d_R_ = nullptr, *d_M_ = nullptr, *d_H_ = nullptr;
     int *d_bcr_ = nullptr, *d_bce_ptr_ = nullptr, *d_bce_pos_ = nullptr;
     double *d_bce_val_ = nullptr;

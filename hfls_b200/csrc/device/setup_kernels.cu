@@ -104,7 +104,6 @@ __global__ void k_assemble(const int *__restrict__ elist, int count, const doubl
     const double E = subE[d], nu = subnu[d];
     const double lam = E * nu / ((1. + nu) * (1. - 2. * nu));
     const double mu = E / (2. * (1. + nu));
-    double *K = Kbuf + sd.K_off;
     for (int idx = t; idx < 576; idx += blockDim.x) {
         const int I = idx % 24, J = idx / 24;
         const int pI = P[I], pJ = P[J];
@@ -116,7 +115,7 @@ __global__ void k_assemble(const int *__restrict__ elist, int count, const doubl
             if (i == j) s += mu * (G[g][a][0] * G[g][b][0] + G[g][a][1] * G[g][b][1] + G[g][a][2] * G[g][b][2]);
             v += s * W[g];
         }
-        K[pI + (size_t)pJ * sd.N] += v;
+        Kbuf[kidx(sd, pI, pJ)] += v;
     }
     if (t < 24) {
         const int i = t >> 3, a = t & 7;
@@ -133,14 +132,14 @@ __global__ void k_regularize(SubDev *subs, int nsub, double *Kbuf) {
     const int d = blockIdx.x;
     if (d >= nsub) return;
     SubDev &sd = subs[d];
-    double *K = Kbuf + sd.K_off;
     if (threadIdx.x < 6) {
         const int f = sd.fix[threadIdx.x];
-        const double v = K[f + (size_t)f * sd.N];
+        const long long a = kidx(sd, f, f);
+        const double v = Kbuf[a];
         sd.fix_diag[threadIdx.x] = v;
-        K[f + (size_t)f * sd.N] = 2.0 * v;
+        Kbuf[a] = 2.0 * v;
     }
-    for (int r = sd.nr + sd.nb + threadIdx.x; r < sd.N; r += blockDim.x) K[r + (size_t)r * sd.N] = 1.0;
+    for (int r = sd.nr + sd.nb + threadIdx.x; r < sd.N; r += blockDim.x) Kbuf[kidx(sd, r, r)] = 1.0;
 }
 
 // ---------------------------------------------------------------------------
@@ -151,9 +150,10 @@ __global__ void k_potrf_diag(const StepDesc *__restrict__ st, const SubDev *__re
     __shared__ double A[32][33];
     const StepDesc s = st[blockIdx.x];
     const SubDev &sd = subs[s.d];
-    double *K = Kbuf + sd.K_off;
-    const int N = sd.N, k = s.k, nb = s.nb, lane = threadIdx.x;
-    for (int c = 0; c < nb; ++c) A[lane][c] = (lane < nb) ? K[(k + lane) + (size_t)(k + c) * N] : 0.0;
+    double *K = Kbuf + kidx(sd, s.k, s.k);        // the step's panel: entry (k+i, k+j) at K[i + j*ld]
+    const int k = s.k, nb = s.nb, lane = threadIdx.x;
+    const long long ld = kld(sd, k);
+    for (int c = 0; c < nb; ++c) A[lane][c] = (lane < nb) ? K[lane + c * ld] : 0.0;
     __syncwarp();
     for (int j = 0; j < nb; ++j) {
         if (lane == j) {
@@ -175,7 +175,7 @@ __global__ void k_potrf_diag(const StepDesc *__restrict__ st, const SubDev *__re
         __syncwarp();
     }
     if (lane < nb)
-        for (int c = 0; c <= lane; ++c) K[(k + lane) + (size_t)(k + c) * N] = A[lane][c];
+        for (int c = 0; c <= lane; ++c) K[lane + c * ld] = A[lane][c];
 }
 
 __global__ void k_trsm_panel(const StepDesc *__restrict__ st, const SubDev *__restrict__ subs,
@@ -183,18 +183,19 @@ __global__ void k_trsm_panel(const StepDesc *__restrict__ st, const SubDev *__re
     __shared__ double L[32][33];
     const StepDesc s = st[blockIdx.x];
     const SubDev &sd = subs[s.d];
-    double *K = Kbuf + sd.K_off;
+    double *K = Kbuf + kidx(sd, s.k, s.k);        // the step's panel: entry (k+i, k+j) at K[i + j*ld]
     const int N = sd.N, k = s.k, nb = s.nb;
+    const long long ld = kld(sd, k);
     for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
         const int r = i % 32, c = i / 32;
-        L[r][c] = (r < nb && c < nb && c <= r) ? K[(k + r) + (size_t)(k + c) * N] : 0.0;
+        L[r][c] = (r < nb && c < nb && c <= r) ? K[r + c * ld] : 0.0;
     }
     __syncthreads();
     const int row = k + nb + blockIdx.y * blockDim.x + threadIdx.x;
     if (row >= N) return;
     double x[32];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) x[j] = (j < nb) ? K[row + (size_t)(k + j) * N] : 0.0;
+    for (int j = 0; j < 32; ++j) x[j] = (j < nb) ? K[(row - k) + j * ld] : 0.0;
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
         if (j < nb) {
@@ -206,7 +207,7 @@ __global__ void k_trsm_panel(const StepDesc *__restrict__ st, const SubDev *__re
     }
 #pragma unroll
     for (int j = 0; j < 32; ++j)
-        if (j < nb) K[row + (size_t)(k + j) * N] = x[j];
+        if (j < nb) K[(row - k) + j * ld] = x[j];
 }
 
 // C(64x64 block, lower part of the trailing matrix) -= P_i P_j^T, P = panel
@@ -228,12 +229,13 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
     while (bi * (bi + 1) / 2 > tri) --bi;
     const int bj = tri - bi * (bi + 1) / 2;
     const int i0 = t0 + 64 * bi, j0 = t0 + 64 * bj;
-    double *K = Kbuf + sd.K_off;
+    const double *P = Kbuf + kidx(sd, k, k);       // the step's panel: entry (k+i, k+j) at P[i + j*ld]
+    const long long ld = kld(sd, k);
     for (int idx = threadIdx.x; idx < 32 * 64; idx += 256) {
         const int r = idx % 64, kk = idx / 64;
         const bool ok = kk < nb;
-        Pa[kk][r] = (ok && i0 + r < N) ? K[(i0 + r) + (size_t)(k + kk) * N] : 0.0;
-        Pb[kk][r] = (ok && j0 + r < N) ? K[(j0 + r) + (size_t)(k + kk) * N] : 0.0;
+        Pa[kk][r] = (ok && i0 + r < N) ? P[(i0 + r - k) + kk * ld] : 0.0;
+        Pb[kk][r] = (ok && j0 + r < N) ? P[(j0 + r - k) + kk * ld] : 0.0;
     }
     __syncthreads();
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -257,11 +259,12 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
     for (int b = 0; b < 4; ++b) {
         const int col = j0 + ty + 16 * b;
         if (col >= N) continue;
+        double *C = Kbuf + kcol(sd, col);
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
             const int row = i0 + tx + 16 * a;
             if (row >= N || row < col) continue;
-            K[row + (size_t)col * N] -= acc[a][b];
+            C[row] -= acc[a][b];
         }
     }
 }
@@ -276,13 +279,12 @@ __global__ void k_snapshot(const int *__restrict__ dlist, const SubDev *__restri
     while ((I + 1) * (I + 2) / 2 <= tile) ++I;
     while (I * (I + 1) / 2 > tile) --I;
     const int J = tile - I * (I + 1) / 2;
-    const double *K = Kbuf + sd.K_off;
     double *T = Sbuf + (sd.T_off + tile) * TILE_ELEMS;
     for (int idx = threadIdx.x; idx < TILE_ELEMS; idx += blockDim.x) {
         const int r = idx / TILE, c = idx % TILE;
         int gr = sd.nr + TILE * I + r, gc = sd.nr + TILE * J + c;
         if (gr < gc) { int tmp = gr; gr = gc; gc = tmp; }
-        double v = K[gr + (size_t)gc * sd.N];
+        double v = Kbuf[kidx(sd, gr, gc)];
         if (gr == gc)
             for (int q = 0; q < 6; ++q)
                 if (sd.fix[q] == gr) v -= sd.fix_diag[q];
@@ -304,7 +306,6 @@ __global__ void __launch_bounds__(256) k_trtri_step(int i, const int *__restrict
     const int j = blockIdx.y;
     if (i >= sd.nt || j > i) return;
     const int N = sd.N, nbp = sd.nbp, base = sd.nr;
-    const double *K = Kbuf + sd.K_off;
     double *X = Xbuf + sd.X_off;
     const int tid = threadIdx.x;
     const int r = tid % 32, c0 = (tid / 32) * 4;
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(256) k_trtri_step(int i, const int *__restrict
     for (int kb = j; kb < i; ++kb) {
         for (int idx = tid; idx < 1024; idx += 256) {
             const int rr = idx % 32, cc = idx / 32;
-            La[rr][cc] = K[(base + 32 * i + rr) + (size_t)(base + 32 * kb + cc) * N];
+            La[rr][cc] = Kbuf[kidx(sd, base + 32 * i + rr, base + 32 * kb + cc)];
             Xb[rr][cc] = X[(32 * kb + rr) + (size_t)(32 * j + cc) * nbp];
         }
         __syncthreads();
@@ -330,7 +331,7 @@ __global__ void __launch_bounds__(256) k_trtri_step(int i, const int *__restrict
     for (int cc = 0; cc < 4; ++cc) T[r][c0 + cc] = acc[cc];
     for (int idx = tid; idx < 1024; idx += 256) {
         const int rr = idx % 32, cc = idx / 32;
-        La[rr][cc] = (cc <= rr) ? K[(base + 32 * i + rr) + (size_t)(base + 32 * i + cc) * N] : 0.0;
+        La[rr][cc] = (cc <= rr) ? Kbuf[kidx(sd, base + 32 * i + rr, base + 32 * i + cc)] : 0.0;
     }
     __syncthreads();
     if (tid < 32) {                        // forward substitution, one column per thread
@@ -443,7 +444,6 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(const SubDev *__restrict__ sub
     __shared__ double part[8][32];
     __shared__ double xs[32];
     const SubDev &sd = subs[blockIdx.x];
-    const double *L = Kbuf + sd.K_off;
     double *x = v + sd.nfull_off + (size_t)blockIdx.y * ldv;
     const int N = sd.N, lane = threadIdx.x % 32, w = threadIdx.x / 32;
     for (int kb = 0; kb < N; kb += 32) {
@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(const SubDev *__restrict__ sub
         double acc = 0.0;
         const int row = kb + lane;
         if (lane < nrow)
-            for (int c = w; c < kb; c += 8) acc += L[row + (size_t)c * N] * x[c];
+            for (int c = w; c < kb; c += 8) acc += Kbuf[kidx(sd, row, c)] * x[c];
         part[w][lane] = acc;
         __syncthreads();
         if (w == 0) {
@@ -459,10 +459,10 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(const SubDev *__restrict__ sub
             for (int q = 0; q < 8; ++q) a -= part[q][lane];
             for (int q = 0; q < nrow; ++q) {
                 double xq = 0.0;
-                if (lane == q) xq = a / L[row + (size_t)row * N];
+                if (lane == q) xq = a / Kbuf[kidx(sd, row, row)];
                 xq = __shfl_sync(0xffffffffu, xq, q);
                 if (lane == q) xs[q] = xq;
-                if (lane > q && lane < nrow) a -= L[row + (size_t)(kb + q) * N] * xq;
+                if (lane > q && lane < nrow) a -= Kbuf[kidx(sd, row, kb + q)] * xq;
             }
             __syncwarp();
             if (lane < nrow) x[row] = xs[lane];
@@ -476,7 +476,6 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(const SubDev *__restrict__ sub
                                                   long long ldv) {
     __shared__ double acc_s[32];
     const SubDev &sd = subs[blockIdx.x];
-    const double *L = Kbuf + sd.K_off;
     double *x = v + sd.nfull_off + (size_t)blockIdx.y * ldv;
     const int N = sd.N, lane = threadIdx.x % 32, w = threadIdx.x / 32;
     const int nblk = (N + 31) / 32;
@@ -484,7 +483,7 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(const SubDev *__restrict__ sub
         const int kb = 32 * b, nrow = min(32, N - kb);
         // acc[r] = x[kb+r] - sum_{c >= kb+nrow} L[c][kb+r] x[c]
         for (int r = w; r < nrow; r += 8) {
-            const double *col = L + (size_t)(kb + r) * N;
+            const double *col = Kbuf + kcol(sd, kb + r);
             double s = 0.0;
             for (int c = kb + nrow + lane; c < N; c += 32) s += col[c] * x[c];
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -495,10 +494,10 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(const SubDev *__restrict__ sub
             double a = (lane < nrow) ? acc_s[lane] : 0.0;
             for (int q = nrow - 1; q >= 0; --q) {
                 double xq = 0.0;
-                if (lane == q) xq = a / L[(kb + q) + (size_t)(kb + q) * N];
+                if (lane == q) xq = a / Kbuf[kidx(sd, kb + q, kb + q)];
                 xq = __shfl_sync(0xffffffffu, xq, q);
                 if (lane == q) acc_s[q] = xq;
-                if (lane < q) a -= L[(kb + q) + (size_t)(kb + lane) * N] * xq;
+                if (lane < q) a -= Kbuf[kidx(sd, kb + q, kb + lane)] * xq;
             }
             __syncwarp();
             if (lane < nrow) x[kb + lane] = acc_s[lane];
@@ -533,7 +532,6 @@ __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict
     const int c0 = 32 * blockIdx.y;
     if (ncols) nrhs = min(32, ncols[blockIdx.x] - c0);
     if (nrhs <= 0) return;
-    const double *L = Kbuf + sd.K_off;
     double *x = v + sd.nfull_off + (size_t)c0 * ld;
     const int N = sd.N, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nblk = (N + 31) / 32;
@@ -546,7 +544,7 @@ __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int c = w + 8 * i;
-                lr[i] = (lane < nrow) ? L[(kb + lane) + (size_t)(32 * cb + c) * N] : 0.0;
+                lr[i] = (lane < nrow) ? Kbuf[kidx(sd, kb + lane, 32 * cb + c)] : 0.0;
                 xr[i] = (c < nrhs) ? x[(32 * cb + lane) + (size_t)c * ld] : 0.0;
             }
         };
@@ -571,7 +569,7 @@ __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int c = w + 8 * i;
-            Ls[lane][c] = (lane < nrow && c <= lane) ? L[(kb + lane) + (size_t)(kb + c) * N] : 0.0;
+            Ls[lane][c] = (lane < nrow && c <= lane) ? Kbuf[kidx(sd, kb + lane, kb + c)] : 0.0;
         }
         __syncthreads();
         if (threadIdx.x < 32) rinv[lane] = (lane < nrow) ? 1.0 / Ls[lane][lane] : 0.0;
@@ -611,7 +609,6 @@ __global__ void __launch_bounds__(256) k_trsm_bwd_multi(const SubDev *__restrict
     const int c0 = 32 * blockIdx.y;
     if (ncols) nrhs = min(32, ncols[blockIdx.x] - c0);
     if (nrhs <= 0) return;
-    const double *L = Kbuf + sd.K_off;
     double *x = v + sd.nfull_off + (size_t)c0 * ld;
     const int N = sd.N, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nblk = (N + 31) / 32;
@@ -625,7 +622,7 @@ __global__ void __launch_bounds__(256) k_trsm_bwd_multi(const SubDev *__restrict
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int r = w + 8 * i;
-                lr[i] = (c < N && r < nrow) ? L[c + (size_t)(kb + r) * N] : 0.0;
+                lr[i] = (c < N && r < nrow) ? Kbuf[kidx(sd, c, kb + r)] : 0.0;
                 xr[i] = (c < N && r < nrhs) ? x[c + (size_t)r * ld] : 0.0;
             }
         };
@@ -650,7 +647,7 @@ __global__ void __launch_bounds__(256) k_trsm_bwd_multi(const SubDev *__restrict
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int r = w + 8 * i;
-            Ls[lane][r] = (lane < nrow && r <= lane) ? L[(kb + lane) + (size_t)(kb + r) * N] : 0.0;
+            Ls[lane][r] = (lane < nrow && r <= lane) ? Kbuf[kidx(sd, kb + lane, kb + r)] : 0.0;
         }
         __syncthreads();
         if (threadIdx.x < 32) rinv[lane] = (lane < nrow) ? 1.0 / Ls[lane][lane] : 0.0;

@@ -215,9 +215,11 @@ int build_problem(Problem &p, std::string &err) {
         if (p.clu[c].subs.empty()) { err = "cluster without subdomains"; return HTF_EINVAL; }
     for (int e = 0; e < ne; ++e) p.sub[m.elem_sub[e]].elems.push_back(e);
     // l2g (Data.cpp:111-144)
+    for (int d = 0; d < ns; ++d)
+        if (p.sub[d].elems.empty()) { err = "subdomain without elements"; return HTF_EINVAL; }
+#pragma omp parallel for schedule(dynamic, 4)
     for (int d = 0; d < ns; ++d) {
         Subdomain &s = p.sub[d];
-        if (s.elems.empty()) { err = "subdomain without elements"; return HTF_EINVAL; }
         std::vector<int> &l = s.l2g;
         l.reserve(s.elems.size() * 24);
         for (int e : s.elems)
@@ -276,14 +278,36 @@ int build_problem(Problem &p, std::string &err) {
                 }
             }
         }
-    for (int d = 0; d < ns; ++d)
-        for (int g : m.dirichlet) {
+    {
+        // Dirichlet rows in the order (subdomain, position in the Dirichlet list)
+        std::vector<std::vector<int>> drows(ns);
+        std::vector<int> dpos(3 * size_t(m.n_nodes), -1);    // position in the Dirichlet list
+        bool dup = false;
+        for (size_t i = 0; i < m.dirichlet.size(); ++i) {
+            int &q = dpos[m.dirichlet[i]];
+            if (q >= 0) dup = true;
+            else q = int(i);
+        }
+#pragma omp parallel for schedule(dynamic, 4)
+        for (int d = 0; d < ns; ++d) {
             const std::vector<int> &l = p.sub[d].l2g;
-            if (std::binary_search(l.begin(), l.end(), g)) {
+            if (dup) {                 // a DOF listed twice gives two rows, as the reference's scan does
+                for (int g : m.dirichlet)
+                    if (std::binary_search(l.begin(), l.end(), g)) drows[d].push_back(g);
+            } else {
+                std::vector<std::pair<int, int>> hit;
+                for (int g : l)
+                    if (dpos[g] >= 0) hit.push_back({dpos[g], g});
+                std::sort(hit.begin(), hit.end());
+                for (auto &h : hit) drows[d].push_back(h.second);
+            }
+        }
+        for (int d = 0; d < ns; ++d)
+            for (int g : drows[d]) {
                 p.rows.push_back(BfRow{{d, -1}, {g, -1}, {1.0, 0.0}});
                 p.weight.push_back(1);
             }
-        }
+    }
     p.n_lam = int(p.rows.size());
     if (p.n_lam == 0) { err = "no dual rows (no interface and no Dirichlet DOF)"; return HTF_EINVAL; }
     // b sets, permutation and Bf gather CSR
@@ -295,6 +319,8 @@ int build_problem(Problem &p, std::string &err) {
                 if (d < 0) continue;
                 ent[d].push_back({local_of(d, p.rows[r].dof[k]), {r, p.rows[r].sign[k]}});
             }
+        int few = -1;
+#pragma omp parallel for schedule(dynamic, 4)
         for (int d = 0; d < ns; ++d) {
             Subdomain &s = p.sub[d];
             std::sort(ent[d].begin(), ent[d].end());
@@ -319,10 +345,15 @@ int build_problem(Problem &p, std::string &err) {
                 s.bf_sign.push_back(e.second.second);
             }
             for (int i = 0; i < s.nb; ++i) s.bf_ptr[i + 1] += s.bf_ptr[i];
-            if (s.nb < 6) { err = "subdomain with fewer than 6 interface/Dirichlet DOFs"; return HTF_EINVAL; }
+            if (s.nb < 6) {
+#pragma omp critical
+                few = (few < 0 || d < few) ? d : few;
+            }
         }
+        if (few >= 0) { err = "subdomain with fewer than 6 interface/Dirichlet DOFs"; return HTF_EINVAL; }
     }
     // kernels and fix DOFs
+#pragma omp parallel for schedule(dynamic, 4)
     for (int d = 0; d < ns; ++d) {
         Subdomain &s = p.sub[d];
         kernel_of(m, s.l2g, s.R);

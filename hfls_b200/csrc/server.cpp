@@ -221,15 +221,18 @@ int Server::wait(long long ticket, double timeout_ms, htf_request_info *out) {
 // with a margin
 size_t Server::estimate(const Problem &p, int nrhs) const {
     const double K = opt_.batch;
-    double b = 0.0, nslots = 0.0, nfull = 0.0;
+    double b = 0.0, nslots = 0.0, nfull = 0.0, xs = 0.0;
     for (const Subdomain &s : p.sub) {
         const double nbp = 32.0 * ((s.nb + 31) / 32), N = (s.n - s.nb) + nbp, nt = nbp / 32;
         const double mb = std::ceil(nbp / 128.0), nks = nbp / 32;
-        b += 8.0 * (N * N + nt * (nt + 1) * 1024.0 + nbp * nbp + nbp * (s.c() + 6) + 6 * N + 2 * nbp);
+        b += 8.0 * (double(kpanel_doubles(s.n - s.nb, int(nbp))) + nt * (nt + 1) * 1024.0 +
+                    nbp * (s.c() + 6) + 6 * N + 2 * nbp);
+        xs += nbp * nbp;
         b += 2.0 * mb * nks * 4096.0 * 4.0;
         nslots += nbp;
         nfull += N;
     }
+    b += 8.0 * std::min(xs, double(1LL << 29));           // L_bb^{-1} scratch of the set-up (one wave)
     for (const Cluster &c : p.clu) b += 8.0 * double(c.ngc()) * c.ngc();
     const double nl = p.n_lam;
     b += nl * 8.0 * (11.0 * K + 12.0) + nslots * (K * (8.0 * 2 + 4.0 * 2) + 8.0 * 4) + nfull * 8.0 * (nrhs + 3);
