@@ -1,0 +1,114 @@
+"""The batched uneven configuration at full size on the GPU: 8 clusters of
+8x8x8 subdomains on a non-uniform grid whose slab widths (elements per
+subdomain per axis) are drawn from {4..12} (seed 0), E log-uniform in
+[1, 1e4] per subdomain, clamped face x = 0, body force (0, 0, -1): 4096
+subdomains of 375-6591 DOFs, about 6.3 M global DOFs, FP64.
+
+The oracle cannot solve a problem of this size, so the test solves at
+eps 1e-10 and checks properties that hold at any size:
+  * PCPG stops on the reference's criterion (sqrt(g'Pz) < eps sqrt(g0'Pz0));
+  * the clamped DOFs stay at zero (within 1e-7 of max |u|: the Dirichlet
+    rows hold to the dual residual);
+  * nodal equilibrium: at 3000 sampled nodes off the clamped face, the sum of
+    the element forces K_e u_e of the elements around the node equals the
+    nodal body-force load (element matrices from the oracle's hex8 element),
+    relative to the largest element-force sum among the sampled nodes,
+    within 1e-5 (an oracle solve of the small case reaches 5e-7 at
+    eps 1e-10 and 4e-5 at eps 1e-8).
+The same construction at a size the oracle solves is checked against it in
+test_uneven_widths_small_matches_oracle."""
+import numpy as np
+import pytest
+
+import hfls_b200 as hb
+from oracle.htfeti_oracle import HTFETI, MeshArrays, Options, element_dofs, hex8_element
+
+pytestmark = pytest.mark.gpu
+
+OPTS = {"typeBc": "cor", "preconditioner": "Dirichlet_explicit", "eps_iter": "1e-8", "max_iter": "5000"}
+
+
+def widths(n, seed, lo=4, hi=12):
+    rng = np.random.default_rng(seed)
+    return [rng.integers(lo, hi + 1, n).astype(np.int32) for _ in range(3)]
+
+
+def spec_uneven(clusters, subs, w, seed=0):
+    return hb.mesh_spec(clusters=clusters, subs=subs, widths=w, jitter=0.1, seed=seed,
+                        material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e4, nu=0.3, bc=hb.HTF_BC_CLAMP_X0,
+                        body_force=(0.0, 0.0, -1.0))
+
+
+def nodal_equilibrium(m, u, nodes):
+    """max over the given nodes of |sum_e K_e u_e - f_e| (3 DOFs each),
+    relative to the largest sum_e |K_e u_e| + |f_e| among them."""
+    el = m.elems.astype(np.int64)
+    flat = el.ravel()
+    order = np.argsort(flat, kind="stable")
+    srt = flat[order]
+    starts = np.searchsorted(srt, nodes, side="left")
+    ends = np.searchsorted(srt, nodes, side="right")
+    res, scale = 0.0, 0.0
+    for a, b in zip(starts, ends):
+        es = order[a:b] // 8
+        loc = order[a:b] % 8
+        Ke, fe = hex8_element(m.coords[el[es]], m.sub_E[m.elem_sub[es]], m.sub_nu[m.elem_sub[es]], m.body_force)
+        Fe = np.einsum("eij,ej->ei", Ke, u[element_dofs(el[es])])
+        rows = np.stack([loc, loc + 8, loc + 16], axis=1)
+        k = np.arange(len(es))[:, None]
+        r = (Fe[k, rows] - fe[k, rows]).sum(axis=0)
+        res = max(res, float(np.max(np.abs(r))))
+        scale = max(scale, float(np.max((np.abs(Fe[k, rows]) + np.abs(fe[k, rows])).sum(axis=0))))
+    return res / scale
+
+
+def test_uneven_widths_full_size():
+    w = widths(16, seed=0)
+    spec = spec_uneven((2, 2, 2), (8, 8, 8), w)
+    m = hb.generate_mesh(spec)
+    assert m.n_sub == 4096
+    s = hb.Solver(dict(OPTS, eps_iter="1e-10"))
+    s.set_mesh(m)
+    s.setup()
+    u, st = s.pcpg()
+    u = u[0]
+    assert st.iterations[0] < 5000
+    assert st.final_rel[0] < 1e-10
+    umax = np.max(np.abs(u))
+    assert umax > 0
+    assert np.max(np.abs(u[m.dirichlet])) < 1e-7 * umax
+    clamped = np.zeros(m.n_nodes, bool)
+    clamped[m.dirichlet // 3] = True
+    rng = np.random.default_rng(1)
+    nodes = rng.choice(np.flatnonzero(~clamped), 3000, replace=False)
+    assert nodal_equilibrium(m, u, nodes) < 1e-5
+
+
+def test_uneven_widths_small_matches_oracle():
+    """Same construction (uneven widths from {2..4}, 8 clusters, E contrast
+    1e4) at 2x2x2 subdomains per cluster against the oracle.  This mesh is
+    ill-conditioned enough that PCPG iteration counts move with round-off:
+    the oracle alone gives 516 or 522 iterations at eps 1e-8 depending on the
+    BLAS build it runs on.  So iterations agree within 2 % at eps 1e-8, and
+    the displacements at eps 1e-10 are within 1e-8 of the oracle's at eps
+    1e-12 (an oracle solve at eps 1e-10 is within 4e-9 of it)."""
+    w = widths(4, seed=3, lo=2, hi=4)
+    spec = spec_uneven((2, 2, 2), (2, 2, 2), w, seed=3)
+    m = hb.generate_mesh(spec)
+    o = HTFETI(MeshArrays(m.coords, m.elems.astype(np.int64), m.elem_sub.astype(np.int64),
+                          m.sub_cluster.astype(np.int64), m.sub_E, m.sub_nu, m.dirichlet.astype(np.int64),
+                          m.corner.astype(np.int64), m.body_force),
+               Options(typeBc="cor", fix_rule="boundary", kerGc="analytic"))
+    s8 = hb.Solver(OPTS)
+    s8.set_mesh(m)
+    s8.setup()
+    _, st8 = s8.pcpg()
+    ref8 = o.pcpg(eps_iter=1e-8, max_iter=5000)
+    assert abs(st8.iterations[0] - ref8["iterations"]) <= max(2, 0.02 * ref8["iterations"])
+    s10 = hb.Solver(dict(OPTS, eps_iter="1e-10"))
+    s10.set_mesh(m)
+    s10.setup()
+    u, st = s10.pcpg()
+    ref = o.pcpg(eps_iter=1e-12, max_iter=5000)
+    assert np.linalg.norm(u[0] - ref["u"]) / np.linalg.norm(ref["u"]) < 1e-8
+    assert nodal_equilibrium(m, u[0], np.arange(m.n_nodes)[m.coords[:, 0] > 1e-12]) < 1e-5
