@@ -212,11 +212,15 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
-def run_mixed(hb, local, dist):
+REDUCED = {"small": dict(clusters=(1, 1, 1), subs=(2, 4, 4)),     # F_i tiles 120 MB, FP32 slabs 100 MB
+           "mid": dict(clusters=(2, 1, 1), subs=(2, 4, 4))}       # F_i tiles 240 MB, FP32 slabs 200 MB
+
+
+def run_mixed(hb, local, dist, reduced=None):
     """Batched mixed-precision solve of MIXED_RHS load cases vs the FP64 form
     on four of them (time per load case; displacement error against FP64 at
     eps 1e-10).  Times are CUDA-event solve times, max over ranks."""
-    spec_kw = dict(SPEC, body_force=(0.0, 0.0, -1.0))
+    spec_kw = dict(SPEC, body_force=(0.0, 0.0, -1.0), **(reduced or {}))
     spec = hb.mesh_spec(material=hb.HTF_MAT_LOGUNIFORM, bc=hb.HTF_BC_CLAMP_X0, **spec_kw)
     mesh = hb.generate_mesh(spec)
     f = hb.traction(spec, seed=3, n_rhs=MIXED_RHS)
@@ -364,9 +368,9 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision multi-load-case measurement")
     ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS,
                     help="requests of the seeded serving stream to serve (0 skips the serving measurement)")
-    ap.add_argument("--workload", default="full", choices=["full", "small"],
-                    help="small: one cluster of 2x4x4 subdomains of 8^3 (F_i + S_i 0.3 GB > L2), "
-                         "for ncu captures only")
+    ap.add_argument("--workload", default="full", choices=["full", "small", "mid"],
+                    help="small: one cluster of 2x4x4 subdomains of 8^3 (F_i + S_i 0.24 GB > L2); mid: two such "
+                         "clusters; reduced cases for ncu captures only (the mixed form runs at the same size)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -375,8 +379,8 @@ def main():
     rank, world, local, dist = dist_setup(args.gpus)
     import hfls_b200 as hb
     spec_kw = dict(SPEC)
-    if args.workload == "small":
-        spec_kw.update(clusters=(1, 1, 1), subs=(2, 4, 4))
+    if args.workload != "full":
+        spec_kw.update(REDUCED[args.workload])
     spec = hb.mesh_spec(material=hb.HTF_MAT_LOGUNIFORM, bc=hb.HTF_BC_CLAMP_X0, **spec_kw)
     mesh = hb.generate_mesh(spec)
     f = hb.traction(spec, seed=2, n_rhs=1)
@@ -406,7 +410,7 @@ def main():
     prof = s.profile(reps=20)
     del s
     # every rank solves its mixed-precision replica too (collective max inside)
-    mixed = None if args.no_mixed or args.workload != "full" else run_mixed(hb, local, dist)
+    mixed = None if args.no_mixed else run_mixed(hb, local, dist, REDUCED.get(args.workload))
     serving = None
     if args.serve_requests > 0 and args.workload == "full":
         barrier(dist)
