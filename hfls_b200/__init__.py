@@ -50,7 +50,8 @@ class ProfileInfo(ctypes.Structure):
                 ("iteration_ms", ctypes.c_double), ("kernels_per_iteration", ctypes.c_int),
                 ("batch_width", ctypes.c_int), ("tc_F_ms", ctypes.c_double), ("tc_F_bytes", ctypes.c_double),
                 ("batch_iteration_ms", ctypes.c_double), ("kernels_per_batch_iteration", ctypes.c_int),
-                ("setup_phase_ms", ctypes.c_double * 8)]
+                ("setup_phase_ms", ctypes.c_double * 8), ("symv_unit_tiles", ctypes.c_int * 5),
+                ("symv_tuned", ctypes.c_int)]
 
 
 class RequestInfo(ctypes.Structure):

@@ -108,16 +108,27 @@ HTF_HD long long kidx(const SubDev &s, int r, int c) { return kcol(s, c) + r; }
 // leading dimension of the panel of the step starting at column k
 HTF_HD long long kld(const SubDev &s, int k) { return s.K_bset < 0 ? s.N : s.N - k; }
 
-// One SYMV work unit: packed tiles [t0, t1) of subdomain d (kind 0), or the
-// V^T x_b product of subdomain d (kind 1).  Units write partial y sums for
-// b rows [0, rows) to scratch at y_off; they are summed in unit order.
+// One SYMV work unit of subdomain d: packed tiles [t0, t1) (kind 0 and 2), or
+// the V^T x_b product (kind 1).  Units write partial y sums over the rows
+// their tiles touch (the unit's window) to scratch at y_off; they are summed
+// in unit order.  Kind 0 (whole tile rows): window rows [row0, row0 + rows).
+// Kind 2 (part of one tile row I, rowI = 32 I): window = rows [row0, row0 +
+// rows - 32) for the column blocks, then rows [rowI, rowI + 32).
 struct SymvUnit {
     int d, kind;
     long long t0, t1;
     long long y_off;
     int rows;
+    int row0;
+    int rowI;
     int pad;
 };
+
+// SYMV schedule: subdomains with nt tile rows fall in bucket b, the first
+// with nt <= SYMV_BUCKET_NT[b]; their tiles are cut into units of tiles[b].
+constexpr int SYMV_BUCKETS = 5;
+constexpr int SYMV_BUCKET_NT[SYMV_BUCKETS] = {8, 16, 32, 64, 1 << 30};
+constexpr int SYMV_DEFAULT_TILES = 48;
 
 // One CTA of the tensor-core multi-RHS product: 128-row block m of
 // subdomain d (slabs (m, 0..ks-1) contiguous at a_off, X slabs at x_off).

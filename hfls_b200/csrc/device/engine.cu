@@ -269,31 +269,9 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     nslots_ = xb;
     nfull_ = nf;
     ntiles_ = T_off;
-    // SYMV work units: ~48 tiles (384 KB in FP64) per unit, sub-contiguous
-    std::vector<SymvUnit> units;
-    long long yoff = 0;
-    const long long UNIT_TILES = 48;
-    for (int d = 0; d < nsub_; ++d) {
-        SubDev &h = hs_[d];
-        const long long nt2 = (long long)h.nt * (h.nt + 1) / 2;
-        h.u0 = int(units.size());
-        for (long long t0 = 0; t0 < nt2; t0 += UNIT_TILES) {
-            const long long t1 = std::min(nt2, t0 + UNIT_TILES);
-            long long I = 0;
-            while ((I + 1) * (I + 2) / 2 <= t1 - 1) ++I;         // tile row of the last tile
-            SymvUnit u{d, 0, t0, t1, yoff, int(TILE * (I + 1)), 0};
-            yoff += u.rows;
-            units.push_back(u);
-        }
-        h.u1 = int(units.size());
-        max_nbp_ = std::max(max_nbp_, h.nbp);
-    }
-    nunits_ = int(units.size());
-    for (int d = 0; d < nsub_; ++d) units.push_back(SymvUnit{d, 1, 0, 0, 0, 0, 0});   // V^T x units
-    d_units_ = alloc<SymvUnit>(units.size(), err, rc);
-    d_ypart_ = alloc<double>(yoff, err, rc);
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(d_units_, units.data(), units.size() * sizeof(SymvUnit), cudaMemcpyHostToDevice, s_));
+    // SYMV work units (default schedule; autotune_symv may replace it after set-up)
+    for (auto &h : hs_) max_nbp_ = std::max(max_nbp_, h.nbp);
+    if ((rc = alloc_units(err))) return rc;
     // clusters
     hc_.assign(ncl_, ClusterDev());
     long long M_off = 0;
@@ -776,25 +754,7 @@ int Engine::setup(Problem &p, std::string &err) {
     lap(5);
     if (!rc) rc = outer_coarse(p, err);
     lap(6);
-    if (!rc) {
-        int max_nbp = 0;
-        for (auto &h : hs_) max_nbp = std::max(max_nbp, h.nbp);
-        symv_smem_ = (1 + 4) * max_nbp * int(sizeof(double));
-        if (symv_smem_ > 48 * 1024) {
-            rc = check(cudaFuncSetAttribute(k_symv_units<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, symv_smem_),
-                       "cudaFuncSetAttribute", err);
-            if (!rc)
-                rc = check(cudaFuncSetAttribute(k_symv_units<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, symv_smem_),
-                           "cudaFuncSetAttribute", err);
-        }
-        if (!rc && symv_smem_ > 48 * 1024) {
-            rc = check(cudaFuncSetAttribute(k_symv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, symv_smem_),
-                       "cudaFuncSetAttribute", err);
-            if (!rc)
-                rc = check(cudaFuncSetAttribute(k_symv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, symv_smem_),
-                           "cudaFuncSetAttribute", err);
-        }
-    }
+    if (!rc) rc = autotune_symv(err);             // SYMV work-unit schedule of this problem class
     if (!rc && opt_.mixed) {
         // FP32 slabs for the tensor-core products of the batched form; the
         // FP64 tiles stay resident for the FP64 residuals
@@ -1056,6 +1016,8 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
     if (!info || reps < 1) { err = "bad arguments"; return HTF_EINVAL; }
     std::memset(info, 0, sizeof(*info));
     for (int i = 0; i < 8; ++i) info->setup_phase_ms[i] = phase_ms[i];
+    for (int b = 0; b < SYMV_BUCKETS && b < int(schedule_.size()); ++b) info->symv_unit_tiles[b] = schedule_[b];
+    info->symv_tuned = tuned_ ? 1 : 0;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));

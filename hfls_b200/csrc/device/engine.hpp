@@ -68,6 +68,8 @@ public:
     int device() const { return opt_.device; }
     int apply(int op, const double *x, double *y, int nrhs, std::string &err);   // 0=F, 1=P, 2=M
     double setup_ms = 0.0;
+    const std::vector<int> &symv_schedule() const { return schedule_; }
+    bool symv_tuned() const { return tuned_; }
     double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // see htf_profile_info::setup_phase_ms
     int status_sub = -1;
 
@@ -90,6 +92,12 @@ private:
     void iteration_batch();
     int check(cudaError_t e, const char *what, std::string &err, const char *file = nullptr, int line = 0);
     int upload_layout(Problem &p, std::string &err);
+    // SYMV work-unit schedules (autotune.cu)
+    void build_units(const std::vector<int> &tiles, std::vector<SymvUnit> &units, long long &yoff, int &smem);
+    int apply_schedule(const std::vector<int> &tiles, bool subs_on_device, std::string &err);
+    int alloc_units(std::string &err);
+    std::string schedule_key() const;
+    int autotune_symv(std::string &err);
     int factorize(Problem &p, std::string &err);
     int coarse(Problem &p, std::string &err);
     int outer_coarse(Problem &p, std::string &err);
@@ -141,6 +149,10 @@ private:
     SymvUnit *d_units_ = nullptr;              // SYMV work units (+ one V^T x unit per subdomain)
     double *d_ypart_ = nullptr;                // partial y sums of the units (scratch)
     int nunits_ = 0, max_nbp_ = 0;
+    long long units_cap_ = 0, ypart_cap_ = 0;    // unit buffers, sized for every candidate schedule
+    int symv_smem_cap_ = 0;
+    std::vector<int> schedule_;                  // unit tiles per size bucket in use
+    bool tuned_ = false;
     // batched mixed-precision form
     int bK_ = 0, nblocks_ = 0, bnpart_ = 0, bnpartP_ = 0;
     float *d_AF_ = nullptr, *d_AS_ = nullptr, *d_Xs_ = nullptr;

@@ -117,8 +117,10 @@ template __global__ void k_symv<double>(const SubDev *, const double *, const do
 template __global__ void k_symv<float>(const SubDev *, const float *, const double *, double *,
                                        const PcpgState *);
 
-// SYMV over work units (kind 0) and V^T x (kind 1) in one launch; partial y
-// of a unit -> ypart[y_off, y_off+rows), summed later in unit order.
+// SYMV over work units (kinds 0 and 2) and V^T x (kind 1) in one launch; the
+// partial y of a unit over its row window -> ypart[y_off, y_off + rows),
+// summed later in unit order.  Shared memory: x and one partial y per warp
+// over the unit's window.
 template <typename T>
 __global__ void __launch_bounds__(SYMV_WARPS * 32) k_symv_units(const SymvUnit *__restrict__ units,
                                                                 const SubDev *__restrict__ subs,
@@ -145,13 +147,17 @@ __global__ void __launch_bounds__(SYMV_WARPS * 32) k_symv_units(const SymvUnit *
         }
         return;
     }
-    const int rows = u.rows;                // 32 * (last tile row + 1)
-    double *xs = sm;                        // rows
+    const int rows = u.rows, r0 = u.row0;
+    // kind 0: window = rows [r0, r0 + rows); kind 2: rows [r0, r0 + seg) of the
+    // column blocks, then the 32 rows of the unit's tile row at rowI
+    const int seg = u.kind == 2 ? rows - TILE : rows;
     double *yp = sm + rows;                 // SYMV_WARPS x rows
-    for (int i = threadIdx.x; i < rows; i += blockDim.x) xs[i] = x[i];
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) sm[i] = x[i < seg ? r0 + i : u.rowI + (i - seg)];
     for (int i = threadIdx.x; i < SYMV_WARPS * rows; i += blockDim.x) yp[i] = 0.0;
     __syncthreads();
-    double *my = yp + warp * rows;
+    const double *xs = sm - r0;             // x of column block J at xs + 32 J
+    double *ys = yp + warp * rows;          // this warp's partial y over the window
+    double *my = ys - r0;                   // column block J at my + 32 J
     const T *base = tiles + sd.T_off * TILE_ELEMS;
     for (long long tt = u.t0 + warp; tt < u.t1; tt += SYMV_WARPS) {
         int I = (int)((sqrt(8.0 * (double)tt + 1.0) - 1.0) * 0.5);
@@ -163,15 +169,17 @@ __global__ void __launch_bounds__(SYMV_WARPS * 32) k_symv_units(const SymvUnit *
 #pragma unroll
         for (int r = 0; r < 32; ++r) v[r] = (double)tp[r * TILE + lane];
         const double xJ = xs[TILE * J + lane];
+        const double *xI = u.kind == 2 ? sm + seg : xs + TILE * I;      // x of row block I
+        double *yI = u.kind == 2 ? ys + seg : my + TILE * I;             // partial y of row block I
         double p[32];
         double col = 0.0;
 #pragma unroll
         for (int r = 0; r < 32; ++r) {
             p[r] = v[r] * xJ;
-            col += v[r] * xs[TILE * I + r];
+            col += v[r] * xI[r];
         }
         reduce_scatter32(p, lane);
-        my[TILE * I + lane] += p[0];
+        yI[lane] += p[0];
         if (I != J) my[TILE * J + lane] += col;
     }
     __syncthreads();
@@ -213,7 +221,9 @@ __global__ void k_reduce_correct(const SubDev *__restrict__ subs, const SymvUnit
     double a = 0.0;
     for (int k = sd.u0; k < sd.u1; ++k) {
         const SymvUnit &u = units[k];
-        if (i < u.rows) a += ypart[u.y_off + i];
+        const int seg = u.kind == 2 ? u.rows - TILE : u.rows;
+        if (i >= u.row0 && i < u.row0 + seg) a += ypart[u.y_off + (i - u.row0)];
+        if (u.kind == 2 && i >= u.rowI && i < u.rowI + TILE) a += ypart[u.y_off + seg + (i - u.rowI)];
     }
     if (s && i < sd.nb) {
         const double *V = Vbuf + sd.V_off + i;

@@ -223,6 +223,8 @@ int parse_options(const char *s, Options &o, std::string &err) {
         } else if (k == "device") o.device = std::atoi(v.c_str());
         else if (k == "check_every") o.check_every = std::max(1, std::atoi(v.c_str()));
         else if (k == "verbose") o.verbose = std::atoi(v.c_str());
+        else if (k == "autotune") o.autotune = std::atoi(v.c_str());
+        else if (k == "tune_file") o.tune_file = v;
         else if (k == "batch") {
             o.batch = std::atoi(v.c_str());
             if (o.batch != 16 && o.batch != 32) { err = "batch must be 16 or 32"; return HTF_EINVAL; }

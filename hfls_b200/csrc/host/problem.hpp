@@ -49,6 +49,9 @@ struct Options {
     int check_every = 8;                              // iterations between host convergence checks
     int batch = 32;                                   // load cases per batched mixed-precision solve (16 | 32)
     int verbose = 0;                                  // progress lines on stderr
+    int autotune = 1;                                 // time SYMV work-unit sizes at setup (once per process and
+                                                      // problem class); 0 = fixed default schedule
+    std::string tune_file;                            // JSON file of tuned schedules, read and extended
 };
 int parse_options(const char *s, Options &o, std::string &err);
 

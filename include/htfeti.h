@@ -80,8 +80,13 @@ int htf_mesh_traction(const htf_mesh_spec *spec, uint64_t seed, int n_rhs, doubl
  * (Driver.cpp:14-18, htfeti.cpp:12-57).  `options` is a ';'-separated list
  * of key=value with the reference's keys (eps_iter, max_iter,
  * preconditioner = Dirichlet_explicit | Dirichlet_implicit | lumped,
- * typeBc = cor | ker | all, Ac_extended_by_kerGc) and this build's keys
- * (precision = fp64 | mixed, device = <cuda ordinal>).                     */
+ * typeBc = cor | ker | all, Ac_extended_by_kerGc) and this library's keys:
+ * precision = fp64 | mixed, device = <cuda ordinal>, batch = 16 | 32 (load
+ * cases per batched mixed solve), check_every = <iterations between host
+ * convergence checks>, autotune = 1 | 0 (time the FP64 SYMV work-unit sizes
+ * per subdomain-size bucket at set-up, once per process and problem
+ * class), tune_file = <path of a JSON file of tuned schedules, read and
+ * extended>, verbose = 0 | 1.                                              */
 typedef struct htf_ctx htf_ctx;
 
 int htf_create(const char *options, htf_ctx **ctx);
@@ -158,8 +163,13 @@ typedef struct htf_profile_info {
      * Bf/Bc, kernels, fix DOFs), 1 device context and stream, 2 layout upload
      * and allocation, 3 assembly + factorisation + F_i/S_i, 4 load and
      * displacement maps, 5 cluster coarse problems, 6 outer coarse problem,
-     * 7 FP32 slabs of the batched form                                       */
+     * 7 SYMV schedule tuning and FP32 slabs of the batched form              */
     double setup_phase_ms[8];
+    /* SYMV schedule in use: work-unit tiles for subdomains with at most
+     * 8, 16, 32, 64 and more tile rows; tuned = 1 when it came from the
+     * autotuner (option autotune=1, the default) or its cache              */
+    int symv_unit_tiles[5];
+    int symv_tuned;
 } htf_profile_info;
 int htf_profile(htf_ctx *ctx, int reps, htf_profile_info *info);
 

@@ -1,0 +1,40 @@
+"""SYMV schedule autotuner: the tuned schedule changes only the work split of
+the FP64 F / S applies, not the result; it is kept per process and written to
+and read back from a tuning file."""
+import json
+
+import numpy as np
+import pytest
+
+import hfls_b200 as hb
+
+pytestmark = pytest.mark.gpu
+
+SPEC = dict(clusters=(2, 1, 1), subs=(2, 2, 2), widths=([3, 5, 4, 6], [4, 7], [2, 5]), jitter=0.1, seed=8,
+            material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e3)
+CANDIDATES = {8, 12, 16, 24, 32, 48, 64, 96}
+
+
+def solve(opts):
+    m = hb.generate_mesh(hb.mesh_spec(**SPEC))
+    s = hb.Solver(dict({"typeBc": "cor", "eps_iter": "1e-10", "max_iter": "2000"}, **opts))
+    s.set_mesh(m)
+    s.setup()
+    u, st = s.pcpg()
+    p = s.profile(reps=2)
+    return u[0], st.iterations[0], list(p.symv_unit_tiles), p.symv_tuned
+
+
+def test_tuned_schedule_gives_the_same_solution(tmp_path):
+    u0, it0, t0, tuned0 = solve({"autotune": "0"})
+    assert tuned0 == 0 and t0 == [48] * 5
+    f = tmp_path / "tune.json"
+    u1, it1, t1, tuned1 = solve({"autotune": "1", "tune_file": str(f)})
+    assert tuned1 == 1 and set(t1) <= CANDIDATES
+    assert abs(it1 - it0) <= 2             # the summation order of the F / S applies changes
+    assert np.linalg.norm(u1 - u0) / np.linalg.norm(u0) < 1e-8
+    doc = json.loads(f.read_text())
+    assert any(e["tiles"] == t1 for e in doc["schedules"])
+    # a second problem of the same class in this process uses the cached schedule
+    _, _, t2, tuned2 = solve({"autotune": "1", "tune_file": str(f)})
+    assert tuned2 == 1 and t2 == t1
