@@ -41,6 +41,7 @@ __global__ void k_symv_units(const SymvUnit *, const SubDev *, const T *, const 
 namespace {
 
 constexpr int SYMV_ROW_DOUBLES = 5;            // shared doubles per window row: x + 4 warp partials
+constexpr long long SYMV_TUNE_MIN_TILES = 1LL << 17;   // 1 GiB of FP64 tiles
 const int CANDIDATES[] = {8, 12, 16, 24, 32, 48, 64, 96};
 
 std::mutex g_mu;
@@ -242,9 +243,14 @@ std::string Engine::schedule_key() const {
     return k;
 }
 
-// After set-up (F tiles resident): the cached or tuned schedule.
+// After set-up (F tiles resident): the cached or tuned schedule.  With
+// autotune=1 only problems of at least SYMV_TUNE_MIN_TILES tiles are tuned:
+// below that the F apply takes tens of microseconds and the default schedule
+// keeps small problems' arithmetic fixed from run to run (a tuned schedule
+// is chosen by timing, and the summation order follows the schedule).
+// autotune=2 tunes every problem.
 int Engine::autotune_symv(std::string &err) {
-    if (!opt_.autotune) return HTF_OK;
+    if (!opt_.autotune || (opt_.autotune == 1 && ntiles_ < SYMV_TUNE_MIN_TILES)) return HTF_OK;
     const std::string key = schedule_key();
     {
         std::lock_guard<std::mutex> lk(g_mu);

@@ -25,8 +25,8 @@
 namespace htf {
 
 __global__ void k_potrf_diag(const StepDesc *, const SubDev *, double *, int *);
-__global__ void k_trsm_panel(const StepDesc *, const SubDev *, double *);
-__global__ void k_syrk_update(const StepDesc *, const SubDev *, double *);
+__global__ void k_trsm_panel(const StepDesc *, int, const SubDev *, double *);
+__global__ void k_syrk_update(const StepDesc *, int, const SubDev *, double *);
 __global__ void k_trsm_fwd_multi(const SubDev *, const double *, double *, long long, int, const int *);
 __global__ void k_trsm_bwd_multi(const SubDev *, const double *, double *, long long, int, const int *);
 __global__ void k_build_Fc(const SubDev *, const double *, const int *, const int *, const double *,
@@ -144,9 +144,9 @@ struct DevTmp {                        // device scratch freed when the coarse s
 void chol_steps(const std::vector<SubDev> &m, std::vector<std::vector<StepDesc>> &steps) {
     steps.clear();
     for (int d = 0; d < int(m.size()); ++d)
-        for (int k = 0, s = 0; k < m[d].N; k += TILE, ++s) {
+        for (int k = 0, s = 0; k < m[d].N; k += CHOL_STEP, ++s) {
             if (int(steps.size()) <= s) steps.resize(s + 1);
-            steps[s].push_back({d, k, std::min(TILE, m[d].N - k)});
+            steps[s].push_back({d, k, std::min(CHOL_STEP, m[d].N - k), 0, 0});
         }
 }
 
@@ -161,7 +161,19 @@ static cudaError_t chol_batched(const std::vector<SubDev> &hm, const SubDev *dm,
     chol_steps(hm, steps);
     std::vector<StepDesc> flat;
     std::vector<size_t> off;
-    for (auto &v : steps) { off.push_back(flat.size()); flat.insert(flat.end(), v.begin(), v.end()); }
+    std::vector<int> ntri, nrb;
+    for (auto &v : steps) {
+        int tri = 0, rb = 0;
+        for (auto &x : v) {
+            const int rows = hm[x.d].N - x.k - x.nb, nbr = (rows + 63) / 64;
+            x.tri0 = tri; tri += nbr * (nbr + 1) / 2;
+            x.rb0 = rb; rb += (rows + 127) / 128;
+        }
+        ntri.push_back(tri);
+        nrb.push_back(rb);
+        off.push_back(flat.size());
+        flat.insert(flat.end(), v.begin(), v.end());
+    }
     if (flat.empty()) return cudaSuccess;
     cudaError_t e = cudaSuccess;
     StepDesc *d = tmp.get<StepDesc>(flat.size(), e);
@@ -170,18 +182,9 @@ static cudaError_t chol_batched(const std::vector<SubDev> &hm, const SubDev *dm,
     if (e != cudaSuccess) return e;
     for (size_t st = 0; st < steps.size(); ++st) {
         const int cnt = int(steps[st].size());
-        int max_rows = 0, max_tri = 0;
-        for (auto &x : steps[st]) {
-            const int rows = hm[x.d].N - x.k - x.nb;
-            max_rows = std::max(max_rows, rows);
-            const int nbr = (rows + 63) / 64;
-            max_tri = std::max(max_tri, nbr * (nbr + 1) / 2);
-        }
-        k_potrf_diag<<<cnt, 32, 0, s>>>(d + off[st], dm, buf, status);
-        if (max_rows > 0) {
-            k_trsm_panel<<<dim3(cnt, cdivc(max_rows, 128)), 128, 0, s>>>(d + off[st], dm, buf);
-            k_syrk_update<<<dim3(cnt, max_tri), 256, 0, s>>>(d + off[st], dm, buf);
-        }
+        k_potrf_diag<<<cnt, CHOL_STEP, 0, s>>>(d + off[st], dm, buf, status);
+        if (nrb[st] > 0) k_trsm_panel<<<nrb[st], 128, 0, s>>>(d + off[st], cnt, dm, buf);
+        if (ntri[st] > 0) k_syrk_update<<<ntri[st], 256, 0, s>>>(d + off[st], cnt, dm, buf);
     }
     return cudaGetLastError();
 }

@@ -36,6 +36,7 @@ __device__ __forceinline__ float tf32_trunc(float a) { return __uint_as_float(__
 #endif
 
 constexpr int TILE = 32;                  // packed tile edge
+constexpr int CHOL_STEP = 64;             // columns per batched Cholesky step (two factor panels)
 constexpr int TC_STAGES = 2;              // pipeline stages of the tensor-core product (2 CTAs per SM)
 constexpr int TILE_ELEMS = TILE * TILE;
 
@@ -159,12 +160,32 @@ struct TcSet {
     const double *sc;                     // coarse solution of the F product
 };
 
-// One 32-column step of the batched Cholesky for one subdomain.
+// One step of the batched Cholesky for one subdomain: columns [k, k + nb),
+// nb <= CHOL_STEP, starting at a factor panel and covering at most two.
+// tri0 / rb0: first trailing 64x64 tile / first 128-row block of this entry
+// in the step's flattened SYRK / panel-solve grid (prefix sums over the step's
+// entries, so the grids have no idle CTAs whatever the subdomain sizes).
 struct StepDesc {
     int d;      // subdomain
     int k;      // first column of the step
-    int nb;     // columns in the step (<= 32)
+    int nb;     // columns in the step
+    int tri0;
+    int rb0;
 };
+
+#ifdef __CUDACC__
+// entry of a step whose flattened range holds block b (the last one starting at or before b)
+template <typename F>
+__device__ __forceinline__ int step_entry(const StepDesc *st, int cnt, int b, F start) {
+    int lo = 0, hi = cnt - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start(st[mid]) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+#endif
 
 // PCPG state in device memory (one per load case).
 struct PcpgState {

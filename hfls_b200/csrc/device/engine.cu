@@ -18,8 +18,8 @@ __global__ void k_assemble(const int *, int, const double *, const int *, const 
                            const double *, const SubDev *, double *, double *, double, double, double);
 __global__ void k_regularize(SubDev *, int, double *);
 __global__ void k_potrf_diag(const StepDesc *, const SubDev *, double *, int *);
-__global__ void k_trsm_panel(const StepDesc *, const SubDev *, double *);
-__global__ void k_syrk_update(const StepDesc *, const SubDev *, double *);
+__global__ void k_trsm_panel(const StepDesc *, int, const SubDev *, double *);
+__global__ void k_syrk_update(const StepDesc *, int, const SubDev *, double *);
 __global__ void k_snapshot(const int *, const SubDev *, const double *, double *);
 __global__ void k_trtri_step(int, const int *, const SubDev *, const double *, double *);
 __global__ void k_lauum_tiles(const int *, const SubDev *, const double *, double *);
@@ -522,18 +522,30 @@ int Engine::factorize(Problem &p, std::string &err) {
     std::vector<int> snap_first;                   // nr == 0
     for (int d = 0; d < nsub_; ++d) {
         const SubDev &h = hs_[d];
-        std::vector<std::pair<int, int>> blocks;
-        for (int k = 0; k < h.nr; k += TILE) blocks.push_back({k, std::min(TILE, h.nr - k)});
+        std::vector<std::pair<int, int>> blocks;      // steps never cross from the interior into the b set
+        for (int k = 0; k < h.nr; k += CHOL_STEP) blocks.push_back({k, std::min(CHOL_STEP, h.nr - k)});
         int interior_steps = int(blocks.size());
-        for (int k = h.nr; k < h.N; k += TILE) blocks.push_back({k, TILE});
+        for (int k = h.nr; k < h.N; k += CHOL_STEP) blocks.push_back({k, std::min(CHOL_STEP, h.N - k)});
         if (steps.size() < blocks.size()) { steps.resize(blocks.size()); snap_after.resize(blocks.size()); }
-        for (size_t s = 0; s < blocks.size(); ++s) steps[s].push_back({d, blocks[s].first, blocks[s].second});
+        for (size_t s = 0; s < blocks.size(); ++s) steps[s].push_back({d, blocks[s].first, blocks[s].second, 0, 0});
         if (interior_steps == 0) snap_first.push_back(d);
         else snap_after[interior_steps - 1].push_back(d);
     }
     std::vector<StepDesc> flat;
     std::vector<size_t> soff;
-    for (auto &v : steps) { soff.push_back(flat.size()); flat.insert(flat.end(), v.begin(), v.end()); }
+    std::vector<int> ntri, nrb;                    // flattened grid sizes per step
+    for (auto &v : steps) {
+        int tri = 0, rb = 0;
+        for (auto &x : v) {
+            const int rows = hs_[x.d].N - x.k - x.nb, nbr = (rows + 63) / 64;
+            x.tri0 = tri; tri += nbr * (nbr + 1) / 2;
+            x.rb0 = rb; rb += (rows + 127) / 128;
+        }
+        ntri.push_back(tri);
+        nrb.push_back(rb);
+        soff.push_back(flat.size());
+        flat.insert(flat.end(), v.begin(), v.end());
+    }
     std::vector<int> snap_flat;
     std::vector<size_t> snap_off;
     for (auto &v : snap_after) { snap_off.push_back(snap_flat.size()); snap_flat.insert(snap_flat.end(), v.begin(), v.end()); }
@@ -551,20 +563,10 @@ int Engine::factorize(Problem &p, std::string &err) {
     }
     for (size_t s = 0; s < steps.size(); ++s) {
         const int cnt = int(steps[s].size());
-        int max_rows = 0, max_tri = 0;
-        for (auto &st : steps[s]) {
-            const SubDev &h = hs_[st.d];
-            int rows = h.N - st.k - st.nb;
-            max_rows = std::max(max_rows, rows);
-            int nbr = (rows + 63) / 64;
-            max_tri = std::max(max_tri, nbr * (nbr + 1) / 2);
-        }
         const StepDesc *ds = d_steps + soff[s];
-        k_potrf_diag<<<cnt, 32, 0, s_>>>(ds, d_subs_, d_K_, d_status_);
-        if (max_rows > 0) {
-            k_trsm_panel<<<dim3(cnt, cdiv(max_rows, 128)), 128, 0, s_>>>(ds, d_subs_, d_K_);
-            k_syrk_update<<<dim3(cnt, max_tri), 256, 0, s_>>>(ds, d_subs_, d_K_);
-        }
+        k_potrf_diag<<<cnt, CHOL_STEP, 0, s_>>>(ds, d_subs_, d_K_, d_status_);
+        if (nrb[s] > 0) k_trsm_panel<<<nrb[s], 128, 0, s_>>>(ds, cnt, d_subs_, d_K_);
+        if (ntri[s] > 0) k_syrk_update<<<ntri[s], 256, 0, s_>>>(ds, cnt, d_subs_, d_K_);
         if (dirichlet && !snap_after[s].empty())
             k_snapshot<<<dim3(int(snap_after[s].size()), max_tiles), 256, 0, s_>>>(d_snap + snap_off[s], d_subs_, d_K_, d_S_);
         CK(cudaGetLastError());

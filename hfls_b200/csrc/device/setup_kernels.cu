@@ -143,61 +143,104 @@ __global__ void k_regularize(SubDev *subs, int nsub, double *Kbuf) {
 }
 
 // ---------------------------------------------------------------------------
-// batched Cholesky steps
+// batched Cholesky steps of up to CHOL_STEP = 64 columns (two 32-column factor
+// panels): the diagonal block in one CTA, the panel below it one row per
+// thread, the trailing update keeping one accumulator per 32-column panel and
+// subtracting them in turn in registers, so each trailing tile is read and
+// written once per 64 columns.  The arithmetic is that of two successive
+// 32-column right-looking steps (per panel: Cholesky of the diagonal block,
+// row-wise substitution with division by the pivot, block update subtracting
+// a 32-term sum), operation for operation.
 // ---------------------------------------------------------------------------
-__global__ void k_potrf_diag(const StepDesc *__restrict__ st, const SubDev *__restrict__ subs,
-                             double *__restrict__ Kbuf, int *__restrict__ status) {
-    __shared__ double A[32][33];
+__global__ void __launch_bounds__(CHOL_STEP) k_potrf_diag(const StepDesc *__restrict__ st,
+                                                          const SubDev *__restrict__ subs,
+                                                          double *__restrict__ Kbuf, int *__restrict__ status) {
+    __shared__ double A[CHOL_STEP][CHOL_STEP + 1];
+    __shared__ int bad;
     const StepDesc s = st[blockIdx.x];
     const SubDev &sd = subs[s.d];
-    double *K = Kbuf + kidx(sd, s.k, s.k);        // the step's panel: entry (k+i, k+j) at K[i + j*ld]
-    const int k = s.k, nb = s.nb, lane = threadIdx.x;
-    const long long ld = kld(sd, k);
-    for (int c = 0; c < nb; ++c) A[lane][c] = (lane < nb) ? K[lane + c * ld] : 0.0;
-    __syncwarp();
-    for (int j = 0; j < nb; ++j) {
-        if (lane == j) {
-            double dj = A[j][j];
-            if (!(dj > 0.0)) {
-                atomicCAS(&status[s.d], 0, k + j + 1);
-                dj = 1.0;
-            }
-            A[j][j] = sqrt(dj);
-        }
-        __syncwarp();
-        const double dj = A[j][j];
-        if (lane > j && lane < nb) A[lane][j] /= dj;
-        __syncwarp();
-        if (lane > j && lane < nb) {
-            const double lj = A[lane][j];
-            for (int c = j + 1; c <= lane; ++c) A[lane][c] -= lj * A[c][j];
-        }
-        __syncwarp();
-    }
-    if (lane < nb)
-        for (int c = 0; c <= lane; ++c) K[lane + c * ld] = A[lane][c];
-}
-
-__global__ void k_trsm_panel(const StepDesc *__restrict__ st, const SubDev *__restrict__ subs,
-                             double *__restrict__ Kbuf) {
-    __shared__ double L[32][33];
-    const StepDesc s = st[blockIdx.x];
-    const SubDev &sd = subs[s.d];
-    double *K = Kbuf + kidx(sd, s.k, s.k);        // the step's panel: entry (k+i, k+j) at K[i + j*ld]
-    const int N = sd.N, k = s.k, nb = s.nb;
-    const long long ld = kld(sd, k);
-    for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
-        const int r = i % 32, c = i / 32;
-        L[r][c] = (r < nb && c < nb && c <= r) ? K[r + c * ld] : 0.0;
+    const int k = s.k, nb = s.nb, t = threadIdx.x;
+    if (t == 0) bad = 0;
+    for (int c = 0; c < nb; ++c) {
+        const double *col = Kbuf + kcol(sd, k + c);
+        A[t][c] = (t < nb && t >= c) ? col[k + t] : 0.0;
     }
     __syncthreads();
-    const int row = k + nb + blockIdx.y * blockDim.x + threadIdx.x;
+    // Cholesky of the 32-column diagonal block starting at column o (rows o .. e-1)
+    auto potrf32 = [&](int o, int e) {
+        for (int j = o; j < e; ++j) {
+            if (t == j) {
+                double dj = A[j][j];
+                if (!(dj > 0.0)) {
+                    if (!bad) bad = k + j + 1;
+                    dj = 1.0;
+                }
+                A[j][j] = sqrt(dj);
+            }
+            __syncthreads();
+            const double dj = A[j][j];
+            if (t > j && t < e) A[t][j] /= dj;
+            __syncthreads();
+            if (t > j && t < e) {
+                const double lj = A[t][j];
+                for (int c = j + 1; c <= t; ++c) A[t][c] -= lj * A[c][j];
+            }
+            __syncthreads();
+        }
+    };
+    const int n1 = min(nb, TILE);
+    potrf32(0, n1);
+    if (nb > TILE) {
+        if (t >= TILE && t < nb) {              // rows of the second panel: substitution with the first
+            for (int j = 0; j < TILE; ++j) {
+                double v = A[t][j];
+                for (int i = 0; i < j; ++i) v -= A[t][i] * A[j][i];
+                A[t][j] = v / A[j][j];
+            }
+        }
+        __syncthreads();
+        if (t >= TILE && t < nb) {              // block update of the second diagonal block
+            for (int c = TILE; c <= t; ++c) {
+                double acc = 0.0;
+                for (int i = 0; i < TILE; ++i) acc += A[t][i] * A[c][i];
+                A[t][c] -= acc;
+            }
+        }
+        __syncthreads();
+        potrf32(TILE, nb);
+    }
+    if (t == 0 && bad) atomicCAS(&status[s.d], 0, bad);
+    for (int c = 0; c < nb; ++c) {
+        double *col = Kbuf + kcol(sd, k + c);
+        if (t < nb && t >= c) col[k + t] = A[t][c];
+    }
+}
+
+// rows below the diagonal block: x = x L_kk^{-T}, one row per thread
+// grid: the step's row blocks of 128 (flattened over its entries)
+__global__ void __launch_bounds__(128) k_trsm_panel(const StepDesc *__restrict__ st, int cnt,
+                                                    const SubDev *__restrict__ subs, double *__restrict__ Kbuf) {
+    __shared__ double L[CHOL_STEP][CHOL_STEP + 1];
+    const int e = step_entry(st, cnt, int(blockIdx.x), [](const StepDesc &x) { return x.rb0; });
+    const StepDesc s = st[e];
+    const int rb = int(blockIdx.x) - s.rb0;
+    const SubDev &sd = subs[s.d];
+    const int N = sd.N, k = s.k, nb = s.nb;
+    for (int i = threadIdx.x; i < CHOL_STEP * CHOL_STEP; i += blockDim.x) {
+        const int r = i % CHOL_STEP, c = i / CHOL_STEP;
+        L[r][c] = (r < nb && c < nb && c <= r) ? Kbuf[kidx(sd, k + r, k + c)] : 0.0;
+    }
+    __syncthreads();
+    const int row = k + nb + rb * blockDim.x + threadIdx.x;
     if (row >= N) return;
-    double x[32];
+    const long long c0 = kcol(sd, k), c1 = kcol(sd, k + TILE);     // the step's two panels
+    const long long ld0 = kld(sd, k), ld1 = kld(sd, k + TILE);
+    double x[CHOL_STEP];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) x[j] = (j < nb) ? K[(row - k) + j * ld] : 0.0;
+    for (int j = 0; j < CHOL_STEP; ++j)
+        x[j] = (j < nb) ? Kbuf[(j < TILE ? c0 + (long long)j * ld0 : c1 + (long long)(j - TILE) * ld1) + row] : 0.0;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
+    for (int j = 0; j < TILE; ++j) {
         if (j < nb) {
             double v = x[j];
 #pragma unroll
@@ -205,56 +248,89 @@ __global__ void k_trsm_panel(const StepDesc *__restrict__ st, const SubDev *__re
             x[j] = v / L[j][j];
         }
     }
+    if (nb > TILE) {
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
-        if (j < nb) K[(row - k) + j * ld] = x[j];
+        for (int j = TILE; j < CHOL_STEP; ++j) {       // block update by the first panel
+            if (j < nb) {
+                double acc = 0.0;
+#pragma unroll
+                for (int i = 0; i < TILE; ++i) acc += x[i] * L[j][i];
+                x[j] -= acc;
+            }
+        }
+#pragma unroll
+        for (int j = TILE; j < CHOL_STEP; ++j) {
+            if (j < nb) {
+                double v = x[j];
+#pragma unroll
+                for (int i = TILE; i < j; ++i) v -= x[i] * L[j][i];
+                x[j] = v / L[j][j];
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < CHOL_STEP; ++j)
+        if (j < nb) Kbuf[(j < TILE ? c0 + (long long)j * ld0 : c1 + (long long)(j - TILE) * ld1) + row] = x[j];
 }
 
-// C(64x64 block, lower part of the trailing matrix) -= P_i P_j^T, P = panel
-__global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict__ st,
+// C(64x64 block, lower part of the trailing matrix) -= P_i P_j^T, P = the
+// step's panel rows; 32 columns of P at a time, one accumulator per panel,
+// C read and written once.  grid: the step's trailing tiles (flattened)
+__global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict__ st, int cnt,
                                                      const SubDev *__restrict__ subs,
                                                      double *__restrict__ Kbuf) {
     __shared__ double Pa[32][64 + 1];
     __shared__ double Pb[32][64 + 1];
-    const StepDesc s = st[blockIdx.x];
+    const int e = step_entry(st, cnt, int(blockIdx.x), [](const StepDesc &x) { return x.tri0; });
+    const StepDesc s = st[e];
     const SubDev &sd = subs[s.d];
     const int N = sd.N, k = s.k, nb = s.nb;
     const int t0 = k + nb;                  // first trailing row/col
     const int m = N - t0;
     const int nbr = (m + 63) / 64;
-    const int tri = blockIdx.y;
+    const int tri = int(blockIdx.x) - s.tri0;
     if (tri >= nbr * (nbr + 1) / 2) return;
     int bi = (int)((sqrt(8.0 * tri + 1.0) - 1.0) * 0.5);
     while ((bi + 1) * (bi + 2) / 2 <= tri) ++bi;
     while (bi * (bi + 1) / 2 > tri) --bi;
     const int bj = tri - bi * (bi + 1) / 2;
     const int i0 = t0 + 64 * bi, j0 = t0 + 64 * bj;
-    const double *P = Kbuf + kidx(sd, k, k);       // the step's panel: entry (k+i, k+j) at P[i + j*ld]
-    const long long ld = kld(sd, k);
-    for (int idx = threadIdx.x; idx < 32 * 64; idx += 256) {
-        const int r = idx % 64, kk = idx / 64;
-        const bool ok = kk < nb;
-        Pa[kk][r] = (ok && i0 + r < N) ? P[(i0 + r - k) + kk * ld] : 0.0;
-        Pb[kk][r] = (ok && j0 + r < N) ? P[(j0 + r - k) + kk * ld] : 0.0;
-    }
-    __syncthreads();
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double acc[4][4];
+    double acc[CHOL_STEP / TILE][4][4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-    for (int kk = 0; kk < nb; ++kk) {
-        double av[4], bv[4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) av[a] = Pa[kk][tx + 16 * a];
-#pragma unroll
-        for (int b = 0; b < 4; ++b) bv[b] = Pb[kk][ty + 16 * b];
+    for (int q = 0; q < CHOL_STEP / TILE; ++q)
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+            for (int b = 0; b < 4; ++b) acc[q][a][b] = 0.0;
+#pragma unroll
+    for (int q = 0; q < CHOL_STEP / TILE; ++q) {
+        const int kc = TILE * q;
+        if (kc >= nb) break;
+        const int kn = min(TILE, nb - kc);
+        const double *P = Kbuf + kidx(sd, k + kc, k + kc);    // panel of columns k+kc..: entry (k+kc+i, k+kc+j) at P[i + j*ld]
+        const long long ld = kld(sd, k + kc);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < 32 * 64; idx += 256) {
+            const int r = idx % 64, kk = idx / 64;
+            const bool ok = kk < kn;
+            Pa[kk][r] = (ok && i0 + r < N) ? P[(i0 + r - k - kc) + kk * ld] : 0.0;
+            Pb[kk][r] = (ok && j0 + r < N) ? P[(j0 + r - k - kc) + kk * ld] : 0.0;
+        }
+        __syncthreads();
+        for (int kk = 0; kk < kn; ++kk) {
+            double av[4], bv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) av[a] = Pa[kk][tx + 16 * a];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) bv[b] = Pb[kk][ty + 16 * b];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[q][a][b] += av[a] * bv[b];
+        }
     }
+    const int nq = (nb + TILE - 1) / TILE;
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
         const int col = j0 + ty + 16 * b;
@@ -264,7 +340,11 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
         for (int a = 0; a < 4; ++a) {
             const int row = i0 + tx + 16 * a;
             if (row >= N || row < col) continue;
-            C[row] -= acc[a][b];
+            double c = C[row];
+#pragma unroll
+            for (int q = 0; q < CHOL_STEP / TILE; ++q)
+                if (q < nq) c -= acc[q][a][b];
+            C[row] = c;
         }
     }
 }

@@ -50,7 +50,8 @@ struct Options {
     int batch = 32;                                   // load cases per batched mixed-precision solve (16 | 32)
     int verbose = 0;                                  // progress lines on stderr
     int autotune = 1;                                 // time SYMV work-unit sizes at setup (once per process and
-                                                      // problem class); 0 = fixed default schedule
+                                                      // problem class) for problems of >= 1 GiB of FP64 tiles;
+                                                      // 2 = every problem; 0 = fixed default schedule
     std::string tune_file;                            // JSON file of tuned schedules, read and extended
 };
 int parse_options(const char *s, Options &o, std::string &err);

@@ -83,10 +83,11 @@ int htf_mesh_traction(const htf_mesh_spec *spec, uint64_t seed, int n_rhs, doubl
  * typeBc = cor | ker | all, Ac_extended_by_kerGc) and this library's keys:
  * precision = fp64 | mixed, device = <cuda ordinal>, batch = 16 | 32 (load
  * cases per batched mixed solve), check_every = <iterations between host
- * convergence checks>, autotune = 1 | 0 (time the FP64 SYMV work-unit sizes
- * per subdomain-size bucket at set-up, once per process and problem
- * class), tune_file = <path of a JSON file of tuned schedules, read and
- * extended>, verbose = 0 | 1.                                              */
+ * convergence checks>, autotune = 1 | 2 | 0 (time the FP64 SYMV work-unit
+ * sizes per subdomain-size bucket at set-up, once per process and problem
+ * class: 1 for problems of at least 1 GiB of FP64 tiles, 2 for every
+ * problem, 0 never), tune_file = <path of a JSON file of tuned schedules,
+ * read and extended>, verbose = 0 | 1.                                     */
 typedef struct htf_ctx htf_ctx;
 
 int htf_create(const char *options, htf_ctx **ctx);
@@ -167,7 +168,7 @@ typedef struct htf_profile_info {
     double setup_phase_ms[8];
     /* SYMV schedule in use: work-unit tiles for subdomains with at most
      * 8, 16, 32, 64 and more tile rows; tuned = 1 when it came from the
-     * autotuner (option autotune=1, the default) or its cache              */
+     * autotuner (option autotune) or its cache                             */
     int symv_unit_tiles[5];
     int symv_tuned;
 } htf_profile_info;

