@@ -48,7 +48,7 @@ REF_SAMPLE = dict(Nx=2, Ny=1, Nz=1, nx=8, ny=8, nz=8)     # subdomains of the wo
 MIXED_RHS = 32
 MIXED_WORKLOAD = ("same cube, body force (0,0,-1) + 32 seeded N(0,1) tractions on x=1, solved as one batch of 32: "
                   "F_i/S_i FP32 slabs, 3xTF32 tcgen05 products, FP64 coarse/projector/residual replacement, eps 1e-8")
-SERVE_REQUESTS = 16          # requests of the seeded stream that one bench run serves
+SERVE_REQUESTS = 12          # requests of the seeded stream that one bench run serves
 SERVE_RATE = 1.0             # Poisson arrivals per second
 SERVE_WORKLOAD = ("seeded Poisson stream (rate %.1f/s): cube meshes of c^3 clusters, (c s)^3 subdomains of e^3 hex8, "
                   "c in 1..4, s in 2..5, e in 4..10, 1..16 load cases (body force + N(0,1) traction on x=1), "

@@ -32,9 +32,6 @@ __global__ void k_trsv_bwd(const SubDev *, const double *, double *, long long);
 __global__ void k_gather_b(int, const int *, const int *, const double *, const double *, double *,
                            const PcpgState *);
 template <typename T>
-__global__ void k_symv(const SubDev *, const T *, const double *, double *, const PcpgState *);
-__global__ void k_vt(const SubDev *, const double *, const double *, double *, const PcpgState *);
-template <typename T>
 __global__ void k_symv_units(const SymvUnit *, const SubDev *, const T *, const double *, const double *, double *,
                              double *, const PcpgState *);
 __global__ void k_reduce_correct(const SubDev *, const SymvUnit *, const double *, const ClusterDev *,
@@ -48,14 +45,8 @@ __global__ void k_correct(const SubDev *, const ClusterDev *, const double *, co
                           double *, const PcpgState *);
 __global__ void k_rows(int, const int *, const double *, const double *, const double *, double *,
                        const double *, double *, const PcpgState *);
-__global__ void k_dot_partial(int, const double *, const double *, double *, const PcpgState *);
-__global__ void k_sum_to(const double *, int, double *, const PcpgState *);
 __global__ void k_gft_partial(const int *, const int *, const int *, const int *, const double *,
                               const double *, double *, const PcpgState *);
-__global__ void k_gft_final(int, const int *, const double *, const double *, double *, double *,
-                            const PcpgState *);
-__global__ void k_gf_apply(int, const int *, const double *, const double *, const double *, double *,
-                           const double *, double *, const PcpgState *);
 __global__ void k_gf_mult(int, const int *, const double *, const double *, double *);
 __global__ void k_update_lam_g(int, const double *, int, const double *, const double *, double *, double *,
                                PcpgState *);
@@ -177,12 +168,6 @@ __global__ void k_gather_u(int ndof, const int *__restrict__ win, const double *
     if (g >= ndof) return;
     const int s = win[g];
     u[g] = (s >= 0) ? uloc[s] : 0.0;
-}
-
-__global__ void k_copy(long long n, const double *__restrict__ a, double *__restrict__ b, const PcpgState *st) {
-    if (st && st->done) return;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        b[i] = a[i];
 }
 
 // ---------------------------------------------------------------------------

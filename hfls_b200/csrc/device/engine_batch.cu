@@ -50,7 +50,6 @@ __global__ void k_update_w_multi(int, int, const double *, const double *, doubl
 __global__ void k_finish_multi(int, const double *, const double *, PcpgState *);
 __global__ void k_col_get(int, int, int, const double *, double *);
 __global__ void k_col_set(int, int, int, const double *, double *);
-__global__ void k_sum_to(const double *, int, double *, const PcpgState *);
 __global__ void k_build_f(int, int, int, const double *, const int *, const double *, double *);
 __global__ void k_trsm_fwd_multi(const SubDev *, const double *, double *, long long, int, const int *);
 __global__ void k_trsm_bwd_multi(const SubDev *, const double *, double *, long long, int, const int *);

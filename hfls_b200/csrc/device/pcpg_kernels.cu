@@ -3,17 +3,17 @@
 // gives the same bits alone and inside a batch.
 //
 //  F w = Bf K_HT^+ Bf^T w   (Cluster::mult_Ff, Cluster.cpp:1114-1188):
-//    k_gather_b   x_b = Bf_d^T w             signed gather over the b slots
-//    k_symv       y_b = F_d x_b              packed 32x32 lower tiles, one pass
-//    k_vt         t_d = V_d^T x_b            V = [F Bc_b^T, -R_b]
-//    k_gc         gc  = sum_d t_d            per cluster (gather map)
-//    k_coarse     s   = M gc                 M = Ac^{-1} restricted
-//    k_correct    y_b -= V_d s_d
-//    k_rows       Fw  = Bf y                 <= 2 entries per row
+//    k_gather_b        x_b = Bf_d^T w             signed gather over the b slots
+//    k_symv_units      y_b = F_d x_b              packed 32x32 lower tiles, one pass, in work
+//                      t_d = V_d^T x_b            units; V = [F Bc_b^T, -R_b]
+//    k_gc              gc  = sum_d t_d            per cluster (gather map)
+//    k_coarse          s   = M gc                 M = Ac^{-1} restricted
+//    k_reduce_correct  y_b = sum of the unit partials - V_d s_d
+//    k_rows            Fw  = Bf y                 <= 2 entries per row
 //  Preconditioner (Cluster::Preconditioning, Cluster.cpp:1043-1112):
-//    k_gather_b(weighted) -> k_symv(S_d or K_bb) -> k_rows(weighted)
+//    k_gather_b(weighted) -> k_symv_units(S_d or K_bb) -> k_reduce_correct -> k_rows(weighted)
 //  Projector (Cluster::Projection, Cluster.cpp:1314-1329):
-//    k_gft_partial -> k_gft_final -> k_gf_apply
+//    k_gft_partial (Gf^T x partials per chunk) -> k_gf_apply_fused (sums, (Gf^T Gf)^{-1}, x - Gf a)
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -63,59 +63,6 @@ __device__ __forceinline__ void reduce_scatter32(double (&p)[32], int lane) {
 
 constexpr int SYMV_WARPS = 4;
 
-template <typename T>
-__global__ void __launch_bounds__(SYMV_WARPS * 32) k_symv(const SubDev *__restrict__ subs,
-                                                          const T *__restrict__ tiles,
-                                                          const double *__restrict__ xb,
-                                                          double *__restrict__ yb,
-                                                          const PcpgState *__restrict__ st) {
-    if (st && st->done) return;
-    extern __shared__ double sm[];
-    const SubDev &sd = subs[blockIdx.x];
-    const int nbp = sd.nbp, nt = sd.nt;
-    double *xs = sm;                       // nbp
-    double *yp = sm + nbp;                 // SYMV_WARPS x nbp
-    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
-    for (int i = threadIdx.x; i < nbp; i += blockDim.x) xs[i] = xb[sd.xb_off + i];
-    for (int i = threadIdx.x; i < SYMV_WARPS * nbp; i += blockDim.x) yp[i] = 0.0;
-    __syncthreads();
-    double *my = yp + warp * nbp;
-    const long long ntiles = (long long)nt * (nt + 1) / 2;
-    const T *base = tiles + sd.T_off * TILE_ELEMS;
-    for (long long t = warp; t < ntiles; t += SYMV_WARPS) {
-        int I = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-        while ((long long)(I + 1) * (I + 2) / 2 <= t) ++I;
-        while ((long long)I * (I + 1) / 2 > t) --I;
-        const int J = (int)(t - (long long)I * (I + 1) / 2);
-        const T *tp = base + t * TILE_ELEMS;
-        double v[32];
-#pragma unroll
-        for (int r = 0; r < 32; ++r) v[r] = (double)tp[r * TILE + lane];    // v[r] = A[r][lane]
-        const double xJ = xs[TILE * J + lane];
-        double p[32];
-        double col = 0.0;
-#pragma unroll
-        for (int r = 0; r < 32; ++r) {
-            p[r] = v[r] * xJ;
-            col += v[r] * xs[TILE * I + r];
-        }
-        reduce_scatter32(p, lane);
-        my[TILE * I + lane] += p[0];                   // row sums -> y_I
-        if (I != J) my[TILE * J + lane] += col;        // column sums -> y_J
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < nbp; i += blockDim.x) {
-        double s = 0.0;
-#pragma unroll
-        for (int q = 0; q < SYMV_WARPS; ++q) s += yp[q * nbp + i];
-        yb[sd.xb_off + i] = s;
-    }
-}
-
-template __global__ void k_symv<double>(const SubDev *, const double *, const double *, double *,
-                                        const PcpgState *);
-template __global__ void k_symv<float>(const SubDev *, const float *, const double *, double *,
-                                       const PcpgState *);
 
 // SYMV over work units (kinds 0 and 2) and V^T x (kind 1) in one launch; the
 // partial y of a unit over its row window -> ypart[y_off, y_off + rows),
@@ -232,23 +179,6 @@ __global__ void k_reduce_correct(const SubDev *__restrict__ subs, const SymvUnit
     yb[sd.xb_off + i] = a;
 }
 
-// t_d = V_d^T x_b  (c+6 values per subdomain)
-__global__ void k_vt(const SubDev *__restrict__ subs, const double *__restrict__ Vbuf,
-                     const double *__restrict__ xb, double *__restrict__ t, const PcpgState *__restrict__ st) {
-    if (st && st->done) return;
-    const SubDev &sd = subs[blockIdx.x];
-    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nw = blockDim.x / 32;
-    const double *x = xb + sd.xb_off;
-    for (int col = warp; col < sd.c + 6; col += nw) {
-        const double *V = Vbuf + sd.V_off + (size_t)col * sd.nbp;
-        double s = 0.0;
-        for (int i = lane; i < sd.nb; i += 32) s += V[i] * x[i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
-        if (lane == 0) t[sd.t_off + col] = s;
-    }
-}
-
 // gc[q] = sum of the t entries listed for q (fixed order)
 __global__ void k_gc(int ngc_total, const int *__restrict__ gptr, const int *__restrict__ gidx,
                      const double *__restrict__ t, double *__restrict__ gc, const PcpgState *__restrict__ st) {
@@ -328,24 +258,6 @@ __global__ void k_rows(int nlam, const int *__restrict__ rslot, const double *__
     if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
 }
 
-// ---------------------------------------------------------------------------
-// deterministic dot products
-// ---------------------------------------------------------------------------
-__global__ void k_dot_partial(int n, const double *__restrict__ a, const double *__restrict__ b,
-                              double *__restrict__ partial, const PcpgState *__restrict__ st) {
-    if (st && st->done) return;
-    __shared__ double red[256];
-    double s = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
-    red[threadIdx.x] = s;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
-}
-
 __device__ double block_sum_fixed(const double *partial, int np) {
     __shared__ double red[256];
     double s = 0.0;
@@ -359,13 +271,6 @@ __device__ double block_sum_fixed(const double *partial, int np) {
     const double r = red[0];
     __syncthreads();
     return r;
-}
-
-__global__ void k_sum_to(const double *__restrict__ partial, int np, double *__restrict__ out,
-                         const PcpgState *__restrict__ st) {
-    if (st && st->done) return;
-    const double s = block_sum_fixed(partial, np);
-    if (threadIdx.x == 0) *out = s;
 }
 
 // ---------------------------------------------------------------------------
@@ -396,28 +301,6 @@ __global__ void k_gft_partial(const int *__restrict__ chunk_cl, const int *__res
         __syncthreads();
     }
     if (threadIdx.x < 6) partial[6 * (size_t)ch + threadIdx.x] = red[threadIdx.x][0];
-}
-
-// one CTA: a = invGtG * (sum of chunk partials per cluster); alpha_out = -a
-__global__ void k_gft_final(int ncl, const int *__restrict__ cl_chunk_ptr, const double *__restrict__ partial,
-                            const double *__restrict__ invGtG, double *__restrict__ a,
-                            double *__restrict__ alpha_out, const PcpgState *__restrict__ st) {
-    if (st && st->done) return;
-    extern __shared__ double gt[];
-    const int m = 6 * ncl;
-    for (int q = threadIdx.x; q < m; q += blockDim.x) {
-        const int c = q / 6, i = q % 6;
-        double s = 0.0;
-        for (int ch = cl_chunk_ptr[c]; ch < cl_chunk_ptr[c + 1]; ++ch) s += partial[6 * (size_t)ch + i];
-        gt[q] = s;
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < m; q += blockDim.x) {
-        double s = 0.0;
-        for (int p = 0; p < m; ++p) s += invGtG[q + (size_t)p * m] * gt[p];
-        a[q] = s;
-        if (alpha_out) alpha_out[q] = -s;
-    }
 }
 
 // Px = x - Gf a with a = invGtG * (chunk partials summed per cluster)
@@ -453,38 +336,6 @@ __global__ void k_gf_apply_fused(int nlam, int ncl, const int *__restrict__ cl_c
         }
     }
     __syncthreads();
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    double prod = 0.0;
-    if (r < nlam) {
-        double v = 0.0;
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int c = gcl[2 * r + k];
-            if (c < 0) continue;
-            const double *g = gval + 6 * (size_t)(2 * r + k);
-#pragma unroll
-            for (int q = 0; q < 6; ++q) v += g[q] * a[6 * c + q];
-        }
-        const double pv = x[r] - v;
-        Px[r] = pv;
-        if (dotv) prod = pv * dotv[r];
-    }
-    if (!partial) return;
-    red[threadIdx.x] = prod;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
-}
-
-__global__ void k_gf_apply(int nlam, const int *__restrict__ gcl, const double *__restrict__ gval,
-                           const double *__restrict__ x, const double *__restrict__ a, double *__restrict__ Px,
-                           const double *__restrict__ dotv, double *__restrict__ partial,
-                           const PcpgState *__restrict__ st) {
-    if (st && st->done) return;
-    __shared__ double red[256];
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     double prod = 0.0;
     if (r < nlam) {
