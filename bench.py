@@ -315,7 +315,11 @@ def run_serving(hb, local, n_req):
     for i, t in enumerate(tickets):
         try:
             u, info = srv.wait(t)
-            served.append((i, u.copy(), info.t_submit_ms, info.t_done_ms, info.iterations_max))
+            served.append((i, u.copy(), info.t_submit_ms, info.t_done_ms, info.iterations_max,
+                           dict(queue_ms=round(info.t_admit_ms - info.t_submit_ms, 1),
+                                setup_ms=round(info.t_start_ms - info.t_admit_ms, 1),
+                                run_ms=round(info.t_done_ms - info.t_start_ms, 1),
+                                iterations=info.iterations_max, gb=round(info.bytes / 1e9, 2))))
         except hb.HTFError as e:
             served.append((i, None, None, None, e.code, str(e)[:200]))
     srv.close()
@@ -325,7 +329,7 @@ def run_serving(hb, local, n_req):
     makespan = (max(x[3] for x in ok) - min(x[2] for x in ok)) / 1e3 if ok else None
     # plain FP64 per-request path: service time of each served request, FIFO on the same arrivals
     service, err = [], 0.0
-    for (i, u, _, _, _) in ok:
+    for (i, u, *_) in ok:
         ta, spec, k, _, _ = stream[i]
         t = time.perf_counter()
         s = hb.Solver(dict(OPTS, device=str(local), max_iter="5000"))
@@ -354,6 +358,7 @@ def run_serving(hb, local, n_req):
                              "service_s": [round(x, 3) for x in service]},
         "u_rel_err_max_vs_fp64": err,
         "sizes": [dict(c=x[4][0], s=x[4][1], e=x[4][2], load_cases=x[2]) for x in stream],
+        "per_request": [dict(request=x[0], **x[5]) for x in ok],
         "errors": [x[5] for x in served if x[1] is None],
     }
 

@@ -6,9 +6,10 @@
 // and runs their setup on each request's own stream, overlapping the
 // iterations of the requests already running.  A run thread advances every
 // live request one batched mixed-precision PCPG iteration at a time: the
-// FP64 phases of each request run back to back on the server stream around
-// ONE tensor-core launch for the F products of all live requests and one for
-// their S products (the F applies of all requests are batched together).
+// FP64 phases of the requests run side by side, each on its own stream forked
+// from and joined back to the server stream, around ONE tensor-core launch
+// for the F products of all live requests and one for their S products (the
+// F applies of all requests are batched together).
 // The sequence is captured as a CUDA graph, re-captured whenever the live set
 // changes; requests join and leave only between groups of check_every
 // iterations, so each request sees the same iteration cadence, and the same
@@ -51,6 +52,8 @@ struct Request {
     std::unique_ptr<Problem> p;
     std::unique_ptr<Engine> eng;
     htf_stats stats{};
+    cudaStream_t rs = nullptr;      // this request's stream while it iterates
+    cudaEvent_t joined = nullptr;   // marks the end of its phase on rs (graph capture)
 };
 
 class Server {
@@ -95,6 +98,7 @@ private:
     std::thread t_setup_, t_run_;
     // run-thread state
     cudaStream_t stream_ = nullptr;
+    cudaEvent_t fork_ = nullptr;               // start of a phase on the server stream (graph capture)
     cudaGraphExec_t graph_ = nullptr;
     bool dirty_ = true;
     GemmBlock *d_blocks_ = nullptr;
@@ -116,6 +120,7 @@ int Server::start(std::string &err) {
     if (opt_.batch != 16 && opt_.batch != 32) { err = "batch width must be 16 or 32"; return HTF_EINVAL; }
     int rc = ck(cudaSetDevice(opt_.device), "cudaSetDevice", err);
     if (!rc) rc = ck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate", err);
+    if (!rc) rc = ck(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate", err);
     if (!rc) rc = ck(cudaMalloc(&d_err_, sizeof(int)), "cudaMalloc", err);
     if (!rc) rc = ck(cudaMemset(d_err_, 0, sizeof(int)), "cudaMemset", err);
     if (rc) return rc;
@@ -143,6 +148,7 @@ Server::~Server() {
     if (d_blocks_) cudaFree(d_blocks_);
     if (d_sets_) cudaFree(d_sets_);
     if (d_err_) cudaFree(d_err_);
+    if (fork_) cudaEventDestroy(fork_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -289,6 +295,10 @@ void Server::finish(Request *r, int rc, const std::string &msg) {
         r->eng->set_stream(nullptr);
         r->eng.reset();
     }
+    if (r->joined) cudaEventDestroy(r->joined);
+    if (r->rs && r->rs != stream_) cudaStreamDestroy(r->rs);
+    r->joined = nullptr;
+    r->rs = nullptr;
     r->p.reset();
     std::lock_guard<std::mutex> lk(mu_);
     if (r->info.status >= HTF_REQ_SETUP) {
@@ -371,12 +381,28 @@ int Server::rebuild_graph(std::string &err) {
     cudaGraph_t g;
     if ((rc = ck(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture", err)))
         return rc;
-    for (Request *r : live_) r->eng->iter_a();
-    tc_launch(opt_.batch, d_blocks_, nblocks_, d_sets_, 0, smem, d_err_, stream_);
-    for (Request *r : live_) r->eng->iter_b();
-    tc_launch(opt_.batch, d_blocks_, nblocks_, d_sets_, 1, smem, d_err_, stream_);
-    for (Request *r : live_) r->eng->iter_c();
-    if ((rc = ck(cudaStreamEndCapture(stream_, &g), "cudaStreamEndCapture", err))) return rc;
+    // each request's phase on its own stream, forked from and joined back to the server stream
+    auto phase = [&](void (Engine::*fn)()) -> int {
+        int e = ck(cudaEventRecord(fork_, stream_), "cudaEventRecord", err);
+        for (Request *r : live_) {
+            if (!e) e = ck(cudaStreamWaitEvent(r->rs, fork_, 0), "cudaStreamWaitEvent", err);
+            if (!e) ((*r->eng).*fn)();
+            if (!e) e = ck(cudaEventRecord(r->joined, r->rs), "cudaEventRecord", err);
+            if (!e) e = ck(cudaStreamWaitEvent(stream_, r->joined, 0), "cudaStreamWaitEvent", err);
+        }
+        return e;
+    };
+    rc = phase(&Engine::iter_a);
+    if (!rc) tc_launch(opt_.batch, d_blocks_, nblocks_, d_sets_, 0, smem, d_err_, stream_);
+    if (!rc) rc = phase(&Engine::iter_b);
+    if (!rc) tc_launch(opt_.batch, d_blocks_, nblocks_, d_sets_, 1, smem, d_err_, stream_);
+    if (!rc) rc = phase(&Engine::iter_c);
+    const int rc_end = ck(cudaStreamEndCapture(stream_, &g), "cudaStreamEndCapture", err);
+    if (rc) {
+        if (!rc_end) cudaGraphDestroy(g);
+        return rc;
+    }
+    if ((rc = rc_end)) return rc;
     rc = ck(cudaGraphInstantiate(&graph_, g, 0), "cudaGraphInstantiate", err);
     cudaGraphDestroy(g);
     dirty_ = false;
@@ -391,7 +417,10 @@ void Server::run_loop() {
             cv_.wait(lk, [&] { return !ready_.empty() || !live_.empty() || (stop_ && outstanding_ == 0); });
             if (live_.empty() && ready_.empty()) return;     // stopping and drained
             for (Request *r : ready_) {
-                r->eng->set_stream(stream_);
+                if (!r->rs && cudaStreamCreateWithFlags(&r->rs, cudaStreamNonBlocking) != cudaSuccess) r->rs = stream_;
+                if (!r->joined && cudaEventCreateWithFlags(&r->joined, cudaEventDisableTiming) != cudaSuccess)
+                    r->joined = nullptr;
+                r->eng->set_stream(r->rs);
                 r->info.status = HTF_REQ_RUNNING;
                 r->info.t_start_ms = now_ms();
                 live_.push_back(r);
@@ -402,6 +431,11 @@ void Server::run_loop() {
         std::string err;
         int rc = HTF_OK;
         if (dirty_) rc = rebuild_graph(err);
+        // work the requests left on their own streams (residual replacements) comes first
+        for (Request *r : live_) {
+            if (!rc && r->rs != stream_) rc = ck(cudaEventRecord(r->joined, r->rs), "cudaEventRecord", err);
+            if (!rc && r->rs != stream_) rc = ck(cudaStreamWaitEvent(stream_, r->joined, 0), "cudaStreamWaitEvent", err);
+        }
         for (int k = 0; !rc && k < opt_.check_every; ++k)
             rc = ck(cudaGraphLaunch(graph_, stream_), "cudaGraphLaunch", err);
         int tcerr = 0;
@@ -433,8 +467,8 @@ void Server::run_loop() {
             if (!rc2) rc2 = r->eng->batch_finish(&r->stats, ms, e2);
             if (rc2 != HTF_ECUDA && r->u_out) {
                 cudaMemcpyAsync(r->u_out, r->eng->u_dev(), (size_t)r->eng->n_dof() * r->nrhs * sizeof(double),
-                                cudaMemcpyDeviceToHost, stream_);
-                if (cudaStreamSynchronize(stream_) != cudaSuccess && !rc2) {
+                                cudaMemcpyDeviceToHost, r->eng->stream());
+                if (cudaStreamSynchronize(r->eng->stream()) != cudaSuccess && !rc2) {
                     rc2 = HTF_ECUDA;
                     e2 = "copy of the displacements failed";
                 }
