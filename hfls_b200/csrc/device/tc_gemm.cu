@@ -145,12 +145,14 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
     constexpr int GW = 3 * K;                              // TMEM columns per accumulator group
     constexpr uint32_t TMEM_COLS = K == 32 ? 256 : 128;   // power of two >= TC_NACC * GW
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // 1024-byte aligned stage buffers: stage s holds A (FP32), A_lo, then X_hi, X_lo
+    // 1024-byte aligned buffers: stage s holds A (FP32) and X_hi, X_lo (copied
+    // from HBM); A_lo of K slab kk is formed in buffer kk mod TC_LO
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    float *sA = reinterpret_cast<float *>(base);                          // TC_STAGES x 2 x 16 KB
-    float *sB = reinterpret_cast<float *>(base + TC_STAGES * 2 * TC_SLAB_A * 4);
-    __shared__ __align__(8) uint64_t full[TC_STAGES], split[TC_STAGES], empty[TC_STAGES], done;
+    float *sA = reinterpret_cast<float *>(base);                          // TC_STAGES x 16 KB
+    float *sB = reinterpret_cast<float *>(base + TC_STAGES * TC_SLAB_A * 4);
+    float *sL = reinterpret_cast<float *>(base + TC_STAGES * (TC_SLAB_A + 2 * SLAB_B) * 4);   // TC_LO x 16 KB
+    __shared__ __align__(8) uint64_t full[TC_STAGES], split[TC_STAGES], empty[TC_STAGES], lo_empty[TC_LO], done;
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
 
@@ -169,6 +171,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
             mbar_init(&split[s], 4);                      // one arrival per splitting warp
             mbar_init(&empty[s], 1);
         }
+        for (int s = 0; s < TC_LO; ++s) mbar_init(&lo_empty[s], 1);
         mbar_init(&done, 1);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -196,7 +199,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                 }
                 if (abort_flag) break;
                 mbar_expect_tx(&full[s], STAGE_TX);
-                bulk_g2s(sA + s * 2 * TC_SLAB_A, A + g.a_off + (long long)kk * TC_SLAB_A, TC_SLAB_A * 4, &full[s]);
+                bulk_g2s(sA + s * TC_SLAB_A, A + g.a_off + (long long)kk * TC_SLAB_A, TC_SLAB_A * 4, &full[s]);
                 bulk_g2s(sB + s * 2 * SLAB_B, Xs + g.x_off + (long long)kk * SLAB_B, SLAB_B * 4, &full[s]);
                 bulk_g2s(sB + (s * 2 + 1) * SLAB_B, Xs + xlo_off + g.x_off + (long long)kk * SLAB_B, SLAB_B * 4,
                          &full[s]);
@@ -218,8 +221,8 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t d = tmem + uint32_t((kk % TC_NACC) * GW);   // [hi-hi | hi-lo | lo-hi]
-                const uint64_t da = sw128_desc(sA + s * 2 * TC_SLAB_A);
-                const uint64_t dal = sw128_desc(sA + (s * 2 + 1) * TC_SLAB_A);
+                const uint64_t da = sw128_desc(sA + s * TC_SLAB_A);
+                const uint64_t dal = sw128_desc(sL + (kk % TC_LO) * TC_SLAB_A);
                 const uint64_t db = sw128_desc(sB + s * 2 * SLAB_B);      // X_hi, X_lo: 2k rows
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {              // 4 x K=8 (32 bytes) per slab
@@ -230,6 +233,9 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&empty[s]))
                              : "memory");
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&lo_empty[kk % TC_LO]))
+                             : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                              smem_u32(&done))
@@ -239,16 +245,17 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
         // warps 2-5: split the A slab of every stage, then the epilogue
         const int t = threadIdx.x - 64;                  // 0..127
         for (int kk = 0; kk < g.ks; ++kk) {
-            const int s = kk % TC_STAGES;
-            bool ok = mbar_wait(&full[s], (kk / TC_STAGES) & 1);
-            ok = __all_sync(0xffffffffu, ok);
-            if (!ok || abort_flag) {
-                if (lane == 0) atomicExch(err, HTF_ETIMEDOUT);
+            const int s = kk % TC_STAGES, lb = kk % TC_LO;
+            // the A_lo buffer of slab kk - TC_LO is free once its MMAs completed; the A slab has landed
+            bool ok = kk < TC_LO || mbar_wait(&lo_empty[lb], ((kk / TC_LO) - 1) & 1);
+            ok = __all_sync(0xffffffffu, ok && mbar_wait(&full[s], (kk / TC_STAGES) & 1));
+            if (!__all_sync(0xffffffffu, ok && !abort_flag)) {          // warp-uniform exit
+                if (lane == 0 && !ok) atomicExch(err, HTF_ETIMEDOUT);
                 abort_flag = 1;
                 break;
             }
-            const float4 *a4 = reinterpret_cast<const float4 *>(sA + s * 2 * TC_SLAB_A);
-            float4 *lo = reinterpret_cast<float4 *>(sA + (s * 2 + 1) * TC_SLAB_A);
+            const float4 *a4 = reinterpret_cast<const float4 *>(sA + s * TC_SLAB_A);
+            float4 *lo = reinterpret_cast<float4 *>(sL + lb * TC_SLAB_A);
 #pragma unroll
             for (int i = t; i < TC_SLAB_A / 4; i += 128) {
                 const float4 v = a4[i];
@@ -273,8 +280,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                 for (int q = 0; q < sd.c + 6; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(Vr + (size_t)q * sd.nbp));
             }
         }
-        bool have = mbar_wait(&done, 0);
-        have = __all_sync(0xffffffffu, have);            // warp-uniform before the .sync.aligned loads
+        const bool have = __all_sync(0xffffffffu, mbar_wait(&done, 0));   // warp-uniform before the .sync.aligned loads
         __syncwarp();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int quarter = warp & 3;                     // TMEM lanes this warp may read
@@ -282,9 +288,10 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
         double acc[K];
 #pragma unroll
         for (int j = 0; j < K; ++j) acc[j] = 0.0;
+        const bool go = __all_sync(0xffffffffu, have && !abort_flag);
         if (!have) {
             if (lane == 0) atomicExch(err, HTF_ETIMEDOUT);
-        } else if (!abort_flag) {
+        } else if (go) {
             const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16);
             const int nacc = g.ks < TC_NACC ? g.ks : TC_NACC;
             for (int a = 0; a < nacc; ++a) {
@@ -326,7 +333,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
             }
             asm volatile("bar.sync 1, 128;" ::: "memory");   // ss is overwritten below
         }
-        if (have && !abort_flag) {
+        if (go) {
             // each warp's 32 output rows are contiguous in yb: transpose them
             // through shared memory (row stride K+1 doubles) and store coalesced
             double *st = reinterpret_cast<double *>(base) + quarter * 32 * (K + 1);
