@@ -84,7 +84,7 @@ private:
     void f_post(double *Fw, const double *dotv, double *partial);
     void m_pre(const double *x);
     void m_post(double *z);
-    int fp64_residual(int j, bool reset_w, std::string &err);
+    int fp64_residual_batch(const std::vector<int> &sel, const std::vector<int> &reset, std::string &err);
     void profile_batch_gather(const double *w);
     void op_F_batch(const double *w, double *Fw, const double *dotv, double *partial);
     void op_M_batch(const double *x, double *z);
@@ -168,6 +168,10 @@ private:
            *b_alpha_ = nullptr, *b_tmp_ = nullptr;
     double *b_fullA_ = nullptr, *b_fullB_ = nullptr;   // full vectors of the batch (nfull x K)
     double *b_srec_ = nullptr;                         // coarse solutions of the reconstruction (ngc x K)
+    double *b_alpha2_ = nullptr;                       // alpha of the FP64 residuals, K-interleaved
+    int *d_mask_ = nullptr;                            // selected / reset columns of an FP64 residual batch
+    void *d_rowblk_ = nullptr;                         // (subdomain, 32-row block) list of the FP64 multi-RHS SYMV
+    int nrowblk_ = 0;
     PcpgState *b_st_ = nullptr;
     cudaGraphExec_t bgraph_ = nullptr;
     int bkernels_per_iter_ = 0;

@@ -15,6 +15,7 @@
 // server can run the phases of several problems around one tensor-core
 // launch over all their blocks.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -51,6 +52,12 @@ __global__ void k_finish_multi(int, const double *, const double *, PcpgState *)
 __global__ void k_col_get(int, int, int, const double *, double *);
 __global__ void k_col_set(int, int, int, const double *, double *);
 __global__ void k_build_f(int, int, int, const double *, const int *, const double *, double *);
+template <int K>
+__global__ void k_symv_rows_multi(const int2 *, const SubDev *, const double *, const double *, double *,
+                                  const ClusterDev *, const double *, const int *, const double *);
+__global__ void k_cols_copy(long long, int, const int *, const double *, double *);
+__global__ void k_alpha_cols(int, int, const int *, const double *, double *);
+__global__ void k_axpby(int, double, const double *, double, double *);
 __global__ void k_trsm_fwd_multi(const SubDev *, const double *, double *, long long, int, const int *);
 __global__ void k_trsm_bwd_multi(const SubDev *, const double *, double *, long long, int, const int *);
 __global__ void k_gather_b(int, const int *, const int *, const double *, const double *, double *,
@@ -148,6 +155,16 @@ int Engine::setup_batch(int K, std::string &err) {
     b_gt_ = alloc<double>((size_t)6 * ncl_ * K, err, rc); b_acoef_ = alloc<double>((size_t)6 * ncl_ * K, err, rc);
     b_alpha_ = alloc<double>((size_t)6 * ncl_ * K, err, rc);
     b_st_ = alloc<PcpgState>(K, err, rc);
+    b_alpha2_ = alloc<double>((size_t)6 * ncl_ * K, err, rc);
+    d_mask_ = alloc<int>(2 * K, err, rc);
+    {
+        std::vector<int2> rb;                       // (subdomain, 32-row block) of the FP64 multi-RHS SYMV
+        for (int d = 0; d < nsub_; ++d)
+            for (int I = 0; I < hs_[d].nt; ++I) rb.push_back(make_int2(d, I));
+        nrowblk_ = int(rb.size());
+        d_rowblk_ = alloc<int2>(rb.size(), err, rc);
+        if (!rc) CKB(cudaMemcpyAsync(d_rowblk_, rb.data(), rb.size() * sizeof(int2), cudaMemcpyHostToDevice, s_));
+    }
     b_fullA_ = alloc<double>((size_t)nfull_ * K, err, rc);
     b_fullB_ = alloc<double>((size_t)nfull_ * K, err, rc);
     b_srec_ = alloc<double>((size_t)ngc_total_ * K, err, rc);
@@ -306,41 +323,85 @@ int Engine::batch_loads(int nrhs, const double *f_nodal, std::string &err) {
     return HTF_OK;
 }
 
-// FP64 residual of load case j of the running chunk (Cluster.cpp:1398-1412
-// from the current lambda): g, Pz, g'Pz; replaces the batch residual column,
-// and the search direction too when reset_w
-int Engine::fp64_residual(int j, bool reset_w, std::string &err) {
+// FP64 residuals of the load cases j with sel[j] (Cluster.cpp:1398-1412 from
+// the current lambda), all in one pass over the FP64 tiles: g = F lambda - d,
+// P g (alpha), z = M P g, P z and g'Pz.  They replace the batch residual
+// columns of the selected load cases, and the search directions of those with
+// reset[j].  Every column is computed independently of the others, so a load
+// case gets the same bits alone and in a batch.
+int Engine::fp64_residual_batch(const std::vector<int> &sel, const std::vector<int> &reset, std::string &err) {
     BatchRun &r = run_;
+    const auto t_start = std::chrono::steady_clock::now();
     const int K = bK_;
-    k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_lam_, d_lam_);
-    k_col_get<<<npart_, 256, 0, s_>>>(nlam_, K, j, b_d_, d_d_);
-    pcpg_start(d_st_);
-    launches_ += 2 + 15;
-    PcpgState h;
-    CKB(cudaMemcpyAsync(&h, d_st_, sizeof(PcpgState), cudaMemcpyDeviceToHost, s_));
-    CKB(cudaMemcpyAsync(b_alpha_ + (size_t)j * 6 * ncl_, d_alpha_, 6 * ncl_ * sizeof(double),
-                        cudaMemcpyDeviceToDevice, s_));
-    CKB(cudaStreamSynchronize(s_));
-    k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_g_, b_g_);
-    launches_ += 1;
-    if (reset_w) {
-        k_col_set<<<npart_, 256, 0, s_>>>(nlam_, K, j, d_Pz_, b_w_);
-        launches_ += 1;
+    const long long nk = (long long)nlam_ * K;
+    int maxg = 0;
+    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
+    auto symv = [&](const double *tiles, const double *scoarse) {
+        if (K == 32)
+            k_symv_rows_multi<32><<<nrowblk_, 256, 0, s_>>>(static_cast<const int2 *>(d_rowblk_), d_subs_, tiles, b_xb_,
+                                                           b_yb_, d_cl_, d_V_, d_bcr_, scoarse);
+        else
+            k_symv_rows_multi<16><<<nrowblk_, 256, 0, s_>>>(static_cast<const int2 *>(d_rowblk_), d_subs_, tiles, b_xb_,
+                                                           b_yb_, d_cl_, d_V_, d_bcr_, scoarse);
+    };
+    // g = F lambda - d
+    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, b_lam_, nullptr, b_xb_, nullptr,
+                                                 nullptr);
+    if (K == 32) k_vt_multi<32><<<dim3(nsub_, vt_nch_), 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
+    else k_vt_multi<16><<<dim3(nsub_, vt_nch_), 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
+    k_gc_multi<<<cdivb((long long)ngc_total_ * K, 256), 256, 0, s_>>>(ngc_total_, K, vt_nch_, d_gptr_, d_gidx_, b_t_,
+                                                                      b_gc_);
+    if (K == 32) k_coarse_multi<32><<<dim3(ncl_, cdivb(maxg, 32)), 128, 0, s_>>>(d_cl_, d_M_, b_gc_, b_s_);
+    else k_coarse_multi<16><<<dim3(ncl_, cdivb(maxg, 32)), 128, 0, s_>>>(d_cl_, d_M_, b_gc_, b_s_);
+    symv(d_F_, b_s_);
+    k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, nullptr, b_tmp_, nullptr, nullptr);
+    k_axpby<<<cdivb(nk, 256), 256, 0, s_>>>(int(nk), -1.0, b_d_, 1.0, b_tmp_);
+    op_P_batch(b_tmp_, b_Pg_, b_alpha2_, nullptr, nullptr);
+    // z = M P g, P z, g'Pz
+    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, b_Pg_, d_weight_, b_xb_,
+                                                 nullptr, nullptr);
+    symv(d_S_, nullptr);
+    k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, d_weight_, b_z_, nullptr, nullptr);
+    op_P_batch(b_z_, b_Pz_, nullptr, b_tmp_, b_part_);
+    k_colsum<<<K, 256, 0, s_>>>(b_part_, bnpart_, K, b_gPz_);
+    // the selected columns back into the recurrence
+    std::vector<int> masks(2 * K, 0);
+    for (int j = 0; j < K; ++j) {
+        masks[j] = sel[j];
+        masks[K + j] = sel[j] && reset[j];
     }
-    PcpgState &st = r.st[j];
-    st.gPz = h.gPz;
-    st.gPz_prev = h.gPz;
-    r.last[j] = h.gPz;
-    if (st.norm0 == 0.0) st.norm0 = std::sqrt(h.gPz);
-    const double cur = std::sqrt(h.gPz);
-    r.rel[j] = st.norm0 > 0 ? cur / st.norm0 : 0.0;
-    if (opt_.verbose)
-        std::fprintf(stderr, "[htf mixed] rhs %d it %d FP64 sqrt(gPz)/norm0 = %.3e\n", r.r0 + j, st.it, r.rel[j]);
-    if (!(h.gPz > 0.0) || !std::isfinite(h.gPz) || cur < opt_.eps_iter * st.norm0) {
-        r.conv[j] = 1;
-        st.done = 1;
-    } else {
-        st.done = 0;
+    CKB(cudaMemcpyAsync(d_mask_, masks.data(), 2 * K * sizeof(int), cudaMemcpyHostToDevice, s_));
+    k_cols_copy<<<cdivb(nk, 256), 256, 0, s_>>>(nlam_, K, d_mask_, b_tmp_, b_g_);
+    k_cols_copy<<<cdivb(nk, 256), 256, 0, s_>>>(nlam_, K, d_mask_ + K, b_Pz_, b_w_);
+    k_alpha_cols<<<1, 256, 0, s_>>>(6 * ncl_, K, d_mask_, b_alpha2_, b_alpha_);
+    CKB(cudaGetLastError());
+    launches_ += 19 + 8;
+    std::vector<double> gPz(K);
+    CKB(cudaMemcpyAsync(gPz.data(), b_gPz_, K * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    CKB(cudaStreamSynchronize(s_));
+    if (opt_.verbose) {
+        int m = 0;
+        for (int j = 0; j < K; ++j) m += sel[j];
+        std::fprintf(stderr, "[htf mixed] FP64 residuals of %d load cases: %.3f ms\n", m,
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
+    }
+    for (int j = 0; j < K; ++j) {
+        if (!sel[j]) continue;
+        PcpgState &st = r.st[j];
+        st.gPz = gPz[j];
+        st.gPz_prev = gPz[j];
+        r.last[j] = gPz[j];
+        if (st.norm0 == 0.0) st.norm0 = std::sqrt(gPz[j]);
+        const double cur = std::sqrt(gPz[j]);
+        r.rel[j] = st.norm0 > 0 ? cur / st.norm0 : 0.0;
+        if (opt_.verbose)
+            std::fprintf(stderr, "[htf mixed] rhs %d it %d FP64 sqrt(gPz)/norm0 = %.3e\n", r.r0 + j, st.it, r.rel[j]);
+        if (!(gPz[j] > 0.0) || !std::isfinite(gPz[j]) || cur < opt_.eps_iter * st.norm0) {
+            r.conv[j] = 1;
+            st.done = 1;
+        } else {
+            st.done = 0;
+        }
     }
     return HTF_OK;
 }
@@ -376,12 +437,14 @@ int Engine::batch_begin(int r0, int kc, std::string &err) {
     CKB(cudaEventRecord(run_e0_, s_));
     for (int j = 0; j < K; ++j) r.st[j].done = 1;
     int rc;
+    std::vector<int> sel(K, 0), reset(K, 0);
     for (int j = 0; j < kc; ++j) {
         r.st[j].eps = opt_.eps_iter;
         r.st[j].max_iter = opt_.max_iter;
         r.st[j].wFw = 1.0;
-        if ((rc = fp64_residual(j, true, err))) return rc;
+        sel[j] = reset[j] = 1;
     }
+    if ((rc = fp64_residual_batch(sel, reset, err))) return rc;
     for (int j = kc; j < K; ++j) r.conv[j] = 1;
     CKB(cudaMemcpyAsync(b_st_, r.st.data(), K * sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
     return HTF_OK;
@@ -400,16 +463,19 @@ int Engine::batch_check(bool &all_done, std::string &err) {
     if (tcerr) { err = "tensor-core product timed out on a barrier"; return tcerr; }
     bool changed = false;
     int rc;
+    std::vector<int> sel(K, 0), reset(K, 0);
     for (int j = 0; j < K; ++j) {
         if (r.conv[j]) continue;
         const bool broke = r.st[j].done == 2;
         if (r.st[j].it >= opt_.max_iter) { r.conv[j] = 2; continue; }
         if (r.st[j].done != 0 || r.st[j].gPz < ru2 * r.last[j]) {
             r.st[j].eps = opt_.eps_iter;
-            if ((rc = fp64_residual(j, broke, err))) return rc;
+            sel[j] = 1;
+            reset[j] = broke;
             changed = true;
         }
     }
+    if (changed && (rc = fp64_residual_batch(sel, reset, err))) return rc;
     if (changed) CKB(cudaMemcpyAsync(b_st_, r.st.data(), K * sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
     all_done = true;
     for (int j = 0; j < K; ++j) all_done &= r.conv[j] != 0;

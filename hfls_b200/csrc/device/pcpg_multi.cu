@@ -453,3 +453,119 @@ __global__ void k_col_set(int n, int K, int j, const double *__restrict__ v, dou
 }
 
 }  // namespace htf
+
+namespace htf {
+
+// ---------------------------------------------------------------------------
+// FP64 residual of several load cases at once (the reliable-update step of
+// the batched form): y_b(:, j) = A_d x_b(:, j) from the packed FP64 tiles for
+// the K columns of a batch vector.  One CTA per (subdomain, 32-row block I)
+// sums the tiles of block row I and, transposed, of block column I, so each
+// output row is written once and no partial sums are needed.  The products
+// run on the FP64 tensor path (mma.sync m8n8k4 .f64): warp w owns the 8-row
+// band w mod 4 and K/16 column bands of 8; shared-memory row strides keep
+// both operand loads free of bank conflicts.  With s given (the F apply),
+// the coarse correction y_b -= V_d s_d is applied before the store.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <int K>
+__global__ void __launch_bounds__(256) k_symv_rows_multi(const int2 *__restrict__ rowblk,
+                                                         const SubDev *__restrict__ subs,
+                                                         const double *__restrict__ tiles,
+                                                         const double *__restrict__ xb, double *__restrict__ yb,
+                                                         const ClusterDev *__restrict__ cl,
+                                                         const double *__restrict__ Vbuf,
+                                                         const int *__restrict__ bcrows,
+                                                         const double *__restrict__ s) {
+    constexpr int NT = K / 16;                      // 8x8 output tiles per warp
+    constexpr int TS = 36, XS = K + 4;              // row strides (doubles): conflict-free fragment loads
+    __shared__ double Ts[32 * TS];
+    __shared__ double Xs[32 * XS];
+    const int2 rb = rowblk[blockIdx.x];
+    const SubDev &sd = subs[rb.x];
+    const int I = rb.y;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int g = lane >> 2, t4 = lane & 3;         // fragment row / column groups
+    const int band = warp & 3, cb0 = (warp >> 2) * NT;
+    const double *base = tiles + sd.T_off * TILE_ELEMS;
+    double acc[NT][2];
+#pragma unroll
+    for (int q = 0; q < NT; ++q) acc[q][0] = acc[q][1] = 0.0;
+    for (int J = 0; J < sd.nt; ++J) {
+        const bool lower = J <= I;
+        const double *tp = base + (lower ? (long long)I * (I + 1) / 2 + J : (long long)J * (J + 1) / 2 + I) * TILE_ELEMS;
+        for (int e = threadIdx.x; e < TILE_ELEMS; e += blockDim.x) {
+            const int rr = e / TILE, cc = e % TILE;
+            const double v = tp[e];                 // stored tile, row rr, column cc
+            if (lower) Ts[rr * TS + cc] = v;        // A[32I + rr][32J + cc]
+            else Ts[cc * TS + rr] = v;              // tile (J, I): A[32I + cc][32J + rr]
+        }
+        for (int e = threadIdx.x; e < TILE * K; e += blockDim.x) {
+            const int c = e / K, j = e % K;
+            Xs[c * XS + j] = xb[(size_t)(sd.xb_off + TILE * J + c) * K + j];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TILE / 4; ++kk) {
+            const double a = Ts[(8 * band + g) * TS + 4 * kk + t4];
+#pragma unroll
+            for (int q = 0; q < NT; ++q) {
+                const double b = Xs[(4 * kk + t4) * XS + 8 * (cb0 + q) + g];
+                dmma_8x8x4(acc[q][0], acc[q][1], a, b);
+            }
+        }
+        __syncthreads();
+    }
+    const int row = TILE * I + 8 * band + g;        // this thread's output row
+    if (s && row < sd.nb) {
+        const int gc_off = cl[sd.cluster].gc_off;
+        const double *Vr = Vbuf + sd.V_off + row;
+        for (int q = 0; q < sd.c + 6; ++q) {
+            const double v = Vr[(size_t)q * sd.nbp];
+            const int pos = q < sd.c ? bcrows[sd.bcr_off + q] : sd.alpha_pos + (q - sd.c);
+            const double *sq = s + ((size_t)gc_off + pos) * K;
+#pragma unroll
+            for (int u = 0; u < NT; ++u) {
+                const int col = 8 * (cb0 + u) + 2 * t4;
+                acc[u][0] -= v * sq[col];
+                acc[u][1] -= v * sq[col + 1];
+            }
+        }
+    }
+    double *y = yb + (size_t)(sd.xb_off + row) * K;
+#pragma unroll
+    for (int u = 0; u < NT; ++u) {
+        const int col = 8 * (cb0 + u) + 2 * t4;
+        y[col] = acc[u][0];
+        y[col + 1] = acc[u][1];
+    }
+}
+template __global__ void k_symv_rows_multi<16>(const int2 *, const SubDev *, const double *, const double *, double *,
+                                               const ClusterDev *, const double *, const int *, const double *);
+template __global__ void k_symv_rows_multi<32>(const int2 *, const SubDev *, const double *, const double *, double *,
+                                               const ClusterDev *, const double *, const int *, const double *);
+
+// B(:, j) = A(:, j) for the columns j with mask[j] (n rows, K-interleaved)
+__global__ void k_cols_copy(long long n, int K, const int *__restrict__ mask, const double *__restrict__ A,
+                            double *__restrict__ B) {
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n * K;
+         o += (long long)gridDim.x * blockDim.x)
+        if (mask[o % K]) B[o] = A[o];
+}
+
+// per-column alpha (m values per column, column-major) of the columns with
+// mask[j] from the projector's K-interleaved output
+__global__ void k_alpha_cols(int m, int K, const int *__restrict__ mask, const double *__restrict__ a,
+                             double *__restrict__ alpha) {
+    for (int o = threadIdx.x; o < m * K; o += blockDim.x) {
+        const int q = o / K, j = o % K;
+        if (mask[j]) alpha[(size_t)j * m + q] = a[o];
+    }
+}
+
+}  // namespace htf
