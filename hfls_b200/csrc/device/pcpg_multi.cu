@@ -236,33 +236,56 @@ __device__ __forceinline__ void block_col_partial(double prod, int K, double *__
 
 // out[r][j] = wt[r] * sum_k sign * y[slot][j]; partial dot with dotv per
 // (block, j).  Blocks stride over groups of 256 / K rows (fixed assignment,
-// so the partials and their sums are the same on every run).
+// so the partials and their sums are the same on every run); each thread
+// has the loads of two of its rows in flight and adds them in row order.
+__device__ __forceinline__ double row_value(int r, int K, int j, const int *__restrict__ rslot,
+                                            const double *__restrict__ rsign, const double *__restrict__ yb,
+                                            const double *__restrict__ weight) {
+    const int2 sl = reinterpret_cast<const int2 *>(rslot)[r];
+    const double2 sg = reinterpret_cast<const double2 *>(rsign)[r];
+    double v = 0.0;
+    if (sl.x >= 0) v += sg.x * yb[(size_t)sl.x * K + j];
+    if (sl.y >= 0) v += sg.y * yb[(size_t)sl.y * K + j];
+    if (weight) v *= weight[r];
+    return v;
+}
+
 __global__ void k_rows_multi(int nlam, int K, const int *__restrict__ rslot, const double *__restrict__ rsign,
                              const double *__restrict__ yb, const double *__restrict__ weight,
                              double *__restrict__ out, const double *__restrict__ dotv,
                              double *__restrict__ partial) {
     const int rows_per_block = 256 / K;
     const int lr = threadIdx.x / K, j = threadIdx.x % K;
+    const int stride = gridDim.x * rows_per_block;
     double prod = 0.0;
-    for (int r0 = blockIdx.x * rows_per_block; r0 < nlam; r0 += gridDim.x * rows_per_block) {
-        const int r = r0 + lr;
-        if (lr < rows_per_block && r < nlam) {
-            double v = 0.0;
-            const int s0 = rslot[2 * r], s1 = rslot[2 * r + 1];
-            if (s0 >= 0) v += rsign[2 * r] * yb[(size_t)s0 * K + j];
-            if (s1 >= 0) v += rsign[2 * r + 1] * yb[(size_t)s1 * K + j];
-            if (weight) v *= weight[r];
-            out[(size_t)r * K + j] = v;
-            if (dotv) prod += v * dotv[(size_t)r * K + j];
+    if (lr < rows_per_block)
+        for (int r0 = blockIdx.x * rows_per_block; r0 < nlam; r0 += 2 * stride) {
+            const int ra = r0 + lr, rb = r0 + stride + lr;
+            const bool ha = ra < nlam, hb = rb < nlam;
+            double va = 0.0, vb = 0.0, da = 0.0, db = 0.0;
+            if (ha) va = row_value(ra, K, j, rslot, rsign, yb, weight);
+            if (hb) vb = row_value(rb, K, j, rslot, rsign, yb, weight);
+            if (dotv) {
+                if (ha) da = dotv[(size_t)ra * K + j];
+                if (hb) db = dotv[(size_t)rb * K + j];
+            }
+            if (ha) {
+                out[(size_t)ra * K + j] = va;
+                if (dotv) prod += va * da;
+            }
+            if (hb) {
+                out[(size_t)rb * K + j] = vb;
+                if (dotv) prod += vb * db;
+            }
         }
-    }
     if (partial) block_col_partial(prod, K, partial);
 }
 
-// Gf^T x per chunk and column: partial[ch][q][j].  Thread (lr, j) walks
-// every (256/K)-th entry of the chunk, four entries per step so the row-index
-// and x loads of consecutive entries are in flight together; the 6 sums are
-// then reduced over lr in one pass through shared memory.
+// Gf^T x per chunk and column: partial[ch][q][j].  The chunk's row indices
+// and Gf values are staged in shared memory 256 entries at a time; thread
+// (lr, j) walks every (256/K)-th entry with eight x loads in flight, adding
+// its entries in the order lr, lr + 256/K, ...; the 6 sums are then reduced
+// over lr in one pass through shared memory.
 __global__ void __launch_bounds__(256) k_gft_partial_multi(int K, const int *__restrict__ chunk_beg,
                                                            const int *__restrict__ chunk_end,
                                                            const int *__restrict__ crow,
@@ -270,29 +293,35 @@ __global__ void __launch_bounds__(256) k_gft_partial_multi(int K, const int *__r
                                                            const double *__restrict__ x,
                                                            double *__restrict__ partial) {
     __shared__ double red[6 * 256];
+    __shared__ double cs[6 * 256];
+    __shared__ int rs[256];
     const int ch = blockIdx.x;
     const int j = threadIdx.x % K, nl = 256 / K, lr = threadIdx.x / K;
     const int beg = chunk_beg[ch], end = chunk_end[ch];
     double s[6] = {0, 0, 0, 0, 0, 0};
-    int e = beg + lr;
-    for (; e + 3 * nl < end; e += 4 * nl) {
-        int r[4];
-        double xv[4];
+    for (int e0 = beg; e0 < end; e0 += 256) {
+        const int n = min(256, end - e0);
+        __syncthreads();                            // the previous stage is consumed
+        if (threadIdx.x < n) rs[threadIdx.x] = crow[e0 + threadIdx.x];
+        for (int o = threadIdx.x; o < 6 * n; o += 256) cs[o] = cval[6 * (size_t)e0 + o];
+        __syncthreads();
+        int e = lr;
+        for (; e + 7 * nl < n; e += 8 * nl) {
+            double xv[8];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) r[u] = crow[e + u * nl];
+            for (int u = 0; u < 8; ++u) xv[u] = x[(size_t)rs[e + u * nl] * K + j];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) xv[u] = x[(size_t)r[u] * K + j];
+            for (int u = 0; u < 8; ++u) {
+                const double *cv = cs + 6 * (e + u * nl);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const double *cv = cval + 6 * (size_t)(e + u * nl);
-#pragma unroll
-            for (int q = 0; q < 6; ++q) s[q] += cv[q] * xv[u];
+                for (int q = 0; q < 6; ++q) s[q] += cv[q] * xv[u];
+            }
         }
-    }
-    for (; e < end; e += nl) {
-        const double xv = x[(size_t)crow[e] * K + j];
+        for (; e < n; e += nl) {
+            const double xv = x[(size_t)rs[e] * K + j];
 #pragma unroll
-        for (int q = 0; q < 6; ++q) s[q] += cval[6 * (size_t)e + q] * xv;
+            for (int q = 0; q < 6; ++q) s[q] += cs[6 * e + q] * xv;
+        }
     }
 #pragma unroll
     for (int q = 0; q < 6; ++q) red[q * 256 + threadIdx.x] = s[q];
