@@ -81,6 +81,7 @@ private:
     double pcpg_start(PcpgState *st);                     // g0, Pg, z, Pz; returns nothing useful
     void tc_apply(int which);
     void f_pre(const double *w);
+    void coarse_batch();
     void f_post(double *Fw, const double *dotv, double *partial);
     void m_pre(const double *x);
     void m_post(double *z);
@@ -175,7 +176,7 @@ private:
     PcpgState *b_st_ = nullptr;
     cudaGraphExec_t bgraph_ = nullptr;
     int bkernels_per_iter_ = 0;
-    int tc_smem_ = 0, vt_nch_ = 1;
+    int tc_smem_ = 0, vt_nch_ = 1, vt_qn_ = 64;
     long long aoff_ = 0;                       // floats per FP32 slab array
     // vectors
     double *d_f_ = nullptr, *d_full_ = nullptr, *d_full2_ = nullptr;

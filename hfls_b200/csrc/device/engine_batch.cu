@@ -30,7 +30,7 @@ __global__ void k_tc_gemm(const GemmBlock *, const TcSet *, int, int *);
 __global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *);
 __global__ void k_gather_multi(int, int, const int *, const int *, const double *, const double *, double *, float *,
                                float *);
-template <int K>
+template <int K, int QN>
 __global__ void k_vt_multi(int, const SubDev *, const double *, const double *, double *);
 __global__ void k_gc_multi(int, int, int, const int *, const int *, const double *, double *);
 template <int K>
@@ -136,10 +136,13 @@ int Engine::setup_batch(int K, std::string &err) {
     const size_t nl = (size_t)nlam_ * K;
     int ntot = 0;
     vt_nch_ = 1;
+    int maxcol = 0;
     for (auto &h : hs_) {
         ntot = std::max(ntot, h.t_off + h.c + 6);
         vt_nch_ = std::max(vt_nch_, (h.nb + 127) / 128);
+        maxcol = std::max(maxcol, h.c + 6);
     }
+    vt_qn_ = maxcol <= 32 ? 32 : maxcol <= 64 ? 64 : 128;     // columns of V^T x_b computed per chunk
     // row kernels stride over row groups with a fixed grid: few partials per column
     bnpart_ = std::min(cdivb(nlam_, 256 / K), 1184);
     b_lam_ = alloc<double>(nl, err, rc); b_g_ = alloc<double>(nl, err, rc); b_w_ = alloc<double>(nl, err, rc);
@@ -207,13 +210,27 @@ void Engine::tc_apply(int which) {
 // tensor-core product, whose epilogue applies the correction
 void Engine::f_pre(const double *w) {
     const int K = bK_;
-    int maxg = 0;
-    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
     const long long xlo = (long long)nslots_ * K;
     k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, w, nullptr, b_xb_, d_Xs_,
                                                  d_Xs_ + xlo);
-    if (K == 32) k_vt_multi<32><<<dim3(nsub_, vt_nch_), 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
-    else k_vt_multi<16><<<dim3(nsub_, vt_nch_), 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
+    coarse_batch();
+}
+
+// s = M_c [Bc_b F x_b ; -R_b^T x_b] per cluster from the batch vector b_xb_:
+// V^T x_b per 128-row chunk, the coarse right-hand side, M G
+void Engine::coarse_batch() {
+    const int K = bK_;
+    int maxg = 0;
+    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
+    const dim3 gv(nsub_, vt_nch_);
+    if (K == 32) {
+        if (vt_qn_ == 32) k_vt_multi<32, 32><<<gv, 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
+        else k_vt_multi<32, 64><<<gv, 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
+    } else {
+        if (vt_qn_ == 32) k_vt_multi<16, 32><<<gv, 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
+        else if (vt_qn_ == 64) k_vt_multi<16, 64><<<gv, 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
+        else k_vt_multi<16, 128><<<gv, 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
+    }
     k_gc_multi<<<cdivb((long long)ngc_total_ * K, 256), 256, 0, s_>>>(ngc_total_, K, vt_nch_, d_gptr_, d_gidx_, b_t_,
                                                                       b_gc_);
     if (K == 32) k_coarse_multi<32><<<dim3(ncl_, cdivb(maxg, 32)), 128, 0, s_>>>(d_cl_, d_M_, b_gc_, b_s_);
@@ -334,8 +351,6 @@ int Engine::fp64_residual_batch(const std::vector<int> &sel, const std::vector<i
     const auto t_start = std::chrono::steady_clock::now();
     const int K = bK_;
     const long long nk = (long long)nlam_ * K;
-    int maxg = 0;
-    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
     auto symv = [&](const double *tiles, const double *scoarse) {
         if (K == 32)
             k_symv_rows_multi<32><<<nrowblk_, 256, 0, s_>>>(static_cast<const int2 *>(d_rowblk_), d_subs_, tiles, b_xb_,
@@ -347,12 +362,7 @@ int Engine::fp64_residual_batch(const std::vector<int> &sel, const std::vector<i
     // g = F lambda - d
     k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, b_lam_, nullptr, b_xb_, nullptr,
                                                  nullptr);
-    if (K == 32) k_vt_multi<32><<<dim3(nsub_, vt_nch_), 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
-    else k_vt_multi<16><<<dim3(nsub_, vt_nch_), 256, 0, s_>>>(vt_nch_, d_subs_, d_V_, b_xb_, b_t_);
-    k_gc_multi<<<cdivb((long long)ngc_total_ * K, 256), 256, 0, s_>>>(ngc_total_, K, vt_nch_, d_gptr_, d_gidx_, b_t_,
-                                                                      b_gc_);
-    if (K == 32) k_coarse_multi<32><<<dim3(ncl_, cdivb(maxg, 32)), 128, 0, s_>>>(d_cl_, d_M_, b_gc_, b_s_);
-    else k_coarse_multi<16><<<dim3(ncl_, cdivb(maxg, 32)), 128, 0, s_>>>(d_cl_, d_M_, b_gc_, b_s_);
+    coarse_batch();
     symv(d_F_, b_s_);
     k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, nullptr, b_tmp_, nullptr, nullptr);
     k_axpby<<<cdivb(nk, 256), 256, 0, s_>>>(int(nk), -1.0, b_d_, 1.0, b_tmp_);

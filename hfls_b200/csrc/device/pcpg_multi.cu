@@ -10,6 +10,15 @@
 
 namespace htf {
 
+// D += A B on the FP64 tensor path: one 8x8x4 product per warp.  Fragments:
+// a = A[g][t4], b = B[t4][g], (d0, d1) = D[g][2 t4], D[g][2 t4 + 1] with
+// g = lane / 4, t4 = lane % 4.
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 // x_b = Bf^T w (optionally weighted; x_b itself only when xb != nullptr) for
 // all K columns; also writes the X
 // slabs of the tensor-core product (TF32 part and TF32 remainder) in the
@@ -52,27 +61,32 @@ __global__ void k_gather_multi(int nslots, int K, const int *__restrict__ ptr, c
 
 // Partial V_d^T x_b over the 128-row chunk ch of subdomain d:
 // tpart[(t_off + q) * nch + ch][j] = sum_{i in chunk} V_d[i][q] x_b[i][j]
-// (chunks past nb write zeros).  32-row pieces of V (stored i-major in
-// shared memory) and x_b are staged; each thread keeps a QPT x (K/8)
-// register tile (q = its q group, j = jg + 8c).  CTA (subdomain, chunk).
-template <int K>
-__device__ __forceinline__ void vt_chunk(int nch, const SubDev &sd, const double *__restrict__ Vbuf,
-                                         const double *__restrict__ xb, double *__restrict__ tpart) {
-    constexpr int QPT = K == 32 ? 2 : 4, CPT = K / 8, VP = 2048 / K + 1;
-    constexpr int UX = 32 * K / 256, UV = 2048 / K * 32 / 256;   // staged values per thread
-    __shared__ double Vs[32 * VP];           // [ii][q]
-    __shared__ double Xs[32 * K];            // [ii][j]
+// for q < c + 6 (QN >= c + 6 columns computed).  32-row pieces of V (stored
+// q-major in shared memory) and x_b are staged, the next piece prefetched
+// into registers; the products run on the FP64 tensor path, warp w owning
+// the 8x8 output tiles w, w + 8, ... (q band = tile % (QN/8)).  Row strides
+// of 36 and K + 4 doubles keep the fragment loads free of bank conflicts.
+// CTA (subdomain, chunk), 256 threads.
+template <int K, int QN>
+__global__ void __launch_bounds__(256) k_vt_multi(int nch, const SubDev *__restrict__ subs,
+                                                  const double *__restrict__ Vbuf, const double *__restrict__ xb,
+                                                  double *__restrict__ tpart) {
+    constexpr int VS = 36, XS = K + 4;
+    constexpr int T = QN * K / 512;                 // 8x8 tiles per warp
+    constexpr int UX = 32 * K / 256, UV = QN / 8;   // staged values per thread
+    __shared__ double Vs[QN * VS];                  // [q][ii]
+    __shared__ double Xs[32 * XS];                  // [ii][j]
+    const SubDev &sd = subs[blockIdx.x];
     const int ch = blockIdx.y;
     const int ncol = sd.c + 6;
     const int r_end = min(sd.nb, ch * 128 + 128);
     const double *V = Vbuf + sd.V_off;
     const double *x = xb + (size_t)sd.xb_off * K;
-    const int jg = threadIdx.x % 8, qg = threadIdx.x / 8;
-    double acc[QPT][CPT];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int g = lane >> 2, t4 = lane & 3;
+    double acc[T][2];
 #pragma unroll
-    for (int a = 0; a < QPT; ++a)
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) acc[a][c] = 0.0;
+    for (int u = 0; u < T; ++u) acc[u][0] = acc[u][1] = 0.0;
     double xr[UX], vr[UV];
     auto fetch = [&](int i0) {
 #pragma unroll
@@ -89,46 +103,48 @@ __device__ __forceinline__ void vt_chunk(int nch, const SubDev &sd, const double
     if (ch * 128 < r_end) fetch(ch * 128);
     for (int i0 = ch * 128; i0 < r_end; i0 += 32) {
 #pragma unroll
-        for (int u = 0; u < UX; ++u) Xs[threadIdx.x + 256 * u] = xr[u];
+        for (int u = 0; u < UX; ++u) {
+            const int o = threadIdx.x + 256 * u;
+            Xs[(o / K) * XS + o % K] = xr[u];
+        }
 #pragma unroll
         for (int u = 0; u < UV; ++u) {
             const int o = threadIdx.x + 256 * u;
-            Vs[(o % 32) * VP + o / 32] = vr[u];
+            Vs[(o / 32) * VS + o % 32] = vr[u];
         }
         __syncthreads();
-        if (i0 + 32 < r_end) fetch(i0 + 32);        // next piece in flight during the FMAs
-#pragma unroll 4
-        for (int ii = 0; ii < 32; ++ii) {
-            double v[QPT], xv[CPT];
+        if (i0 + 32 < r_end) fetch(i0 + 32);        // next piece in flight during the products
 #pragma unroll
-            for (int a = 0; a < QPT; ++a) v[a] = Vs[ii * VP + qg * QPT + a];
+        for (int kk = 0; kk < 8; ++kk) {
 #pragma unroll
-            for (int c = 0; c < CPT; ++c) xv[c] = Xs[ii * K + jg + 8 * c];
-#pragma unroll
-            for (int a = 0; a < QPT; ++a)
-#pragma unroll
-                for (int c = 0; c < CPT; ++c) acc[a][c] += v[a] * xv[c];
+            for (int u = 0; u < T; ++u) {
+                const int tile = warp + 8 * u, qb = tile % (QN / 8), jb = tile / (QN / 8);
+                const double av = Vs[(8 * qb + g) * VS + 4 * kk + t4];
+                const double bv = Xs[(4 * kk + t4) * XS + 8 * jb + g];
+                dmma_8x8x4(acc[u][0], acc[u][1], av, bv);
+            }
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int a = 0; a < QPT; ++a) {
-        const int q = qg * QPT + a;
-        if (q < ncol)
-#pragma unroll
-            for (int c = 0; c < CPT; ++c)
-                tpart[(((size_t)sd.t_off + q) * nch + ch) * K + jg + 8 * c] = acc[a][c];
+    for (int u = 0; u < T; ++u) {
+        const int tile = warp + 8 * u, qb = tile % (QN / 8), jb = tile / (QN / 8);
+        const int q = 8 * qb + g, j = 8 * jb + 2 * t4;
+        if (q < ncol) {
+            double *o = tpart + (((size_t)sd.t_off + q) * nch + ch) * K + j;
+            o[0] = acc[u][0];
+            o[1] = acc[u][1];
+        }
     }
 }
-
-template <int K>
-__global__ void __launch_bounds__(256) k_vt_multi(int nch, const SubDev *__restrict__ subs,
-                                                  const double *__restrict__ Vbuf, const double *__restrict__ xb,
-                                                  double *__restrict__ tpart) {
-    vt_chunk<K>(nch, subs[blockIdx.x], Vbuf, xb, tpart);
-}
-template __global__ void k_vt_multi<16>(int, const SubDev *, const double *, const double *, double *);
-template __global__ void k_vt_multi<32>(int, const SubDev *, const double *, const double *, double *);
+#define HTF_VT(K, QN) \
+    template __global__ void k_vt_multi<K, QN>(int, const SubDev *, const double *, const double *, double *);
+HTF_VT(16, 32)
+HTF_VT(16, 64)
+HTF_VT(16, 128)
+HTF_VT(32, 32)
+HTF_VT(32, 64)
+#undef HTF_VT
 
 // gc[q][j] = sum over the t entries of coarse row q and their row chunks
 __global__ void k_gc_multi(int ngc_total, int K, int nch, const int *__restrict__ gptr, const int *__restrict__ gidx,
@@ -143,78 +159,72 @@ __global__ void k_gc_multi(int ngc_total, int K, int nch, const int *__restrict_
 }
 
 // S = M G per cluster (M symmetric ngc x ngc, G = gc ngc x K): CTA
-// (cluster, 32-row block) of 128 threads, 32-column tiles of M and 32-row
-// tiles of G staged in shared memory; each thread keeps a 4-row x (K/16)
-// register tile (rows 4 rg .. 4 rg + 3, columns cg + 16 c).
+// (cluster, 32-row block) of 128 threads; 32 x 64 tiles of M and 64-row
+// tiles of G staged in shared memory, the next pair prefetched into
+// registers.  Products on the FP64 tensor path: warp w owns rows
+// 8w .. 8w + 7 and all K columns (K / 8 tiles sharing one A fragment).
 template <int K>
-__device__ __forceinline__ void coarse_tile(const ClusterDev &c, const double *__restrict__ Mbuf,
-                                            const double *__restrict__ gc, double *__restrict__ s) {
-    constexpr int CPT = K / 16, UG = 32 * K / 128;
-    __shared__ double Ms[32 * 33];
-    __shared__ double Gs[32 * K];
+__global__ void __launch_bounds__(128) k_coarse_multi(const ClusterDev *__restrict__ cl,
+                                                      const double *__restrict__ Mbuf, const double *__restrict__ gc,
+                                                      double *__restrict__ s) {
+    constexpr int PK = 64, MS = PK + 4, GS = K + 4, NT = K / 8;
+    constexpr int UM = 32 * PK / 128, UG = PK * K / 128;
+    __shared__ double Ms[32 * MS];                  // [r][p]
+    __shared__ double Gs[PK * GS];                  // [p][j]
+    const ClusterDev c = cl[blockIdx.x];
     const int row0 = blockIdx.y * 32;
+    if (row0 >= c.ngc) return;
     const double *M = Mbuf + c.M_off;
-    const double *g = gc + (size_t)c.gc_off * K;
-    const int cg = threadIdx.x % 16, rg = threadIdx.x / 16;
-    double acc[4][CPT];
+    const double *G = gc + (size_t)c.gc_off * K;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int g = lane >> 2, t4 = lane & 3;
+    double acc[NT][2];
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int cc = 0; cc < CPT; ++cc) acc[r][cc] = 0.0;
-    double mr[8], gr[UG];
+    for (int u = 0; u < NT; ++u) acc[u][0] = acc[u][1] = 0.0;
+    double mr[UM], gr[UG];
     auto fetch = [&](int p0) {
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int o = threadIdx.x + 128 * u, r = o / 32, pp = o % 32;
+        for (int u = 0; u < UM; ++u) {
+            const int o = threadIdx.x + 128 * u, r = o / PK, pp = o % PK;
             mr[u] = (row0 + r < c.ngc && p0 + pp < c.ngc) ? M[(size_t)(row0 + r) * c.ngc + p0 + pp] : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < UG; ++u) {
             const int o = threadIdx.x + 128 * u, pp = o / K;
-            gr[u] = (p0 + pp < c.ngc) ? g[(size_t)(p0 + pp) * K + (o % K)] : 0.0;
+            gr[u] = (p0 + pp < c.ngc) ? G[(size_t)(p0 + pp) * K + (o % K)] : 0.0;
         }
     };
     fetch(0);
-    for (int p0 = 0; p0 < c.ngc; p0 += 32) {
+    for (int p0 = 0; p0 < c.ngc; p0 += PK) {
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+        for (int u = 0; u < UM; ++u) {
             const int o = threadIdx.x + 128 * u;
-            Ms[(o / 32) * 33 + o % 32] = mr[u];
+            Ms[(o / PK) * MS + o % PK] = mr[u];
         }
 #pragma unroll
-        for (int u = 0; u < UG; ++u) Gs[threadIdx.x + 128 * u] = gr[u];
+        for (int u = 0; u < UG; ++u) {
+            const int o = threadIdx.x + 128 * u;
+            Gs[(o / K) * GS + o % K] = gr[u];
+        }
         __syncthreads();
-        if (p0 + 32 < c.ngc) fetch(p0 + 32);          // next tile in flight during the FMAs
-#pragma unroll 4
-        for (int pp = 0; pp < 32; ++pp) {
-            double m[4], gv[CPT];
+        if (p0 + PK < c.ngc) fetch(p0 + PK);        // next tiles in flight during the products
 #pragma unroll
-            for (int r = 0; r < 4; ++r) m[r] = Ms[(4 * rg + r) * 33 + pp];
+        for (int kk = 0; kk < PK / 4; ++kk) {
+            const double av = Ms[(8 * warp + g) * MS + 4 * kk + t4];
 #pragma unroll
-            for (int cc = 0; cc < CPT; ++cc) gv[cc] = Gs[pp * K + cg + 16 * cc];
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int cc = 0; cc < CPT; ++cc) acc[r][cc] += m[r] * gv[cc];
+            for (int u = 0; u < NT; ++u)
+                dmma_8x8x4(acc[u][0], acc[u][1], av, Gs[(4 * kk + t4) * GS + 8 * u + g]);
         }
         __syncthreads();
     }
+    const int row = row0 + 8 * warp + g;
+    if (row < c.ngc)
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const int row = row0 + 4 * rg + r;
-        if (row < c.ngc)
-#pragma unroll
-            for (int cc = 0; cc < CPT; ++cc) s[((size_t)c.gc_off + row) * K + cg + 16 * cc] = acc[r][cc];
-    }
-}
-
-template <int K>
-__global__ void __launch_bounds__(128) k_coarse_multi(const ClusterDev *__restrict__ cl,
-                                                      const double *__restrict__ Mbuf, const double *__restrict__ gc,
-                                                      double *__restrict__ s) {
-    const ClusterDev c = cl[blockIdx.x];
-    if (blockIdx.y * 32 >= c.ngc) return;
-    coarse_tile<K>(c, Mbuf, gc, s);
+        for (int u = 0; u < NT; ++u) {
+            double *o = s + ((size_t)c.gc_off + row) * K + 8 * u + 2 * t4;
+            o[0] = acc[u][0];
+            o[1] = acc[u][1];
+        }
 }
 template __global__ void k_coarse_multi<16>(const ClusterDev *, const double *, const double *, double *);
 template __global__ void k_coarse_multi<32>(const ClusterDev *, const double *, const double *, double *);
@@ -496,11 +506,6 @@ namespace htf {
 // both operand loads free of bank conflicts.  With s given (the F apply),
 // the coarse correction y_b -= V_d s_d is applied before the store.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
-}
 
 template <int K>
 __global__ void __launch_bounds__(256) k_symv_rows_multi(const int2 *__restrict__ rowblk,
