@@ -18,7 +18,8 @@ lib = ctypes.CDLL(LIB_PATH)
 HTF_BC_ROLLERS, HTF_BC_CLAMP_X0 = 0, 1
 HTF_MAT_CONST, HTF_MAT_CHECKER, HTF_MAT_LOGUNIFORM = 0, 1, 2
 ERRORS = {0: "HTF_OK", -1: "HTF_EINVAL", -2: "HTF_ENOMEM", -3: "HTF_ECUDA", -4: "HTF_ENOTSPD",
-          -5: "HTF_EBREAKDOWN", -6: "HTF_ENOCONV", -7: "HTF_ESTATE", -8: "HTF_ETIMEDOUT", -9: "HTF_ENODEV"}
+          -5: "HTF_EBREAKDOWN", -6: "HTF_ENOCONV", -7: "HTF_ESTATE", -8: "HTF_ETIMEDOUT", -9: "HTF_ENODEV",
+          -10: "HTF_EIO"}
 for _c, _n in ERRORS.items():
     globals()[_n] = _c
 
@@ -67,6 +68,7 @@ _SIGS = {
     "htf_mesh_sizes": [ctypes.POINTER(MeshSpec)] + [_ip] * 6,
     "htf_mesh_fill": [ctypes.POINTER(MeshSpec), _dp, _ip, _ip, _ip, _dp, _dp, _ip, _ip],
     "htf_mesh_traction": [ctypes.POINTER(MeshSpec), ctypes.c_uint64, ctypes.c_int, ctypes.c_double, _dp],
+    "htf_write_vtk": [ctypes.c_char_p, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, _ip, _dp],
     "htf_create": [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)],
     "htf_destroy": [ctypes.c_void_p],
     "htf_set_mesh": [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, ctypes.c_int, _ip, _dp, _dp,
@@ -183,6 +185,22 @@ def traction(spec, seed, n_rhs, scale=1.0):
     if rc:
         raise HTFError(rc, "htf_mesh_traction")
     return f
+
+
+def write_vtk(path, mesh, u, material=None):
+    """Mesh::SaveVTK (Mesh.cpp:292-351): the displacement field u (one load
+    case, 3*n_nodes) written as the reference's box.vtk.  material: one id
+    per element; None applies the reference's rule, remainder(subdomain, 2)."""
+    u = np.ascontiguousarray(u, dtype=np.float64).ravel()
+    if u.size != 3 * mesh.n_nodes:
+        raise HTFError(-1, f"htf_write_vtk: u has {u.size} values, expected {3 * mesh.n_nodes}")
+    mat = None if material is None else np.ascontiguousarray(material, dtype=np.int32)
+    if mat is not None and mat.size != len(mesh.elem_sub):
+        raise HTFError(-1, "htf_write_vtk: one material id per element expected")
+    rc = lib.htf_write_vtk(os.fsencode(path), mesh.n_nodes, _d(mesh.coords), len(mesh.elem_sub), _i(mesh.elems),
+                           _i(mesh.elem_sub), None if mat is None else _i(mat), _d(u))
+    if rc:
+        raise HTFError(rc, f"htf_write_vtk({path})")
 
 
 class Solver:

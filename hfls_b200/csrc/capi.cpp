@@ -56,6 +56,11 @@ int htf_mesh_traction(const htf_mesh_spec *spec, uint64_t seed, int n_rhs, doubl
     return htf::mesh_traction(*spec, seed, n_rhs, scale, f, err);
 }
 
+int htf_write_vtk(const char *path, int n_nodes, const double *coords, int n_elems, const int *elems,
+                  const int *elem_sub, const int *elem_mat, const double *u) {
+    return htf::write_vtk(path, n_nodes, coords, n_elems, elems, elem_sub, elem_mat, u);
+}
+
 int htf_create(const char *options, htf_ctx **ctx) {
     if (!ctx) return HTF_EINVAL;
     *ctx = nullptr;

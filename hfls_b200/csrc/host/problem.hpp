@@ -38,6 +38,9 @@ int mesh_sizes(const htf_mesh_spec &s, int *nn, int *ne, int *ns, int *nc, int *
                std::string &err);
 int mesh_traction(const htf_mesh_spec &s, uint64_t seed, int n_rhs, double scale, double *f,
                   std::string &err);
+// box.vtk of the displacement field (vtk.cpp)
+int write_vtk(const char *path, int n_nodes, const double *coords, int n_elems, const int *elems,
+              const int *elem_sub, const int *elem_mat, const double *u);
 
 struct Options {
     std::string typeBc = "cor";                       // cor | ker | all

@@ -32,6 +32,7 @@ extern "C" {
 #define HTF_ESTATE -7       /* call out of order (e.g. pcpg before setup)      */
 #define HTF_ETIMEDOUT -8    /* a bounded device wait gave up                   */
 #define HTF_ENODEV -9       /* no CUDA device                                  */
+#define HTF_EIO -10         /* a file could not be written                     */
 
 /* ---- mesh generation ----------------------------------------------------
  * Replaces Mesh::createMesh (Mesh.cpp:69-289), generalised to clusters,
@@ -74,6 +75,19 @@ int htf_mesh_fill(const htf_mesh_spec *spec, double *coords, int *elems, int *el
  * f[3*n_nodes*n_rhs] (column-major: load case k at f + k*3*n_nodes).  The
  * reference has no traction; it is a configuration load.                   */
 int htf_mesh_traction(const htf_mesh_spec *spec, uint64_t seed, int n_rhs, double scale, double *f);
+
+/* ---- solution output ----------------------------------------------------
+ * Replaces Mesh::SaveVTK (Mesh.cpp:292-351), which Cluster::printVTK
+ * (Cluster.cpp:1648-1678) calls with the displacement field at the end of
+ * the solve: writes `path` as the reference's box.vtk (legacy ASCII VTK,
+ * unstructured grid of hex8 cells, same layout and number formats), with
+ * u[3*n_nodes] as the point field "displacements", elem_sub as the cell field
+ * "decomposition" and elem_mat as "materialId".  elem_mat may be NULL: the
+ * reference's rule is used, remainder(elem_sub, 2) (Mesh.cpp:280-281; 0, 1
+ * or -1).  Host only, no context.  HTF_EINVAL for a NULL array or a node id
+ * out of range, HTF_EIO if the file cannot be written.                     */
+int htf_write_vtk(const char *path, int n_nodes, const double *coords, int n_elems, const int *elems,
+                  const int *elem_sub, const int *elem_mat, const double *u);
 
 /* ---- solver context ------------------------------------------------------
  * Replaces Driver::Driver(map) / Cluster::initialization's options map

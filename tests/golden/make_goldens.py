@@ -4,7 +4,8 @@ Builds the reference from its sources (oracle/ref_build/Makefile ->
 oracle/_ref/hfls_ref), runs it on the cases below and stores, per case, the
 reference's mesh, dual layout (Bf, weights), projected-operator probes,
 element matrices, iteration count and displacement field (read from the
-box.vtk the reference writes) in tests/golden/<case>.npz.
+box.vtk the reference writes) in tests/golden/<case>.npz, and one case's box.vtk
+verbatim (tests/golden/<case>_box.vtk).
 
 Young's modulus is scaled to ~1e-3 so the displacements printed with "%f"
 by Mesh::SaveVTK (Mesh.cpp:346-349) keep about 12 significant digits; the
@@ -125,11 +126,29 @@ def run_case(name, args):
     print(f"{name}: nsub={nsub} iterations={its[-1] - 1} nlam={len(rec['weight'])}")
 
 
+VTK_CASE = "ref_ker_dirichlet_3"
+
+
+def write_vtk_fixture():
+    """The reference's own box.vtk (Mesh::SaveVTK) of VTK_CASE, kept verbatim
+    as tests/golden/<case>_box.vtk: the byte-for-byte target of htf_write_vtk."""
+    work = os.path.join(ROOT, "oracle", "_ref", "runs", VTK_CASE + "_vtk")
+    os.makedirs(work, exist_ok=True)
+    argv = [REF_BIN, f"out={work}"] + [f"{k}={v}" for k, v in CASES[VTK_CASE].items()]
+    subprocess.run(argv, capture_output=True, text=True, check=True)
+    with open(os.path.join(work, "box.vtk"), "rb") as f:
+        data = f.read()
+    with open(os.path.join(OUTDIR, VTK_CASE + "_box.vtk"), "wb") as f:
+        f.write(data)
+    print(f"{VTK_CASE}_box.vtk: {len(data)} bytes")
+
+
 def main():
     if not os.path.exists(REF_BIN):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle", "ref_build")], check=True)
     for name, args in CASES.items():
         run_case(name, args)
+    write_vtk_fixture()
 
 
 if __name__ == "__main__":
