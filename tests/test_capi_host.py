@@ -104,3 +104,36 @@ def test_options_and_errors():
     with pytest.raises(hb.HTFError) as e:
         s.setup()
     assert e.value.code == -7
+
+
+def _broken(mesh, **changes):
+    a = dict(coords=mesh.coords, elems=mesh.elems, elem_sub=mesh.elem_sub, sub_cluster=mesh.sub_cluster,
+             sub_E=mesh.sub_E, sub_nu=mesh.sub_nu, dirichlet=mesh.dirichlet, corner=mesh.corner,
+             body_force=mesh.body_force)
+    a.update(changes)
+    return hb.Mesh(**a)
+
+
+@pytest.mark.parametrize("what, change", [
+    ("element node id out of range", lambda m: dict(elems=np.where(np.arange(m.elems.size).reshape(m.elems.shape) == 5,
+                                                                   m.n_nodes, m.elems))),
+    ("elem_sub out of range", lambda m: dict(elem_sub=np.where(np.arange(len(m.elem_sub)) == 0, m.n_sub,
+                                                               m.elem_sub))),
+    ("subdomain without elements", lambda m: dict(sub_cluster=np.append(m.sub_cluster, 0),
+                                                  sub_E=np.append(m.sub_E, 1.0), sub_nu=np.append(m.sub_nu, 0.3))),
+    ("negative cluster id", lambda m: dict(sub_cluster=np.where(np.arange(m.n_sub) == 1, -1, m.sub_cluster))),
+    ("Dirichlet DOF out of range", lambda m: dict(dirichlet=np.append(m.dirichlet, 3 * m.n_nodes))),
+    ("no dual rows", lambda m: dict(elem_sub=np.zeros_like(m.elem_sub), sub_cluster=m.sub_cluster[:1],
+                                    sub_E=m.sub_E[:1], sub_nu=m.sub_nu[:1], dirichlet=m.dirichlet[:0],
+                                    corner=m.corner[:0])),
+])
+def test_malformed_meshes_are_rejected_before_any_device_work(what, change):
+    """The host problem build checks the mesh arrays and returns HTF_EINVAL
+    with a message (the reference reads past its arrays or exits instead);
+    it runs before any device call, so these need no GPU."""
+    m = hb.generate_mesh(hb.mesh_spec(subs=(2, 2, 1), elems=(2, 2, 2)))
+    s = hb.Solver({"typeBc": "cor"})
+    s.set_mesh(_broken(m, **change(m)))
+    with pytest.raises(hb.HTFError) as e:
+        s.setup()
+    assert e.value.code == -1 and what in str(e.value)
