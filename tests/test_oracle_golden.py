@@ -112,3 +112,21 @@ def test_multi_cluster_matches_direct_solve(typeBc):
     s = h.pcpg(eps_iter=1e-10, max_iter=1000)
     assert h.Gf.shape[1] == 12
     assert rel(s["u"], _direct(h)) < 1e-8
+
+
+def test_uneven_slabs_match_direct_solve():
+    """Subdomains of different sizes in two clusters with a 1e3 material
+    contrast (the shape of the 4 096-subdomain configuration at a size the
+    oracle solves in a second): u equals a direct global solve."""
+    import hfls_b200 as hb
+    from oracle.htfeti_oracle import MeshArrays, Options
+    spec = hb.mesh_spec(clusters=(2, 1, 1), subs=(2, 2, 1), widths=([2, 4, 3, 1], [3, 1], [2]), jitter=0.1,
+                        seed=5, material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e3)
+    m = hb.generate_mesh(spec)
+    ma = MeshArrays(m.coords, m.elems.astype(np.int64), m.elem_sub.astype(np.int64), m.sub_cluster.astype(np.int64),
+                    m.sub_E, m.sub_nu, m.dirichlet.astype(np.int64), m.corner.astype(np.int64), m.body_force)
+    h = HTFETI(ma, Options(typeBc="cor", fix_rule="boundary", kerGc="analytic"))
+    sizes = [len(h.l2g[d]) for d in range(m.n_sub)]
+    assert min(sizes) < max(sizes) / 2                      # really uneven
+    s = h.pcpg(eps_iter=1e-11, max_iter=3000)
+    assert rel(s["u"], _direct(h)) < 1e-8
