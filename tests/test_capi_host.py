@@ -137,3 +137,52 @@ def test_malformed_meshes_are_rejected_before_any_device_work(what, change):
     with pytest.raises(hb.HTFError) as e:
         s.setup()
     assert e.value.code == -1 and what in str(e.value)
+
+
+C_CALLER = r"""
+#include <stdio.h>
+#include <stdlib.h>
+#include "htfeti.h"
+
+int main(int argc, char **argv) {
+    htf_mesh_spec s = {{1, 1, 1}, {2, 2, 2}, {2, 2, 2}, {NULL, NULL, NULL}, 0.0, 7u, HTF_BC_CLAMP_X0,
+                       HTF_MAT_CONST, 2.1e5, 1.0, 0.3, {0.0, 0.0, -1.0}};
+    int nn, ne, ns, nc, nd, ncr;
+    if (htf_mesh_sizes(&s, &nn, &ne, &ns, &nc, &nd, &ncr) != HTF_OK) return 1;
+    double *xyz = malloc(sizeof(double) * 3 * nn), *u = calloc(3 * nn, sizeof(double));
+    int *el = malloc(sizeof(int) * 8 * ne), *part = malloc(sizeof(int) * ne);
+    if (htf_mesh_fill(&s, xyz, el, part, NULL, NULL, NULL, NULL, NULL) != HTF_OK) return 2;
+    if (htf_write_vtk(argv[1], nn, xyz, ne, el, part, NULL, u) != HTF_OK) return 3;
+    htf_ctx *ctx = NULL;
+    if (htf_create("typeBc=cor;preconditioner=bogus", &ctx) != HTF_EINVAL || ctx) return 4;
+    if (htf_create("typeBc=cor;eps_iter=1e-8", &ctx) != HTF_OK) return 5;
+    if (htf_setup(ctx) != HTF_ESTATE) return 6;
+    printf("%d %d %d %s\n", nn, ne, ns, htf_last_error(ctx));
+    htf_destroy(ctx);
+    free(xyz); free(u); free(el); free(part);
+    return 0;
+}
+"""
+
+
+def test_header_and_library_from_plain_c(tmp_path):
+    """The boundary as a C caller (cgo, JNI or any FFI) sees it: htfeti.h
+    compiles as C99 and the library links and runs from C, with no C++ or
+    torch types in the signatures (host entry points only: no GPU here)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "caller.c"
+    src.write_text(C_CALLER)
+    exe = tmp_path / "caller"
+    lib_dir = os.path.join(ROOT, "hfls_b200")
+    subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L" + lib_dir, "-lhtfeti_b200", "-Wl,-rpath," + lib_dir], check=True, capture_output=True)
+    out = subprocess.run([str(exe), str(tmp_path / "box.vtk")], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0, out.stderr
+    nn, ne, ns, msg = out.stdout.split(" ", 3)
+    assert (int(nn), int(ne), int(ns)) == (125, 64, 8)
+    assert "before htf_set_mesh" in msg
+    assert (tmp_path / "box.vtk").read_text().startswith("# vtk DataFile Version 3.0\n")
