@@ -1,26 +1,36 @@
-"""HTFETI solve benchmark (plain FP64 form at scale).
+"""HTFETI solve benchmark.
 
-Workload (one step = one PCPG solve, g0 -> convergence at 1e-8, with the
-factors and F_i / S_i resident on the device):
-  2x2x2 clusters x 4x4x4 subdomains x 8x8x8 trilinear hex8 elements on the
-  unit cube, interior nodes jittered by U(-0.1h, 0.1h), E_i log-uniform in
-  [1e3, 1e6] per subdomain, nu = 0.3, u = 0 on x = 0, seeded N(0,1) nodal
-  traction on x = 1, corner gluing inside clusters, Dirichlet preconditioner,
-  F_i stored dense FP64 (packed triangular tiles).
+Headline workload (one step = one PCPG solve, g0 -> convergence at 1e-8, with
+the factors and F_i / S_i resident on the device), the largest configuration
+that fits one GPU:
+  the uneven cube: 16 subdomain slabs per axis whose element counts are drawn
+  from {4..12} (seed 0), grouped into 2x2x2 clusters of 8x8x8 subdomains
+  (4096 subdomains of 375-6591 DOFs, 5.47 M DOFs), interior nodes jittered by
+  U(-0.1h, 0.1h), E_i log-uniform in [1, 1e4] per subdomain, nu 0.3, u = 0 on
+  x = 0, body force (0, 0, -1), corner gluing inside clusters, Dirichlet
+  preconditioner, F_i / S_i dense FP64 (packed triangular tiles).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Alongside it (same mesh, body force (0, 0, -1), 32 seeded N(0,1) traction
-load cases): the batched mixed-precision form (F_i / S_i FP32 on the tensor
-cores, FP64 residual replacement) against the FP64 form on the same load
-cases, with the displacement error against an FP64 solve at eps 1e-10
-("mixed" in the JSON line; --no-mixed skips it).
+Beside it in the same JSON line:
+  cube512   the regular cube (2x2x2 clusters x 4x4x4 subdomains x 8^3 hex8,
+            E logU[1e3, 1e6], N(0,1) traction on x = 1) in FP64, with its
+            iteration count against the oracle golden;
+  mixed     the same cube with body force and 32 seeded traction load cases
+            solved as one batch in mixed precision (F_i / S_i FP32 on the
+            tensor cores, FP64 residual replacement), the displacement error
+            of every load case against the oracle golden;
+  serving   a prefix of the seeded serving stream through htf_server against
+            the plain FP64 per-request path;
+  cpu_baseline  the reference (oracle/_ref/hfls_ref, built from the reference
+            sources, one core) solving its own CPU configuration in full -
+            2x2x2 subdomains x 5^3 hex8 - with the GPU's time on the same
+            configuration beside it.
 
-Under torchrun (N > 1) every rank solves its own replica of the workload on
-its own GPU (the solve has no cross-GPU exchange on one node here), timing
-is the max over ranks.  --impl reference times the reference CPU solver
-(oracle/_ref/hfls_ref, built from the reference sources) on a bounded
-sample and scales it to the same metric.
+Under torchrun (N > 1) every rank solves its own replica on its own GPU (the
+solve has no cross-GPU exchange here), timing is the max over ranks.
+--impl reference reports that the reference cannot solve the headline
+workload (it has one cluster) and times it on its own configuration instead.
 """
 import argparse
 import json
@@ -37,16 +47,21 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "HTFETI solve s & F-apply GB/s at 1e-8 rel res; mixed vs FP64 GPU; p99 latency"
-WORKLOAD = ("HTFETI cube: 2x2x2 clusters x 4x4x4 subdomains x 8^3 hex8 (512 subdomains, 1.12M local DOFs), "
-            "jitter 0.1h, E logU[1e3,1e6], nu 0.3, clamp x=0, N(0,1) traction x=1, corner Bc, "
-            "Dirichlet preconditioner, F_i dense FP64, eps 1e-8")
-SPEC = dict(clusters=(2, 2, 2), subs=(4, 4, 4), elems=(8, 8, 8), jitter=0.1, seed=1,
-            E=1e3, E_hi=1e6, nu=0.3, body_force=(0.0, 0.0, 0.0))
-WORKLOAD_ITERATIONS = 638   # PCPG iterations of the workload at 1e-8 (measured by the GPU arm)
 OPTS = {"typeBc": "cor", "preconditioner": "Dirichlet_explicit", "eps_iter": "1e-8", "max_iter": "5000"}
-REF_SAMPLE = dict(Nx=2, Ny=1, Nz=1, nx=8, ny=8, nz=8)     # subdomains of the workload's size, one cluster
+
+UNEVEN_WORKLOAD = ("HTFETI uneven cube: 16 slabs/axis of {4..12} hex8 (seed 0), 2x2x2 clusters x 8x8x8 subdomains "
+                   "(4096 subdomains, 375-6591 DOFs each), jitter 0.1h, E logU[1,1e4], nu 0.3, clamp x=0, body force "
+                   "(0,0,-1), corner Bc, Dirichlet preconditioner, F_i/S_i dense FP64, eps 1e-8")
+CUBE_WORKLOAD = ("HTFETI cube: 2x2x2 clusters x 4x4x4 subdomains x 8^3 hex8 (512 subdomains, 823875 DOFs), "
+                 "jitter 0.1h, E logU[1e3,1e6], nu 0.3, clamp x=0, N(0,1) traction x=1, corner Bc, "
+                 "Dirichlet preconditioner, F_i dense FP64, eps 1e-8")
+CUBE = dict(clusters=(2, 2, 2), subs=(4, 4, 4), elems=(8, 8, 8), jitter=0.1, seed=1,
+            E=1e3, E_hi=1e6, nu=0.3, body_force=(0.0, 0.0, 0.0))
+SMALL_WORKLOAD = ("the reference's CPU configuration: 2x2x2 subdomains x 5^3 hex8 on the unit cube (one cluster), "
+                  "E 2.1e5, nu 0.3, u = 0 on x = 0, body force, interior nodes jittered by 0.1h, "
+                  "Bc of kernel type, Dirichlet preconditioner, eps 1e-8")
 MIXED_RHS = 32
-MIXED_WORKLOAD = ("same cube, body force (0,0,-1) + 32 seeded N(0,1) tractions on x=1, solved as one batch of 32: "
+MIXED_WORKLOAD = ("cube512 mesh, body force (0,0,-1) + 32 seeded N(0,1) tractions on x=1, solved as one batch of 32: "
                   "F_i/S_i FP32 slabs, 3xTF32 tcgen05 products, FP64 coarse/projector/residual replacement, eps 1e-8")
 SERVE_REQUESTS = 12          # requests of the seeded stream that one bench run serves
 SERVE_RATE = 1.0             # Poisson arrivals per second
@@ -55,6 +70,26 @@ SERVE_WORKLOAD = ("seeded Poisson stream (rate %.1f/s): cube meshes of c^3 clust
                   "E logU[1,1e4] per subdomain, nu U[0.2,0.4] per request, clamp x=0, jitter 0.1h, eps 1e-8; "
                   "served by htf_server (mixed precision, batch 16) vs the plain FP64 per-request path "
                   "(set up and solve one request after another, FIFO on the same arrivals)" % SERVE_RATE)
+PROFILE_UNEVEN = os.path.join(ROOT, "profiles", "k_symv_fp64_uneven.md")
+PROFILE_CUBE = os.path.join(ROOT, "profiles", "k_symv_fp64_cfg1.md")
+
+
+def uneven_widths(n=16, seed=0, lo=4, hi=12):
+    rng = np.random.default_rng(seed)
+    return [rng.integers(lo, hi + 1, n).astype(np.int32) for _ in range(3)]
+
+
+def uneven_spec(hb, clusters=(2, 2, 2), subs=(8, 8, 8), widths=None):
+    w = widths if widths is not None else uneven_widths(clusters[0] * subs[0])
+    return hb.mesh_spec(clusters=clusters, subs=subs, widths=w, jitter=0.1, seed=0,
+                        material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e4, nu=0.3, bc=hb.HTF_BC_CLAMP_X0,
+                        body_force=(0.0, 0.0, -1.0))
+
+
+# reduced meshes of the same constructions, for ncu captures only
+REDUCED = {"uneven-small": dict(clusters=(1, 1, 1), subs=(8, 8, 8)),     # 512 subdomains, ~2.4 GB of FP64 tiles
+           "small": dict(clusters=(1, 1, 1), subs=(2, 4, 4)),            # cube: F_i tiles 120 MB
+           "mid": dict(clusters=(2, 1, 1), subs=(2, 4, 4))}              # cube: F_i tiles 240 MB
 
 
 def peaks():
@@ -80,7 +115,7 @@ class ClockSampler:
                  "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
         except OSError:
@@ -155,83 +190,176 @@ def barrier(dist):
         dist.barrier()
 
 
+def traffic_from_profile(path, key="traffic_bytes_per_launch_scaled"):
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"^%s:\s*([0-9.eE+]+)" % key, open(path).read(), re.M)
+    return float(m.group(1)) if m else None
+
+
 # ---------------------------------------------------------------------------
-# reference CPU solver on a bounded sample
+# reference CPU solver on its own configuration
 # ---------------------------------------------------------------------------
+REF_SMALL = dict(Nx=2, Ny=2, Nz=2, nx=5, ny=5, nz=5, young_modulus="2.1e5", poissons_ratio="0.3", clamp="true",
+                 jitter_seed=1, typeBc="ker", preconditioner="Dirichlet_explicit", eps_iter="1e-8", max_iter=500)
+
+
 def ref_binary():
     return os.path.join(ROOT, "oracle", "_ref", "hfls_ref")
 
 
-def ref_iteration_seconds(iters_a=1, iters_b=101):
-    """Wall seconds per PCPG iteration of the reference on REF_SAMPLE
-    (difference of two runs that differ only in max_iter)."""
-    out = {}
+def ref_run_small():
+    """One run of the reference on REF_SMALL: its own timed intervals (wall
+    seconds of Cluster::initialization's setup and Cluster::pcpg,
+    Cluster.cpp:24-379, 1364-1451), the process wall time and the PCPG
+    iteration count it prints."""
     with tempfile.TemporaryDirectory() as td:
-        for it in (iters_a, iters_b):
-            args = [ref_binary(), f"out={td}/r{it}", "typeBc=cor", "preconditioner=Dirichlet_explicit",
-                    "clamp=true", "young_modulus=1e3", "ratio_mat=1", "eps_iter=1e-30", f"max_iter={it}"]
-            args += [f"{k}={v}" for k, v in REF_SAMPLE.items()]
-            t0 = time.perf_counter()
-            r = subprocess.run(args, capture_output=True, text=True, env=dict(os.environ, OMP_NUM_THREADS="1"))
-            out[it] = time.perf_counter() - t0
-            if r.returncode != 0:
-                raise RuntimeError("reference run failed: " + r.stderr[-400:])
-    nsub = REF_SAMPLE["Nx"] * REF_SAMPLE["Ny"] * REF_SAMPLE["Nz"]
-    per_iter = (out[iters_b] - out[iters_a]) / (iters_b - iters_a)
-    return per_iter, nsub, out
+        args = [ref_binary(), f"out={td}", "dumps=false"] + [f"{k}={v}" for k, v in REF_SMALL.items()]
+        t0 = time.perf_counter()
+        r = subprocess.run(args, capture_output=True, text=True, env=dict(os.environ, OMP_NUM_THREADS="1",
+                                                                           OPENBLAS_NUM_THREADS="1"))
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError("reference run failed: " + r.stderr[-400:])
+        t = {}
+        for ln in open(os.path.join(td, "timing.txt")):
+            k, v = ln.split()
+            t[k] = float(v)
+    its = [int(m.group(1)) for m in re.finditer(r"^\s*(\d+)\s+[0-9.eE+-]+\s*$", r.stdout, re.M)]
+    return dict(setup_s=t["setup_s"], pcpg_s=t["pcpg_s"], total_s=t["total_s"], wall_s=wall,
+                iterations=max(its) if its else None)
 
 
-def cpu_baseline(iterations, n_sub_cfg):
-    if not os.path.exists(ref_binary()):
-        return None
-    per_iter, nsub, runs = ref_iteration_seconds()
-    value = per_iter / nsub * n_sub_cfg * iterations
-    return {"value": value, "unit": "s", "cores": 1, "kind": "reference",
-            "sample": (f"reference (oracle/_ref/hfls_ref, PARDISO stand-in = skyline Cholesky) on one cluster of "
-                       f"{nsub} subdomains of 8^3 hex8: {per_iter:.4f} s per PCPG iteration from runs of "
-                       f"{runs[1]:.1f}s (1 it) and {runs[101]:.1f}s (101 it); scaled to {n_sub_cfg} subdomains x "
-                       f"{iterations} iterations")}
+def ref_small_measure(steps, warmup):
+    for _ in range(warmup):
+        ref_run_small()
+    runs = [ref_run_small() for _ in range(steps)]
+    return {k: statistics.mean(r[k] for r in runs) for k in ("setup_s", "pcpg_s", "total_s", "wall_s")} | \
+        {"iterations": runs[-1]["iterations"], "runs": len(runs)}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    if not os.path.exists(ref_binary()):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/hfls_ref was not built"}))
-        return 0
-    # the reference cannot run the multi-cluster workload; it times PCPG iterations on
-    # subdomains of the workload's size and scales by the workload's iteration count,
-    # which the FP64 GPU solve of the same problem measures (checked by the GPU arm).
-    iterations = WORKLOAD_ITERATIONS
-    for _ in range(args.warmup):
-        ref_iteration_seconds()
-    vals = []
-    for _ in range(args.steps):
-        per_iter, nsub, _ = ref_iteration_seconds()
-        vals.append(per_iter / nsub * 512 * iterations)
-    v = statistics.mean(vals)
-    line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "iterations_scaled_to": iterations},
-            "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "reference",
-                             "sample": f"{REF_SAMPLE} one cluster, per-iteration time scaled to 512 subdomains"},
-            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    why = ("the reference solves one cluster only (one Cluster object, Driver.cpp:29; Mesh::createMesh builds one "
+           "cluster) and cannot solve the 8-cluster 4096-subdomain workload; its single-cluster form of that mesh "
+           "needs a coarse problem of ~10^5 unknowns that takes hours on one core. Measured instead on its own CPU "
+           "configuration (reference_small), which bench.py's GPU line also solves (cpu_baseline)")
+    line = {"impl": "reference", "unavailable": why}
+    if os.path.exists(ref_binary()):
+        m = ref_small_measure(args.steps, args.warmup)
+        line["reference_small"] = {"workload": SMALL_WORKLOAD, "unit": "s", "cores": 1, "kind": "reference",
+                                   "pcpg_s_per_solve": m["pcpg_s"], "setup_s": m["setup_s"],
+                                   "setup_and_solve_s": m["total_s"], "process_wall_s": m["wall_s"],
+                                   "iterations": m["iterations"], "runs": m["runs"]}
     print(json.dumps(line))
     return 0
 
 
+def cpu_baseline_small(hb, local, steps=5, warmup=1):
+    """The reference on its own configuration, measured in full, and the GPU
+    on the same configuration (same mesh construction and options)."""
+    if not os.path.exists(ref_binary()):
+        return None
+    ref = ref_small_measure(steps, warmup)
+    spec = hb.mesh_spec(subs=(2, 2, 2), elems=(5, 5, 5), jitter=0.1, seed=1, E=2.1e5, nu=0.3,
+                        bc=hb.HTF_BC_CLAMP_X0, body_force=(0.0, 0.0, -1.0))
+    mesh = hb.generate_mesh(spec)
+    opts = dict(OPTS, typeBc="ker", device=str(local))
+    t0 = time.perf_counter()
+    s = hb.Solver(opts)
+    s.set_mesh(mesh)
+    s.setup()
+    setup_wall = time.perf_counter() - t0
+    u = np.zeros((1, 3 * mesh.n_nodes))
+    for _ in range(3):
+        s.solve(None, u=u)
+    ms, e2e, its = [], [], []
+    for _ in range(20):
+        t = time.perf_counter()
+        _, st = s.solve(None, u=u)
+        e2e.append(time.perf_counter() - t)
+        ms.append(st.solve_ms)
+        its.append(st.iterations[0])
+    s.close()
+    gpu = statistics.mean(ms) / 1e3
+    return {"value": ref["pcpg_s"], "unit": "s", "cores": 1, "kind": "reference",
+            "sample": ("not a sample: the reference (oracle/_ref/hfls_ref, built -O2 from the reference sources, "
+                       "PARDISO stand-in = skyline Cholesky, 1 thread) solving its own CPU configuration in full, "
+                       "mean of %d runs; value = its Cluster::pcpg interval (Cluster.cpp:1364-1451) in wall seconds"
+                       % ref["runs"]),
+            "workload": SMALL_WORKLOAD, "same_config": True,
+            "reference": {"pcpg_s": ref["pcpg_s"], "setup_s": ref["setup_s"], "setup_and_solve_s": ref["total_s"],
+                          "iterations": ref["iterations"]},
+            "gpu_same_config": {"pcpg_s": gpu, "e2e_solve_s": statistics.mean(e2e), "setup_wall_s": setup_wall,
+                                "iterations": int(statistics.median(its)),
+                                "speedup_pcpg": ref["pcpg_s"] / gpu,
+                                "speedup_setup_and_solve": ref["total_s"] / (setup_wall + statistics.mean(e2e))}}
+
+
 # ---------------------------------------------------------------------------
-REDUCED = {"small": dict(clusters=(1, 1, 1), subs=(2, 4, 4)),     # F_i tiles 120 MB, FP32 slabs 100 MB
-           "mid": dict(clusters=(2, 1, 1), subs=(2, 4, 4))}       # F_i tiles 240 MB, FP32 slabs 200 MB
+def oracle_golden(name):
+    p = os.path.join(ROOT, "tests", "golden", f"oracle_{name}.npz")
+    return np.load(p) if os.path.exists(p) else None
+
+
+def golden_rel_err(g, u, k):
+    """Relative displacement error of load case k against an oracle golden:
+    the larger of the error on the golden's seeded DOF sample and on its
+    seeded projections of the whole field."""
+    idx = g["sample_idx"]
+    e1 = np.linalg.norm(u[idx] - g["u_sample"][k]) / np.linalg.norm(g["u_sample"][k])
+    P = np.random.default_rng(777).standard_normal((g["u_proj"].shape[1], u.size))
+    e2 = np.linalg.norm(P @ u - g["u_proj"][k]) / np.linalg.norm(g["u_proj"][k])
+    return float(max(e1, e2))
+
+
+def run_cube(hb, local, dist, steps):
+    """The regular 512-subdomain cube in FP64: seconds per solve, F apply
+    bandwidth and the iteration count against the oracle golden."""
+    spec = hb.mesh_spec(material=hb.HTF_MAT_LOGUNIFORM, bc=hb.HTF_BC_CLAMP_X0, **CUBE)
+    mesh = hb.generate_mesh(spec)
+    f = hb.traction(spec, seed=2, n_rhs=1)
+    s = hb.Solver(dict(OPTS, device=str(local)))
+    s.set_mesh(mesh)
+    s.set_loads(f)
+    t0 = time.perf_counter()
+    s.setup()
+    setup_wall = time.perf_counter() - t0
+    u = np.zeros((1, 3 * mesh.n_nodes))
+    for _ in range(3):
+        s.solve(f, u=u)
+    barrier(dist)
+    ms, e2e, its = [], [], []
+    for _ in range(steps):
+        t = time.perf_counter()
+        _, st = s.solve(f, u=u)
+        e2e.append(time.perf_counter() - t)
+        ms.append(st.solve_ms)
+        its.append(st.iterations[0])
+    prof = s.profile(reps=20)
+    s.close()
+    peak, peak_kind = peaks()
+    g = oracle_golden("cube1")
+    achieved = prof.symv_F_bytes / (prof.symv_F_ms * 1e-3) / 1e9
+    return {"workload": CUBE_WORKLOAD, "solve_s": max_over_ranks(dist, statistics.mean(ms)) / 1e3,
+            "e2e_s": max_over_ranks(dist, statistics.mean(e2e)), "setup_s": setup_wall,
+            "iterations": int(statistics.median(its)),
+            "iterations_oracle": int(g["iterations"][0]) if g is not None else None,
+            "fapply_gbs": prof.fapply_bytes / (prof.fapply_ms * 1e-3) / 1e9, "fapply_ms": prof.fapply_ms,
+            "iteration_ms": prof.iteration_ms,
+            "symv_F": {"kernel": "k_symv_units<double>", "ms": prof.symv_F_ms, "bytes": prof.symv_F_bytes,
+                       "gbs": achieved, "frac": achieved / peak, "peak_kind": peak_kind,
+                       "traffic": traffic_from_profile(PROFILE_CUBE)}}
 
 
 def run_mixed(hb, local, dist, reduced=None):
     """Batched mixed-precision solve of MIXED_RHS load cases vs the FP64 form
-    on four of them (time per load case; displacement error against FP64 at
-    eps 1e-10).  Times are CUDA-event solve times, max over ranks."""
-    spec_kw = dict(SPEC, body_force=(0.0, 0.0, -1.0), **(reduced or {}))
+    on four of them (time per load case); displacement error of every load
+    case against the oracle golden (full size) or an FP64 solve at eps 1e-10
+    (reduced meshes).  Times are CUDA-event solve times, max over ranks."""
+    spec_kw = dict(CUBE, body_force=(0.0, 0.0, -1.0), **(reduced or {}))
     spec = hb.mesh_spec(material=hb.HTF_MAT_LOGUNIFORM, bc=hb.HTF_BC_CLAMP_X0, **spec_kw)
     mesh = hb.generate_mesh(spec)
     f = hb.traction(spec, seed=3, n_rhs=MIXED_RHS)
@@ -249,20 +377,31 @@ def run_mixed(hb, local, dist, reduced=None):
     wall = max_over_ranks(dist, wall)
     its = list(st.iterations[:MIXED_RHS])
     prof = s.profile(reps=10)
-    del s
+    s.close()
     s64 = hb.Solver(dict(OPTS, device=str(local)))
     s64.set_mesh(mesh)
     s64.setup()
     u64, st64 = s64.solve(f[pick])
     fp64_ms = max_over_ranks(dist, st64.solve_ms) / len(pick)
     its64 = list(st64.iterations[:len(pick)])
-    del s64
-    sref = hb.Solver(dict(OPTS, device=str(local), eps_iter="1e-10", max_iter="10000"))
-    sref.set_mesh(mesh)
-    sref.setup()
-    uref, _ = sref.solve(f[pick])
-    del sref
-    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    s64.close()
+    g = oracle_golden("cube32") if reduced is None else None
+    if g is not None:
+        err = [golden_rel_err(g, u[k], k) for k in range(MIXED_RHS)]
+        err64 = [golden_rel_err(g, u64[i], k) for i, k in enumerate(pick)]
+        against = "oracle golden (tests/golden/oracle_cube32.npz, eps 1e-11), every load case"
+        its_oracle = [int(x) for x in g["iterations"]]
+    else:
+        sref = hb.Solver(dict(OPTS, device=str(local), eps_iter="1e-10", max_iter="10000"))
+        sref.set_mesh(mesh)
+        sref.setup()
+        uref, _ = sref.solve(f[pick])
+        sref.close()
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        err = [rel(u[k], uref[i]) for i, k in enumerate(pick)]
+        err64 = [rel(u64[i], uref[i]) for i in range(len(pick))]
+        against = "FP64 GPU solve at eps 1e-10 of load cases %s" % pick
+        its_oracle = None
     peak, peak_kind = peaks()
     tc_gbs = prof.tc_F_bytes / (prof.tc_F_ms * 1e-3) / 1e9
     return {
@@ -272,10 +411,8 @@ def run_mixed(hb, local, dist, reduced=None):
         "speedup_vs_fp64": fp64_ms / (mixed_ms / MIXED_RHS),
         "e2e_s_per_load_case": wall / MIXED_RHS,
         "iterations_median": int(statistics.median(its)), "iterations_max": int(max(its)),
-        "fp64_iterations": its64,
-        "u_rel_err_max": max(rel(u[k], uref[i]) for i, k in enumerate(pick)),
-        "fp64_u_rel_err_max": max(rel(u64[i], uref[i]) for i in range(len(pick))),
-        "u_err_reference": "FP64 GPU solve at eps 1e-10 of load cases %s" % pick,
+        "fp64_iterations": its64, "oracle_iterations_fp64": its_oracle,
+        "u_rel_err_max": max(err), "fp64_u_rel_err_max": max(err64), "u_err_against": against,
         "batch_iteration_ms": prof.batch_iteration_ms,
         "tc_F": {"kernel": "k_tc_gemm<32> (F_i FP32 slabs x 32 load cases)", "ms": prof.tc_F_ms,
                  "bytes": prof.tc_F_bytes, "gbs": tc_gbs, "frac": tc_gbs / peak, "peak_kind": peak_kind},
@@ -308,11 +445,7 @@ def run_serving(hb, local, n_req):
     free, _ = torch.cuda.mem_get_info(local)
     budget = 0.85 * free
     stream = serve_stream(hb, n_req)
-    loads = []
-    for (_, spec, k, fseed, dims) in stream:
-        c, s, e = dims
-        lower = 8.0 * 9.0 * ((c * s) * (e + 1) ** 2) ** 3      # dense factors alone
-        loads.append(hb.traction(spec, seed=fseed, n_rhs=k) if lower <= budget else None)
+    loads = [hb.traction(spec, seed=fseed, n_rhs=k) for (_, spec, k, fseed, _) in stream]
     opts = dict(OPTS, device=str(local), precision="mixed", batch="16", max_iter="3000")
     srv = hb.Server(opts, hbm_budget_bytes=budget, max_live=8)
     tickets = []
@@ -321,16 +454,23 @@ def run_serving(hb, local, n_req):
         dt = t0 + ta - time.perf_counter()
         if dt > 0:
             time.sleep(dt)
-        tickets.append(srv.submit(spec, f, n_rhs=k))
+        try:
+            tickets.append(srv.submit(spec, f, n_rhs=k))
+        except hb.HTFError as e:
+            tickets.append(e)
     served = []
     for i, t in enumerate(tickets):
+        if isinstance(t, hb.HTFError):
+            served.append((i, None, None, None, t.code, str(t)[:200]))
+            continue
         try:
             u, info = srv.wait(t)
             served.append((i, u.copy(), info.t_submit_ms, info.t_done_ms, info.iterations_max,
                            dict(queue_ms=round(info.t_admit_ms - info.t_submit_ms, 1),
                                 setup_ms=round(info.t_start_ms - info.t_admit_ms, 1),
                                 run_ms=round(info.t_done_ms - info.t_start_ms, 1),
-                                iterations=info.iterations_max, gb=round(info.bytes / 1e9, 2))))
+                                iterations=info.iterations_max, gb=round(info.bytes / 1e9, 2),
+                                gb_estimate=round(info.bytes_estimate / 1e9, 2))))
         except hb.HTFError as e:
             served.append((i, None, None, None, e.code, str(e)[:200]))
     srv.close()
@@ -347,7 +487,7 @@ def run_serving(hb, local, n_req):
         s.set_mesh(hb.generate_mesh(spec))
         s.setup()
         u64, _ = s.solve(loads[i])
-        del s
+        s.close()
         service.append(time.perf_counter() - t)
         err = max(err, max(float(np.linalg.norm(u[j] - u64[j]) / np.linalg.norm(u64[j])) for j in range(k)))
     fin, lat64 = 0.0, []
@@ -377,16 +517,18 @@ def run_serving(hb, local, n_req):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision multi-load-case measurement")
+    ap.add_argument("--no-cube", action="store_true", help="skip the 512-subdomain cube measurement")
     ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS,
                     help="requests of the seeded serving stream to serve (0 skips the serving measurement)")
-    ap.add_argument("--workload", default="full", choices=["full", "small", "mid"],
-                    help="small: one cluster of 2x4x4 subdomains of 8^3 (F_i + S_i 0.24 GB > L2); mid: two such "
-                         "clusters; reduced cases for ncu captures only (the mixed form runs at the same size)")
+    ap.add_argument("--workload", default="full", choices=["full"] + sorted(REDUCED),
+                    help="reduced meshes of the same constructions, for ncu captures only: uneven-small is one "
+                         "cluster of the uneven cube; small / mid are one / two clusters of 2x4x4 cube subdomains "
+                         "and run the cube in place of the uneven headline (the mixed form runs at the same size)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -394,15 +536,27 @@ def main():
 
     rank, world, local, dist = dist_setup(args.gpus)
     import hfls_b200 as hb
-    spec_kw = dict(SPEC)
-    if args.workload != "full":
-        spec_kw.update(REDUCED[args.workload])
-    spec = hb.mesh_spec(material=hb.HTF_MAT_LOGUNIFORM, bc=hb.HTF_BC_CLAMP_X0, **spec_kw)
+    reduced = REDUCED.get(args.workload)
+    if args.workload in ("small", "mid"):
+        spec = hb.mesh_spec(material=hb.HTF_MAT_LOGUNIFORM, bc=hb.HTF_BC_CLAMP_X0, **dict(CUBE, **reduced))
+        workload = CUBE_WORKLOAD + " (reduced: %s)" % args.workload
+        f = hb.traction(spec, seed=2, n_rhs=1)
+    else:
+        spec = uneven_spec(hb, **(reduced or {}))
+        workload = UNEVEN_WORKLOAD + ("" if reduced is None else " (reduced: %s)" % args.workload)
+        f = None
     mesh = hb.generate_mesh(spec)
-    f = hb.traction(spec, seed=2, n_rhs=1)
+    if f is None:
+        # the load case is the body force; htf_solve still takes the (zero) extra nodal load from
+        # host memory, as a caller solving a new load case does
+        f = np.zeros((1, 3 * mesh.n_nodes))
+        s_loads = False
+    else:
+        s_loads = True
     s = hb.Solver(dict(OPTS, device=str(local)))
     s.set_mesh(mesh)
-    s.set_loads(f)
+    if s_loads:
+        s.set_loads(f)
     t0 = time.perf_counter()
     s.setup()
     setup_wall = time.perf_counter() - t0
@@ -423,35 +577,37 @@ def main():
         barrier(dist)
     ms = max_over_ranks(dist, statistics.mean(solve_ms))
     e2e = max_over_ranks(dist, statistics.mean(e2e_s))
-    prof = s.profile(reps=20)
-    del s
-    # every rank solves its mixed-precision replica too (collective max inside)
-    mixed = None if args.no_mixed else run_mixed(hb, local, dist, REDUCED.get(args.workload))
+    prof = s.profile(reps=10)
+    n_lambda = st.n_lambda
+    s.close()
+    full = args.workload == "full"
+    cube = None if (args.no_cube or not full) else run_cube(hb, local, dist, min(args.steps, 5))
+    mixed = None if args.no_mixed else run_mixed(hb, local, dist, None if full else REDUCED.get(
+        args.workload if args.workload in ("small", "mid") else "mid"))
     serving = None
-    if args.serve_requests > 0 and args.workload == "full":
+    if args.serve_requests > 0 and full:
         barrier(dist)
         serving = run_serving(hb, local, args.serve_requests)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return 0
+    cpu = None if args.no_cpu_baseline else cpu_baseline_small(hb, local)
     peak, peak_kind = peaks()
     achieved = prof.symv_F_bytes / (prof.symv_F_ms * 1e-3) / 1e9
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "k_symv_fp64_cfg1.md")
-    if os.path.exists(tf) and args.workload == "full":
-        m = re.search(r"^traffic_bytes_per_launch_scaled:\s*([0-9.eE+]+)", open(tf).read(), re.M)
-        traffic = float(m.group(1)) if m else None
-    iterations = int(statistics.median(iters))
-    cpu = None if args.no_cpu_baseline else cpu_baseline(iterations, mesh.n_sub)
     ndof = 3 * mesh.n_nodes
     line = {
         "metric": METRIC, "value": whole_job_seconds_per_solve(ms, world), "unit": "s", "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_sub": mesh.n_sub, "n_lambda": st.n_lambda,
-                   "iterations": iterations, "iterations_expected": WORKLOAD_ITERATIONS, "setup_s": setup_wall, "setup_device_ms": st.setup_ms,
+        "config": {"workload": workload, "n_sub": mesh.n_sub, "n_dof": ndof, "n_lambda": n_lambda,
+                   "iterations": int(statistics.median(iters)), "setup_s": setup_wall,
+                   "setup_device_ms": st.setup_ms,
+                   "setup_phase_ms": {k: round(v, 1) for k, v in zip(
+                       ["problem_build", "device_context", "layout_upload", "assembly_factor_FS", "load_maps",
+                        "cluster_coarse", "outer_coarse", "symv_tuning_fp32_slabs"], prof.setup_phase_ms)},
+                   "symv_unit_tiles": list(prof.symv_unit_tiles), "symv_tuned": int(prof.symv_tuned),
                    "l2": "inputs larger than L2 (F_i and S_i tiles: %.2f GB per PCPG iteration)"
                          % ((prof.symv_F_bytes + prof.symv_S_bytes) / 1e9),
                    "parallelism": f"replicas x{world}",
@@ -459,14 +615,18 @@ def main():
         "fapply_gbs": prof.fapply_bytes / (prof.fapply_ms * 1e-3) / 1e9,
         "fapply_ms": prof.fapply_ms, "iteration_ms": prof.iteration_ms,
         "e2e": {"value": whole_job_seconds_per_solve(e2e * 1e3, world), "unit": "s",
-                "h2d_bytes_per_step": 8 * ndof, "d2h_bytes_per_step": 8 * ndof},
+                "h2d_bytes_per_step": 8 * ndof, "d2h_bytes_per_step": 8 * ndof,
+                "note": "htf_solve with host buffers: the nodal load vector in (zero on the body-force headline, "
+                        "whose load the library assembles from the mesh) and the displacement field out"},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "k_symv<double> (F_i packed tiles)", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+        "roofline": {"bound": "hbm", "kernel": "k_symv_units<double> (F_i packed tiles)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic_from_profile(PROFILE_UNEVEN) if full else None,
                      "peak_kind": peak_kind, "bytes_per_launch": prof.symv_F_bytes,
                      "launch_ms": prof.symv_F_ms},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
+        "cube512": cube,
         "mixed": mixed,
         "serving": serving,
     }

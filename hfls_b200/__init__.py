@@ -97,6 +97,8 @@ for _name, _args in _SIGS.items():
     _f = getattr(lib, _name)
     _f.argtypes = _args
     _f.restype = ctypes.c_int
+lib.htf_status_sub.argtypes = [ctypes.c_void_p]
+lib.htf_status_sub.restype = ctypes.c_int
 lib.htf_last_error.argtypes = [ctypes.c_void_p]
 lib.htf_last_error.restype = ctypes.c_char_p
 lib.htf_server_error.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
@@ -237,6 +239,10 @@ class Solver:
                                      m.n_sub, _i(m.sub_cluster), _d(m.sub_E), _d(m.sub_nu), len(m.dirichlet),
                                      _i(m.dirichlet), len(m.corner), _i(m.corner), _d(m.body_force)),
                     "htf_set_mesh")
+
+    def status_sub(self):
+        """Subdomain of the last HTF_ENOTSPD set-up failure, or -1."""
+        return lib.htf_status_sub(self._h)
 
     def set_loads(self, f_nodal):
         f = np.ascontiguousarray(np.atleast_2d(f_nodal), dtype=np.float64)

@@ -82,6 +82,8 @@ int htf_destroy(htf_ctx *ctx) {
 
 const char *htf_last_error(const htf_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+int htf_status_sub(const htf_ctx *ctx) { return ctx && ctx->eng ? ctx->eng->status_sub : -1; }
+
 int htf_set_mesh(htf_ctx *ctx, int n_nodes, const double *coords, int n_elems, const int *elems,
                  const int *elem_sub, int n_sub, const int *sub_cluster, const double *sub_E,
                  const double *sub_nu, int n_dirichlet, const int *dirichlet, int n_corner, const int *corner,
@@ -173,6 +175,21 @@ int htf_projection_noalloc(htf_ctx *ctx, const double *x_dev, double *Px_dev, vo
     if (cudaGetDevice(&prev) != cudaSuccess) return fail(ctx, HTF_ECUDA, "cudaGetDevice failed");
     if (prev != ctx->eng->device() && cudaSetDevice(ctx->eng->device()) != cudaSuccess)
         return fail(ctx, HTF_ECUDA, "cudaSetDevice failed");
+    // both vectors must be device (or managed) memory of the context's device: a host pointer or a
+    // pointer on another GPU would reach the kernels as an invalid address
+    for (const void *ptr : {static_cast<const void *>(x_dev), static_cast<const void *>(Px_dev)}) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+            cudaGetLastError();
+            if (prev != ctx->eng->device()) cudaSetDevice(prev);
+            return fail(ctx, HTF_EINVAL, "htf_projection_noalloc: a vector is not CUDA memory");
+        }
+        if ((a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) || a.device != ctx->eng->device()) {
+            if (prev != ctx->eng->device()) cudaSetDevice(prev);
+            return fail(ctx, HTF_EINVAL,
+                        "htf_projection_noalloc: both vectors must be device memory of the context's device");
+        }
+    }
     int rc = ctx->eng->project_noalloc(x_dev, Px_dev, static_cast<cudaStream_t>(stream), ctx->err);
     if (prev != ctx->eng->device()) cudaSetDevice(prev);
     return rc;

@@ -711,6 +711,20 @@ int Engine::setup(Problem &p, std::string &err) {
     lap(1);
     int rc = upload_layout(p, err);
     if (!rc) rc = check(cudaStreamSynchronize(s_), "sync", err);
+    if (!rc) {                    // the projector keeps 12 doubles per cluster in shared memory
+        const int smem = 12 * ncl_ * int(sizeof(double));
+        int optin = 0;
+        rc = check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, opt_.device),
+                   "cudaDeviceGetAttribute", err);
+        if (!rc && smem > optin) {
+            err = "projector: " + std::to_string(ncl_) + " clusters need " + std::to_string(smem) +
+                  " bytes of shared memory, the device allows " + std::to_string(optin) + " per block";
+            rc = HTF_EINVAL;
+        }
+        if (!rc && smem > 48 * 1024)
+            rc = check(cudaFuncSetAttribute(k_gf_apply_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                       "cudaFuncSetAttribute(k_gf_apply_fused)", err);
+    }
     lap(2);
     if (!rc) rc = factorize(p, err);
     lap(3);
@@ -985,7 +999,7 @@ int Engine::project_noalloc(const double *x, double *Px, cudaStream_t stream, st
     size_t cap = 0;
     int rc = noalloc_scratch(&scr, &cap, err);
     if (rc) return rc;
-    const size_t need = 6 * (size_t)nchunks_ + 6 * (size_t)ncl_;
+    const size_t need = 6 * (size_t)nchunks_;
     if (need > cap) {
         err = "htf_projection_noalloc: problem needs " + std::to_string(need) +
               " doubles of scratch, the static array holds " + std::to_string(cap);
@@ -994,7 +1008,7 @@ int Engine::project_noalloc(const double *x, double *Px, cudaStream_t stream, st
     k_gft_partial<<<nchunks_, 256, 0, stream>>>(d_chunk_cl_, d_chunk_beg_, d_chunk_end_, d_crow_, d_cval_, x, scr,
                                                 nullptr);
     k_gf_apply_fused<<<npart_, 256, 12 * ncl_ * sizeof(double), stream>>>(
-        nlam_, ncl_, d_cl_chunk_ptr_, scr, d_invGtG_, d_gcl_, d_gval_, x, scr + 6 * (size_t)nchunks_, nullptr, Px,
+        nlam_, ncl_, d_cl_chunk_ptr_, scr, d_invGtG_, d_gcl_, d_gval_, x, nullptr, nullptr, Px,
         nullptr, nullptr, nullptr);
     return check(cudaGetLastError(), "htf_projection_noalloc launch", err);
 }

@@ -406,7 +406,7 @@ int Engine::fp64_residual_batch(const std::vector<int> &sel, const std::vector<i
         r.rel[j] = st.norm0 > 0 ? cur / st.norm0 : 0.0;
         if (opt_.verbose)
             std::fprintf(stderr, "[htf mixed] rhs %d it %d FP64 sqrt(gPz)/norm0 = %.3e\n", r.r0 + j, st.it, r.rel[j]);
-        if (!(gPz[j] > 0.0) || !std::isfinite(gPz[j]) || cur < opt_.eps_iter * st.norm0) {
+        if (!(gPz[j] > 0.0) || !std::isfinite(gPz[j]) || cur < opt_.eps_iter * opt_.mixed_eps_factor * st.norm0) {
             r.conv[j] = 1;
             st.done = 1;
         } else {
@@ -449,7 +449,7 @@ int Engine::batch_begin(int r0, int kc, std::string &err) {
     int rc;
     std::vector<int> sel(K, 0), reset(K, 0);
     for (int j = 0; j < kc; ++j) {
-        r.st[j].eps = opt_.eps_iter;
+        r.st[j].eps = opt_.eps_iter * opt_.mixed_eps_factor;
         r.st[j].max_iter = opt_.max_iter;
         r.st[j].wFw = 1.0;
         sel[j] = reset[j] = 1;
@@ -479,7 +479,7 @@ int Engine::batch_check(bool &all_done, std::string &err) {
         const bool broke = r.st[j].done == 2;
         if (r.st[j].it >= opt_.max_iter) { r.conv[j] = 2; continue; }
         if (r.st[j].done != 0 || r.st[j].gPz < ru2 * r.last[j]) {
-            r.st[j].eps = opt_.eps_iter;
+            r.st[j].eps = opt_.eps_iter * opt_.mixed_eps_factor;
             sel[j] = 1;
             reset[j] = broke;
             changed = true;

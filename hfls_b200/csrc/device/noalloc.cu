@@ -1,21 +1,21 @@
 // Projector on caller-owned device vectors with no allocation at all.
 //
-// Callers that cannot call cudaMalloc at the time they project: code that
-// records the PCPG step into its own CUDA graph (allocation calls are not
-// allowed while a stream is being captured in global mode), serving loops
-// that admit work against a fixed device-memory budget and must not grow it
-// per call, and latency-bound loops where an allocation's implicit device
-// synchronisation would stall the other streams.  For them the reduction
-// scratch of the projector (6 partial sums per Gf chunk plus the 6 coarse
-// coefficients per cluster) lives in the static array below instead of the
-// context's own buffer.
+// Some callers of the PCPG building blocks cannot call cudaMalloc at the
+// moment they project: a serving loop that admits work against a fixed
+// device-memory budget must not grow its footprint per call, and a
+// latency-bound loop that shares the GPU with other streams cannot afford
+// the device-wide synchronisation an allocation may cause.  For them the
+// reduction scratch of the projector (6 partial sums per Gf chunk) lives in
+// the static array below instead of the context's own buffer.
 //
 // The array is HTF_NOALLOC_SCRATCH_DOUBLES doubles (8 MiB); every GPU that
 // loads the library holds it until the process exits.  All calls share it
 // and it keeps the last call's contents; each call overwrites every entry it
 // reads before reading it, so nothing needs to start at zero.  Calls whose
 // kernels overlap on the GPU (different streams without ordering) race on
-// the array and must be serialised by the caller.
+// the array and must be serialised by the caller.  The first call on a
+// device looks the array's device address up (once per device, with that
+// device current) and should come before any stream capture.
 #include <cuda_runtime.h>
 
 #include <mutex>

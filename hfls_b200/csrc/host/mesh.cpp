@@ -70,17 +70,20 @@ int mesh_sizes(const htf_mesh_spec &s, int *nn, int *ne, int *ns, int *nc, int *
     return HTF_OK;
 }
 
-double dense_factor_bytes(const htf_mesh_spec &s) {
+double factor_panel_bytes(const htf_mesh_spec &s) {
     Axes ax;
     std::string err;
     if (make_axes(s, ax, err)) return 0.0;
-    double sum[3] = {0.0, 0.0, 0.0};          // sum of (w+1)^2 over the slabs of each axis
+    // per subdomain n = 3 (w_x+1)(w_y+1)(w_z+1) DOFs; its lower-triangular
+    // column-panel factor holds at least n^2/2 + 16 n doubles
+    double sq[3] = {0.0, 0.0, 0.0}, lin[3] = {0.0, 0.0, 0.0};
     for (int a = 0; a < 3; ++a)
         for (int k = 0; k < ax.NS[a]; ++k) {
             const double w = ax.bound[a][k + 1] - ax.bound[a][k] + 1;
-            sum[a] += w * w;
+            sq[a] += w * w;
+            lin[a] += w;
         }
-    return 8.0 * 9.0 * sum[0] * sum[1] * sum[2];
+    return 8.0 * (0.5 * 9.0 * sq[0] * sq[1] * sq[2] + 16.0 * 3.0 * lin[0] * lin[1] * lin[2]);
 }
 
 int generate_mesh(const htf_mesh_spec &s, Mesh &m, std::string &err) {
@@ -216,6 +219,13 @@ int parse_options(const char *s, Options &o, std::string &err) {
             }
             o.preconditioner = v;
         } else if (k == "eps_iter") o.eps_iter = std::atof(v.c_str());
+        else if (k == "mixed_eps_factor") {
+            o.mixed_eps_factor = std::atof(v.c_str());
+            if (!(o.mixed_eps_factor > 0.0 && o.mixed_eps_factor <= 1.0)) {
+                err = "mixed_eps_factor must be in (0, 1]";
+                return HTF_EINVAL;
+            }
+        }
         else if (k == "max_iter") o.max_iter = std::atoi(v.c_str());
         else if (k == "precision") {
             if (v != "fp64" && v != "mixed") { err = "precision must be fp64|mixed"; return HTF_EINVAL; }

@@ -90,10 +90,15 @@ std::vector<int> null_pivots(const std::vector<double> &R, int n, int m) {
 
 // Right-looking Cholesky, column-contiguous updates.
 bool chol_lower(int n, double *A, int lda) {
+    // a pivot below 1e-12 of its column's original diagonal means the matrix
+    // is singular to working precision (a rank-deficient Gram matrix leaves
+    // round-off of either sign there), which is reported like a negative one
+    std::vector<double> diag(n);
+    for (int k = 0; k < n; ++k) diag[k] = A[k + size_t(k) * lda];
     for (int k = 0; k < n; ++k) {
         double *ck = A + size_t(k) * lda;
         const double d = ck[k];
-        if (!(d > 0.0)) return false;
+        if (!(d > 1e-12 * diag[k])) return false;
         const double r = std::sqrt(d);
         ck[k] = r;
         for (int i = k + 1; i < n; ++i) ck[i] /= r;

@@ -31,9 +31,10 @@ struct Mesh {
 
 // Mesh::createMesh generalised (Mesh.cpp:69-289).
 int generate_mesh(const htf_mesh_spec &s, Mesh &m, std::string &err);
-// sum over subdomains of 8 n_d^2 (n_d = 3 x nodes of subdomain d): the dense
-// factors alone, a lower bound of the device footprint of a spec's problem
-double dense_factor_bytes(const htf_mesh_spec &s);
+// sum over subdomains of 8 (n_d^2/2 + 16 n_d) (n_d = 3 x nodes of subdomain
+// d): the column-panel factors alone, a lower bound of the device footprint
+// of a spec's problem
+double factor_panel_bytes(const htf_mesh_spec &s);
 int mesh_sizes(const htf_mesh_spec &s, int *nn, int *ne, int *ns, int *nc, int *nd, int *ncr,
                std::string &err);
 int mesh_traction(const htf_mesh_spec &s, uint64_t seed, int n_rhs, double scale, double *f,
@@ -48,6 +49,10 @@ struct Options {
     double eps_iter = 1e-8;
     int max_iter = 500;
     bool mixed = false;                               // precision=mixed
+    double mixed_eps_factor = 0.1;                    // the batched mixed form stops at eps_iter x this factor:
+                                                      // the reference's criterion at eps_iter alone leaves the
+                                                      // displacements ~1e-7 from converged on ill-conditioned
+                                                      // meshes, the mixed form's bound against the FP64 oracle
     int device = 0;
     int check_every = 8;                              // iterations between host convergence checks
     int batch = 32;                                   // load cases per batched mixed-precision solve (16 | 32)
@@ -117,7 +122,7 @@ void kernel_of(const Mesh &m, const std::vector<int> &l2g, std::vector<double> &
 std::vector<int> null_pivots(const std::vector<double> &R, int n, int m);
 
 // ---- small dense FP64 helpers (column-major) ----
-bool chol_lower(int n, double *A, int lda);                          // in place
+bool chol_lower(int n, double *A, int lda);   // in place; false if not numerically SPD
 void chol_solve(int n, const double *L, int lda, double *B, int ldb, int nrhs);
 void sym_eig(int n, std::vector<double> &A, std::vector<double> &w, std::vector<double> &V);
 

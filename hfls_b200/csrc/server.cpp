@@ -169,8 +169,8 @@ int Server::submit(const htf_mesh_spec &spec, int nrhs, const double *f, double 
             r->spec.widths[a] = r->widths[a].data();
         }
     r->nrhs = nrhs;
-    // the dense factors alone exceed the budget: fail at once, before any host work
-    const double lower = dense_factor_bytes(r->spec);
+    // the factor panels alone exceed the budget: fail at once, before any host work
+    const double lower = factor_panel_bytes(r->spec);
     if (f && lower <= budget_) r->f.assign(f, f + (size_t)3 * nn * nrhs);
     r->u_out = u;
     r->info.status = HTF_REQ_QUEUED;
@@ -186,7 +186,7 @@ int Server::submit(const htf_mesh_spec &spec, int nrhs, const double *f, double 
         r->info.status = HTF_REQ_FAILED;
         r->info.t_done_ms = r->info.t_submit_ms;
         r->err = "request needs more than " + std::to_string(size_t(lower) >> 20) +
-                 " MiB for its dense factors, more than the server budget";
+                 " MiB for its factor panels, more than the server budget";
         all_[r->id] = std::move(r);
         cv_.notify_all();
         return HTF_OK;

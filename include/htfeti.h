@@ -107,6 +107,11 @@ typedef struct htf_ctx htf_ctx;
 int htf_create(const char *options, htf_ctx **ctx);
 int htf_destroy(htf_ctx *ctx);
 const char *htf_last_error(const htf_ctx *ctx);
+/* Subdomain whose regularised K_i was found not positive definite by the
+ * last htf_setup that returned HTF_ENOTSPD (-1 otherwise; also reported as
+ * htf_stats.status_sub by later solves).  The reference exits from inside
+ * PARDISO's factorisation instead (Matrix.cpp:1174-1178).                  */
+int htf_status_sub(const htf_ctx *ctx);
 
 /* Mesh of one problem.  Replaces the Mesh& argument of
  * Cluster::initialization (Cluster.cpp:21, 42) and the public Mesh fields
@@ -202,12 +207,15 @@ int htf_preconditioning(htf_ctx *ctx, const double *x, double *Mx, int nrhs);
  * without waiting.  It allocates nothing: its reduction scratch is a static
  * device array of HTF_NOALLOC_SCRATCH_DOUBLES doubles (8 MiB, held by every
  * GPU that loads the library until exit), for callers that cannot allocate
- * while they project — their own CUDA-graph capture, a fixed device-memory
- * budget, latency-bound loops.  No counterpart in the reference.  The first
- * call on a device looks the array up and should come before any stream
- * capture; all calls share the array, so calls that overlap on the GPU race.
- * Returns HTF_EINVAL when the problem needs more scratch (6 doubles per 1024
- * Gf entries plus 6 per cluster) than the array holds.                    */
+ * while they project — a serving loop held to a fixed device-memory budget,
+ * or a latency-bound loop that must not trigger the synchronisation an
+ * allocation can cause.  No counterpart in the reference.  The first call on
+ * a device looks the array up and should come before any stream capture;
+ * all calls share the array, so calls that overlap on the GPU race.
+ * Returns HTF_EINVAL when the problem needs more scratch than the array
+ * holds (6 doubles per chunk of up to 1024 dual rows of one cluster: about
+ * 170 million (row, cluster) entries of Gf), or when a vector is not device
+ * memory of the context's device.                                         */
 #define HTF_NOALLOC_SCRATCH_DOUBLES 1048576
 int htf_projection_noalloc(htf_ctx *ctx, const double *x_dev, double *Px_dev, void *stream);
 

@@ -8,7 +8,18 @@
 //   probe.txt   w, P F P w and P M P w for a seeded w (Projection, mult_Ff,
 //               Preconditioning of the reference, Cluster.cpp:1043-1188,1314-1329)
 //   elem.txt    Data::stf_mtrx_solid45 on an axis-aligned and a distorted hex
+//   timing.txt  wall seconds of the reference's own timed intervals (below)
 // The displacement field is the reference's own box.vtk in path2data.
+//
+// Timing: clock() is wrapped too (--wrap=clock).  The reference calls it four
+// times in a run: at the start of Cluster::initialization (Cluster.cpp:24),
+// at the start and end of Cluster::pcpg's timed region (Cluster.cpp:1364,
+// 1451; the final printVTK is outside it) and at the end of the setup +
+// solve (Cluster.cpp:374).  The wrapper returns the real clock() and records
+// a steady-clock wall time per call, so timing.txt holds the reference's own
+// "Solver time" and "Total time" intervals in wall seconds at microsecond
+// resolution (the reference prints them with one decimal).  `dumps=false`
+// skips the layout, probe and element dumps.
 //
 // Two process-level measures keep the run deterministic without touching the
 // sources: time() is wrapped (link flag --wrap=time) so the srand(time(NULL))
@@ -16,6 +27,7 @@
 // the global allocator pads every block with 0xFF bytes so the read past the
 // end of nullPivots in Matrix::num_factor (Matrix.cpp:1040) sees -1 and never
 // triggers the out-of-bounds write at Matrix.cpp:1043.
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -31,6 +43,14 @@
 extern "C" time_t __wrap_time(time_t *t) {
     if (t) *t = 12345;
     return 12345;
+}
+
+extern "C" clock_t __real_clock(void);
+static std::vector<double> g_clock_wall;
+extern "C" clock_t __wrap_clock(void) {
+    g_clock_wall.push_back(std::chrono::duration<double>(
+        std::chrono::steady_clock::now().time_since_epoch()).count());
+    return __real_clock();
 }
 
 static const size_t kPad = 64;
@@ -94,6 +114,7 @@ int main(int argc, char **argv) {
     long jitter_seed = -1;
     bool clamp = false;
     long probe_seed = 7;
+    bool dumps = true;
     for (int i = 1; i < argc; ++i) {
         std::string a = argv[i];
         size_t eq = a.find('=');
@@ -103,6 +124,7 @@ int main(int argc, char **argv) {
         else if (k == "jitter_seed") jitter_seed = std::atol(v.c_str());
         else if (k == "clamp") clamp = (v == "true");
         else if (k == "probe_seed") probe_seed = std::atol(v.c_str());
+        else if (k == "dumps") dumps = (v != "false");
         else o[k] = v;
     }
     mkdir(out.c_str(), 0755);
@@ -152,7 +174,17 @@ int main(int argc, char **argv) {
     std::fclose(fm);
 
     Cluster cluster;
+    g_clock_wall.clear();
     cluster.initialization(o, mesh);          // setup + PCPG + box.vtk
+    FILE *ft = std::fopen((out + "/timing.txt").c_str(), "w");
+    if (g_clock_wall.size() == 4) {           // Cluster.cpp:24, 1364, 1451, 374
+        const std::vector<double> &c = g_clock_wall;
+        std::fprintf(ft, "setup_s %.6f\npcpg_s %.6f\ntotal_s %.6f\n", c[1] - c[0], c[2] - c[1], c[3] - c[0]);
+    } else {
+        std::fprintf(ft, "clock_calls %zu\n", g_clock_wall.size());
+    }
+    std::fclose(ft);
+    if (!dumps) return 0;
 
     FILE *fl = std::fopen((out + "/layout.txt").c_str(), "w");
     int ns = cluster.get_nSubClst();

@@ -145,7 +145,8 @@ def write_vtk_fixture():
 
 def main():
     if not os.path.exists(REF_BIN):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle", "ref_build")], check=True)
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle", "ref_build"),
+                        "REF=" + os.environ.get("HFLS_REFERENCE", "/root/reference")], check=True)
     for name, args in CASES.items():
         run_case(name, args)
     write_vtk_fixture()

@@ -40,3 +40,19 @@ def mesh_from_golden(g, args, clusters=None):
 def options_from_args(args, **kw):
     return Options(typeBc=args["typeBc"], preconditioner=args["preconditioner"],
                    eps_iter=float(args.get("eps_iter", "1e-8")), **kw)
+
+
+def oracle_golden(name):
+    """Full-size oracle golden written by tests/golden/make_large_goldens.py."""
+    return np.load(os.path.join(GOLDEN_DIR, f"oracle_{name}.npz"))
+
+
+def golden_rel_err(g, u, k):
+    """Relative displacement error of load case k against an oracle golden:
+    the larger of the error on its seeded DOF sample and on its seeded
+    N(0,1) projections of the whole field (make_large_goldens.py)."""
+    idx = g["sample_idx"]
+    e1 = np.linalg.norm(u[idx] - g["u_sample"][k]) / np.linalg.norm(g["u_sample"][k])
+    P = np.random.default_rng(777).standard_normal((g["u_proj"].shape[1], u.size))
+    e2 = np.linalg.norm(P @ u - g["u_proj"][k]) / np.linalg.norm(g["u_proj"][k])
+    return float(max(e1, e2))

@@ -67,7 +67,7 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
     import bench
     monkeypatch.setenv("RANK", "1")
     called = []
-    monkeypatch.setattr(bench, "ref_iteration_seconds", lambda: called.append(1))
+    monkeypatch.setattr(bench, "ref_small_measure", lambda *a: called.append(1))
 
     class A:
         warmup, steps = 3, 1
