@@ -133,19 +133,23 @@ constexpr int SYMV_BUCKET_NT[SYMV_BUCKETS] = {8, 16, 32, 64, 1 << 30};
 constexpr int SYMV_DEFAULT_TILES = 48;
 
 // One CTA of the tensor-core multi-RHS product: 128-row block m of
-// subdomain d (slabs (m, 0..ks-1) contiguous at a_off, X slabs at x_off).
-// `set` names the TcSet (problem) the block belongs to: one launch can cover
-// the blocks of several problems.
+// subdomain d.  The symmetric A_d is stored as its lower triangle at 128-row
+// block granularity: block m holds the slabs (m, 0 .. kd-1), kd =
+// min(4 (m + 1), ks), contiguous at a_off, and the subdomain's blocks follow
+// one another, so block m' starts 2 m' (m' + 1) slabs after block 0.  Column
+// slabs kk >= kd of block m (above the diagonal block) are read transposed
+// from the blocks below.  X slabs at x_off.  `set` names the TcSet (problem)
+// the block belongs to: one launch can cover the blocks of several problems.
 struct GemmBlock {
     int d;                                // subdomain within its problem
     int m;                                // 128-row block index
-    long long a_off;                      // first slab (floats) in the set's A arrays
-    int ks;                               // K slabs (32 columns each)
+    long long a_off;                      // first stored slab (floats) of this block in the set's A arrays
+    int ks;                               // K slabs (32 columns each) of the full row
     int rows;                             // valid rows of the block
     long long x_off;                      // first X slab (floats)
     long long y_row0;                     // first output row (b-space slot)
     int set;
-    int pad;
+    int kd;                               // slabs stored in this block row (the rest are read transposed)
 };
 
 // Operands of the tensor-core products of one problem.

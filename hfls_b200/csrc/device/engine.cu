@@ -1073,10 +1073,15 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
         CK(cudaMemsetAsync(b_s_, 0, (size_t)ngc_total_ * K * sizeof(double), s_));
         profile_batch_gather(b_tmp_);
         info->tc_F_ms = timeit([&] { tc_apply(0); });
-        // FP32 slabs, X_hi + X_lo, Y, and the V columns of the epilogue's correction
-        double vbytes = 0.0;
-        for (auto &h : hs_) vbytes += 8.0 * h.nbp * (h.c + 6);
-        info->tc_F_bytes = 4.0 * aoff_ + 2.0 * 4.0 * nslots_ * K + 8.0 * nslots_ * K + vbytes;
+        // algorithmic bytes of one launch (the F apply's per-subdomain terms for k
+        // load cases): the FP32 triangle n_b (n_b + 1) / 2, the coupling columns
+        // V = [F Bc_b^T, -R_b] (FP64, n_b (c + 6)), X_hi + X_lo in (FP32) and Y out
+        // (FP64) per load case; padding rows and the diagonal blocks' upper halves
+        // the kernel also reads are not counted
+        double bytes = 0.0;
+        for (auto &h : hs_)
+            bytes += 4.0 * h.nb * (h.nb + 1.0) / 2.0 + 8.0 * h.nb * (h.c + 6) + (4.0 + 4.0 + 8.0) * h.nb * K;
+        info->tc_F_bytes = bytes;
         if (bgraph_) {
             std::vector<PcpgState> st(K), saved(K);
             for (auto &x : st) {

@@ -89,18 +89,24 @@ int Engine::setup_batch(int K, std::string &err) {
             err = "too many Bc rows for the batched form";
             return HTF_EINVAL;
         }
-    // tensor-core blocks and FP32 slabs
+    // tensor-core blocks and FP32 slabs: the lower triangle at 128-row block
+    // granularity (block m stores its slabs kk < min(4 (m + 1), ks), so the
+    // block's first slab is 2 m (m + 1) slabs after the subdomain's first)
     std::vector<GemmBlock> blocks;
     long long aoff = 0;
     for (int d = 0; d < nsub_; ++d) {
         const SubDev &h = hs_[d];
         const int mb = (h.nbp + 127) / 128, ks = h.nbp / 32;
+        long long stored = 0;
         for (int m = 0; m < mb; ++m) {
-            GemmBlock g{d, m, aoff + (long long)m * ks * 4096, ks, std::min(128, h.nb - 128 * m),
-                        (long long)h.xb_off * K, (long long)h.xb_off + 128 * m, 0, 0};
+            const int kd = std::min(4 * (m + 1), ks);
+            if (stored != 2LL * m * (m + 1)) { err = "tensor-core slab layout"; return HTF_EINVAL; }
+            GemmBlock g{d, m, aoff + stored * 4096, ks, std::min(128, h.nb - 128 * m),
+                        (long long)h.xb_off * K, (long long)h.xb_off + 128 * m, 0, kd};
             blocks.push_back(g);
+            stored += kd;
         }
-        aoff += (long long)mb * ks * 4096;
+        aoff += stored * 4096;
     }
     nblocks_ = int(blocks.size());
     d_blocks_ = alloc<GemmBlock>(blocks.size(), err, rc);

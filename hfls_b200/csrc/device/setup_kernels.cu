@@ -275,12 +275,25 @@ __global__ void __launch_bounds__(128) k_trsm_panel(const StepDesc *__restrict__
 
 // C(64x64 block, lower part of the trailing matrix) -= P_i P_j^T, P = the
 // step's panel rows; 32 columns of P at a time, one accumulator per panel,
-// C read and written once.  grid: the step's trailing tiles (flattened)
+// C read and written once.  The products run on the FP64 tensor path
+// (mma.sync m8n8k4 .f64): warp w owns rows 32 (w / 4) .. +31 and columns
+// 16 (w % 4) .. +15 of the block, 4 x 2 tiles of 8 x 8, so per k-group of 4
+// a warp loads 6 operand fragments for 8 MMAs (the CUDA-core form loaded 8
+// values per 16 FMAs per thread and was bound by shared-memory loads).  A
+// row stride of 68 doubles keeps both fragment loads free of bank
+// conflicts.  grid: the step's trailing tiles (flattened)
+__device__ __forceinline__ void dmma_syrk(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict__ st, int cnt,
                                                      const SubDev *__restrict__ subs,
                                                      double *__restrict__ Kbuf) {
-    __shared__ double Pa[32][64 + 1];
-    __shared__ double Pb[32][64 + 1];
+    constexpr int LDP = 68;
+    __shared__ double Pa[32][LDP];
+    __shared__ double Pb[32][LDP];
     const int e = step_entry(st, cnt, int(blockIdx.x), [](const StepDesc &x) { return x.tri0; });
     const StepDesc s = st[e];
     const SubDev &sd = subs[s.d];
@@ -295,14 +308,16 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
     while (bi * (bi + 1) / 2 > tri) --bi;
     const int bj = tri - bi * (bi + 1) / 2;
     const int i0 = t0 + 64 * bi, j0 = t0 + 64 * bj;
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double acc[CHOL_STEP / TILE][4][4];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int wr = 32 * (warp >> 2), wc = 16 * (warp & 3);
+    double acc[CHOL_STEP / TILE][4][2][2];
 #pragma unroll
     for (int q = 0; q < CHOL_STEP / TILE; ++q)
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[q][a][b] = 0.0;
+            for (int b = 0; b < 2; ++b) acc[q][a][b][0] = acc[q][a][b][1] = 0.0;
 #pragma unroll
     for (int q = 0; q < CHOL_STEP / TILE; ++q) {
         const int kc = TILE * q;
@@ -318,35 +333,39 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
             Pb[kk][r] = (ok && j0 + r < N) ? P[(j0 + r - k - kc) + kk * ld] : 0.0;
         }
         __syncthreads();
-        for (int kk = 0; kk < kn; ++kk) {
-            double av[4], bv[4];
+        const int kgs = (kn + 3) >> 2;
+        for (int kg = 0; kg < kgs; ++kg) {
+            const int kr = 4 * kg + t4;
+            double av[4], bv[2];
 #pragma unroll
-            for (int a = 0; a < 4; ++a) av[a] = Pa[kk][tx + 16 * a];
+            for (int a = 0; a < 4; ++a) av[a] = Pa[kr][wr + 8 * a + g];
 #pragma unroll
-            for (int b = 0; b < 4; ++b) bv[b] = Pb[kk][ty + 16 * b];
+            for (int b = 0; b < 2; ++b) bv[b] = Pb[kr][wc + 8 * b + g];
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) acc[q][a][b] += av[a] * bv[b];
+                for (int b = 0; b < 2; ++b) dmma_syrk(acc[q][a][b][0], acc[q][a][b][1], av[a], bv[b]);
         }
     }
     const int nq = (nb + TILE - 1) / TILE;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        const int col = j0 + ty + 16 * b;
-        if (col >= N) continue;
-        double *C = Kbuf + kcol(sd, col);
+    for (int b = 0; b < 2; ++b)
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int row = i0 + tx + 16 * a;
-            if (row >= N || row < col) continue;
-            double c = C[row];
+        for (int h = 0; h < 2; ++h) {
+            const int col = j0 + wc + 8 * b + 2 * t4 + h;
+            if (col >= N) continue;
+            double *C = Kbuf + kcol(sd, col);
 #pragma unroll
-            for (int q = 0; q < CHOL_STEP / TILE; ++q)
-                if (q < nq) c -= acc[q][a][b];
-            C[row] = c;
+            for (int a = 0; a < 4; ++a) {
+                const int row = i0 + wr + 8 * a + g;
+                if (row >= N || row < col) continue;
+                double c = C[row];
+#pragma unroll
+                for (int q = 0; q < CHOL_STEP / TILE; ++q)
+                    if (q < nq) c -= acc[q][a][b][h];
+                C[row] = c;
+            }
         }
-    }
 }
 
 // Copy the trailing nbp x nbp block into packed tiles, minus the fix diagonal.

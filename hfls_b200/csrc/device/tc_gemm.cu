@@ -1,25 +1,34 @@
 // Multi-right-hand-side F_i / S_i apply on the 5th-generation tensor cores.
 //
-// Y_b(:, 0:k) = A_i X_b(:, 0:k) for every subdomain i, with A_i the full
+// Y_b(:, 0:k) = A_i X_b(:, 0:k) for every subdomain i, with A_i the
 // symmetric F_i (or S_i) stored in FP32 and the products formed as 3xTF32
 // (A_hi X_hi + A_hi X_lo + A_lo X_hi) on the tensor cores
 // (Cluster::mult_Ff's local solves, Cluster.cpp:1125-1126, applied to k
 // load cases at once).
 //
-// Storage: A_i is cut into 128 x 32 slabs (128 rows of an M block, 32
-// columns of a K slab), each 16 KB and already in the SWIZZLE_128B K-major
-// layout the MMA reads from shared memory (byte b of the logical row-major
-// slab lives at b ^ (((b >> 7) & 7) << 4)), so one cp.async.bulk per slab
-// lands it ready for tcgen05.mma.  X is written by the gather kernel in the
-// same layout as k x 32 slabs (one 128-byte row per load case), already
-// split into its TF32 part and the TF32 remainder.
+// Storage: the lower triangle of A_i at 128-row block granularity, cut into
+// 128 x 32 slabs (128 rows of an M block, 32 columns of a K slab), each
+// 16 KB and already in the SWIZZLE_128B K-major layout the MMA reads from
+// shared memory (byte b of the logical row-major slab lives at
+// b ^ (((b >> 7) & 7) << 4)), so one cp.async.bulk per slab lands it ready
+// for tcgen05.mma.  Block m keeps its slabs up to and including its
+// diagonal 128 x 128 block; the K steps right of it read the transpose of
+// the blocks below, 32 rows of four stored slabs (4 x 4 KB bulk copies),
+// which the splitting warps transpose in shared memory.  Each off-diagonal
+// slab is thus read from HBM by its own block and, through L2, by the block
+// its columns belong to: half the bytes of full symmetric storage.  X is
+// written by the gather kernel in the same layout as k x 32 slabs (one
+// 128-byte row per load case), already split into its TF32 part and the
+// TF32 remainder.
 //
 // One CTA of 6 warps per (subdomain, 128-row block):
-//   * warp 0, one thread: bulk-copy producer (A slab, X_hi, X_lo per stage);
+//   * warp 0, one thread: bulk-copy producer (A slab or its four transposed
+//     pieces, X_hi, X_lo per stage);
 //   * warps 2-5: form A_lo = rna_tf32(A - trunc_tf32(A)) of every landed A
 //     slab (the MMA reads the FP32 slab itself as A_hi: a TF32 operand's
-//     low 13 mantissa bits do not take part in the product), then hand the
-//     stage to the MMA issuer;
+//     low 13 mantissa bits do not take part in the product; a transposed
+//     step is first transposed in place, each warp inside its own 4 KB),
+//     then hand the stage to the MMA issuer;
 //     at the end they read the accumulators out of TMEM (warp w owns TMEM
 //     lanes 32 (w mod 4) .. +31) and write y in FP64;
 //   * warp 1, one thread: issues the MMAs (M=128, N=k, K=8 per instruction,
@@ -87,6 +96,32 @@ __device__ __forceinline__ uint32_t tf32_idesc(int M, int N) {
            | (2u << 7)          // A format TF32
            | (2u << 10)         // B format TF32
            | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);   // A, B K-major
+}
+
+// One warp's 4 KB of a transposed K step: pa holds 32 rows x 32 columns of
+// a stored slab (SWIZZLE_128B rows), whose column `lane` becomes row `lane`
+// of the same 4 KB in the K-major slab the MMA reads; its A_lo row goes to
+// the same place in lo.  Kept out of line so its 32 live values do not
+// compete with the epilogue's registers.
+__device__ __noinline__ void split_transposed(float *pa, float *lo, int lane) {
+    float v[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = pa[j * 32 + (lane ^ ((j & 7) << 2))];
+    __syncwarp();
+    float *hrow = pa + lane * 32;
+    float *lrow = lo + lane * 32;
+#pragma unroll
+    for (int g4 = 0; g4 < 8; ++g4) {
+        const int ph = (g4 ^ (lane & 7)) * 4;     // SWIZZLE_128B position of granule g4 in this row
+        const float4 h = make_float4(v[4 * g4], v[4 * g4 + 1], v[4 * g4 + 2], v[4 * g4 + 3]);
+        float4 l;
+        l.x = tf32_rna(h.x - tf32_trunc(h.x));
+        l.y = tf32_rna(h.y - tf32_trunc(h.y));
+        l.z = tf32_rna(h.z - tf32_trunc(h.z));
+        l.w = tf32_rna(h.w - tf32_trunc(h.w));
+        *reinterpret_cast<float4 *>(hrow + ph) = h;
+        *reinterpret_cast<float4 *>(lrow + ph) = l;
+    }
 }
 
 constexpr int TC_NACC = 2;                   // rotating accumulator groups
@@ -190,6 +225,8 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
     if (warp == 0) {
         if (lane == 0) {                                  // producer
             int issued = 0;
+            // first stored slab of the subdomain: block m' starts 2 m' (m' + 1) slabs after it
+            const long long a0 = g.a_off - 2LL * g.m * (g.m + 1) * TC_SLAB_A;
             for (int kk = 0; kk < g.ks; ++kk) {
                 const int s = kk % TC_STAGES;
                 if (kk >= TC_STAGES && !mbar_wait(&empty[s], ((kk / TC_STAGES) - 1) & 1)) {
@@ -199,7 +236,18 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                 }
                 if (abort_flag) break;
                 mbar_expect_tx(&full[s], STAGE_TX);
-                bulk_g2s(sA + s * TC_SLAB_A, A + g.a_off + (long long)kk * TC_SLAB_A, TC_SLAB_A * 4, &full[s]);
+                if (kk < g.kd) {
+                    bulk_g2s(sA + s * TC_SLAB_A, A + g.a_off + (long long)kk * TC_SLAB_A, TC_SLAB_A * 4, &full[s]);
+                } else {
+                    // above the diagonal block: rows [32 kk, 32 kk + 32) of the stored slabs
+                    // (kk / 4, 4 m + p), p = 0..3, i.e. 32 rows x 128 columns of the transpose;
+                    // each 32-row piece is 4 KB contiguous (8-row swizzle groups of 1 KB)
+                    const int mp = kk >> 2, q = kk & 3;
+                    const float *src = A + a0 + (2LL * mp * (mp + 1) + 4LL * g.m) * TC_SLAB_A + q * 1024;
+#pragma unroll
+                    for (int p = 0; p < 4; ++p)
+                        bulk_g2s(sA + s * TC_SLAB_A + p * 1024, src + (long long)p * TC_SLAB_A, 4096, &full[s]);
+                }
                 bulk_g2s(sB + s * 2 * SLAB_B, Xs + g.x_off + (long long)kk * SLAB_B, SLAB_B * 4, &full[s]);
                 bulk_g2s(sB + (s * 2 + 1) * SLAB_B, Xs + xlo_off + g.x_off + (long long)kk * SLAB_B, SLAB_B * 4,
                          &full[s]);
@@ -254,17 +302,25 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                 abort_flag = 1;
                 break;
             }
-            const float4 *a4 = reinterpret_cast<const float4 *>(sA + s * TC_SLAB_A);
-            float4 *lo = reinterpret_cast<float4 *>(sL + lb * TC_SLAB_A);
+            if (kk < g.kd) {                              // stored slab: A_lo beside it
+                const float4 *a4 = reinterpret_cast<const float4 *>(sA + s * TC_SLAB_A);
+                float4 *lo = reinterpret_cast<float4 *>(sL + lb * TC_SLAB_A);
 #pragma unroll
-            for (int i = t; i < TC_SLAB_A / 4; i += 128) {
-                const float4 v = a4[i];
-                float4 l;
-                l.x = tf32_rna(v.x - tf32_trunc(v.x));
-                l.y = tf32_rna(v.y - tf32_trunc(v.y));
-                l.z = tf32_rna(v.z - tf32_trunc(v.z));
-                l.w = tf32_rna(v.w - tf32_trunc(v.w));
-                lo[i] = l;
+                for (int i = t; i < TC_SLAB_A / 4; i += 128) {
+                    const float4 v = a4[i];
+                    float4 l;
+                    l.x = tf32_rna(v.x - tf32_trunc(v.x));
+                    l.y = tf32_rna(v.y - tf32_trunc(v.y));
+                    l.z = tf32_rna(v.z - tf32_trunc(v.z));
+                    l.w = tf32_rna(v.w - tf32_trunc(v.w));
+                    lo[i] = l;
+                }
+            } else {
+                // transposed pieces: warp p (0..3) owns piece p (4 KB at p * 1024 floats), whose
+                // column l is row 32 p + l of this K step's A; the output rows 32 p .. 32 p + 31
+                // of the K-major slab occupy the same 4 KB, so the transpose stays inside the warp
+                split_transposed(sA + s * TC_SLAB_A + (warp - 2) * 1024, sL + lb * TC_SLAB_A + (warp - 2) * 1024,
+                                 lane);
             }
             // generic-proxy writes become visible to the tensor core's async proxy
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -357,14 +413,15 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
 template __global__ void k_tc_gemm<16>(const GemmBlock *, const TcSet *, int, int *);
 template __global__ void k_tc_gemm<32>(const GemmBlock *, const TcSet *, int, int *);
 
-// Full FP32 slabs of a packed symmetric FP64 tile matrix: slab (m, kk) of
-// subdomain d holds rows [128m, 128m+128) x columns [32kk, 32kk+32) of the
-// symmetric block, swizzled for SWIZZLE_128B K-major.  grid (block, kk).
+// FP32 slabs of the lower triangle (at 128-row block granularity) of a packed
+// symmetric FP64 tile matrix: slab (m, kk), kk < kd, of subdomain d holds
+// rows [128m, 128m+128) x columns [32kk, 32kk+32) of the symmetric block,
+// swizzled for SWIZZLE_128B K-major.  grid (block, kk).
 __global__ void k_make_slabs(const GemmBlock *__restrict__ blocks, const SubDev *__restrict__ subs,
                              const double *__restrict__ tiles, float *__restrict__ A) {
     const GemmBlock g = blocks[blockIdx.x];
     const int kk = blockIdx.y;
-    if (kk >= g.ks) return;
+    if (kk >= g.kd) return;
     const SubDev &sd = subs[g.d];
     float *slab = A + g.a_off + (long long)kk * TC_SLAB_A;
     for (int idx = threadIdx.x; idx < TC_SLAB_A; idx += blockDim.x) {

@@ -231,10 +231,12 @@ size_t Server::estimate(const Problem &p, int nrhs) const {
     for (const Subdomain &s : p.sub) {
         const double nbp = 32.0 * ((s.nb + 31) / 32), N = (s.n - s.nb) + nbp, nt = nbp / 32;
         const double mb = std::ceil(nbp / 128.0), nks = nbp / 32;
+        double stored = 0.0;                              // FP32 slabs: lower triangle of 128-row blocks
+        for (int m = 0; m < int(mb); ++m) stored += std::min(4.0 * (m + 1), nks);
         b += 8.0 * (double(kpanel_doubles(s.n - s.nb, int(nbp))) + nt * (nt + 1) * 1024.0 +
                     nbp * (s.c() + 6) + 6 * N + 2 * nbp);
         xs += nbp * nbp;
-        b += 2.0 * mb * nks * 4096.0 * 4.0;
+        b += 2.0 * stored * 4096.0 * 4.0;
         nslots += nbp;
         nfull += N;
     }
