@@ -52,7 +52,7 @@ class ProfileInfo(ctypes.Structure):
                 ("batch_width", ctypes.c_int), ("tc_F_ms", ctypes.c_double), ("tc_F_bytes", ctypes.c_double),
                 ("batch_iteration_ms", ctypes.c_double), ("kernels_per_batch_iteration", ctypes.c_int),
                 ("setup_phase_ms", ctypes.c_double * 8), ("symv_unit_tiles", ctypes.c_int * 5),
-                ("symv_tuned", ctypes.c_int)]
+                ("symv_tuned", ctypes.c_int), ("device_bytes", ctypes.c_double)]
 
 
 class RequestInfo(ctypes.Structure):
@@ -84,6 +84,7 @@ _SIGS = {
     "htf_dual_sizes": [ctypes.c_void_p, _ip, _ip, _ip],
     "htf_dual_layout": [ctypes.c_void_p, _ip, _ip, _dp, _dp],
     "htf_fix_dofs": [ctypes.c_void_p, _ip],
+    "htf_residual_history": [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_int],
     "htf_projection_noalloc": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "htf_server_create": [ctypes.c_char_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
     "htf_server_destroy": [ctypes.c_void_p],
@@ -291,6 +292,15 @@ class Solver:
         sg = np.zeros(2 * nl); w = np.zeros(nl)
         self._check(lib.htf_dual_layout(self._h, _i(rs), _i(rd), _d(sg), _d(w)), "htf_dual_layout")
         return rs.reshape(-1, 2), rd.reshape(-1, 2), sg.reshape(-1, 2), w
+
+    def residual_history(self, rhs=0):
+        """Relative residual per PCPG iteration of load case rhs of the last plain solve."""
+        n = lib.htf_residual_history(self._h, rhs, None, 0)
+        if n < 0:
+            self._check(n, "htf_residual_history")
+        h = np.zeros(n)
+        self._check(min(0, lib.htf_residual_history(self._h, rhs, _d(h), n)), "htf_residual_history")
+        return h
 
     def fix_dofs(self):
         ns = self.mesh.n_sub

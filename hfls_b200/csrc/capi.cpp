@@ -195,6 +195,12 @@ int htf_projection_noalloc(htf_ctx *ctx, const double *x_dev, double *Px_dev, vo
     return rc;
 }
 
+int htf_residual_history(htf_ctx *ctx, int rhs, double *hist, int cap) {
+    if (!ctx) return HTF_EINVAL;
+    if (!ctx->is_setup) return fail(ctx, HTF_ESTATE, "htf_residual_history before htf_setup");
+    return ctx->eng->history(rhs, hist, cap, ctx->err);
+}
+
 int htf_dual_sizes(htf_ctx *ctx, int *n_lambda, int *n_sub, int *n_clusters) {
     if (!ctx) return HTF_EINVAL;
     if (ctx->p.rows.empty()) {

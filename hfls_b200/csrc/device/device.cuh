@@ -69,6 +69,9 @@ struct ClusterDev {
     long long M_off;                      // M = (Ac^{-1}) restricted, ngc x ngc (col-major)
     int gc_off;                           // offset in the concatenated coarse vectors
     int gmap_off;                         // gather map: ptr array offset (ngc+1 entries)
+    long long MT_off;                     // M as packed lower 32x32 tiles (the plain form's copy): first tile
+    int mt;                               // tile rows, ceil(ngc / 32)
+    int mt_row_off;                       // first tile row of this cluster in the per-row arrays
 };
 
 #ifdef __CUDACC__

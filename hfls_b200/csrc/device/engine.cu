@@ -36,6 +36,14 @@ __global__ void k_symv_units(const SymvUnit *, const SubDev *, const T *, const 
                              double *, const PcpgState *);
 __global__ void k_reduce_correct(const SubDev *, const SymvUnit *, const double *, const ClusterDev *,
                                  const double *, const int *, const double *, double *, const PcpgState *);
+__global__ void k_lbt_x(const int2 *, const SubDev *, const double *, const double *, double *, const PcpgState *);
+__global__ void k_lb_t(const int2 *, const SubDev *, const double *, const double *, const double *, double *,
+                       const PcpgState *);
+__global__ void k_pack_M(const int2 *, const ClusterDev *, const double *, double *);
+__global__ void k_msym_rows(const int2 *, const ClusterDev *, const double *, const double *, double *, double *,
+                            const PcpgState *);
+__global__ void k_msym_reduce(const int2 *, const ClusterDev *, const double *, const double *, double *,
+                              const PcpgState *);
 __global__ void k_gf_apply_fused(int, int, const int *, const double *, const double *, const int *,
                                  const double *, const double *, double *, double *, double *, const double *,
                                  double *, const PcpgState *);
@@ -51,7 +59,7 @@ __global__ void k_gf_mult(int, const int *, const double *, const double *, doub
 __global__ void k_update_lam_g(int, const double *, int, const double *, const double *, double *, double *,
                                PcpgState *);
 __global__ void k_update_w(int, const double *, int, const double *, double *, PcpgState *);
-__global__ void k_finish_iter(const double *, int, PcpgState *);
+__global__ void k_finish_iter(const double *, int, PcpgState *, double *);
 __global__ void k_init_state(const double *, int, PcpgState *, double, int);
 __global__ void k_axpby(int, double, const double *, double, double *);
 
@@ -171,6 +179,22 @@ __global__ void k_gather_u(int ndof, const int *__restrict__ win, const double *
 }
 
 // ---------------------------------------------------------------------------
+// free one of the engine's buffers before the end of its life
+void Engine::release(void *p) {
+    for (size_t i = 0; i < bufs_.size(); ++i)
+        if (bufs_[i].p == p) {
+            cudaFree(p);
+            bufs_.erase(bufs_.begin() + i);
+            return;
+        }
+}
+
+// s = M gc for every cluster (M = [Ac^{-1}] restricted), from the packed symmetric tiles
+void Engine::coarse_apply(const double *gc, double *s, const PcpgState *st) {
+    k_msym_rows<<<nmt_, 128, 0, s_>>>(d_mt_, d_cl_, d_MT_, gc, d_mD_, d_mP_, st);
+    k_msym_reduce<<<nmt_, TILE, 0, s_>>>(d_mt_, d_cl_, d_mD_, d_mP_, s, st);
+}
+
 Engine::~Engine() {
     if (own_s_) cudaStreamSynchronize(own_s_);
     if (s_ && s_ != own_s_) cudaStreamSynchronize(s_);
@@ -261,11 +285,18 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     hc_.assign(ncl_, ClusterDev());
     long long M_off = 0;
     int gc_off = 0;
+    long long MT_off = 0;
+    int mt_rows = 0;
+    std::vector<int2> mtl;
     for (int c = 0; c < ncl_; ++c) {
         hc_[c].nlam_c = p.clu[c].nlam_c;
         hc_[c].ngc = p.clu[c].ngc();
         hc_[c].M_off = M_off; M_off += (long long)hc_[c].ngc * hc_[c].ngc;
         hc_[c].gc_off = gc_off; gc_off += hc_[c].ngc;
+        hc_[c].mt = (hc_[c].ngc + TILE - 1) / TILE;
+        hc_[c].MT_off = MT_off; MT_off += (long long)hc_[c].mt * (hc_[c].mt + 1) / 2;
+        hc_[c].mt_row_off = mt_rows; mt_rows += hc_[c].mt;
+        for (int I = 0; I < hc_[c].mt; ++I) mtl.push_back(make_int2(c, I));
     }
     ngc_total_ = gc_off;
     // device allocations
@@ -274,10 +305,19 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     d_all_subs_ = alloc<int>(nsub_, err, rc);
     d_K_ = alloc<double>(K_off, err, rc);
     d_F_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);
-    d_S_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);
+    implicit_ = opt_.preconditioner == "Dirichlet_implicit";
+    if (!implicit_) d_S_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);   // implicit: S applied through L_bb
     d_V_ = alloc<double>(V_off, err, rc);
     d_R_ = alloc<double>(R_off, err, rc);
     d_M_ = alloc<double>(M_off, err, rc);
+    // the plain form's coarse solves read M as packed symmetric tiles (the dense M is freed after
+    // set-up unless the batched mixed form needs it)
+    nmt_ = int(mtl.size());
+    d_mt_ = alloc<int2>(mtl.size(), err, rc);
+    d_MT_ = alloc<double>(MT_off * TILE_ELEMS, err, rc);
+    d_mP_ = alloc<double>(MT_off * TILE, err, rc);
+    d_mD_ = alloc<double>((size_t)mt_rows * TILE, err, rc);
+    if (!rc) CK(cudaMemcpyAsync(d_mt_, mtl.data(), mtl.size() * sizeof(int2), cudaMemcpyHostToDevice, s_));
     d_H_ = alloc<double>(36 * (size_t)nsub_, err, rc);
     d_status_ = alloc<int>(nsub_, err, rc);
     if (rc) return rc;
@@ -393,6 +433,15 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     d_tmp_ = alloc<double>(nlam_, err, rc);
     d_xb_ = alloc<double>(nslots_, err, rc);
     d_yb_ = alloc<double>(nslots_, err, rc);
+    if (implicit_) {              // (subdomain, 32-block) list of the two L_bb passes and their b-space vector
+        std::vector<int2> lb;
+        for (int d = 0; d < nsub_; ++d)
+            for (int q = 0; q < hs_[d].nt; ++q) lb.push_back(make_int2(d, q));
+        nlblk_ = int(lb.size());
+        d_lblk_ = alloc<int2>(lb.size(), err, rc);
+        d_tb_ = alloc<double>(nslots_, err, rc);
+        if (!rc) CK(cudaMemcpyAsync(d_lblk_, lb.data(), lb.size() * sizeof(int2), cudaMemcpyHostToDevice, s_));
+    }
     d_t_ = alloc<double>(t_off, err, rc);
     d_gc_ = alloc<double>(ngc_total_, err, rc);
     d_s_ = alloc<double>(ngc_total_, err, rc);
@@ -401,6 +450,7 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     npart_ = cdiv(nlam_, 256);
     d_partial_ = alloc<double>(npart_, err, rc);
     d_st_ = alloc<PcpgState>(1, err, rc);
+    d_hist_ = alloc<double>(size_t(std::max(opt_.max_iter, 0)) + 1, err, rc);
     if (rc) return rc;
     {
         std::vector<int> csp(ncl_ + 1, 0), cs;
@@ -494,7 +544,8 @@ int Engine::factorize(Problem &p, std::string &err) {
     CK(cudaGetLastError());
     k_regularize<<<nsub_, 128, 0, s_>>>(d_subs_, nsub_, d_K_);
     CK(cudaGetLastError());
-    const bool dirichlet = opt_.preconditioner != "lumped";
+    // explicit Dirichlet: snapshot S_reg - D_fix as tiles; implicit: nothing (L_bb stays in the factor)
+    const bool dirichlet = opt_.preconditioner == "Dirichlet_explicit";
     int max_nt = 0, max_tiles = 0;
     for (auto &h : hs_) { max_nt = std::max(max_nt, h.nt); max_tiles = std::max(max_tiles, h.nt * (h.nt + 1) / 2); }
     if (!dirichlet) {          // lumped: K_bb before any elimination
@@ -752,6 +803,15 @@ int Engine::setup(Problem &p, std::string &err) {
     }
     lap(4);
     if (!rc) rc = coarse(p, err);
+    if (!rc) {
+        k_pack_M<<<nmt_, 256, 0, s_>>>(d_mt_, d_cl_, d_M_, d_MT_);
+        rc = check(cudaGetLastError(), "k_pack_M", err);
+        if (!rc) rc = check(cudaStreamSynchronize(s_), "sync", err);
+        if (!rc && !opt_.mixed) {
+            release(d_M_);
+            d_M_ = nullptr;
+        }
+    }
     lap(5);
     if (!rc) rc = outer_coarse(p, err);
     lap(6);
@@ -788,9 +848,7 @@ void Engine::op_F(const double *w, double *Fw, const double *dotv, double *parti
     k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, w, nullptr, d_xb_, st);
     k_symv_units<double><<<nunits_ + nsub_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, st);
     k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, st);
-    int maxg = 0;
-    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
-    k_coarse<<<dim3(ncl_, cdiv(maxg, 8)), 256, 0, s_>>>(d_cl_, d_M_, d_gc_, d_s_, st);
+    coarse_apply(d_gc_, d_s_, st);
     k_reduce_correct<<<dim3(nsub_, cdiv(max_nbp_, 256)), 256, 0, s_>>>(d_subs_, d_units_, d_ypart_, d_cl_, d_V_, d_bcr_,
                                                                        d_s_, d_yb_, st);
     k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, nullptr, Fw, dotv, partial, st);
@@ -798,6 +856,12 @@ void Engine::op_F(const double *w, double *Fw, const double *dotv, double *parti
 
 void Engine::op_M(const double *x, double *z, PcpgState *st) {
     k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, x, d_weight_, d_xb_, st);
+    if (implicit_) {
+        k_lbt_x<<<nlblk_, 128, 0, s_>>>(d_lblk_, d_subs_, d_K_, d_xb_, d_tb_, st);
+        k_lb_t<<<nlblk_, 128, 0, s_>>>(d_lblk_, d_subs_, d_K_, d_tb_, d_xb_, d_yb_, st);
+        k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, d_weight_, z, nullptr, nullptr, st);
+        return;
+    }
     k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_, st);
     k_reduce_correct<<<dim3(nsub_, cdiv(max_nbp_, 256)), 256, 0, s_>>>(d_subs_, d_units_, d_ypart_, d_cl_, d_V_, d_bcr_,
                                                                        nullptr, d_yb_, st);
@@ -819,7 +883,7 @@ void Engine::iteration(PcpgState *st) {
     op_M(d_Pg_, d_z_, st);
     op_P(d_z_, d_Pz_, nullptr, d_g_, d_partial_, st);
     k_update_w<<<std::min(npart_, 1184), 256, 0, s_>>>(nlam_, d_partial_, npart_, d_Pz_, d_w_, st);
-    k_finish_iter<<<1, 256, 0, s_>>>(d_partial_, npart_, st);
+    k_finish_iter<<<1, 256, 0, s_>>>(d_partial_, npart_, st, d_hist_);
 }
 
 int Engine::apply(int op, const double *x, double *y, int nrhs, std::string &err) {
@@ -841,8 +905,6 @@ int Engine::apply(int op, const double *x, double *y, int nrhs, std::string &err
 // with x_solved the triangular solves K_reg^{-1} f were done already (for
 // several load cases at once) and x_solved holds them
 void Engine::init_rhs(const double *f, const double *x_solved) {
-    int maxg = 0;
-    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
     const double *x = x_solved;
     if (!x) {
         cudaMemcpyAsync(d_full_, f, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_);
@@ -852,7 +914,7 @@ void Engine::init_rhs(const double *f, const double *x_solved) {
     }
     k_bc_rt<<<nsub_, 256, 0, s_>>>(d_subs_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_R_, x, f, d_t_);
     k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, nullptr);
-    k_coarse<<<dim3(ncl_, cdiv(maxg, 8)), 256, 0, s_>>>(d_cl_, d_M_, d_gc_, d_s_, nullptr);
+    coarse_apply(d_gc_, d_s_, nullptr);
     k_full_to_b<<<nsub_, 256, 0, s_>>>(d_subs_, x, d_yb_);
     k_correct<<<nsub_, 256, 0, s_>>>(d_subs_, d_cl_, d_V_, d_bcr_, d_s_, d_yb_, nullptr);
     k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, nullptr, d_d_, nullptr, nullptr, nullptr);
@@ -874,8 +936,6 @@ double Engine::pcpg_start(PcpgState *st) {
 
 // u = K_HT^+(f - Bf^T lambda) - Rf alpha  (Cluster.cpp:1648-1678)
 void Engine::reconstruct(const double *f, double *u_dev) {
-    int maxg = 0;
-    for (auto &c : hc_) maxg = std::max(maxg, c.ngc);
     cudaMemcpyAsync(d_full_, f, nfull_ * sizeof(double), cudaMemcpyDeviceToDevice, s_);
     k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, d_lam_, nullptr, d_xb_, nullptr);
     k_full_minus_b<<<nsub_, 256, 0, s_>>>(d_subs_, d_xb_, d_full_);
@@ -884,7 +944,7 @@ void Engine::reconstruct(const double *f, double *u_dev) {
     k_trsv_bwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full2_, 0);
     k_bc_rt<<<nsub_, 256, 0, s_>>>(d_subs_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_R_, d_full2_, d_full_, d_t_);
     k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, nullptr);
-    k_coarse<<<dim3(ncl_, cdiv(maxg, 8)), 256, 0, s_>>>(d_cl_, d_M_, d_gc_, d_s_, nullptr);
+    coarse_apply(d_gc_, d_s_, nullptr);
     k_sub_bct<<<nsub_, 32, 0, s_>>>(d_subs_, d_cl_, d_bcr_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_s_, d_full_);
     k_trsv_fwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full_, 0);
     k_trsv_bwd<<<dim3(nsub_, 1), 256, 0, s_>>>(d_subs_, d_K_, d_full_, 0);
@@ -934,12 +994,30 @@ int Engine::solve_one(Problem &p, int rhs, double *u_dev, int &iters, double &no
     iters = hst.it;
     norm0 = hst.norm0;
     rel = hst.rel;
+    if (rhs < 64) {                           // relative residual per iteration, for htf_residual_history
+        std::vector<double> h(size_t(std::min(hst.it, opt_.max_iter)) + 1, 1.0);
+        if (h.size() > 1)
+            CK(cudaMemcpy(h.data() + 1, d_hist_ + 1, (h.size() - 1) * sizeof(double), cudaMemcpyDeviceToHost));
+        if (int(hist_.size()) <= rhs) hist_.resize(rhs + 1);
+        hist_[rhs] = std::move(h);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     reconstruct(f, u_dev);
     CK(cudaGetLastError());
     if (hst.done == 2) { err = "PCPG breakdown (w'Fw <= 0 or non-finite)"; return HTF_EBREAKDOWN; }
     return HTF_OK;
+}
+
+int Engine::history(int rhs, double *out, int cap, std::string &err) const {
+    if (rhs < 0 || rhs >= int(hist_.size()) || hist_[rhs].empty()) {
+        err = "no residual history for load case " + std::to_string(rhs) +
+              " (the plain FP64 form records the first 64 load cases of the last solve)";
+        return HTF_EINVAL;
+    }
+    const int n = int(hist_[rhs].size());
+    if (out) std::copy(hist_[rhs].begin(), hist_[rhs].begin() + std::min(n, std::max(cap, 0)), out);
+    return n;
 }
 
 int Engine::ensure_rhs(int nrhs, std::string &err) {
@@ -1019,6 +1097,7 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
     for (int i = 0; i < 8; ++i) info->setup_phase_ms[i] = phase_ms[i];
     for (int b = 0; b < SYMV_BUCKETS && b < int(schedule_.size()); ++b) info->symv_unit_tiles[b] = schedule_[b];
     info->symv_tuned = tuned_ ? 1 : 0;
+    info->device_bytes = double(device_bytes());
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1040,10 +1119,19 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
         k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
     });
     info->symv_F_bytes = tri + vec;
-    info->symv_S_ms = timeit([&] {
-        k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
-    });
-    info->symv_S_bytes = tri + vec;
+    if (implicit_) {              // the two passes over L_bb (its triangle read twice)
+        info->symv_S_ms = timeit([&] {
+            k_lbt_x<<<nlblk_, 128, 0, s_>>>(d_lblk_, d_subs_, d_K_, d_xb_, d_tb_, nullptr);
+            k_lb_t<<<nlblk_, 128, 0, s_>>>(d_lblk_, d_subs_, d_K_, d_tb_, d_xb_, d_yb_, nullptr);
+        });
+        info->symv_S_bytes = 2.0 * tri + 2.0 * vec;
+    } else {
+        info->symv_S_ms = timeit([&] {
+            k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_,
+                                                                   nullptr);
+        });
+        info->symv_S_bytes = tri + vec;
+    }
     info->fapply_ms = timeit([&] { op_F(d_lam_, d_Fw_, nullptr, nullptr, nullptr); });
     info->fapply_bytes = fapply_bytes_;
     if (graph_) {

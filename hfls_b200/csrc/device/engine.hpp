@@ -41,6 +41,8 @@ public:
     int solve(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err);
     int profile(int reps, htf_profile_info *info, std::string &err);
     int project_noalloc(const double *x, double *Px, cudaStream_t stream, std::string &err);
+    // relative residuals per iteration of load case rhs of the last plain solve; returns their count
+    int history(int rhs, double *out, int cap, std::string &err) const;
     // batched mixed-precision form (engine_batch.cu)
     int setup_batch(int K, std::string &err);
     int solve_batch(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err);
@@ -108,6 +110,8 @@ private:
     void op_P(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial,
               PcpgState *st);
     void iteration(PcpgState *st);
+    void coarse_apply(const double *gc, double *s, const PcpgState *st);
+    void release(void *p);
     int solve_one(Problem &p, int rhs, double *u_dev, int &iters, double &norm0, double &rel,
                   double &solve_ms, std::string &err);
     int ensure_rhs(int nrhs, std::string &err);
@@ -126,6 +130,9 @@ private:
     std::vector<int> xwave_;             // subdomain boundaries of the L_bb^{-1} scratch waves
     long long xwave_max_ = 0;            // doubles of the largest wave
     double *d_V_ = nullptr, *d_R_ = nullptr, *d_M_ = nullptr, *d_H_ = nullptr;
+    double *d_MT_ = nullptr, *d_mP_ = nullptr, *d_mD_ = nullptr;   // packed symmetric M, its partial sums
+    int2 *d_mt_ = nullptr;                     // (cluster, tile row) pairs of M
+    int nmt_ = 0;
     int *d_bcr_ = nullptr, *d_bce_ptr_ = nullptr, *d_bce_pos_ = nullptr;
     double *d_bce_val_ = nullptr;
     int *d_slot_ptr_ = nullptr, *d_slot_ent_ = nullptr;
@@ -185,9 +192,15 @@ private:
     double *d_xb_ = nullptr, *d_yb_ = nullptr, *d_t_ = nullptr, *d_gc_ = nullptr, *d_s_ = nullptr;
     double *d_a_ = nullptr, *d_alpha_ = nullptr, *d_partial_ = nullptr, *d_gpart_ = nullptr;
     PcpgState *d_st_ = nullptr;
+    double *d_hist_ = nullptr;                 // relative residual per iteration of the running solve
+    std::vector<std::vector<double>> hist_;    // per load case (first 64) of the last plain solve
     int npart_ = 0;
     int symv_smem_ = 0;
     bool mixed_ = false;
+    bool implicit_ = false;                    // Dirichlet_implicit: S_d applied through L_bb, no S tiles
+    int2 *d_lblk_ = nullptr;                   // (subdomain, 32-block) pairs of the L_bb passes
+    int nlblk_ = 0;
+    double *d_tb_ = nullptr;                   // b-space L_bb^T x of the implicit preconditioner
     cudaGraphExec_t graph_ = nullptr;
     double fapply_ms_ = 0.0, fapply_bytes_ = 0.0;
     std::vector<std::vector<double>> Hd_;   // per subdomain 6x6 rows of ker(Gc)

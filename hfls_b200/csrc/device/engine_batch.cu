@@ -83,6 +83,10 @@ static inline int cdivb(long long a, long long b) { return int((a + b - 1) / b);
 
 int Engine::setup_batch(int K, std::string &err) {
     if (K != 16 && K != 32) { err = "batch width must be 16 or 32"; return HTF_EINVAL; }
+    if (implicit_) {
+        err = "precision=mixed needs the explicit preconditioner blocks (Dirichlet_explicit or lumped)";
+        return HTF_EINVAL;
+    }
     int rc = HTF_OK;
     for (auto &h : hs_)
         if ((h.c + 6) * K > 2048) {

@@ -417,8 +417,11 @@ __global__ void k_update_w(int n, const double *__restrict__ partial, int np, co
     // st->gPz is committed by k_finish_iter, launched after this kernel
 }
 
-// end of one iteration: commit gPz/gamma, count it, test convergence
-__global__ void k_finish_iter(const double *__restrict__ partial, int np, PcpgState *__restrict__ st) {
+// end of one iteration: commit gPz/gamma, count it, test convergence; the
+// relative residual sqrt(g'Pz)/sqrt(g0'Pz0) of iteration it goes to hist[it]
+// (hist holds max_iter + 1 entries)
+__global__ void k_finish_iter(const double *__restrict__ partial, int np, PcpgState *__restrict__ st,
+                              double *__restrict__ hist) {
     if (st->done) return;
     const double gPz = block_sum_fixed(partial, np);
     if (threadIdx.x == 0) {
@@ -427,6 +430,7 @@ __global__ void k_finish_iter(const double *__restrict__ partial, int np, PcpgSt
         st->gPz = gPz;
         st->it += 1;
         st->rel = sqrt(gPz) / st->norm0;
+        if (hist && st->it <= st->max_iter) hist[st->it] = st->rel;
         if (!(st->wFw > 0.0) || !isfinite(gPz)) st->done = 2;          // breakdown
         else if (sqrt(gPz) < st->eps * st->norm0) st->done = 1;        // converged
         else if (st->it >= st->max_iter) st->done = 3;                  // max_iter
@@ -453,6 +457,161 @@ __global__ void k_init_state(const double *__restrict__ partial, int np, PcpgSta
 // generic: y = a*x + b*y on n entries
 __global__ void k_axpby(int n, double a, const double *__restrict__ x, double b, double *__restrict__ y) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a * x[i] + b * y[i];
+}
+
+// ---------------------------------------------------------------------------
+// Dirichlet preconditioner without the dense S_d (preconditioner =
+// Dirichlet_implicit, the reference's Cluster.cpp:1082-1104 variant that
+// keeps no explicit S_d): the factor of K_reg,d eliminates the interior
+// first, so its trailing b-set columns hold L_bb with L_bb L_bb^T = S_reg =
+// S_d + D_fix (D_fix = the original diagonal at the 6 fix DOFs).  y_b =
+// S_d x_b = L_bb (L_bb^T x_b) - D_fix x_b, two passes over the b-set
+// column panels of the resident factor, no S_d stored.
+//   k_lbt_x: t = L_bb^T x_b, one CTA per (subdomain, 32-column block p):
+//            4 warps over the 32-row blocks R >= p, lane l row 32 R + l,
+//            32 column sums per lane, reduce-scatter, warps added in order;
+//   k_lb_t:  y = L_bb t - D_fix x_b, one CTA per (subdomain, 32-row block R):
+//            4 warps over the column blocks p <= R, warps added in order.
+// Each block of L_bb is read once per pass, 32 contiguous rows of a column
+// per warp load.  `blk` lists (subdomain, block) pairs.
+// ---------------------------------------------------------------------------
+__global__ void k_lbt_x(const int2 *__restrict__ blk, const SubDev *__restrict__ subs, const double *__restrict__ K,
+                        const double *__restrict__ xb, double *__restrict__ tb, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    __shared__ double part[4][32];
+    const int2 b = blk[blockIdx.x];
+    const SubDev sd = subs[b.x];
+    const int p = b.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cb = sd.nr + 32 * p;
+    double acc[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+    // the 32 columns are one factor panel: (r, cb + j) at pbase + j * ld + r
+    const double *pbase = K + kcol(sd, cb);
+    const long long ld = kld(sd, cb);
+    for (int R = p + warp; R < sd.nt; R += 4) {
+        const int r = sd.nr + 32 * R + lane;
+        const double xr = xb[sd.xb_off + 32 * R + lane];
+        const double *col = pbase + r;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const double l = (R > p || lane >= j) ? col[j * ld] : 0.0;
+            acc[j] += l * xr;
+        }
+    }
+    reduce_scatter32(acc, lane);
+    part[warp][lane] = acc[0];
+    __syncthreads();
+    if (warp == 0)
+        tb[sd.xb_off + 32 * p + lane] = ((part[0][lane] + part[1][lane]) + part[2][lane]) + part[3][lane];
+}
+
+__global__ void k_lb_t(const int2 *__restrict__ blk, const SubDev *__restrict__ subs, const double *__restrict__ K,
+                       const double *__restrict__ tb, const double *__restrict__ xb, double *__restrict__ yb,
+                       const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    __shared__ double part[4][32];
+    const int2 b = blk[blockIdx.x];
+    const SubDev sd = subs[b.x];
+    const int R = b.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = sd.nr + 32 * R + lane;
+    double z = 0.0;
+    for (int p = warp; p <= R; p += 4) {
+        const int cb = sd.nr + 32 * p;
+        const double tl = tb[sd.xb_off + 32 * p + lane];
+        const double *col = K + kcol(sd, cb) + r;      // (r, cb + j) at col + j * ld
+        const long long ld = kld(sd, cb);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const double tj = __shfl_sync(FULL, tl, j);
+            const double l = (p < R || lane >= j) ? col[j * ld] : 0.0;
+            z += l * tj;
+        }
+    }
+    part[warp][lane] = z;
+    __syncthreads();
+    if (warp == 0) {
+        double y = ((part[0][lane] + part[1][lane]) + part[2][lane]) + part[3][lane];
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+            if (sd.fix[k] == r) y -= sd.fix_diag[k] * xb[sd.xb_off + 32 * R + lane];
+        yb[sd.xb_off + 32 * R + lane] = y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Coarse solve s = M gc with the symmetric M stored once, as packed lower
+// 32x32 tiles (tile (I, J), J <= I, at MT_off + I (I + 1) / 2 + J, row-major
+// inside, diagonal tiles full): half the bytes of the dense M every F apply
+// reads.  `mt` lists (cluster, tile row) pairs.
+//   k_pack_M:      tiles of tile row I from the dense M (set-up);
+//   k_msym_rows:   CTA (cluster, I), 4 warps over the tiles of row I: the
+//                  direct product M_IJ x_J summed per warp then in warp
+//                  order into D[I]; the transposed M_IJ^T x_I (J < I) of each
+//                  tile into its own 32-value slot P[(I, J)];
+//   k_msym_reduce: s_J = D[J] + sum over I > J of P[(I, J)], in I order.
+// Every tile is read once and every sum has a fixed order.
+// ---------------------------------------------------------------------------
+__global__ void k_pack_M(const int2 *__restrict__ mt, const ClusterDev *__restrict__ cl,
+                         const double *__restrict__ M, double *__restrict__ T) {
+    const int2 b = mt[blockIdx.x];
+    const ClusterDev c = cl[b.x];
+    const int I = b.y;
+    double *row = T + (c.MT_off + (long long)I * (I + 1) / 2) * TILE_ELEMS;
+    for (int idx = threadIdx.x; idx < (I + 1) * TILE_ELEMS; idx += blockDim.x) {
+        const int J = idx / TILE_ELEMS, e = idx % TILE_ELEMS, r = e / TILE, j = e % TILE;
+        const int gr = TILE * I + r, gcn = TILE * J + j;
+        row[idx] = (gr < c.ngc && gcn < c.ngc) ? M[c.M_off + gr + (size_t)gcn * c.ngc] : 0.0;
+    }
+}
+
+__global__ void k_msym_rows(const int2 *__restrict__ mt, const ClusterDev *__restrict__ cl,
+                            const double *__restrict__ T, const double *__restrict__ gc, double *__restrict__ D,
+                            double *__restrict__ P, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    __shared__ double xI[TILE];
+    __shared__ double part[4][TILE];
+    const int2 b = mt[blockIdx.x];
+    const ClusterDev c = cl[b.x];
+    const int I = b.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const double *g = gc + c.gc_off;
+    if (threadIdx.x < TILE) xI[threadIdx.x] = (TILE * I + threadIdx.x < c.ngc) ? g[TILE * I + threadIdx.x] : 0.0;
+    __syncthreads();
+    const long long t0 = c.MT_off + (long long)I * (I + 1) / 2;
+    double dir = 0.0;
+    for (int J = warp; J <= I; J += 4) {
+        const double *tp = T + (t0 + J) * TILE_ELEMS;
+        double v[32];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) v[r] = tp[r * TILE + lane];
+        const double xJ = (TILE * J + lane < c.ngc) ? g[TILE * J + lane] : 0.0;
+        double p[32];
+        double col = 0.0;
+#pragma unroll
+        for (int r = 0; r < 32; ++r) {
+            p[r] = v[r] * xJ;
+            col += v[r] * xI[r];
+        }
+        reduce_scatter32(p, lane);
+        dir += p[0];
+        if (J < I) P[(t0 + J) * TILE + lane] = col;
+    }
+    part[warp][lane] = dir;
+    __syncthreads();
+    if (warp == 0)
+        D[((long long)c.mt_row_off + I) * TILE + lane] = ((part[0][lane] + part[1][lane]) + part[2][lane]) + part[3][lane];
+}
+
+__global__ void k_msym_reduce(const int2 *__restrict__ mt, const ClusterDev *__restrict__ cl,
+                              const double *__restrict__ D, const double *__restrict__ P, double *__restrict__ s,
+                              const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    const int2 b = mt[blockIdx.x];
+    const ClusterDev c = cl[b.x];
+    const int J = b.y, lane = threadIdx.x;
+    double y = D[((long long)c.mt_row_off + J) * TILE + lane];
+    for (int I = J + 1; I < c.mt; ++I) y += P[(c.MT_off + (long long)I * (I + 1) / 2 + J) * TILE + lane];
+    if (TILE * J + lane < c.ngc) s[c.gc_off + TILE * J + lane] = y;
 }
 
 }  // namespace htf

@@ -241,7 +241,10 @@ size_t Server::estimate(const Problem &p, int nrhs) const {
         nfull += N;
     }
     b += 8.0 * std::min(xs, double(1LL << 29));           // L_bb^{-1} scratch of the set-up (one wave)
-    for (const Cluster &c : p.clu) b += 8.0 * double(c.ngc()) * c.ngc();
+    for (const Cluster &c : p.clu) {          // dense M (batched coarse solves) + its packed tiles and partials
+        const double mt = std::ceil(c.ngc() / 32.0);
+        b += 8.0 * double(c.ngc()) * c.ngc() + 8.0 * mt * (mt + 1) / 2 * (1024.0 + 32.0) + 8.0 * 32.0 * mt;
+    }
     const double nl = p.n_lam;
     b += nl * 8.0 * (11.0 * K + 12.0) + nslots * (K * (8.0 * 2 + 4.0 * 2) + 8.0 * 4) + nfull * 8.0 * (nrhs + 3);
     b += 3.0 * p.mesh.n_nodes * 8.0 * 2 * nrhs;

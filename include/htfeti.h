@@ -190,6 +190,7 @@ typedef struct htf_profile_info {
      * autotuner (option autotune) or its cache                             */
     int symv_unit_tiles[5];
     int symv_tuned;
+    double device_bytes;                /* device memory the context holds          */
 } htf_profile_info;
 int htf_profile(htf_ctx *ctx, int reps, htf_profile_info *info);
 
@@ -218,6 +219,13 @@ int htf_preconditioning(htf_ctx *ctx, const double *x, double *Mx, int nrhs);
  * memory of the context's device.                                         */
 #define HTF_NOALLOC_SCRATCH_DOUBLES 1048576
 int htf_projection_noalloc(htf_ctx *ctx, const double *x_dev, double *Px_dev, void *stream);
+
+/* Relative residual sqrt(g'Pz)/sqrt(g0'Pz0) at every PCPG iteration of load
+ * case rhs (< 64) of the last plain FP64 htf_pcpg / htf_solve: hist[0] = 1,
+ * hist[i] after iteration i, as the reference prints them (Cluster.cpp:
+ * 1422-1424).  Copies at most cap values; returns their total count (or a
+ * negative code).                                                         */
+int htf_residual_history(htf_ctx *ctx, int rhs, double *hist, int cap);
 
 /* Dual layout for checking: n_lambda, and for every Bf row its entries as
  * (subdomain, global DOF, sign) with up to two entries per row

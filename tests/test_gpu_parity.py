@@ -40,8 +40,10 @@ SMALL = [
     (dict(subs=(2, 2, 2), elems=(3, 3, 3), jitter=0.1, seed=5), dict(typeBc="ker", preconditioner="lumped")),
     (dict(clusters=(2, 1, 1), subs=(2, 2, 2), elems=(3, 2, 3), jitter=0.1, seed=7,
           material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e4), dict(typeBc="cor", preconditioner="Dirichlet_explicit")),
+    (dict(clusters=(2, 1, 1), subs=(2, 2, 2), elems=(3, 3, 2), jitter=0.1, seed=8,
+          material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e3), dict(typeBc="cor", preconditioner="Dirichlet_implicit")),
 ]
-IDS = ["cor-dirichlet", "ker-lumped-jitter", "2clusters-cor-logE"]
+IDS = ["cor-dirichlet", "ker-lumped-jitter", "2clusters-cor-logE", "2clusters-cor-implicit"]
 
 
 @pytest.fixture(scope="module", params=list(range(len(SMALL))), ids=IDS)
@@ -125,3 +127,39 @@ def test_failed_setup_leaves_the_library_usable():
     m, s, o = make(spec, opts)
     u, st = s.pcpg()
     assert rel(u[0], o.pcpg()["u"]) < 1e-6
+
+
+def test_implicit_preconditioner_keeps_no_s_blocks():
+    """Dirichlet_implicit applies S_d through the resident factor's L_bb: the
+    same operator as the explicit blocks (1e-11), without their device
+    memory (at least the algorithmic bytes of the S_d triangles less)."""
+    spec = dict(subs=(2, 2, 2), elems=(5, 5, 5), jitter=0.1, seed=9)
+    m = hb.generate_mesh(hb.mesh_spec(**spec))
+    out = {}
+    for pre in ("Dirichlet_explicit", "Dirichlet_implicit"):
+        s = hb.Solver({"typeBc": "cor", "preconditioner": pre})
+        s.set_mesh(m)
+        s.setup()
+        rng = np.random.default_rng(3)
+        w = rng.standard_normal((1, s.n_lambda()))
+        out[pre] = (s.preconditioning(w)[0], s.profile(reps=2))
+        s.close()
+    (me, pe), (mi, pi) = out["Dirichlet_explicit"], out["Dirichlet_implicit"]
+    assert rel(mi, me) < 1e-11
+    assert pe.device_bytes - pi.device_bytes >= 0.99 * pe.symv_S_bytes
+
+
+def test_residual_history_is_the_stopping_record():
+    """htf_residual_history: hist[0] = 1, one value per iteration, the last
+    one below eps and all earlier ones not (the reference's criterion,
+    Cluster.cpp:1422-1426), equal to the solve's final_rel."""
+    spec, opts = SMALL[2]
+    m, s, o = make(spec, opts)
+    u, st = s.pcpg()
+    h = s.residual_history(0)
+    assert len(h) == st.iterations[0] + 1 and h[0] == 1.0
+    assert h[-1] < 1e-8 and np.all(h[:-1] >= 1e-8)
+    assert h[-1] == st.final_rel[0]
+    ref = o.pcpg()
+    n = min(len(h), len(ref["hist"]), 40)
+    assert np.max(np.abs(h[:n] - ref["hist"][:n]) / ref["hist"][:n]) < 1e-6
