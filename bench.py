@@ -87,7 +87,7 @@ def uneven_spec(hb, clusters=(2, 2, 2), subs=(8, 8, 8), widths=None):
 
 
 # reduced meshes of the same constructions, for ncu captures only
-REDUCED = {"uneven-small": dict(clusters=(1, 1, 1), subs=(8, 8, 8)),     # 512 subdomains, ~2.4 GB of FP64 tiles
+REDUCED = {"uneven-small": dict(clusters=(1, 1, 1), subs=(4, 4, 4)),     # 64 subdomains: FP64 tiles ~0.3 GB > L2
            "small": dict(clusters=(1, 1, 1), subs=(2, 4, 4)),            # cube: F_i tiles 120 MB
            "mid": dict(clusters=(2, 1, 1), subs=(2, 4, 4))}              # cube: F_i tiles 240 MB
 
