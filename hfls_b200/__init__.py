@@ -84,6 +84,7 @@ _SIGS = {
     "htf_dual_sizes": [ctypes.c_void_p, _ip, _ip, _ip],
     "htf_dual_layout": [ctypes.c_void_p, _ip, _ip, _dp, _dp],
     "htf_fix_dofs": [ctypes.c_void_p, _ip],
+    "htf_dump": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int],
     "htf_residual_history": [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_int],
     "htf_projection_noalloc": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "htf_server_create": [ctypes.c_char_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
@@ -301,6 +302,10 @@ class Solver:
         h = np.zeros(n)
         self._check(min(0, lib.htf_residual_history(self._h, rhs, _d(h), n)), "htf_residual_history")
         return h
+
+    def dump(self, folder, level):
+        """MatrixMarket files of the problem (htf_dump) in folder."""
+        self._check(lib.htf_dump(self._h, os.fsencode(folder), int(level)), "htf_dump")
 
     def fix_dofs(self):
         ns = self.mesh.n_sub

@@ -24,7 +24,8 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 CU_SOURCES = ["device/setup_kernels.cu", "device/pcpg_kernels.cu", "device/engine.cu", "device/noalloc.cu",
               "device/tc_gemm.cu", "device/pcpg_multi.cu", "device/engine_batch.cu", "device/coarse.cu",
               "device/autotune.cu"]
-CPP_SOURCES = ["host/mesh.cpp", "host/problem.cpp", "host/vtk.cpp", "capi.cpp", "server.cpp"]
+CPP_SOURCES = ["host/mesh.cpp", "host/problem.cpp", "host/vtk.cpp", "host/dump.cpp", "capi.cpp", "server.cpp",
+               "cxx/surface.cpp"]
 HEADERS = ["device/device.cuh", "device/engine.hpp", "host/problem.hpp"]
 
 INC = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
@@ -38,6 +39,7 @@ def _stale(obj, src):
         return True
     t = os.path.getmtime(obj)
     deps = [src] + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "htfeti.h")]
+    deps += [os.path.join(ROOT, "include", "hfls", h) for h in os.listdir(os.path.join(ROOT, "include", "hfls"))]
     return any(os.path.getmtime(d) > t for d in deps)
 
 

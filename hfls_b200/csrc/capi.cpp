@@ -201,6 +201,13 @@ int htf_residual_history(htf_ctx *ctx, int rhs, double *hist, int cap) {
     return ctx->eng->history(rhs, hist, cap, ctx->err);
 }
 
+int htf_dump(htf_ctx *ctx, const char *folder, int level) {
+    if (!ctx) return HTF_EINVAL;
+    if (!ctx->is_setup) return fail(ctx, HTF_ESTATE, "htf_dump before htf_setup");
+    if (!folder) return fail(ctx, HTF_EINVAL, "htf_dump: null folder");
+    return ctx->eng->dump(ctx->p, folder, level, ctx->err);
+}
+
 int htf_dual_sizes(htf_ctx *ctx, int *n_lambda, int *n_sub, int *n_clusters) {
     if (!ctx) return HTF_EINVAL;
     if (ctx->p.rows.empty()) {

@@ -304,6 +304,7 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     d_cl_ = alloc<ClusterDev>(ncl_, err, rc);
     d_all_subs_ = alloc<int>(nsub_, err, rc);
     d_K_ = alloc<double>(K_off, err, rc);
+    kpanel_total_ = K_off;
     d_F_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);
     implicit_ = opt_.preconditioner == "Dirichlet_implicit";
     if (!implicit_) d_S_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);   // implicit: S applied through L_bb
@@ -544,6 +545,11 @@ int Engine::factorize(Problem &p, std::string &err) {
     CK(cudaGetLastError());
     k_regularize<<<nsub_, 128, 0, s_>>>(d_subs_, nsub_, d_K_);
     CK(cudaGetLastError());
+    if (opt_.print_matrices >= 2) {               // K_reg panels before the factorisation, for htf_dump
+        dumpK_.assign(size_t(kpanel_total_), 0.0);
+        CK(cudaMemcpyAsync(dumpK_.data(), d_K_, dumpK_.size() * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        CK(cudaStreamSynchronize(s_));
+    }
     // explicit Dirichlet: snapshot S_reg - D_fix as tiles; implicit: nothing (L_bb stays in the factor)
     const bool dirichlet = opt_.preconditioner == "Dirichlet_explicit";
     int max_nt = 0, max_tiles = 0;
@@ -689,6 +695,11 @@ int Engine::outer_coarse(Problem &p, std::string &err) {
                         GtG[(6 * c1 + a) + size_t(6 * c2 + b) * m] +=
                             gval[6 * (2 * (size_t)r + k1) + a] * gval[6 * (2 * (size_t)r + k2) + b];
             }
+    if (opt_.print_matrices >= 2) {               // for htf_dump
+        gtg_ = GtG;
+        gcl_ = gcl;
+        gval_ = gval;
+    }
     std::vector<double> L(GtG);
     if (!chol_lower(m, L.data(), m)) { err = "Gf^T Gf is not positive definite"; return HTF_ENOTSPD; }
     invGtG_.assign(size_t(m) * m, 0.0);

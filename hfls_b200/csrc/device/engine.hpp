@@ -41,6 +41,8 @@ public:
     int solve(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err);
     int profile(int reps, htf_profile_info *info, std::string &err);
     int project_noalloc(const double *x, double *Px, cudaStream_t stream, std::string &err);
+    // MatrixMarket files of the problem's matrices (dump.cpp)
+    int dump(const Problem &p, const std::string &folder, int level, std::string &err);
     // relative residuals per iteration of load case rhs of the last plain solve; returns their count
     int history(int rhs, double *out, int cap, std::string &err) const;
     // batched mixed-precision form (engine_batch.cu)
@@ -204,6 +206,10 @@ private:
     cudaGraphExec_t graph_ = nullptr;
     double fapply_ms_ = 0.0, fapply_bytes_ = 0.0;
     std::vector<std::vector<double>> Hd_;   // per subdomain 6x6 rows of ker(Gc)
+    long long kpanel_total_ = 0;            // doubles of all factor panels
+    std::vector<double> dumpK_;             // K_reg panels before the factorisation (print_matrices >= 2)
+    std::vector<double> gtg_, gval_;        // Gf^T Gf and the Gf rows (print_matrices >= 2)
+    std::vector<int> gcl_;
     std::vector<double> invGtG_;
 };
 

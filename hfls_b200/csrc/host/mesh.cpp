@@ -227,6 +227,7 @@ int parse_options(const char *s, Options &o, std::string &err) {
             }
         }
         else if (k == "max_iter") o.max_iter = std::atoi(v.c_str());
+        else if (k == "print_matrices") o.print_matrices = std::atoi(v.c_str());
         else if (k == "precision") {
             if (v != "fp64" && v != "mixed") { err = "precision must be fp64|mixed"; return HTF_EINVAL; }
             o.mixed = (v == "mixed");
@@ -242,7 +243,7 @@ int parse_options(const char *s, Options &o, std::string &err) {
         // reference keys without effect on this path (kept for drop-in option maps)
         else if (k == "vtkWithinIter" || k == "metis" || k == "Ac_clust_explicit" || k == "path2data" ||
                  k == "young_modulus" || k == "ratio_mat" || k == "poissons_ratio" || k == "linear_solver" ||
-                 k == "print_matrices" || k == "Ac_extended_by_kerGc" || k == "GcTGc_assembl_block_by_block" ||
+                 k == "Ac_extended_by_kerGc" || k == "GcTGc_assembl_block_by_block" ||
                  k == "Bc_fullRank" || k == "create_analytic_ker_K" || k == "Nx" || k == "Ny" || k == "Nz" ||
                  k == "nx" || k == "ny" || k == "nz" || k == "nparts") {
         } else {

@@ -57,6 +57,8 @@ struct Options {
     int check_every = 8;                              // iterations between host convergence checks
     int batch = 32;                                   // load cases per batched mixed-precision solve (16 | 32)
     int verbose = 0;                                  // progress lines on stderr
+    int print_matrices = 0;                           // the reference's dump level (Cluster.cpp:31): >= 2 keeps
+                                                      // K_i for htf_dump (MatrixMarket files)
     int autotune = 1;                                 // time SYMV work-unit sizes at setup (once per process and
                                                       // problem class) for problems of >= 1 GiB of FP64 tiles;
                                                       // 2 = every problem; 0 = fixed default schedule

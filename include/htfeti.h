@@ -227,6 +227,17 @@ int htf_projection_noalloc(htf_ctx *ctx, const double *x_dev, double *Px_dev, vo
  * negative code).                                                         */
 int htf_residual_history(htf_ctx *ctx, int rhs, double *hist, int cap);
 
+/* MatrixMarket files of the set-up problem, written as the reference's
+ * Matrix::printToFile writes them (Matrix.cpp:556-632; names
+ * <folder>/dump_<name>_<index>.txt, 1-based coordinates, "%.16e" values) at
+ * the reference's print_matrices levels (Cluster.cpp:118-358): level >= 2
+ * K_i (upper triangle, symmetric), rhs_i (the element load), Bc_i, Bf_i;
+ * >= 3 also R_i, Rf_i, Gf_clust, GfTGf, iGfTGf; >= 4 also S_i (explicit
+ * Dirichlet preconditioner).  K_i needs the option print_matrices >= 2 at
+ * htf_create (the set-up keeps a host copy before factorising; HTF_ESTATE
+ * otherwise).  HTF_EIO if a file cannot be written.                       */
+int htf_dump(htf_ctx *ctx, const char *folder, int level);
+
 /* Dual layout for checking: n_lambda, and for every Bf row its entries as
  * (subdomain, global DOF, sign) with up to two entries per row
  * (Cluster.cpp:846-924); weights (Cluster.cpp:893-895, 918).  Arrays of

@@ -1,0 +1,54 @@
+"""htf_dump: the set-up problem's matrices as the reference's MatrixMarket
+dump files (Matrix::printToFile, Matrix.cpp:556-632), read back with
+scipy.io.mmread and compared with the oracle's: K_i, rhs_i, Bf_i, R_i, S_i
+(explicit Dirichlet) and GfTGf, for every subdomain."""
+import os
+
+import numpy as np
+import pytest
+import scipy.io
+
+import hfls_b200 as hb
+from oracle.htfeti_oracle import HTFETI, MeshArrays, Options
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_dump_matches_oracle_matrices(tmp_path):
+    spec = hb.mesh_spec(clusters=(2, 1, 1), subs=(2, 1, 2), elems=(3, 2, 3), jitter=0.1, seed=4,
+                        material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e2)
+    m = hb.generate_mesh(spec)
+    s = hb.Solver({"typeBc": "cor", "preconditioner": "Dirichlet_explicit", "print_matrices": "4"})
+    s.set_mesh(m)
+    s.setup()
+    s.dump(str(tmp_path), 4)
+    o = HTFETI(MeshArrays(m.coords, m.elems.astype(np.int64), m.elem_sub.astype(np.int64),
+                          m.sub_cluster.astype(np.int64), m.sub_E, m.sub_nu, m.dirichlet.astype(np.int64),
+                          m.corner.astype(np.int64), m.body_force),
+               Options(typeBc="cor", fix_rule="boundary", kerGc="analytic"))
+    read = lambda name, d: scipy.io.mmread(os.path.join(tmp_path, f"dump_{name}_{d}.txt"))
+    with open(os.path.join(tmp_path, "dump_K_0.txt")) as f:
+        assert f.readline().startswith("%%MatrixMarket matrix coordinate real symmetric")
+    for d in range(m.n_sub):
+        assert rel(read("K", d).toarray(), o.K[d]) < 1e-13
+        assert rel(read("rhs", d).toarray()[:, 0], o.f[d][:, 0]) < 1e-13
+        Bf = read("Bf", d).toarray()
+        ref = np.zeros_like(Bf)
+        ref[o.bf_l2g[d][o.bf_rowloc[d]], o.bf_col[d]] = o.bf_val[d]
+        assert np.array_equal(Bf, ref)
+        assert rel(read("R", d).toarray(), o.R[d]) < 1e-13
+        assert rel(read("S", d).toarray(), o.S[d]) < 1e-11
+    assert rel(scipy.io.mmread(os.path.join(tmp_path, "dump_GfTGf_0.txt")).toarray(), o.GfTGf) < 1e-12
+
+
+def test_dump_needs_the_option_at_setup(tmp_path):
+    s = hb.Solver({"typeBc": "cor"})
+    s.set_mesh(hb.generate_mesh(hb.mesh_spec(subs=(2, 1, 1), elems=(2, 2, 2))))
+    s.setup()
+    with pytest.raises(hb.HTFError) as e:
+        s.dump(str(tmp_path), 2)
+    assert e.value.code == hb.HTF_ESTATE
