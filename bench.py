@@ -438,9 +438,10 @@ def pct(v, q):
     return float(np.percentile(np.asarray(v), q)) if len(v) else None
 
 
-def run_serving(hb, local, n_req):
+def run_serving(hb, local, n_req, fp64_requests=None):
     """Continuous-batching server on a bounded prefix of the serving stream,
-    then the plain FP64 per-request path on the same requests."""
+    then the plain FP64 per-request path on the first fp64_requests served
+    requests (all by default), FIFO on their own arrival times."""
     import torch
     free, _ = torch.cuda.mem_get_info(local)
     budget = 0.85 * free
@@ -480,7 +481,8 @@ def run_serving(hb, local, n_req):
     makespan = (max(x[3] for x in ok) - min(x[2] for x in ok)) / 1e3 if ok else None
     # plain FP64 per-request path: service time of each served request, FIFO on the same arrivals
     service, err = [], 0.0
-    for (i, u, *_) in ok:
+    ok64 = ok if fp64_requests is None else ok[:fp64_requests]
+    for (i, u, *_) in ok64:
         ta, spec, k, _, _ = stream[i]
         t = time.perf_counter()
         s = hb.Solver(dict(OPTS, device=str(local), max_iter="5000"))
@@ -491,11 +493,12 @@ def run_serving(hb, local, n_req):
         service.append(time.perf_counter() - t)
         err = max(err, max(float(np.linalg.norm(u[j] - u64[j]) / np.linalg.norm(u64[j])) for j in range(k)))
     fin, lat64 = 0.0, []
-    for (i, *_), sv in zip(ok, service):
+    for (i, *_), sv in zip(ok64, service):
         ta = stream[i][0]
         fin = max(fin, ta) + sv
         lat64.append(1e3 * (fin - ta))
-    first = stream[ok[0][0]][0] if ok else 0.0
+    first = stream[ok64[0][0]][0] if ok64 else 0.0
+    cases64 = sum(stream[x[0]][2] for x in ok64)
     return {
         "workload": SERVE_WORKLOAD, "requests": n_req, "served": len(ok),
         "rejected_oversize": sum(1 for x in served if x[1] is None and x[4] == hb.HTF_ENOMEM),
@@ -504,8 +507,8 @@ def run_serving(hb, local, n_req):
         "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "mean_ms": float(np.mean(lat)) if lat else None,
         "solves_per_s": cases / makespan if makespan else None,
         "requests_per_s": len(ok) / makespan if makespan else None,
-        "fp64_per_request": {"p50_ms": pct(lat64, 50), "p99_ms": pct(lat64, 99),
-                             "solves_per_s": cases / (fin - first) if ok else None,
+        "fp64_per_request": {"requests": len(ok64), "p50_ms": pct(lat64, 50), "p99_ms": pct(lat64, 99),
+                             "solves_per_s": cases64 / (fin - first) if ok64 else None,
                              "service_s": [round(x, 3) for x in service]},
         "u_rel_err_max_vs_fp64": err,
         "sizes": [dict(c=x[4][0], s=x[4][1], e=x[4][2], load_cases=x[2]) for x in stream],
@@ -525,6 +528,10 @@ def main():
     ap.add_argument("--no-cube", action="store_true", help="skip the 512-subdomain cube measurement")
     ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS,
                     help="requests of the seeded serving stream to serve (0 skips the serving measurement)")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="only the serving measurement (its own JSON line); the plain FP64 comparison runs on the "
+                         "first --serve-fp64 served requests")
+    ap.add_argument("--serve-fp64", type=int, default=None)
     ap.add_argument("--workload", default="full", choices=["full"] + sorted(REDUCED),
                     help="reduced meshes of the same constructions, for ncu captures only: uneven-small is one "
                          "cluster of the uneven cube; small / mid are one / two clusters of 2x4x4 cube subdomains "
@@ -536,6 +543,13 @@ def main():
 
     rank, world, local, dist = dist_setup(args.gpus)
     import hfls_b200 as hb
+    if args.serve_only:
+        out = run_serving(hb, local, args.serve_requests, args.serve_fp64)
+        if rank == 0:
+            print(json.dumps({"serving": out}))
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
     reduced = REDUCED.get(args.workload)
     if args.workload in ("small", "mid"):
         spec = hb.mesh_spec(material=hb.HTF_MAT_LOGUNIFORM, bc=hb.HTF_BC_CLAMP_X0, **dict(CUBE, **reduced))
