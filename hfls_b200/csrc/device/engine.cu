@@ -554,7 +554,12 @@ int Engine::factorize(Problem &p, std::string &err) {
     const bool dirichlet = opt_.preconditioner == "Dirichlet_explicit";
     int max_nt = 0, max_tiles = 0;
     for (auto &h : hs_) { max_nt = std::max(max_nt, h.nt); max_tiles = std::max(max_tiles, h.nt * (h.nt + 1) / 2); }
-    if (!dirichlet) {          // lumped: K_bb before any elimination
+    const bool lumped = opt_.preconditioner == "lumped";
+    if ((dirichlet || lumped) && !d_S_) {
+        err = "preconditioner blocks were not allocated";
+        return HTF_EINVAL;
+    }
+    if (lumped) {              // lumped: K_bb before any elimination
         k_snapshot<<<dim3(nsub_, max_tiles), 256, 0, s_>>>(d_all_subs_, d_subs_, d_K_, d_S_);
         CK(cudaGetLastError());
     }

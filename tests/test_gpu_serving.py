@@ -111,3 +111,28 @@ def test_admission_by_budget_and_oversize_request():
     u1, _ = srv.wait(srv.submit(spec, f))
     srv.close()
     assert rel(u1, u0) < 1e-12
+
+
+def test_largest_request_of_a_mix_against_tight_fp64():
+    """The largest request of a served mix (4x3x3 clusters of 2x2x2
+    subdomains of 5^3 hex8, E contrast 1e4, 4 load cases) against the plain
+    FP64 form solved to eps 1e-11: within the mixed form's 1e-7 bound (the
+    served form stops at eps_iter x mixed_eps_factor = 1e-9)."""
+    big = dict(clusters=(4, 3, 3), subs=(2, 2, 2), elems=(5, 5, 5), jitter=0.1, seed=11,
+               material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e4, nu=0.3)
+    spec = hb.mesh_spec(**big)
+    f = hb.traction(spec, seed=77, n_rhs=4)
+    srv = hb.Server(OPTS, max_live=8)
+    small = [srv.submit(*spec_and_loads(i)) for i in range(2)]
+    t = srv.submit(spec, f)
+    u, info = srv.wait(t)
+    for x in small:
+        srv.wait(x)
+    srv.close()
+    s = hb.Solver(dict(OPTS, precision="fp64", eps_iter="1e-11", max_iter="6000"))
+    s.set_mesh(hb.generate_mesh(spec))
+    s.setup()
+    u64, _ = s.solve(f)
+    s.close()
+    for k in range(4):
+        assert rel(u[k], u64[k]) < 1e-7, k
