@@ -1177,14 +1177,13 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
         CK(cudaMemsetAsync(b_s_, 0, (size_t)ngc_total_ * K * sizeof(double), s_));
         profile_batch_gather(b_tmp_);
         info->tc_F_ms = timeit([&] { tc_apply(0); });
-        // algorithmic bytes of one launch (the F apply's per-subdomain terms for k
-        // load cases): the FP32 triangle n_b (n_b + 1) / 2, the coupling columns
-        // V = [F Bc_b^T, -R_b] (FP64, n_b (c + 6)), X_hi + X_lo in (FP32) and Y out
-        // (FP64) per load case; padding rows and the diagonal blocks' upper halves
-        // the kernel also reads are not counted
+        // algorithmic bytes of one launch (the product's per-subdomain terms for k
+        // load cases): the FP32 triangle n_b (n_b + 1) / 2, X_hi + X_lo in (FP32)
+        // and Y out (FP64) per load case; padding rows and the diagonal blocks'
+        // upper halves the kernel also reads are not counted (the coarse
+        // correction runs in its own kernel after it)
         double bytes = 0.0;
-        for (auto &h : hs_)
-            bytes += 4.0 * h.nb * (h.nb + 1.0) / 2.0 + 8.0 * h.nb * (h.c + 6) + (4.0 + 4.0 + 8.0) * h.nb * K;
+        for (auto &h : hs_) bytes += 4.0 * h.nb * (h.nb + 1.0) / 2.0 + (4.0 + 4.0 + 8.0) * h.nb * K;
         info->tc_F_bytes = bytes;
         if (bgraph_) {
             std::vector<PcpgState> st(K), saved(K);

@@ -35,6 +35,9 @@ __global__ void k_vt_multi(int, const SubDev *, const double *, const double *, 
 __global__ void k_gc_multi(int, int, int, const int *, const int *, const double *, double *);
 template <int K>
 __global__ void k_coarse_multi(const ClusterDev *, const double *, const double *, double *);
+template <int K>
+__global__ void k_correct_multi(const SubDev *, const ClusterDev *, const double *, const int *, const double *,
+                                double *);
 __global__ void k_rows_multi(int, int, const int *, const double *, const double *, const double *, double *,
                              const double *, double *);
 __global__ void k_gft_partial_multi(int, const int *, const int *, const int *, const double *, const double *,
@@ -189,8 +192,10 @@ int Engine::setup_batch(int K, std::string &err) {
     return HTF_OK;
 }
 
+// the coarse correction of the F product runs after it (k_correct_multi in
+// f_post), so the product's epilogue gets no coarse solution
 TcSet Engine::tc_set() const {
-    return TcSet{d_AF_, d_AS_, d_Xs_, (long long)nslots_ * bK_, b_yb_, d_subs_, d_cl_, d_V_, d_bcr_, b_s_};
+    return TcSet{d_AF_, d_AS_, d_Xs_, (long long)nslots_ * bK_, b_yb_, d_subs_, d_cl_, d_V_, d_bcr_, nullptr};
 }
 
 // X slabs of a batch vector (for timing the tensor-core product alone)
@@ -248,6 +253,9 @@ void Engine::coarse_batch() {
 }
 
 void Engine::f_post(double *Fw, const double *dotv, double *partial) {
+    const dim3 gc(nsub_, cdivb(max_nbp_, 128));
+    if (bK_ == 32) k_correct_multi<32><<<gc, 256, 0, s_>>>(d_subs_, d_cl_, d_V_, d_bcr_, b_s_, b_yb_);
+    else k_correct_multi<16><<<gc, 256, 0, s_>>>(d_subs_, d_cl_, d_V_, d_bcr_, b_s_, b_yb_);
     k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, bK_, d_rslot_, d_rsign_, b_yb_, nullptr, Fw, dotv, partial);
 }
 

@@ -260,6 +260,49 @@ __device__ __forceinline__ double row_value(int r, int K, int j, const int *__re
     return v;
 }
 
+// y_b -= V_d s_d for all K load cases of a batch vector: the coarse
+// correction of the F apply (Cluster.cpp:1114-1188, y = F_d x_b - V_d s_d
+// with V_d = [F_d Bc_d^T, -R_d], s_d the cluster coarse solution at the
+// subdomain's Bc rows and alpha slot), after the tensor-core product so the
+// product's CTAs end without an FP64 epilogue.  CTA (subdomain, 128-row
+// chunk): s_d staged in shared memory ((c + 6) K <= 2048 doubles, checked at
+// set-up); lane j of a warp is load case j of a row (two rows per warp for
+// K = 16), so the row's y is read and written coalesced and V is a broadcast.
+template <int K>
+__global__ void __launch_bounds__(256) k_correct_multi(const SubDev *__restrict__ subs,
+                                                       const ClusterDev *__restrict__ cl,
+                                                       const double *__restrict__ V, const int *__restrict__ bcr,
+                                                       const double *__restrict__ s, double *__restrict__ yb) {
+    __shared__ double ss[2048];
+    const SubDev &sd = subs[blockIdx.x];
+    const int r0 = blockIdx.y * 128;
+    if (r0 >= sd.nb) return;
+    const int nc = sd.c + 6;
+    const int gc_off = cl[sd.cluster].gc_off;
+    for (int o = threadIdx.x; o < nc * K; o += blockDim.x) {
+        const int q = o / K, j = o % K;
+        const int pos = q < sd.c ? bcr[sd.bcr_off + q] : sd.alpha_pos + (q - sd.c);
+        ss[o] = s[((size_t)gc_off + pos) * K + j];
+    }
+    __syncthreads();
+    constexpr int RPW = 32 / K;                       // rows per warp step
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sub = lane / K, j = lane % K;
+    const int rend = min(128, sd.nb - r0);
+    for (int rr = warp * RPW + sub; rr < rend; rr += 8 * RPW) {
+        const int row = r0 + rr;
+        const double *Vr = V + sd.V_off + row;
+        double a = 0.0;
+        for (int q = 0; q < nc; ++q) a += Vr[(size_t)q * sd.nbp] * ss[q * K + j];
+        yb[((size_t)sd.xb_off + row) * K + j] -= a;
+    }
+}
+
+template __global__ void k_correct_multi<16>(const SubDev *, const ClusterDev *, const double *, const int *,
+                                             const double *, double *);
+template __global__ void k_correct_multi<32>(const SubDev *, const ClusterDev *, const double *, const int *,
+                                             const double *, double *);
+
 __global__ void k_rows_multi(int nlam, int K, const int *__restrict__ rslot, const double *__restrict__ rsign,
                              const double *__restrict__ yb, const double *__restrict__ weight,
                              double *__restrict__ out, const double *__restrict__ dotv,
