@@ -3,18 +3,21 @@ tests/golden/make_large_goldens.py: the oracle solves the same seeded mesh
 on the host, iteration counts at eps 1e-8 and displacements at eps 1e-11).
 
   cube1:  2x2x2 clusters x 4x4x4 subdomains x 8^3 hex8 (823 875 DOFs), one
-          N(0,1) traction load case, plain FP64 form: PCPG iterations within
-          +-2 of the oracle's at eps 1e-8, displacements at eps 1e-10 within
+          N(0,1) traction load case, plain FP64 form: the residual history
+          equal to the oracle's to 1e-9 over the first 20 iterations, the
+          stopping iteration at eps 1e-8 on the oracle's plateau (same_stop:
+          the oracle stops at 627 with its residual between 0.92 and 1.18 x
+          eps from iteration 620 to 635), displacements at eps 1e-10 within
           1e-8 of the oracle's;
   cube32: the same mesh, body force + 32 traction load cases: the batched
           mixed-precision form's displacements within 1e-7 of the oracle's
-          for every load case, and the plain FP64 form's iteration counts on
-          four of them within +-2."""
+          for every load case, and the plain FP64 form's stopping iterations
+          on four of them on the oracle's plateau (same_stop)."""
 import numpy as np
 import pytest
 
 import hfls_b200 as hb
-from tests.golden_util import golden_rel_err, oracle_golden
+from tests.golden_util import golden_rel_err, oracle_golden, same_stop
 
 pytestmark = pytest.mark.gpu
 
@@ -37,8 +40,12 @@ def test_cube1_fp64_matches_oracle():
     f = hb.traction(spec, seed=2, n_rhs=1)
     s = solver(spec, f, eps_iter="1e-8")
     _, st = s.pcpg()
+    h = s.residual_history(0)
     s.close()
-    assert abs(st.iterations[0] - int(g["iterations"][0])) <= 2
+    ho = g["hist"][:, 0]
+    # the same arithmetic up to round-off for the first iterations, the same plateau at the stop
+    assert np.max(np.abs(h[:20] - ho[:20]) / ho[:20]) < 1e-9
+    assert same_stop(st.iterations[0], h, int(g["iterations"][0]), ho, 1e-8)
     s = solver(spec, f, eps_iter="1e-10")
     u, st = s.pcpg()
     s.close()
@@ -60,6 +67,5 @@ def test_cube32_mixed_and_fp64_match_oracle():
     s.set_mesh(hb.generate_mesh(spec))
     s.setup()
     _, st = s.solve(f[pick])
-    s.close()
     for i, k in enumerate(pick):
-        assert abs(st.iterations[i] - int(g["iterations"][k])) <= 2
+        assert same_stop(st.iterations[i], s.residual_history(i), int(g["iterations"][k]), g["hist"][:, k], 1e-8)
