@@ -139,7 +139,7 @@ int Engine::setup_batch(int K, std::string &err) {
     k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_F_, d_AF_);
     k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_S_, d_AS_);
     CKB(cudaGetLastError());
-    // TC_STAGES stages of A (16 KB), X_hi, X_lo (k x 128 B each), TC_LO A_lo buffers (16 KB each) + alignment slack
+    // TC_STAGES stages of A (16 KB), X_hi, X_lo (k x 128 B each) + alignment slack (A_lo lives in TMEM)
     tc_smem_ = tc_smem_bytes(K);
     if (K == 16)
         CKB(cudaFuncSetAttribute(k_tc_gemm<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_));
@@ -215,7 +215,7 @@ int tc_launch(int K, const GemmBlock *blocks, int nblocks, const TcSet *sets, in
     return 0;
 }
 
-int tc_smem_bytes(int K) { return 1024 + (TC_STAGES * (128 * 32 + 2 * K * 32) + TC_LO * 128 * 32) * 4; }
+int tc_smem_bytes(int K) { return 1024 + TC_STAGES * (128 * 32 + 2 * K * 32) * 4; }
 
 void Engine::tc_apply(int which) {
     tc_launch(bK_, static_cast<const GemmBlock *>(d_blocks_), nblocks_, d_tcset_, which, tc_smem_, d_tcerr_, s_);

@@ -98,30 +98,63 @@ __device__ __forceinline__ uint32_t tf32_idesc(int M, int N) {
            | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);   // A, B K-major
 }
 
+// A_lo = rna_tf32(a - trunc_tf32(a)) of one row of 32 values into 32
+// consecutive TMEM columns of this thread's lane (taddr: the warp's lane
+// quarter and the first column), where the MMA reads it as its A operand.
+__device__ __forceinline__ void store_lo_row(const float (&v)[32], uint32_t taddr) {
+    uint32_t r[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) r[j] = __float_as_uint(tf32_rna(v[j] - tf32_trunc(v[j])));
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+        "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]),
+        "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]),
+        "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// A stored slab: this thread's row (its TMEM lane) of the SWIZZLE_128B slab
+// at a, A_lo of it into TMEM.  Out of line so its live values do not compete
+// with the epilogue's registers.
+__device__ __noinline__ void split_direct(const float *a, int row, uint32_t taddr) {
+    float v[32];
+#pragma unroll
+    for (int g4 = 0; g4 < 8; ++g4) {
+        const float4 h = *reinterpret_cast<const float4 *>(a + row * 32 + ((g4 ^ (row & 7)) * 4));
+        v[4 * g4] = h.x; v[4 * g4 + 1] = h.y; v[4 * g4 + 2] = h.z; v[4 * g4 + 3] = h.w;
+    }
+    store_lo_row(v, taddr);
+}
+
 // One warp's 4 KB of a transposed K step: pa holds 32 rows x 32 columns of
 // a stored slab (SWIZZLE_128B rows), whose column `lane` becomes row `lane`
-// of the same 4 KB in the K-major slab the MMA reads; its A_lo row goes to
-// the same place in lo.  Kept out of line so its 32 live values do not
-// compete with the epilogue's registers.
-__device__ __noinline__ void split_transposed(float *pa, float *lo, int lane) {
+// of the same 4 KB in the K-major slab the MMA reads (A_hi, in place); the
+// row's A_lo goes to TMEM.
+__device__ __noinline__ void split_transposed(float *pa, int lane, uint32_t taddr) {
     float v[32];
 #pragma unroll
     for (int j = 0; j < 32; ++j) v[j] = pa[j * 32 + (lane ^ ((j & 7) << 2))];
     __syncwarp();
     float *hrow = pa + lane * 32;
-    float *lrow = lo + lane * 32;
 #pragma unroll
     for (int g4 = 0; g4 < 8; ++g4) {
         const int ph = (g4 ^ (lane & 7)) * 4;     // SWIZZLE_128B position of granule g4 in this row
-        const float4 h = make_float4(v[4 * g4], v[4 * g4 + 1], v[4 * g4 + 2], v[4 * g4 + 3]);
-        float4 l;
-        l.x = tf32_rna(h.x - tf32_trunc(h.x));
-        l.y = tf32_rna(h.y - tf32_trunc(h.y));
-        l.z = tf32_rna(h.z - tf32_trunc(h.z));
-        l.w = tf32_rna(h.w - tf32_trunc(h.w));
-        *reinterpret_cast<float4 *>(hrow + ph) = h;
-        *reinterpret_cast<float4 *>(lrow + ph) = l;
+        *reinterpret_cast<float4 *>(hrow + ph) = make_float4(v[4 * g4], v[4 * g4 + 1], v[4 * g4 + 2], v[4 * g4 + 3]);
     }
+    store_lo_row(v, taddr);
+}
+
+// tcgen05.mma with A from TMEM (a_tmem: lanes = the 128 rows, 8 columns of K)
+__device__ __forceinline__ void mma_tf32_ts(uint32_t d, uint32_t a_tmem, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d),
+        "r"(a_tmem), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
 }
 
 constexpr int TC_NACC = 2;                   // rotating accumulator groups
@@ -178,15 +211,17 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
     constexpr int SLAB_B = K * 32;                        // floats per X slab
     constexpr unsigned STAGE_TX = (TC_SLAB_A + 2 * SLAB_B) * 4;
     constexpr int GW = 3 * K;                              // TMEM columns per accumulator group
-    constexpr uint32_t TMEM_COLS = K == 32 ? 256 : 128;   // power of two >= TC_NACC * GW
+    // TMEM: the accumulator groups (TC_NACC x GW columns), then TC_LO A_lo
+    // buffers of 32 columns each (A_lo of K slab kk in buffer kk mod TC_LO)
+    constexpr uint32_t LO_COL = TC_NACC * GW;
+    constexpr uint32_t TMEM_COLS = 256;                   // power of two >= LO_COL + 32 TC_LO
+    static_assert(LO_COL + 32 * TC_LO <= TMEM_COLS, "TMEM columns");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // 1024-byte aligned buffers: stage s holds A (FP32) and X_hi, X_lo (copied
-    // from HBM); A_lo of K slab kk is formed in buffer kk mod TC_LO
+    // 1024-byte aligned buffers: stage s holds A (FP32) and X_hi, X_lo (copied from HBM)
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     float *sA = reinterpret_cast<float *>(base);                          // TC_STAGES x 16 KB
     float *sB = reinterpret_cast<float *>(base + TC_STAGES * TC_SLAB_A * 4);
-    float *sL = reinterpret_cast<float *>(base + TC_STAGES * (TC_SLAB_A + 2 * SLAB_B) * 4);   // TC_LO x 16 KB
     __shared__ __align__(8) uint64_t full[TC_STAGES], split[TC_STAGES], empty[TC_STAGES], lo_empty[TC_LO], done;
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
@@ -270,13 +305,13 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t d = tmem + uint32_t((kk % TC_NACC) * GW);   // [hi-hi | hi-lo | lo-hi]
                 const uint64_t da = sw128_desc(sA + s * TC_SLAB_A);
-                const uint64_t dal = sw128_desc(sL + (kk % TC_LO) * TC_SLAB_A);
+                const uint32_t tal = tmem + LO_COL + 32u * uint32_t(kk % TC_LO);   // A_lo in TMEM
                 const uint64_t db = sw128_desc(sB + s * 2 * SLAB_B);      // X_hi, X_lo: 2k rows
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {              // 4 x K=8 (32 bytes) per slab
                     const uint32_t acc = (kk >= TC_NACC || q > 0) ? 1u : 0u;
                     mma_tf32(d, da + 2ull * q, db + 2ull * q, idesc2, acc);
-                    mma_tf32(d + 2 * K, dal + 2ull * q, db + 2ull * q, idesc, acc);
+                    mma_tf32_ts(d + 2 * K, tal + 8u * q, db + 2ull * q, idesc, acc);
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&empty[s]))
@@ -291,7 +326,6 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
         }
     } else {
         // warps 2-5: split the A slab of every stage, then the epilogue
-        const int t = threadIdx.x - 64;                  // 0..127
         for (int kk = 0; kk < g.ks; ++kk) {
             const int s = kk % TC_STAGES, lb = kk % TC_LO;
             // the A_lo buffer of slab kk - TC_LO is free once its MMAs completed; the A slab has landed
@@ -302,28 +336,21 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                 abort_flag = 1;
                 break;
             }
-            if (kk < g.kd) {                              // stored slab: A_lo beside it
-                const float4 *a4 = reinterpret_cast<const float4 *>(sA + s * TC_SLAB_A);
-                float4 *lo = reinterpret_cast<float4 *>(sL + lb * TC_SLAB_A);
-#pragma unroll
-                for (int i = t; i < TC_SLAB_A / 4; i += 128) {
-                    const float4 v = a4[i];
-                    float4 l;
-                    l.x = tf32_rna(v.x - tf32_trunc(v.x));
-                    l.y = tf32_rna(v.y - tf32_trunc(v.y));
-                    l.z = tf32_rna(v.z - tf32_trunc(v.z));
-                    l.w = tf32_rna(v.w - tf32_trunc(v.w));
-                    lo[i] = l;
-                }
+            // warp w handles rows 32 (w mod 4) .. +31, the TMEM lanes it may access
+            const int quarter = warp & 3;
+            const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16) + LO_COL + 32u * uint32_t(lb);
+            if (kk < g.kd) {                              // stored slab: A_lo of this warp's rows
+                split_direct(sA + s * TC_SLAB_A, quarter * 32 + lane, taddr);
             } else {
-                // transposed pieces: warp p (0..3) owns piece p (4 KB at p * 1024 floats), whose
+                // transposed pieces: the warp owns piece p = quarter (4 KB at p * 1024 floats), whose
                 // column l is row 32 p + l of this K step's A; the output rows 32 p .. 32 p + 31
                 // of the K-major slab occupy the same 4 KB, so the transpose stays inside the warp
-                split_transposed(sA + s * TC_SLAB_A + (warp - 2) * 1024, sL + lb * TC_SLAB_A + (warp - 2) * 1024,
-                                 lane);
+                split_transposed(sA + s * TC_SLAB_A + quarter * 1024, lane, taddr);
             }
-            // generic-proxy writes become visible to the tensor core's async proxy
+            // generic-proxy writes become visible to the tensor core's async proxy, TMEM stores
+            // are ordered before the hand-off
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&split[s]);
         }
