@@ -123,7 +123,7 @@ int htf_setup(htf_ctx *ctx) {
     if (!ctx->has_mesh) return fail(ctx, HTF_ESTATE, "htf_setup before htf_set_mesh");
     if (ctx->is_setup) return fail(ctx, HTF_ESTATE, "htf_setup called twice");
     const auto t0 = std::chrono::steady_clock::now();
-    int rc = htf::build_problem(ctx->p, ctx->err);
+    int rc = htf::build_problem(ctx->p, ctx->err, true);
     if (rc) return rc;
     ctx->eng.reset(new (std::nothrow) htf::Engine(ctx->p.opt));
     if (!ctx->eng) return fail(ctx, HTF_ENOMEM, "engine allocation failed");

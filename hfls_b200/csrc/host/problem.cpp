@@ -194,7 +194,7 @@ bool bc_rank_full(const std::vector<double> &A, int rows, int cols) {
 }
 }  // namespace
 
-int build_problem(Problem &p, std::string &err) {
+int build_problem(Problem &p, std::string &err, bool on_device) {
     Mesh &m = p.mesh;
     const int ns = m.n_sub(), ne = m.n_elems();
     if (ns < 1 || ne < 1) { err = "empty mesh"; return HTF_EINVAL; }
@@ -357,7 +357,12 @@ int build_problem(Problem &p, std::string &err) {
         }
         if (few >= 0) { err = "subdomain with fewer than 6 interface/Dirichlet DOFs"; return HTF_EINVAL; }
     }
-    // kernels and fix DOFs
+    // kernels and fix DOFs: on the device for a set-up (kernel_fix.cu), on the
+    // host for the layout inspection entry points, bit for bit the same
+    if (on_device) {
+        const int rc = kernels_fix_on_device(m, p.sub, p.opt.device, err);
+        if (rc) return rc;
+    } else {
 #pragma omp parallel for schedule(dynamic, 4)
     for (int d = 0; d < ns; ++d) {
         Subdomain &s = p.sub[d];
@@ -369,6 +374,7 @@ int build_problem(Problem &p, std::string &err) {
         s.fix.resize(6);
         for (int i = 0; i < 6; ++i) s.fix[i] = s.b[pv[i]];
         std::sort(s.fix.begin(), s.fix.end());
+    }
     }
     // neighbour lists (subdomains sharing at least one DOF)
     std::vector<std::vector<int>> neigh(ns);

@@ -114,7 +114,11 @@ struct Problem {
 
 // Data::buildMappingStruct + Cluster::create_cluster_constraints +
 // kernels/fix DOFs.  Returns HTF_OK or an error code with err set.
-int build_problem(Problem &p, std::string &err);
+// on_device: kernels and fix DOFs on the GPU (kernel_fix.cu), bit-identical
+// to the host code used otherwise
+int build_problem(Problem &p, std::string &err, bool on_device = false);
+// kernel bases and fix DOFs of all subdomains on the GPU (kernel_fix.cu)
+int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int device, std::string &err);
 
 // Analytic rigid body modes of the nodes of l2g (column order of
 // Data::create_analytic_ker_K, Data.cpp:61-109), Gram-Schmidt'ed

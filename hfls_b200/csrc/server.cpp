@@ -260,7 +260,7 @@ int Server::prepare(Request &r, std::string &err) {
     if (rc) return rc;
     p.nrhs = r.nrhs;
     if (!r.f.empty()) p.f_nodal = r.f;
-    if ((rc = build_problem(p, err))) return rc;
+    if ((rc = build_problem(p, err, true))) return rc;
     const size_t est = estimate(p, r.nrhs);
     {
         std::unique_lock<std::mutex> lk(mu_);

@@ -52,3 +52,34 @@ def test_dump_needs_the_option_at_setup(tmp_path):
     with pytest.raises(hb.HTFError) as e:
         s.dump(str(tmp_path), 2)
     assert e.value.code == hb.HTF_ESTATE
+
+
+@pytest.mark.parametrize("typeBc", ["cor", "ker"])
+def test_kernel_and_fix_dofs_on_device_are_the_host_ones(tmp_path, typeBc):
+    """A set-up computes the kernel bases R_i and the fix DOFs on the GPU
+    (kernel_fix.cu); the layout inspection without a set-up computes them on
+    the host.  Both are bit-identical, and R_i equals the oracle's
+    (Data.cpp:61-109 + Matrix.cpp:2450-2472) bit for bit."""
+    w = [np.array(v, np.int32) for v in ([3, 5, 2, 4], [4, 2, 3, 5], [2, 4, 5, 3])]
+    spec = hb.mesh_spec(clusters=(2, 2, 1), subs=(2, 2, 4), widths=w, jitter=0.1, seed=6,
+                        material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e3)
+    m = hb.generate_mesh(spec)
+    host = hb.Solver({"typeBc": typeBc})
+    host.set_mesh(m)
+    fix_host = host.fix_dofs()
+    host.close()
+    dev = hb.Solver({"typeBc": typeBc, "print_matrices": "3"})
+    dev.set_mesh(m)
+    dev.setup()
+    assert np.array_equal(dev.fix_dofs(), fix_host)
+    dev.dump(str(tmp_path), 3)
+    dev.close()
+    o = HTFETI(MeshArrays(m.coords, m.elems.astype(np.int64), m.elem_sub.astype(np.int64),
+                          m.sub_cluster.astype(np.int64), m.sub_E, m.sub_nu, m.dirichlet.astype(np.int64),
+                          m.corner.astype(np.int64), m.body_force),
+               Options(typeBc=typeBc, fix_rule="boundary", kerGc="analytic"))
+    for d in range(m.n_sub):
+        R = scipy.io.mmread(os.path.join(tmp_path, f"dump_R_{d}.txt")).toarray()
+        assert np.array_equal(R, o.R[d])
+        assert np.array_equal(np.sort(fix_host[d] if fix_host.ndim == 2 else fix_host[6 * d:6 * d + 6]),
+                              np.sort(o.l2g[d][o.fix[d]]))
