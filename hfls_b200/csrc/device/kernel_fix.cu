@@ -27,9 +27,19 @@ namespace {
 
 constexpr int KF_THREADS = 128;
 
+// left-to-right sum of a[k] b[k]: the adds stay in order, the loads of b
+// (global memory) are issued eight at a time ahead of them
 __device__ double seq_dot(const double *a, const double *b, int n) {
     double s = 0.0;
-    for (int k = 0; k < n; ++k) s = __dadd_rn(s, __dmul_rn(a[k], b[k]));
+    int k = 0;
+    for (; k + 8 <= n; k += 8) {
+        double r[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) r[u] = b[k + u];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s = __dadd_rn(s, __dmul_rn(a[k + u], r[u]));
+    }
+    for (; k < n; ++k) s = __dadd_rn(s, __dmul_rn(a[k], b[k]));
     return s;
 }
 
@@ -42,13 +52,16 @@ __global__ void __launch_bounds__(KF_THREADS) k_kernel_fix(const double *__restr
                                                            const int *__restrict__ bidx,
                                                            const long long *__restrict__ r_off, double *__restrict__ R,
                                                            const long long *__restrict__ n_off,
-                                                           double *__restrict__ N, double *__restrict__ W,
+                                                           double *__restrict__ N, double *__restrict__ Wg,
                                                            int *__restrict__ piv_buf, int *__restrict__ fix) {
     const int d = blockIdx.x, t = threadIdx.x;
     const int nn = node_ptr[d + 1] - node_ptr[d], n = 3 * nn;
     const int nb = b_ptr[d + 1] - b_ptr[d];
+    extern __shared__ double wsm[];
+    // the column being orthogonalised (n doubles): shared memory, or global
+    // scratch for subdomains too large for it
+    double *w = Wg ? Wg + r_off[d] / 6 : wsm;
     double *Rd = R + r_off[d];
-    double *w = W + r_off[d] / 6;                   // one column of scratch (n doubles)
     double *Nd = N + n_off[d];
     int *piv = piv_buf + n_off[d] / 6;
     const int *bd = bidx + b_ptr[d];
@@ -160,8 +173,8 @@ __global__ void __launch_bounds__(KF_THREADS) k_kernel_fix(const double *__restr
     }
 }
 
-template <typename T> int upload(T *&dst, const std::vector<T> &src, std::string &err) {
-    const size_t bytes = std::max<size_t>(src.size(), 1) * sizeof(T);
+template <typename T> int upload(T *&dst, const std::vector<T> &src, std::string &err, size_t n_alloc = 0) {
+    const size_t bytes = std::max<size_t>(std::max(src.size(), n_alloc), 1) * sizeof(T);
     cudaError_t e = cudaMalloc(&dst, bytes);
     if (e == cudaSuccess && !src.empty()) e = cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
@@ -177,6 +190,7 @@ int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int devic
     const int ns = int(subs.size());
     if (ns == 0) return HTF_OK;
     int count = 0;
+    cudaGetLastError();                 // an error left by an earlier, failed call is not this one's
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
         cudaGetLastError();
         err = "no CUDA device";
@@ -188,8 +202,10 @@ int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int devic
     }
     std::vector<int> node_ptr(ns + 1, 0), nodes, b_ptr(ns + 1, 0), bidx;
     std::vector<long long> r_off(ns + 1, 0), n_off(ns + 1, 0);
+    int max_n = 0;
     for (int d = 0; d < ns; ++d) {
         const Subdomain &s = subs[d];
+        max_n = std::max(max_n, s.n);
         for (int i = 0; i < s.n / 3; ++i) nodes.push_back(s.l2g[3 * i] / 3);
         node_ptr[d + 1] = int(nodes.size());
         bidx.insert(bidx.end(), s.b.begin(), s.b.end());
@@ -207,15 +223,24 @@ int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int devic
     if (!rc) rc = upload(db, bidx, err);
     if (!rc) rc = upload(dro, r_off, err);
     if (!rc) rc = upload(dno, n_off, err);
-    if (!rc) rc = upload(dR, std::vector<double>(r_off[ns]), err);
-    if (!rc) rc = upload(dW, std::vector<double>(r_off[ns] / 6 + 1), err);
-    if (!rc) rc = upload(dN, std::vector<double>(n_off[ns] + 1), err);
-    if (!rc) rc = upload(dpiv, std::vector<int>(n_off[ns] / 6 + 1), err);
-    if (!rc) rc = upload(dfix, std::vector<int>(6 * ns), err);
+    if (!rc) rc = upload(dR, std::vector<double>(), err, size_t(r_off[ns]));
+    if (!rc) rc = upload(dN, std::vector<double>(), err, size_t(n_off[ns]) + 1);
+    if (!rc) rc = upload(dpiv, std::vector<int>(), err, size_t(n_off[ns] / 6) + 1);
+    if (!rc) rc = upload(dfix, std::vector<int>(), err, size_t(6 * ns));
     std::vector<double> R(r_off[ns]);
     std::vector<int> fix(6 * ns);
+    int smem = max_n * int(sizeof(double)), optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (!rc && smem > optin - 4096) {          // too large for shared memory: global scratch
+        smem = 0;
+        rc = upload(dW, std::vector<double>(), err, size_t(r_off[ns] / 6) + 1);
+    } else if (!rc && smem > 48 * 1024 &&
+               cudaFuncSetAttribute(k_kernel_fix, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
+        err = "kernel detection: cudaFuncSetAttribute failed";
+        rc = HTF_ECUDA;
+    }
     if (!rc) {
-        k_kernel_fix<<<ns, KF_THREADS>>>(dc, dnp, dn, dbp, db, dro, dR, dno, dN, dW, dpiv, dfix);
+        k_kernel_fix<<<ns, KF_THREADS, smem>>>(dc, dnp, dn, dbp, db, dro, dR, dno, dN, dW, dpiv, dfix);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpy(R.data(), dR, R.size() * sizeof(double), cudaMemcpyDeviceToHost);
         if (e == cudaSuccess) e = cudaMemcpy(fix.data(), dfix, fix.size() * sizeof(int), cudaMemcpyDeviceToHost);

@@ -67,8 +67,7 @@ def test_pcpg_matches_oracle(small):
     m, s, o = small
     u, st = s.pcpg()
     ref = o.pcpg()
-    longer = o.pcpg(eps_iter=1e-9)              # the oracle's history past its own stop
-    assert same_stop(st.iterations[0], s.residual_history(0), ref["iterations"], longer["hist"], 1e-8)
+    assert same_stop(st.iterations[0], ref["iterations"])
     assert rel(u[0], ref["u"]) < 1e-6          # both stop at eps_iter 1e-8
 
 

@@ -105,8 +105,7 @@ def test_uneven_widths_small_matches_oracle():
     s8.setup()
     _, st8 = s8.pcpg()
     ref8 = o.pcpg(eps_iter=1e-8, max_iter=5000)
-    ref9 = o.pcpg(eps_iter=1e-9, max_iter=5000)
-    assert same_stop(st8.iterations[0], s8.residual_history(0), ref8["iterations"], ref9["hist"], 1e-8)
+    assert same_stop(st8.iterations[0], ref8["iterations"])
     s10 = hb.Solver(dict(OPTS, eps_iter="1e-10"))
     s10.set_mesh(m)
     s10.setup()
