@@ -234,18 +234,29 @@ int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int devic
     if (!rc && smem > optin - 4096) {          // too large for shared memory: global scratch
         smem = 0;
         rc = upload(dW, std::vector<double>(), err, size_t(r_off[ns] / 6) + 1);
-    } else if (!rc && smem > 48 * 1024 &&
-               cudaFuncSetAttribute(k_kernel_fix, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
-        err = "kernel detection: cudaFuncSetAttribute failed";
-        rc = HTF_ECUDA;
+    } else if (!rc && smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(k_kernel_fix, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) {
+            err = std::string("kernel detection: shared memory opt-in of ") + std::to_string(smem) +
+                  " B: " + cudaGetErrorString(e);
+            rc = HTF_ECUDA;
+        }
     }
     if (!rc) {
+        const char *step = "launch";
         k_kernel_fix<<<ns, KF_THREADS, smem>>>(dc, dnp, dn, dbp, db, dro, dR, dno, dN, dW, dpiv, dfix);
         cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpy(R.data(), dR, R.size() * sizeof(double), cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess) e = cudaMemcpy(fix.data(), dfix, fix.size() * sizeof(int), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) {
+            step = "copy of R";
+            e = cudaMemcpy(R.data(), dR, R.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        }
+        if (e == cudaSuccess) {
+            step = "copy of the fix DOFs";
+            e = cudaMemcpy(fix.data(), dfix, fix.size() * sizeof(int), cudaMemcpyDeviceToHost);
+        }
         if (e != cudaSuccess) {
-            err = std::string("kernel detection: ") + cudaGetErrorString(e);
+            err = std::string("kernel detection: ") + step + " (" + std::to_string(ns) + " CTAs, " +
+                  std::to_string(smem) + " B dynamic shared memory): " + cudaGetErrorString(e);
             rc = HTF_ECUDA;
         }
     }
