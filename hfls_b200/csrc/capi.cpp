@@ -127,9 +127,14 @@ int htf_setup(htf_ctx *ctx) {
     if (rc) return rc;
     ctx->eng.reset(new (std::nothrow) htf::Engine(ctx->p.opt));
     if (!ctx->eng) return fail(ctx, HTF_ENOMEM, "engine allocation failed");
-    ctx->eng->phase_ms[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    // phase 0 without the device context creation, which the kernel detection
+    // triggers and which belongs to phase 1
+    ctx->eng->phase_ms[0] =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() - ctx->p.context_ms;
+    ctx->eng->kernel_detection_ms = ctx->p.kernel_ms;
     rc = ctx->eng->setup(ctx->p, ctx->err);
     if (rc) return rc;
+    ctx->eng->phase_ms[1] += ctx->p.context_ms;
     ctx->is_setup = true;
     return HTF_OK;
 }

@@ -1114,6 +1114,7 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
     for (int b = 0; b < SYMV_BUCKETS && b < int(schedule_.size()); ++b) info->symv_unit_tiles[b] = schedule_[b];
     info->symv_tuned = tuned_ ? 1 : 0;
     info->device_bytes = double(device_bytes());
+    info->kernel_detection_ms = kernel_detection_ms;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));

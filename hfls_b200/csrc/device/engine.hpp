@@ -75,6 +75,7 @@ public:
     const std::vector<int> &symv_schedule() const { return schedule_; }
     bool symv_tuned() const { return tuned_; }
     double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // see htf_profile_info::setup_phase_ms
+    double kernel_detection_ms = 0.0;                 // part of phase 0 run on the device
     int status_sub = -1;
 
 private:

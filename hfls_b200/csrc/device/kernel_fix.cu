@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <string>
 #include <vector>
 
@@ -186,7 +187,8 @@ template <typename T> int upload(T *&dst, const std::vector<T> &src, std::string
 
 }  // namespace
 
-int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int device, std::string &err) {
+int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int device, std::string &err,
+                          double *timing_ms) {
     const int ns = int(subs.size());
     if (ns == 0) return HTF_OK;
     int count = 0;
@@ -196,10 +198,12 @@ int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int devic
         err = "no CUDA device";
         return HTF_ENODEV;
     }
-    if (cudaSetDevice(device) != cudaSuccess) {
+    const auto t0 = std::chrono::steady_clock::now();
+    if (cudaSetDevice(device) != cudaSuccess || cudaFree(nullptr) != cudaSuccess) {
         err = "kernel detection: cudaSetDevice failed";
         return HTF_ECUDA;
     }
+    const auto t1 = std::chrono::steady_clock::now();
     std::vector<int> node_ptr(ns + 1, 0), nodes, b_ptr(ns + 1, 0), bidx;
     std::vector<long long> r_off(ns + 1, 0), n_off(ns + 1, 0);
     int max_n = 0;
@@ -264,6 +268,10 @@ int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int devic
                     (void *)dpiv, (void *)dfix, (void *)dro, (void *)dno})
         if (p) cudaFree(p);
     if (rc) return rc;
+    if (timing_ms) {
+        timing_ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        timing_ms[1] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
+    }
     for (int d = 0; d < ns; ++d) {
         Subdomain &s = subs[d];
         s.R.assign(R.begin() + r_off[d], R.begin() + r_off[d + 1]);

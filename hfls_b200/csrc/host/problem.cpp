@@ -360,7 +360,10 @@ int build_problem(Problem &p, std::string &err, bool on_device) {
     // kernels and fix DOFs: on the device for a set-up (kernel_fix.cu), on the
     // host for the layout inspection entry points, bit for bit the same
     if (on_device) {
-        const int rc = kernels_fix_on_device(m, p.sub, p.opt.device, err);
+        double t[2] = {0.0, 0.0};
+        const int rc = kernels_fix_on_device(m, p.sub, p.opt.device, err, t);
+        p.context_ms = t[0];
+        p.kernel_ms = t[1];
         if (rc) return rc;
     } else {
 #pragma omp parallel for schedule(dynamic, 4)

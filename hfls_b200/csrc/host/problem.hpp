@@ -110,6 +110,8 @@ struct Problem {
     int n_lam = 0;
     int nrhs = 1;
     std::vector<double> f_nodal;            // 3*n_nodes*nrhs (optional)
+    double context_ms = 0.0;                // host wall of the device context creation (set-up only)
+    double kernel_ms = 0.0;                 // host wall of the device kernel detection (set-up only)
 };
 
 // Data::buildMappingStruct + Cluster::create_cluster_constraints +
@@ -118,7 +120,10 @@ struct Problem {
 // to the host code used otherwise
 int build_problem(Problem &p, std::string &err, bool on_device = false);
 // kernel bases and fix DOFs of all subdomains on the GPU (kernel_fix.cu)
-int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int device, std::string &err);
+// timing_ms (optional): [0] device context creation, [1] the rest (uploads,
+// kernel, copies back), host wall milliseconds
+int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int device, std::string &err,
+                          double *timing_ms = nullptr);
 
 // Analytic rigid body modes of the nodes of l2g (column order of
 // Data::create_analytic_ker_K, Data.cpp:61-109), Gram-Schmidt'ed

@@ -191,6 +191,9 @@ typedef struct htf_profile_info {
     int symv_unit_tiles[5];
     int symv_tuned;
     double device_bytes;                /* device memory the context holds          */
+    double kernel_detection_ms;         /* host wall of the kernel bases and fix
+                                           DOFs computed on the device (part of
+                                           setup phase 0)                           */
 } htf_profile_info;
 int htf_profile(htf_ctx *ctx, int reps, htf_profile_info *info);
 
