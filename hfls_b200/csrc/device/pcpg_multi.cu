@@ -265,15 +265,22 @@ __device__ __forceinline__ double row_value(int r, int K, int j, const int *__re
 // with V_d = [F_d Bc_d^T, -R_d], s_d the cluster coarse solution at the
 // subdomain's Bc rows and alpha slot), after the tensor-core product so the
 // product's CTAs end without an FP64 epilogue.  CTA (subdomain, 128-row
-// chunk): s_d staged in shared memory ((c + 6) K <= 2048 doubles, checked at
-// set-up); lane j of a warp is load case j of a row (two rows per warp for
-// K = 16), so the row's y is read and written coalesced and V is a broadcast.
+// chunk), a 128 x K by (c + 6) x K product: s_d staged in shared memory
+// ((c + 6) K <= 2048 doubles, checked at set-up), V in chunks of 16 columns
+// (coalesced column reads); thread (row group, case group) keeps 128 K / 256
+// outputs in registers (rows rg + RG i, cases jg + JG c: conflict-free
+// shared-memory reads), summed over the columns in order.
 template <int K>
 __global__ void __launch_bounds__(256) k_correct_multi(const SubDev *__restrict__ subs,
                                                        const ClusterDev *__restrict__ cl,
                                                        const double *__restrict__ V, const int *__restrict__ bcr,
                                                        const double *__restrict__ s, double *__restrict__ yb) {
+    constexpr int QC = 16;                            // V columns per shared-memory chunk
+    constexpr int JG = K / 4;                         // case groups (4 cases per thread)
+    constexpr int RG = 256 / JG;                      // row groups
+    constexpr int RPT = 128 / RG;                     // rows per thread
     __shared__ double ss[2048];
+    __shared__ double vs[QC][128];
     const SubDev &sd = subs[blockIdx.x];
     const int r0 = blockIdx.y * 128;
     if (r0 >= sd.nb) return;
@@ -284,17 +291,43 @@ __global__ void __launch_bounds__(256) k_correct_multi(const SubDev *__restrict_
         const int pos = q < sd.c ? bcr[sd.bcr_off + q] : sd.alpha_pos + (q - sd.c);
         ss[o] = s[((size_t)gc_off + pos) * K + j];
     }
-    __syncthreads();
-    constexpr int RPW = 32 / K;                       // rows per warp step
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int sub = lane / K, j = lane % K;
     const int rend = min(128, sd.nb - r0);
-    for (int rr = warp * RPW + sub; rr < rend; rr += 8 * RPW) {
-        const int row = r0 + rr;
-        const double *Vr = V + sd.V_off + row;
-        double a = 0.0;
-        for (int q = 0; q < nc; ++q) a += Vr[(size_t)q * sd.nbp] * ss[q * K + j];
-        yb[((size_t)sd.xb_off + row) * K + j] -= a;
+    const int jg = threadIdx.x % JG, rg = threadIdx.x / JG;
+    const double *Vd = V + sd.V_off + r0;
+    double acc[RPT][4];
+#pragma unroll
+    for (int i = 0; i < RPT; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[i][c] = 0.0;
+    for (int q0 = 0; q0 < nc; q0 += QC) {
+        const int qn = min(QC, nc - q0);
+        __syncthreads();                              // s_d staged, the previous chunk consumed
+        for (int o = threadIdx.x; o < qn * 128; o += blockDim.x) {
+            const int q = o >> 7, r = o & 127;
+            vs[q][r] = r < rend ? Vd[(size_t)(q0 + q) * sd.nbp + r] : 0.0;
+        }
+        __syncthreads();
+        for (int q = 0; q < qn; ++q) {
+            const double *sq = ss + (q0 + q) * K + jg;
+            double sv[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) sv[c] = sq[JG * c];
+#pragma unroll
+            for (int i = 0; i < RPT; ++i) {
+                const double v = vs[q][rg + RG * i];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[i][c] += v * sv[c];
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        const int row = rg + RG * i;
+        if (row < rend) {
+            double *y = yb + ((size_t)sd.xb_off + r0 + row) * K + jg;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) y[JG * c] -= acc[i][c];
+        }
     }
 }
 

@@ -25,19 +25,21 @@
 //   * warp 0, one thread: bulk-copy producer (A slab or its four transposed
 //     pieces, X_hi, X_lo per stage);
 //   * warps 2-5: form A_lo = rna_tf32(A - trunc_tf32(A)) of every landed A
-//     slab (the MMA reads the FP32 slab itself as A_hi: a TF32 operand's
-//     low 13 mantissa bits do not take part in the product; a transposed
-//     step is first transposed in place, each warp inside its own 4 KB),
-//     then hand the stage to the MMA issuer;
+//     slab and store it into one of TC_LO 32-column TMEM buffers
+//     (tcgen05.st; the MMA reads the FP32 slab itself as A_hi: a TF32
+//     operand's low 13 mantissa bits do not take part in the product; a
+//     transposed step is first transposed in place, each warp inside its own
+//     4 KB), then hand the stage to the MMA issuer;
 //     at the end they read the accumulators out of TMEM (warp w owns TMEM
 //     lanes 32 (w mod 4) .. +31) and write y in FP64;
 //   * warp 1, one thread: issues the MMAs (M=128, N=k, K=8 per instruction,
 //     4 per slab).
 // Products per K step of 8: A_hi [X_hi | X_lo] as one N = 2k MMA (A_hi read
-// from shared memory once) and A_lo X_hi.  Accumulation: K slab kk goes to
-// accumulator group kk mod 2 (hi-hi, hi-lo and lo-hi columns), so every FP32
-// accumulator in TMEM sums half of the K range; the groups are added in
-// FP64 in the epilogue.  Every mbarrier wait is bounded; on time-out the
+// from shared memory once) and A_lo X_hi (A from TMEM).  Accumulation: K slab
+// kk goes to accumulator group kk mod 2 (hi-hi columns, and hi-lo + lo-hi
+// columns: the two correction terms are ~2^-11 of the product and share one
+// FP32 accumulator), so every FP32 accumulator in TMEM sums half of the K
+// range; the groups are added in FP64 in the epilogue.  Every mbarrier wait is bounded; on time-out the
 // CTA records HTF_ETIMEDOUT in err and stops issuing work.
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -210,9 +212,11 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
     static_assert(K == 16 || K == 32, "N of the MMA");
     constexpr int SLAB_B = K * 32;                        // floats per X slab
     constexpr unsigned STAGE_TX = (TC_SLAB_A + 2 * SLAB_B) * 4;
-    constexpr int GW = 3 * K;                              // TMEM columns per accumulator group
-    // TMEM: the accumulator groups (TC_NACC x GW columns), then TC_LO A_lo
-    // buffers of 32 columns each (A_lo of K slab kk in buffer kk mod TC_LO)
+    constexpr int GW = 2 * K;                              // TMEM columns per accumulator group
+    // TMEM: the accumulator groups (TC_NACC x GW columns: A_hi X_hi, then
+    // A_hi X_lo + A_lo X_hi, the two small terms sharing one FP32 accumulator),
+    // then TC_LO A_lo buffers of 32 columns each (A_lo of K slab kk in buffer
+    // kk mod TC_LO)
     constexpr uint32_t LO_COL = TC_NACC * GW;
     constexpr uint32_t TMEM_COLS = 256;                   // power of two >= LO_COL + 32 TC_LO
     static_assert(LO_COL + 32 * TC_LO <= TMEM_COLS, "TMEM columns");
@@ -303,7 +307,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t d = tmem + uint32_t((kk % TC_NACC) * GW);   // [hi-hi | hi-lo | lo-hi]
+                const uint32_t d = tmem + uint32_t((kk % TC_NACC) * GW);   // [hi-hi | hi-lo + lo-hi]
                 const uint64_t da = sw128_desc(sA + s * TC_SLAB_A);
                 const uint32_t tal = tmem + LO_COL + 32u * uint32_t(kk % TC_LO);   // A_lo in TMEM
                 const uint64_t db = sw128_desc(sB + s * 2 * SLAB_B);      // X_hi, X_lo: 2k rows
@@ -311,7 +315,8 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                 for (int q = 0; q < 4; ++q) {              // 4 x K=8 (32 bytes) per slab
                     const uint32_t acc = (kk >= TC_NACC || q > 0) ? 1u : 0u;
                     mma_tf32(d, da + 2ull * q, db + 2ull * q, idesc2, acc);
-                    mma_tf32_ts(d + 2 * K, tal + 8u * q, db + 2ull * q, idesc, acc);
+                    // issued after the first, which initialised these columns
+                    mma_tf32_ts(d + K, tal + 8u * q, db + 2ull * q, idesc, 1u);
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&empty[s]))
@@ -380,7 +385,6 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
             for (int a = 0; a < nacc; ++a) {
                 tmem_add<K>(taddr + uint32_t(a * GW), acc);
                 tmem_add<K>(taddr + uint32_t(a * GW + K), acc);
-                tmem_add<K>(taddr + uint32_t(a * GW + 2 * K), acc);
             }
         }
         if (scoarse) {
