@@ -783,12 +783,13 @@ int Engine::setup(Problem &p, std::string &err) {
         int optin = 0;
         rc = check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, opt_.device),
                    "cudaDeviceGetAttribute", err);
-        if (!rc && smem > optin) {
-            err = "projector: " + std::to_string(ncl_) + " clusters need " + std::to_string(smem) +
+        // the kernel's 2 KB of static shared memory count against the same limits
+        if (!rc && smem + 2048 > optin) {
+            err = "projector: " + std::to_string(ncl_) + " clusters need " + std::to_string(smem + 2048) +
                   " bytes of shared memory, the device allows " + std::to_string(optin) + " per block";
             rc = HTF_EINVAL;
         }
-        if (!rc && smem > 48 * 1024)
+        if (!rc)
             rc = check(cudaFuncSetAttribute(k_gf_apply_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                        "cudaFuncSetAttribute(k_gf_apply_fused)", err);
     }

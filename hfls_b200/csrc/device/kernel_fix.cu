@@ -238,7 +238,9 @@ int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int devic
     if (!rc && smem > optin - 4096) {          // too large for shared memory: global scratch
         smem = 0;
         rc = upload(dW, std::vector<double>(), err, size_t(r_off[ns] / 6) + 1);
-    } else if (!rc && smem > 48 * 1024) {
+    } else if (!rc && smem > 0) {
+        // static + dynamic shared memory above 48 KB needs the opt-in; set it
+        // for every size (the static arrays count against the same 48 KB)
         const cudaError_t e = cudaFuncSetAttribute(k_kernel_fix, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) {
             err = std::string("kernel detection: shared memory opt-in of ") + std::to_string(smem) +
