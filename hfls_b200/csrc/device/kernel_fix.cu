@@ -192,13 +192,13 @@ int kernels_fix_on_device(const Mesh &m, std::vector<Subdomain> &subs, int devic
     const int ns = int(subs.size());
     if (ns == 0) return HTF_OK;
     int count = 0;
+    const auto t0 = std::chrono::steady_clock::now();   // runtime initialisation and context creation
     cudaGetLastError();                 // an error left by an earlier, failed call is not this one's
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
         cudaGetLastError();
         err = "no CUDA device";
         return HTF_ENODEV;
     }
-    const auto t0 = std::chrono::steady_clock::now();
     if (cudaSetDevice(device) != cudaSuccess || cudaFree(nullptr) != cudaSuccess) {
         err = "kernel detection: cudaSetDevice failed";
         return HTF_ECUDA;
