@@ -39,6 +39,7 @@ constexpr int TILE = 32;                  // packed tile edge
 constexpr int CHOL_STEP = 64;             // columns per batched Cholesky step (two factor panels)
 constexpr int TC_STAGES = 4;              // pipeline stages of the tensor-core product (2 CTAs per SM)
 constexpr int TC_LO = 4;                  // A_lo buffers (in TMEM) of the tensor-core product
+constexpr int TC_THREADS = 320;           // threads of the tensor-core product: producer, MMA, 8 splitting warps
 constexpr int TILE_ELEMS = TILE * TILE;
 
 struct SubDev {
@@ -161,11 +162,6 @@ struct TcSet {
     const float *Xs;                      // X_hi slabs; X_lo slabs at Xs + xlo
     long long xlo;
     double *yb;                           // b-space output, RHS-interleaved
-    const SubDev *subs;
-    const ClusterDev *cl;
-    const double *V;                      // coarse-correction columns
-    const int *bcr;                       // Bc row ids per subdomain
-    const double *sc;                     // coarse solution of the F product
 };
 
 // One step of the batched Cholesky for one subdomain: columns [k, k + nb),

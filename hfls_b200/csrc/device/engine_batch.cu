@@ -195,7 +195,7 @@ int Engine::setup_batch(int K, std::string &err) {
 // the coarse correction of the F product runs after it (k_correct_multi in
 // f_post), so the product's epilogue gets no coarse solution
 TcSet Engine::tc_set() const {
-    return TcSet{d_AF_, d_AS_, d_Xs_, (long long)nslots_ * bK_, b_yb_, d_subs_, d_cl_, d_V_, d_bcr_, nullptr};
+    return TcSet{d_AF_, d_AS_, d_Xs_, (long long)nslots_ * bK_, b_yb_};
 }
 
 // X slabs of a batch vector (for timing the tensor-core product alone)
@@ -205,13 +205,13 @@ void Engine::profile_batch_gather(const double *w) {
                                                  d_Xs_ + xlo);
 }
 
-// one tensor-core launch over the given blocks / operand sets (which: 0 = F
-// with coarse correction, 1 = S)
+// one tensor-core launch over the given blocks / operand sets (which: 0 = F,
+// 1 = S; the coarse correction of F follows in k_correct_multi)
 int tc_launch(int K, const GemmBlock *blocks, int nblocks, const TcSet *sets, int which, int smem, int *err,
               cudaStream_t s) {
     if (nblocks <= 0) return 0;
-    if (K == 16) k_tc_gemm<16><<<nblocks, 192, smem, s>>>(blocks, sets, which, err);
-    else k_tc_gemm<32><<<nblocks, 192, smem, s>>>(blocks, sets, which, err);
+    if (K == 16) k_tc_gemm<16><<<nblocks, TC_THREADS, smem, s>>>(blocks, sets, which, err);
+    else k_tc_gemm<32><<<nblocks, TC_THREADS, smem, s>>>(blocks, sets, which, err);
     return 0;
 }
 

@@ -21,17 +21,19 @@
 // 128-byte row per load case), already split into its TF32 part and the
 // TF32 remainder.
 //
-// One CTA of 6 warps per (subdomain, 128-row block):
+// One CTA of 10 warps per (subdomain, 128-row block), two CTAs per SM:
 //   * warp 0, one thread: bulk-copy producer (A slab or its four transposed
 //     pieces, X_hi, X_lo per stage);
-//   * warps 2-5: form A_lo = rna_tf32(A - trunc_tf32(A)) of every landed A
+//   * warps 2-9 (two per TMEM lane quarter, taking alternate K steps, so
+//     two K steps are split at once): form A_lo = rna_tf32(A - trunc_tf32(A)) of every landed A
 //     slab and store it into one of TC_LO 32-column TMEM buffers
 //     (tcgen05.st; the MMA reads the FP32 slab itself as A_hi: a TF32
 //     operand's low 13 mantissa bits do not take part in the product; a
 //     transposed step is first transposed in place, each warp inside its own
 //     4 KB), then hand the stage to the MMA issuer;
 //     at the end they read the accumulators out of TMEM (warp w owns TMEM
-//     lanes 32 (w mod 4) .. +31) and write y in FP64;
+//     lanes 32 (w mod 4) .. +31, and half of the load cases) and write y in
+//     FP64;
 //   * warp 1, one thread: issues the MMAs (M=128, N=k, K=8 per instruction,
 //     4 per slab).
 // Products per K step of 8: A_hi [X_hi | X_lo] as one N = 2k MMA (A_hi read
@@ -160,7 +162,6 @@ __device__ __forceinline__ void mma_tf32_ts(uint32_t d, uint32_t a_tmem, uint64_
 }
 
 constexpr int TC_NACC = 2;                   // rotating accumulator groups
-constexpr int TC_THREADS = 192;
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -175,11 +176,16 @@ __device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uin
         : "memory");
 }
 
-// 16 or 32 consecutive FP32 columns of this warp's 32 TMEM lanes, added into acc
+// 8, 16 or 32 consecutive FP32 columns of this warp's 32 TMEM lanes, added into acc
 template <int N>
 __device__ __forceinline__ void tmem_add(uint32_t taddr, double *acc) {
     uint32_t r[N];
-    if constexpr (N == 16) {
+    if constexpr (N == 8) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                       "=r"(r[7])
+                     : "r"(taddr));
+    } else if constexpr (N == 16) {
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
@@ -201,10 +207,9 @@ __device__ __forceinline__ void tmem_add(uint32_t taddr, double *acc) {
     for (int j = 0; j < N; ++j) acc[j] += (double)__uint_as_float(r[j]);
 }
 
-// which = 0: F product (A = the set's F slabs) with the coarse correction
-// y_b -= V_d s_d in the epilogue (V_d = [F_d Bc_d^T, -R_d] FP64, s_d the
-// cluster coarse solution at the subdomain's Bc rows and alpha slot);
-// which = 1: S product (A = the set's S slabs), no correction.
+// which = 0: F product (A = the set's F slabs; its coarse correction
+// y_b -= V_d s_d runs afterwards in k_correct_multi); which = 1: S product
+// (A = the set's S slabs).
 template <int K>
 __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__restrict__ blocks,
                                                            const TcSet *__restrict__ sets, int which,
@@ -236,13 +241,12 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
     const float *__restrict__ Xs = ts.Xs;
     const long long xlo_off = ts.xlo;
     double *__restrict__ yb = ts.yb;
-    const double *__restrict__ scoarse = which == 0 ? ts.sc : nullptr;
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&split[s], 4);                      // one arrival per splitting warp
+            mbar_init(&split[s], 4);                      // one arrival per splitting warp of the stage
             mbar_init(&empty[s], 1);
         }
         for (int s = 0; s < TC_LO; ++s) mbar_init(&lo_empty[s], 1);
@@ -329,9 +333,13 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                              smem_u32(&done))
                          : "memory");
         }
-    } else {
-        // warps 2-5: split the A slab of every stage, then the epilogue
-        for (int kk = 0; kk < g.ks; ++kk) {
+    } else if (warp >= 2) {
+        // warps 2-9: split the A slab of every stage, then the epilogue.  Warp w
+        // may access TMEM lanes 32 (w mod 4) .. +31 (its quarter); the two warps
+        // of a quarter take alternate K steps (h = (w - 2) / 4: steps kk with
+        // kk mod 2 = h), so a stage is always split by the same four warps
+        const int quarter = warp & 3, h = (warp - 2) >> 2;
+        for (int kk = h; kk < g.ks; kk += 2) {
             const int s = kk % TC_STAGES, lb = kk % TC_LO;
             // the A_lo buffer of slab kk - TC_LO is free once its MMAs completed; the A slab has landed
             bool ok = kk < TC_LO || mbar_wait(&lo_empty[lb], ((kk / TC_LO) - 1) & 1);
@@ -341,8 +349,6 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
                 abort_flag = 1;
                 break;
             }
-            // warp w handles rows 32 (w mod 4) .. +31, the TMEM lanes it may access
-            const int quarter = warp & 3;
             const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16) + LO_COL + 32u * uint32_t(lb);
             if (kk < g.kd) {                              // stored slab: A_lo of this warp's rows
                 split_direct(sA + s * TC_SLAB_A, quarter * 32 + lane, taddr);
@@ -360,77 +366,35 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__re
             if (lane == 0) mbar_arrive(&split[s]);
         }
         __syncwarp();
-        if (scoarse) {                                   // warm L2 with this row's V entries while the last MMAs run
-            const SubDev &sd = ts.subs[g.d];
-            const int prow = (warp & 3) * 32 + lane;
-            if (prow < g.rows) {
-                const double *Vr = ts.V + sd.V_off + 128 * g.m + prow;
-                for (int q = 0; q < sd.c + 6; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(Vr + (size_t)q * sd.nbp));
-            }
-        }
+        // epilogue: this warp's 32 rows x the K/2 load cases of half h
+        constexpr int KH = K / 2;
         const bool have = __all_sync(0xffffffffu, mbar_wait(&done, 0));   // warp-uniform before the .sync.aligned loads
         __syncwarp();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const int quarter = warp & 3;                     // TMEM lanes this warp may read
-        const int row = quarter * 32 + lane;
-        double acc[K];
+        double acc[KH];
 #pragma unroll
-        for (int j = 0; j < K; ++j) acc[j] = 0.0;
+        for (int j = 0; j < KH; ++j) acc[j] = 0.0;
         const bool go = __all_sync(0xffffffffu, have && !abort_flag);
         if (!have) {
             if (lane == 0) atomicExch(err, HTF_ETIMEDOUT);
         } else if (go) {
-            const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16);
+            const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(h * KH);
             const int nacc = g.ks < TC_NACC ? g.ks : TC_NACC;
             for (int a = 0; a < nacc; ++a) {
-                tmem_add<K>(taddr + uint32_t(a * GW), acc);
-                tmem_add<K>(taddr + uint32_t(a * GW + K), acc);
+                tmem_add<KH>(taddr + uint32_t(a * GW), acc);
+                tmem_add<KH>(taddr + uint32_t(a * GW + K), acc);
             }
-        }
-        if (scoarse) {
-            // s_d staged in the (now idle) stage buffers by the four epilogue warps
-            const SubDev &sd = ts.subs[g.d];
-            const int gc_off = ts.cl[sd.cluster].gc_off;
-            const int nc = sd.c + 6;
-            double *ss = reinterpret_cast<double *>(base);
-            for (int o = threadIdx.x - 64; o < nc * K; o += 128) {
-                const int q = o / K, j = o % K;
-                const int pos = q < sd.c ? ts.bcr[sd.bcr_off + q] : sd.alpha_pos + (q - sd.c);
-                ss[o] = scoarse[((size_t)gc_off + pos) * K + j];
-            }
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-            if (row < g.rows) {
-                // V entries in groups of 8 independent loads
-                const double *Vr = ts.V + sd.V_off + 128 * g.m + row;
-                int q = 0;
-                for (; q + 8 <= nc; q += 8) {
-                    double v[8];
+            // the warp's 32 rows x KH columns through shared memory (row stride KH + 1
+            // doubles; the stage buffers are idle: every copy landed before the last
+            // MMA completed), stored as 32 segments of KH contiguous doubles
+            double *st = reinterpret_cast<double *>(base) + (warp - 2) * 32 * (KH + 1);
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) v[u] = Vr[(size_t)(q + u) * sd.nbp];
-#pragma unroll
-                    for (int u = 0; u < 8; ++u)
-#pragma unroll
-                        for (int j = 0; j < K; ++j) acc[j] -= v[u] * ss[(q + u) * K + j];
-                }
-                for (; q < nc; ++q) {
-                    const double vq = Vr[(size_t)q * sd.nbp];
-#pragma unroll
-                    for (int j = 0; j < K; ++j) acc[j] -= vq * ss[q * K + j];
-                }
-            }
-            asm volatile("bar.sync 1, 128;" ::: "memory");   // ss is overwritten below
-        }
-        if (go) {
-            // each warp's 32 output rows are contiguous in yb: transpose them
-            // through shared memory (row stride K+1 doubles) and store coalesced
-            double *st = reinterpret_cast<double *>(base) + quarter * 32 * (K + 1);
-#pragma unroll
-            for (int j = 0; j < K; ++j) st[lane * (K + 1) + j] = acc[j];
+            for (int j = 0; j < KH; ++j) st[lane * (KH + 1) + j] = acc[j];
             __syncwarp();
             const int r0 = quarter * 32;
             const int nrow = min(32, g.rows - r0);
-            double *y = yb + (g.y_row0 + r0) * K;
-            for (int e = lane; e < nrow * K; e += 32) y[e] = st[(e / K) * (K + 1) + (e % K)];
+            double *y = yb + (g.y_row0 + r0) * K + h * KH;
+            for (int e = lane; e < nrow * KH; e += 32) y[(e / KH) * K + (e % KH)] = st[(e / KH) * (KH + 1) + (e % KH)];
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
