@@ -37,10 +37,9 @@ __device__ __forceinline__ float tf32_trunc(float a) { return __uint_as_float(__
 
 constexpr int TILE = 32;                  // packed tile edge
 constexpr int CHOL_STEP = 64;             // columns per batched Cholesky step (two factor panels)
-constexpr int TC_STAGES = 8;              // pipeline stages of the tensor-core product (one CTA per SM)
+constexpr int TC_STAGES = 4;              // pipeline stages of the tensor-core product (2 CTAs per SM)
 constexpr int TC_LO = 4;                  // A_lo buffers (in TMEM) of the tensor-core product
-constexpr int TC_THREADS = 448;           // threads of the tensor-core product: producer, MMA, 8 splitting
-                                          // warps, 4 epilogue warps
+constexpr int TC_THREADS = 320;           // threads of the tensor-core product: producer, MMA, 8 splitting warps
 constexpr int TILE_ELEMS = TILE * TILE;
 
 struct SubDev {

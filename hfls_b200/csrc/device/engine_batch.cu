@@ -26,7 +26,7 @@
 namespace htf {
 
 template <int K>
-__global__ void k_tc_gemm(const GemmBlock *, int, const TcSet *, int, int *);
+__global__ void k_tc_gemm(const GemmBlock *, const TcSet *, int, int *);
 __global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *);
 __global__ void k_gather_multi(int, int, const int *, const int *, const double *, const double *, double *, float *,
                                float *);
@@ -139,6 +139,7 @@ int Engine::setup_batch(int K, std::string &err) {
     k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_F_, d_AF_);
     k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_S_, d_AS_);
     CKB(cudaGetLastError());
+    // TC_STAGES stages of A (16 KB), X_hi, X_lo (k x 128 B each) + alignment slack (A_lo lives in TMEM)
     tc_smem_ = tc_smem_bytes(K);
     if (K == 16)
         CKB(cudaFuncSetAttribute(k_tc_gemm<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_));
@@ -209,21 +210,12 @@ void Engine::profile_batch_gather(const double *w) {
 int tc_launch(int K, const GemmBlock *blocks, int nblocks, const TcSet *sets, int which, int smem, int *err,
               cudaStream_t s) {
     if (nblocks <= 0) return 0;
-    // persistent: one CTA per SM (the SM count cached per device)
-    static int sms[64] = {0};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
-    if (sms[dev] == 0 && cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-        return 1;
-    const int grid = std::min(nblocks, sms[dev]);
-    if (K == 16) k_tc_gemm<16><<<grid, TC_THREADS, smem, s>>>(blocks, nblocks, sets, which, err);
-    else k_tc_gemm<32><<<grid, TC_THREADS, smem, s>>>(blocks, nblocks, sets, which, err);
+    if (K == 16) k_tc_gemm<16><<<nblocks, TC_THREADS, smem, s>>>(blocks, sets, which, err);
+    else k_tc_gemm<32><<<nblocks, TC_THREADS, smem, s>>>(blocks, sets, which, err);
     return 0;
 }
 
-// TC_STAGES stages of A (16 KB), X_hi, X_lo (k x 128 B each), the epilogue's
-// transpose buffers (4 warps x 32 rows x (k/2 + 1) doubles), alignment slack
-int tc_smem_bytes(int K) { return 1024 + TC_STAGES * (128 * 32 + 2 * K * 32) * 4 + 4 * 32 * (K / 2 + 1) * 8; }
+int tc_smem_bytes(int K) { return 1024 + TC_STAGES * (128 * 32 + 2 * K * 32) * 4; }
 
 void Engine::tc_apply(int which) {
     tc_launch(bK_, static_cast<const GemmBlock *>(d_blocks_), nblocks_, d_tcset_, which, tc_smem_, d_tcerr_, s_);

@@ -210,48 +210,38 @@ __device__ __forceinline__ void tmem_add(uint32_t taddr, double *acc) {
 // which = 0: F product (A = the set's F slabs; its coarse correction
 // y_b -= V_d s_d runs afterwards in k_correct_multi); which = 1: S product
 // (A = the set's S slabs).
-//
-// Persistent: one CTA per SM (grid = min(blocks, SMs)); CTA c takes the
-// work items (subdomain, 128-row block) c, c + G, c + 2G, ... and every
-// role walks them in that order, counting K steps t across items, so the
-// copy pipeline runs on from one item into the next: stage t mod TC_STAGES,
-// A_lo buffer t mod TC_LO.  Accumulators ping-pong between two TMEM sets
-// (item l in set l mod 2): the MMAs of item l + 1 run while the epilogue
-// warps read item l out.  TC_STAGES and TC_LO are even so that a stage (and
-// an A_lo buffer) is always split by the same four warps, which wait on its
-// phases in order.
 template <int K>
-__global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__restrict__ blocks, int nblocks,
+__global__ void __launch_bounds__(TC_THREADS, 2) k_tc_gemm(const GemmBlock *__restrict__ blocks,
                                                            const TcSet *__restrict__ sets, int which,
                                                            int *__restrict__ err) {
     static_assert(K == 16 || K == 32, "N of the MMA");
-    static_assert(TC_STAGES % 2 == 0 && TC_LO % 2 == 0, "stages and A_lo buffers alternate between split groups");
     constexpr int SLAB_B = K * 32;                        // floats per X slab
     constexpr unsigned STAGE_TX = (TC_SLAB_A + 2 * SLAB_B) * 4;
-    constexpr int KH = K / 2;                             // load cases per epilogue pass
-    constexpr int GW = 2 * K;                             // TMEM columns per accumulator group
-    constexpr int SETW = TC_NACC * GW;                    // TMEM columns per accumulator set
-    // TMEM: two accumulator sets of TC_NACC groups (A_hi X_hi, then A_hi X_lo +
-    // A_lo X_hi, the two small terms sharing one FP32 accumulator), then TC_LO
-    // A_lo buffers of 32 columns each
-    constexpr uint32_t LO_COL = 2 * SETW;
-    constexpr uint32_t TMEM_COLS = (LO_COL + 32 * TC_LO) <= 256 ? 256 : 512;
+    constexpr int GW = 2 * K;                              // TMEM columns per accumulator group
+    // TMEM: the accumulator groups (TC_NACC x GW columns: A_hi X_hi, then
+    // A_hi X_lo + A_lo X_hi, the two small terms sharing one FP32 accumulator),
+    // then TC_LO A_lo buffers of 32 columns each (A_lo of K slab kk in buffer
+    // kk mod TC_LO)
+    constexpr uint32_t LO_COL = TC_NACC * GW;
+    constexpr uint32_t TMEM_COLS = 256;                   // power of two >= LO_COL + 32 TC_LO
     static_assert(LO_COL + 32 * TC_LO <= TMEM_COLS, "TMEM columns");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // 1024-byte aligned buffers: stage s holds A (FP32) and X_hi, X_lo (copied
-    // from HBM); then the epilogue's transpose buffers (4 warps x 32 x (KH + 1))
+    // 1024-byte aligned buffers: stage s holds A (FP32) and X_hi, X_lo (copied from HBM)
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     float *sA = reinterpret_cast<float *>(base);                          // TC_STAGES x 16 KB
     float *sB = reinterpret_cast<float *>(base + TC_STAGES * TC_SLAB_A * 4);
-    double *sY = reinterpret_cast<double *>(base + TC_STAGES * (TC_SLAB_A + 2 * SLAB_B) * 4);
-    __shared__ __align__(8) uint64_t full[TC_STAGES], split[TC_STAGES], empty[TC_STAGES], lo_empty[TC_LO];
-    __shared__ __align__(8) uint64_t acc_full[2], acc_empty[2];
+    __shared__ __align__(8) uint64_t full[TC_STAGES], split[TC_STAGES], empty[TC_STAGES], lo_empty[TC_LO], done;
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
 
+    const GemmBlock g = blocks[blockIdx.x];
+    const TcSet &ts = sets[g.set];
+    const float *__restrict__ A = which == 0 ? ts.AF : ts.AS;
+    const float *__restrict__ Xs = ts.Xs;
+    const long long xlo_off = ts.xlo;
+    double *__restrict__ yb = ts.yb;
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const int G = gridDim.x;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; ++s) {
@@ -260,10 +250,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__re
             mbar_init(&empty[s], 1);
         }
         for (int s = 0; s < TC_LO; ++s) mbar_init(&lo_empty[s], 1);
-        for (int s = 0; s < 2; ++s) {
-            mbar_init(&acc_full[s], 1);
-            mbar_init(&acc_empty[s], 4);                  // one arrival per epilogue warp
-        }
+        mbar_init(&done, 1);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -280,172 +267,134 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__re
 
     if (warp == 0) {
         if (lane == 0) {                                  // producer
-            long long t = 0, issued = 0;
-            for (int item = blockIdx.x; item < nblocks && !abort_flag; item += G) {
-                const GemmBlock g = blocks[item];
-                const TcSet &ts = sets[g.set];
-                const float *__restrict__ A = which == 0 ? ts.AF : ts.AS;
-                // first stored slab of the subdomain: block m' starts 2 m' (m' + 1) slabs after it
-                const long long a0 = g.a_off - 2LL * g.m * (g.m + 1) * TC_SLAB_A;
-                for (int kk = 0; kk < g.ks; ++kk, ++t) {
-                    const int s = int(t % TC_STAGES);
-                    if (t >= TC_STAGES && !mbar_wait(&empty[s], unsigned((t / TC_STAGES) - 1) & 1u)) {
-                        atomicExch(err, HTF_ETIMEDOUT);
-                        abort_flag = 1;
-                    }
-                    if (abort_flag) break;
-                    mbar_expect_tx(&full[s], STAGE_TX);
-                    if (kk < g.kd) {
-                        bulk_g2s(sA + s * TC_SLAB_A, A + g.a_off + (long long)kk * TC_SLAB_A, TC_SLAB_A * 4,
-                                 &full[s]);
-                    } else {
-                        // above the diagonal block: rows [32 kk, 32 kk + 32) of the stored slabs
-                        // (kk / 4, 4 m + p), p = 0..3, i.e. 32 rows x 128 columns of the transpose;
-                        // each 32-row piece is 4 KB contiguous (8-row swizzle groups of 1 KB)
-                        const int mp = kk >> 2, q = kk & 3;
-                        const float *src = A + a0 + (2LL * mp * (mp + 1) + 4LL * g.m) * TC_SLAB_A + q * 1024;
-#pragma unroll
-                        for (int p = 0; p < 4; ++p)
-                            bulk_g2s(sA + s * TC_SLAB_A + p * 1024, src + (long long)p * TC_SLAB_A, 4096, &full[s]);
-                    }
-                    bulk_g2s(sB + s * 2 * SLAB_B, ts.Xs + g.x_off + (long long)kk * SLAB_B, SLAB_B * 4, &full[s]);
-                    bulk_g2s(sB + (s * 2 + 1) * SLAB_B, ts.Xs + ts.xlo + g.x_off + (long long)kk * SLAB_B,
-                             SLAB_B * 4, &full[s]);
-                    ++issued;
+            int issued = 0;
+            // first stored slab of the subdomain: block m' starts 2 m' (m' + 1) slabs after it
+            const long long a0 = g.a_off - 2LL * g.m * (g.m + 1) * TC_SLAB_A;
+            for (int kk = 0; kk < g.ks; ++kk) {
+                const int s = kk % TC_STAGES;
+                if (kk >= TC_STAGES && !mbar_wait(&empty[s], ((kk / TC_STAGES) - 1) & 1)) {
+                    atomicExch(err, HTF_ETIMEDOUT);
+                    abort_flag = 1;
+                    break;
                 }
+                if (abort_flag) break;
+                mbar_expect_tx(&full[s], STAGE_TX);
+                if (kk < g.kd) {
+                    bulk_g2s(sA + s * TC_SLAB_A, A + g.a_off + (long long)kk * TC_SLAB_A, TC_SLAB_A * 4, &full[s]);
+                } else {
+                    // above the diagonal block: rows [32 kk, 32 kk + 32) of the stored slabs
+                    // (kk / 4, 4 m + p), p = 0..3, i.e. 32 rows x 128 columns of the transpose;
+                    // each 32-row piece is 4 KB contiguous (8-row swizzle groups of 1 KB)
+                    const int mp = kk >> 2, q = kk & 3;
+                    const float *src = A + a0 + (2LL * mp * (mp + 1) + 4LL * g.m) * TC_SLAB_A + q * 1024;
+#pragma unroll
+                    for (int p = 0; p < 4; ++p)
+                        bulk_g2s(sA + s * TC_SLAB_A + p * 1024, src + (long long)p * TC_SLAB_A, 4096, &full[s]);
+                }
+                bulk_g2s(sB + s * 2 * SLAB_B, Xs + g.x_off + (long long)kk * SLAB_B, SLAB_B * 4, &full[s]);
+                bulk_g2s(sB + (s * 2 + 1) * SLAB_B, Xs + xlo_off + g.x_off + (long long)kk * SLAB_B, SLAB_B * 4,
+                         &full[s]);
+                ++issued;
             }
             // before the CTA may exit: the last copy into every stage has landed (bounded)
-            for (long long u = (issued > TC_STAGES ? issued - TC_STAGES : 0); u < issued; ++u)
-                if (!mbar_wait(&full[u % TC_STAGES], unsigned(u / TC_STAGES) & 1u)) atomicExch(err, HTF_ETIMEDOUT);
+            for (int kk = (issued > TC_STAGES ? issued - TC_STAGES : 0); kk < issued; ++kk)
+                if (!mbar_wait(&full[kk % TC_STAGES], (kk / TC_STAGES) & 1)) atomicExch(err, HTF_ETIMEDOUT);
         }
     } else if (warp == 1) {
         if (lane == 0) {                                  // MMA issuer
             const uint32_t idesc = tf32_idesc(128, K), idesc2 = tf32_idesc(128, 2 * K);
-            long long t = 0;
-            int li = 0;
-            for (int item = blockIdx.x; item < nblocks && !abort_flag; item += G, ++li) {
-                const GemmBlock g = blocks[item];
-                const int set = li & 1;
-                // the epilogue has read this set out of TMEM (item li - 2)
-                if (li >= 2 && !mbar_wait(&acc_empty[set], unsigned((li >> 1) - 1) & 1u)) {
+            for (int kk = 0; kk < g.ks; ++kk) {
+                const int s = kk % TC_STAGES;
+                if (abort_flag || !mbar_wait(&split[s], (kk / TC_STAGES) & 1)) {
                     atomicExch(err, HTF_ETIMEDOUT);
                     abort_flag = 1;
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t d0 = tmem + uint32_t(set * SETW);
-                for (int kk = 0; kk < g.ks; ++kk, ++t) {
-                    const int s = int(t % TC_STAGES);
-                    if (abort_flag || !mbar_wait(&split[s], unsigned(t / TC_STAGES) & 1u)) {
-                        atomicExch(err, HTF_ETIMEDOUT);
-                        abort_flag = 1;
-                        break;
-                    }
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t d = d0 + uint32_t((kk % TC_NACC) * GW);   // [hi-hi | hi-lo + lo-hi]
-                    const uint64_t da = sw128_desc(sA + s * TC_SLAB_A);
-                    const uint32_t tal = tmem + LO_COL + 32u * uint32_t(t % TC_LO);   // A_lo in TMEM
-                    const uint64_t db = sw128_desc(sB + s * 2 * SLAB_B);      // X_hi, X_lo: 2k rows
+                const uint32_t d = tmem + uint32_t((kk % TC_NACC) * GW);   // [hi-hi | hi-lo + lo-hi]
+                const uint64_t da = sw128_desc(sA + s * TC_SLAB_A);
+                const uint32_t tal = tmem + LO_COL + 32u * uint32_t(kk % TC_LO);   // A_lo in TMEM
+                const uint64_t db = sw128_desc(sB + s * 2 * SLAB_B);      // X_hi, X_lo: 2k rows
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {          // 4 x K=8 (32 bytes) per slab
-                        const uint32_t acc = (kk >= TC_NACC || q > 0) ? 1u : 0u;
-                        mma_tf32(d, da + 2ull * q, db + 2ull * q, idesc2, acc);
-                        // issued after the first, which initialised these columns
-                        mma_tf32_ts(d + K, tal + 8u * q, db + 2ull * q, idesc, 1u);
-                    }
-                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                     smem_u32(&empty[s]))
-                                 : "memory");
-                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                     smem_u32(&lo_empty[t % TC_LO]))
-                                 : "memory");
+                for (int q = 0; q < 4; ++q) {              // 4 x K=8 (32 bytes) per slab
+                    const uint32_t acc = (kk >= TC_NACC || q > 0) ? 1u : 0u;
+                    mma_tf32(d, da + 2ull * q, db + 2ull * q, idesc2, acc);
+                    // issued after the first, which initialised these columns
+                    mma_tf32_ts(d + K, tal + 8u * q, db + 2ull * q, idesc, 1u);
                 }
-                if (abort_flag) break;
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 smem_u32(&acc_full[set]))
+                                 smem_u32(&empty[s]))
+                             : "memory");
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&lo_empty[kk % TC_LO]))
                              : "memory");
             }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&done))
+                         : "memory");
         }
-    } else if (warp < 10) {
-        // warps 2-9: split the A slab of every step.  Warp w may access TMEM
-        // lanes 32 (w mod 4) .. +31 (its quarter); the two warps of a quarter
-        // take alternate steps (h = (w - 2) / 4: steps t with t mod 2 = h)
+    } else if (warp >= 2) {
+        // warps 2-9: split the A slab of every stage, then the epilogue.  Warp w
+        // may access TMEM lanes 32 (w mod 4) .. +31 (its quarter); the two warps
+        // of a quarter take alternate K steps (h = (w - 2) / 4: steps kk with
+        // kk mod 2 = h), so a stage is always split by the same four warps
         const int quarter = warp & 3, h = (warp - 2) >> 2;
-        long long t = 0;
-        bool stop = false;
-        for (int item = blockIdx.x; item < nblocks && !stop; item += G) {
-            const GemmBlock g = blocks[item];
-            for (int kk = 0; kk < g.ks; ++kk, ++t) {
-                if (int(t & 1) != h) continue;
-                const int s = int(t % TC_STAGES), lb = int(t % TC_LO);
-                // the A_lo buffer of step t - TC_LO is free once its MMAs completed; the A slab has landed
-                bool ok = t < TC_LO || mbar_wait(&lo_empty[lb], unsigned((t / TC_LO) - 1) & 1u);
-                ok = __all_sync(0xffffffffu, ok && mbar_wait(&full[s], unsigned(t / TC_STAGES) & 1u));
-                if (!__all_sync(0xffffffffu, ok && !abort_flag)) {      // warp-uniform exit
-                    if (lane == 0 && !ok) atomicExch(err, HTF_ETIMEDOUT);
-                    abort_flag = 1;
-                    stop = true;
-                    break;
-                }
-                const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16) + LO_COL + 32u * uint32_t(lb);
-                if (kk < g.kd) {                          // stored slab: A_lo of this warp's rows
-                    split_direct(sA + s * TC_SLAB_A, quarter * 32 + lane, taddr);
-                } else {
-                    // transposed pieces: the warp owns piece p = quarter (4 KB at p * 1024 floats),
-                    // whose column l is row 32 p + l of this K step's A; the output rows 32 p ..
-                    // 32 p + 31 of the K-major slab occupy the same 4 KB, so the transpose stays
-                    // inside the warp
-                    split_transposed(sA + s * TC_SLAB_A + quarter * 1024, lane, taddr);
-                }
-                // generic-proxy writes become visible to the tensor core's async proxy, TMEM
-                // stores are ordered before the hand-off
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&split[s]);
-            }
-        }
-    } else {
-        // warps 10-13: the epilogue of every item, TMEM lanes of quarter warp mod 4,
-        // in two passes of KH load cases; y in FP64 through shared memory
-        const int quarter = warp & 3;
-        double *st = sY + (warp - 10) * 32 * (KH + 1);
-        int li = 0;
-        for (int item = blockIdx.x; item < nblocks; item += G, ++li) {
-            const GemmBlock g = blocks[item];
-            const int set = li & 1;
-            const bool have = __all_sync(0xffffffffu, !abort_flag && mbar_wait(&acc_full[set], unsigned(li >> 1) & 1u));
-            if (!have) {
-                if (lane == 0 && !abort_flag) atomicExch(err, HTF_ETIMEDOUT);
+        for (int kk = h; kk < g.ks; kk += 2) {
+            const int s = kk % TC_STAGES, lb = kk % TC_LO;
+            // the A_lo buffer of slab kk - TC_LO is free once its MMAs completed; the A slab has landed
+            bool ok = kk < TC_LO || mbar_wait(&lo_empty[lb], ((kk / TC_LO) - 1) & 1);
+            ok = __all_sync(0xffffffffu, ok && mbar_wait(&full[s], (kk / TC_STAGES) & 1));
+            if (!__all_sync(0xffffffffu, ok && !abort_flag)) {          // warp-uniform exit
+                if (lane == 0 && !ok) atomicExch(err, HTF_ETIMEDOUT);
                 abort_flag = 1;
                 break;
             }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(set * SETW);
-            const int nacc = g.ks < TC_NACC ? g.ks : TC_NACC;
-            double *y = sets[g.set].yb + (g.y_row0 + quarter * 32) * K;
-            const int nrow = min(32, g.rows - quarter * 32);
-#pragma unroll 1
-            for (int half = 0; half < 2; ++half) {
-                double acc[KH];
-#pragma unroll
-                for (int j = 0; j < KH; ++j) acc[j] = 0.0;
-                for (int a = 0; a < nacc; ++a) {
-                    tmem_add<KH>(taddr + uint32_t(a * GW + half * KH), acc);
-                    tmem_add<KH>(taddr + uint32_t(a * GW + K + half * KH), acc);
-                }
-                if (half == 1) {                          // the set is read out: the MMAs of item li + 2 may start
-                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&acc_empty[set]);
-                }
-#pragma unroll
-                for (int j = 0; j < KH; ++j) st[lane * (KH + 1) + j] = acc[j];
-                __syncwarp();
-                for (int e = lane; e < nrow * KH; e += 32)
-                    y[(e / KH) * K + half * KH + (e % KH)] = st[(e / KH) * (KH + 1) + (e % KH)];
-                __syncwarp();
+            const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16) + LO_COL + 32u * uint32_t(lb);
+            if (kk < g.kd) {                              // stored slab: A_lo of this warp's rows
+                split_direct(sA + s * TC_SLAB_A, quarter * 32 + lane, taddr);
+            } else {
+                // transposed pieces: the warp owns piece p = quarter (4 KB at p * 1024 floats), whose
+                // column l is row 32 p + l of this K step's A; the output rows 32 p .. 32 p + 31
+                // of the K-major slab occupy the same 4 KB, so the transpose stays inside the warp
+                split_transposed(sA + s * TC_SLAB_A + quarter * 1024, lane, taddr);
             }
+            // generic-proxy writes become visible to the tensor core's async proxy, TMEM stores
+            // are ordered before the hand-off
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&split[s]);
+        }
+        __syncwarp();
+        // epilogue: this warp's 32 rows x the K/2 load cases of half h
+        constexpr int KH = K / 2;
+        const bool have = __all_sync(0xffffffffu, mbar_wait(&done, 0));   // warp-uniform before the .sync.aligned loads
+        __syncwarp();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        double acc[KH];
+#pragma unroll
+        for (int j = 0; j < KH; ++j) acc[j] = 0.0;
+        const bool go = __all_sync(0xffffffffu, have && !abort_flag);
+        if (!have) {
+            if (lane == 0) atomicExch(err, HTF_ETIMEDOUT);
+        } else if (go) {
+            const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(h * KH);
+            const int nacc = g.ks < TC_NACC ? g.ks : TC_NACC;
+            for (int a = 0; a < nacc; ++a) {
+                tmem_add<KH>(taddr + uint32_t(a * GW), acc);
+                tmem_add<KH>(taddr + uint32_t(a * GW + K), acc);
+            }
+            // the warp's 32 rows x KH columns through shared memory (row stride KH + 1
+            // doubles; the stage buffers are idle: every copy landed before the last
+            // MMA completed), stored as 32 segments of KH contiguous doubles
+            double *st = reinterpret_cast<double *>(base) + (warp - 2) * 32 * (KH + 1);
+#pragma unroll
+            for (int j = 0; j < KH; ++j) st[lane * (KH + 1) + j] = acc[j];
+            __syncwarp();
+            const int r0 = quarter * 32;
+            const int nrow = min(32, g.rows - r0);
+            double *y = yb + (g.y_row0 + r0) * K + h * KH;
+            for (int e = lane; e < nrow * KH; e += 32) y[(e / KH) * K + (e % KH)] = st[(e / KH) * (KH + 1) + (e % KH)];
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -456,8 +405,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_gemm(const GemmBlock *__re
     }
 }
 
-template __global__ void k_tc_gemm<16>(const GemmBlock *, int, const TcSet *, int, int *);
-template __global__ void k_tc_gemm<32>(const GemmBlock *, int, const TcSet *, int, int *);
+template __global__ void k_tc_gemm<16>(const GemmBlock *, const TcSet *, int, int *);
+template __global__ void k_tc_gemm<32>(const GemmBlock *, const TcSet *, int, int *);
 
 // FP32 slabs of the lower triangle (at 128-row block granularity) of a packed
 // symmetric FP64 tile matrix: slab (m, kk), kk < kd, of subdomain d holds
