@@ -112,6 +112,53 @@ __global__ void __launch_bounds__(256) k_gemm_batched(const GemmDesc *__restrict
     }
 }
 
+// Cluster Fc = sum_d Bc_d F_d Bc_d^T (Cluster.cpp:190-198) assembled in place
+// from the subdomains' c x c blocks: one CTA per cluster adds its subdomains'
+// blocks one after another (in cluster order, the host's order; the targets
+// inside one block are distinct), so every entry gets its contributions in
+// the same order as a sequential host loop.  F is zero on entry.
+__global__ void __launch_bounds__(1024) k_assemble_Fc(const SubDev *__restrict__ subs,
+                                                      const int *__restrict__ cl_ptr, const int *__restrict__ cl_subs,
+                                                      const int *__restrict__ bcr, const long long *__restrict__ fco,
+                                                      const double *__restrict__ Fc, const long long *__restrict__ oF,
+                                                      const int *__restrict__ ncs, double *__restrict__ F) {
+    const int ci = blockIdx.x, nc = ncs[ci];
+    double *Fcl = F + oF[ci];
+    for (int k = cl_ptr[ci]; k < cl_ptr[ci + 1]; ++k) {
+        const int d = cl_subs[k];
+        const SubDev &sd = subs[d];
+        const int c = sd.c;
+        const int *rows = bcr + sd.bcr_off;
+        const double *B = Fc + fco[d];
+        for (int e = threadIdx.x; e < c * c; e += blockDim.x) {
+            const int i = e % c, j = e / c;
+            double *t = Fcl + rows[i] + (size_t)rows[j] * nc;
+            *t = __dadd_rn(*t, B[i + (size_t)j * c]);
+        }
+        __syncthreads();
+    }
+}
+
+// Cluster Gc = -Bc R (Cluster.cpp:190-198): thread (subdomain d, mode j) owns
+// column 6 k + j of its cluster's Gc (k = d's position in the cluster) and
+// subtracts its Bc entries' products in the host's entry order, rounded as
+// the host rounds them (product, then difference).  G is zero on entry.
+__global__ void k_assemble_Gc(int ns, const SubDev *__restrict__ subs, const int *__restrict__ cl_index,
+                              const int *__restrict__ e_ptr, const int *__restrict__ e_row,
+                              const int *__restrict__ e_pl, const double *__restrict__ e_val,
+                              const double *__restrict__ R, const long long *__restrict__ oG,
+                              const int *__restrict__ ncs, double *__restrict__ G) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 6 * ns) return;
+    const int d = t / 6, j = t % 6;
+    const SubDev &sd = subs[d];
+    const int nc = ncs[sd.cluster];
+    double *col = G + oG[sd.cluster] + (size_t)(6 * cl_index[d] + j) * nc;
+    const double *Rj = R + sd.R_off + (size_t)j * sd.N;
+    for (int e = e_ptr[d]; e < e_ptr[d + 1]; ++e)
+        col[e_row[e]] = __dsub_rn(col[e_row[e]], __dmul_rn(e_val[e], Rj[e_pl[e]]));
+}
+
 // grid: (blocks of the largest copy, copies)
 __global__ void k_copy_batched(const CopyDesc *__restrict__ desc) {
     const CopyDesc c = desc[blockIdx.y];
@@ -175,7 +222,8 @@ static cudaError_t chol_batched(const std::vector<SubDev> &hm, const SubDev *dm,
         flat.insert(flat.end(), v.begin(), v.end());
     }
     if (flat.empty()) return cudaSuccess;
-    cudaError_t e = cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_syrk_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM);
+    if (e != cudaSuccess) return e;
     StepDesc *d = tmp.get<StepDesc>(flat.size(), e);
     if (e != cudaSuccess) return e;
     e = cudaMemcpyAsync(d, flat.data(), flat.size() * sizeof(StepDesc), cudaMemcpyHostToDevice, s);
@@ -184,7 +232,7 @@ static cudaError_t chol_batched(const std::vector<SubDev> &hm, const SubDev *dm,
         const int cnt = int(steps[st].size());
         k_potrf_diag<<<cnt, CHOL_STEP, 0, s>>>(d + off[st], dm, buf, status);
         if (nrb[st] > 0) k_trsm_panel<<<nrb[st], 128, 0, s>>>(d + off[st], cnt, dm, buf);
-        if (ntri[st] > 0) k_syrk_update<<<ntri[st], 256, 0, s>>>(d + off[st], cnt, dm, buf);
+        if (ntri[st] > 0) k_syrk_update<<<ntri[st], 256, SYRK_SMEM, s>>>(d + off[st], cnt, dm, buf);
     }
     return cudaGetLastError();
 }
@@ -260,10 +308,8 @@ int Engine::coarse(Problem &p, std::string &err) {
     CKC(cudaMemcpyAsync(d_fco, fco.data(), nsub_ * sizeof(long long), cudaMemcpyHostToDevice, s_));
     k_build_Fc<<<nsub_, 256, 0, s_>>>(d_subs_, d_V_, d_bce_ptr_, d_bce_pos_, d_bce_val_, d_fco, d_Fc);
     CKC(cudaGetLastError());
-    std::vector<double> Fc(std::max<long long>(fct, 1));
-    CKC(cudaMemcpyAsync(Fc.data(), d_Fc, fct * sizeof(double), cudaMemcpyDeviceToHost, s_));
-    CKC(cudaStreamSynchronize(s_));
-    // host: cluster Fc, Gc = -Bc R (Cluster.cpp:190-198) and H = ker(Gc) (orthonormal rigid modes of the cluster)
+    // cluster Fc and Gc = -Bc R (Cluster.cpp:190-198) on the device (below);
+    // host: H = ker(Gc) (orthonormal rigid modes of the cluster)
     std::vector<long long> oF(ncl_), oW(ncl_), oG(ncl_), oH(ncl_), oS(ncl_), oZS(ncl_);
     long long nF = 0, nW = 0, nG = 0, nH = 0, nS = 0, nZS = 0;
     for (int c = 0; c < ncl_; ++c) {
@@ -276,22 +322,16 @@ int Engine::coarse(Problem &p, std::string &err) {
         oZS[c] = nZS; nZS += nc * na;
     }
     if (nW > 0x7fffffffLL || nS > 0x7fffffffLL) { err = "cluster coarse problems too large"; return HTF_EINVAL; }
-    std::vector<double> hF(nF, 0.0), hG(nG, 0.0), hH(nH, 0.0);
+    std::vector<double> hH(nH, 0.0);
     Hd_.assign(nsub_, std::vector<double>(36, 0.0));
 #pragma omp parallel for schedule(dynamic)
     for (int ci = 0; ci < ncl_; ++ci) {
         const Cluster &cl = p.clu[ci];
-        const int nc = cl.nlam_c, ns = int(cl.subs.size()), na = 6 * ns;
-        double *F = hF.data() + oF[ci], *G = hG.data() + oG[ci], *H = hH.data() + oH[ci];
+        const int ns = int(cl.subs.size()), na = 6 * ns;
+        double *H = hH.data() + oH[ci];
         for (int k = 0; k < ns; ++k) {
             const int d = cl.subs[k];
             const Subdomain &s = p.sub[d];
-            const int c = hs_[d].c;
-            for (int j = 0; j < c; ++j)
-                for (int i = 0; i < c; ++i) F[s.bc_rows[i] + size_t(s.bc_rows[j]) * nc] += Fc[fco[d] + i + (size_t)j * c];
-            for (size_t e = 0; e < s.bc_row.size(); ++e)
-                for (int j = 0; j < 6; ++j)
-                    G[s.bc_row[e] + size_t(6 * k + j) * nc] -= s.bc_val[e] * s.R[s.bc_col[e] + size_t(j) * s.n];
             // ker(Gc): alpha_d = R_d^T r for the (unnormalised) rigid modes r of the cluster
             const int n = s.n;
             for (int q = 0; q < 6; ++q)
@@ -340,9 +380,56 @@ int Engine::coarse(Problem &p, std::string &err) {
     SubDev *dmF = tmp.get<SubDev>(ncl_, ce), *dmS = tmp.get<SubDev>(ncl_, ce);
     int *dst = tmp.get<int>(2 * ncl_, ce);
     CKC(ce);
-    CKC(cudaMemcpyAsync(dF, hF.data(), nF * sizeof(double), cudaMemcpyHostToDevice, s_));
-    CKC(cudaMemcpyAsync(dG, hG.data(), nG * sizeof(double), cudaMemcpyHostToDevice, s_));
     CKC(cudaMemcpyAsync(dH, hH.data(), nH * sizeof(double), cudaMemcpyHostToDevice, s_));
+    {
+        // cluster Fc and Gc assembled on the device, in the host loop's order
+        std::vector<int> cl_ptr(ncl_ + 1, 0), cl_subs, cl_index(nsub_), ncs(ncl_), e_ptr(nsub_ + 1, 0), e_row, e_pl;
+        std::vector<double> e_val;
+        for (int c = 0; c < ncl_; ++c) {
+            ncs[c] = p.clu[c].nlam_c;
+            for (size_t k = 0; k < p.clu[c].subs.size(); ++k) {
+                cl_subs.push_back(p.clu[c].subs[k]);
+                cl_index[p.clu[c].subs[k]] = int(k);
+            }
+            cl_ptr[c + 1] = int(cl_subs.size());
+        }
+        for (int d = 0; d < nsub_; ++d) {
+            const Subdomain &s = p.sub[d];
+            for (size_t e = 0; e < s.bc_row.size(); ++e) {
+                e_row.push_back(s.bc_row[e]);
+                e_pl.push_back(s.perm[s.bc_col[e]]);
+                e_val.push_back(s.bc_val[e]);
+            }
+            e_ptr[d + 1] = int(e_row.size());
+        }
+        int *d_clp = tmp.get<int>(cl_ptr.size(), ce), *d_cls = tmp.get<int>(cl_subs.size(), ce);
+        int *d_cli = tmp.get<int>(cl_index.size(), ce), *d_ncs = tmp.get<int>(ncs.size(), ce);
+        int *d_ep = tmp.get<int>(e_ptr.size(), ce), *d_er = tmp.get<int>(e_row.size(), ce);
+        int *d_epl = tmp.get<int>(e_pl.size(), ce);
+        double *d_ev = tmp.get<double>(e_val.size(), ce);
+        long long *d_oF = tmp.get<long long>(ncl_, ce), *d_oG = tmp.get<long long>(ncl_, ce);
+        CKC(ce);
+        auto up = [&](void *dst, const void *src, size_t bytes) {
+            return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s_) : cudaSuccess;
+        };
+        CKC(up(d_clp, cl_ptr.data(), cl_ptr.size() * sizeof(int)));
+        CKC(up(d_cls, cl_subs.data(), cl_subs.size() * sizeof(int)));
+        CKC(up(d_cli, cl_index.data(), cl_index.size() * sizeof(int)));
+        CKC(up(d_ncs, ncs.data(), ncs.size() * sizeof(int)));
+        CKC(up(d_ep, e_ptr.data(), e_ptr.size() * sizeof(int)));
+        CKC(up(d_er, e_row.data(), e_row.size() * sizeof(int)));
+        CKC(up(d_epl, e_pl.data(), e_pl.size() * sizeof(int)));
+        CKC(up(d_ev, e_val.data(), e_val.size() * sizeof(double)));
+        CKC(up(d_oF, oF.data(), ncl_ * sizeof(long long)));
+        CKC(up(d_oG, oG.data(), ncl_ * sizeof(long long)));
+        CKC(cudaMemsetAsync(dF, 0, std::max<long long>(nF, 1) * sizeof(double), s_));
+        CKC(cudaMemsetAsync(dG, 0, std::max<long long>(nG, 1) * sizeof(double), s_));
+        k_assemble_Fc<<<ncl_, 1024, 0, s_>>>(d_subs_, d_clp, d_cls, d_bcr_, d_fco, d_Fc, d_oF, d_ncs, dF);
+        k_assemble_Gc<<<cdivc(6LL * nsub_, 256), 256, 0, s_>>>(nsub_, d_subs_, d_cli, d_ep, d_er, d_epl, d_ev, d_R_,
+                                                              d_oG, d_ncs, dG);
+        CKC(cudaGetLastError());
+        // the scratch above is released with tmp at the end of the coarse set-up, after the stream's work
+    }
     CKC(cudaMemsetAsync(dst, 0, 2 * ncl_ * sizeof(int), s_));
     std::vector<SubDev> mF(ncl_), mS(ncl_);
     std::vector<int> colsW(ncl_), colsS(ncl_);

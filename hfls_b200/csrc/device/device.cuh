@@ -37,6 +37,9 @@ __device__ __forceinline__ float tf32_trunc(float a) { return __uint_as_float(__
 
 constexpr int TILE = 32;                  // packed tile edge
 constexpr int CHOL_STEP = 64;             // columns per batched Cholesky step (two factor panels)
+// dynamic shared memory of k_syrk_update: two 32-column panels of 64 rows for
+// each operand (row stride 68) and the 64 x 64 C block (column stride 65)
+constexpr int SYRK_SMEM = (4 * 32 * 68 + 64 * 65) * 8;
 constexpr int TC_STAGES = 4;              // pipeline stages of the tensor-core product (2 CTAs per SM)
 constexpr int TC_LO = 4;                  // A_lo buffers (in TMEM) of the tensor-core product
 constexpr int TC_THREADS = 320;           // threads of the tensor-core product: producer, MMA, 8 splitting warps

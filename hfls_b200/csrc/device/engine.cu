@@ -608,12 +608,13 @@ int Engine::factorize(Problem &p, std::string &err) {
         k_snapshot<<<dim3(int(snap_first.size()), max_tiles), 256, 0, s_>>>(d_snap + snap_first_off, d_subs_, d_K_, d_S_);
         CK(cudaGetLastError());
     }
+    CK(cudaFuncSetAttribute(k_syrk_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
     for (size_t s = 0; s < steps.size(); ++s) {
         const int cnt = int(steps[s].size());
         const StepDesc *ds = d_steps + soff[s];
         k_potrf_diag<<<cnt, CHOL_STEP, 0, s_>>>(ds, d_subs_, d_K_, d_status_);
         if (nrb[s] > 0) k_trsm_panel<<<nrb[s], 128, 0, s_>>>(ds, cnt, d_subs_, d_K_);
-        if (ntri[s] > 0) k_syrk_update<<<ntri[s], 256, 0, s_>>>(ds, cnt, d_subs_, d_K_);
+        if (ntri[s] > 0) k_syrk_update<<<ntri[s], 256, SYRK_SMEM, s_>>>(ds, cnt, d_subs_, d_K_);
         if (dirichlet && !snap_after[s].empty())
             k_snapshot<<<dim3(int(snap_after[s].size()), max_tiles), 256, 0, s_>>>(d_snap + snap_off[s], d_subs_, d_K_, d_S_);
         CK(cudaGetLastError());

@@ -281,19 +281,32 @@ __global__ void __launch_bounds__(128) k_trsm_panel(const StepDesc *__restrict__
 // a warp loads 6 operand fragments for 8 MMAs (the CUDA-core form loaded 8
 // values per 16 FMAs per thread and was bound by shared-memory loads).  A
 // row stride of 68 doubles keeps both fragment loads free of bank
-// conflicts.  grid: the step's trailing tiles (flattened)
+// conflicts.  All loads are cp.async into shared memory, issued at the start
+// in three groups (the C block, panel 0, panel 1), so panel 1 and C land
+// while panel 0 multiplies.  grid: the step's trailing tiles (flattened);
+// dynamic shared memory SYRK_SMEM.
 __device__ __forceinline__ void dmma_syrk(double &d0, double &d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
 }
 
+// 8-byte asynchronous copy global -> shared; src_bytes 0 writes a zero
+__device__ __forceinline__ void cp_async8(double *dst, const double *src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(
+                     static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                 "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
 __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict__ st, int cnt,
                                                      const SubDev *__restrict__ subs,
                                                      double *__restrict__ Kbuf) {
-    constexpr int LDP = 68;
-    __shared__ double Pa[32][LDP];
-    __shared__ double Pb[32][LDP];
+    constexpr int LDP = 68, LDC = 65;
+    extern __shared__ double syrk_sm[];
+    double(*Pa)[32][LDP] = reinterpret_cast<double(*)[32][LDP]>(syrk_sm);                 // [2][32][LDP]
+    double(*Pb)[32][LDP] = reinterpret_cast<double(*)[32][LDP]>(syrk_sm + 2 * 32 * LDP);  // [2][32][LDP]
+    double *Cs = syrk_sm + 4 * 32 * LDP;                                                    // [64 cols][LDC]
     const int e = step_entry(st, cnt, int(blockIdx.x), [](const StepDesc &x) { return x.tri0; });
     const StepDesc s = st[e];
     const SubDev &sd = subs[s.d];
@@ -311,6 +324,31 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t4 = lane & 3;
     const int wr = 32 * (warp >> 2), wc = 16 * (warp & 3);
+    const int nq = (nb + TILE - 1) / TILE;
+    // group 0: the lower part of the C block (rows >= columns, inside the matrix)
+    for (int idx = threadIdx.x; idx < 64 * 64; idx += 256) {
+        const int r = idx % 64, c = idx / 64;
+        const int row = i0 + r, col = j0 + c;
+        const bool ok = row < N && col < N && row >= col;
+        cp_async8(&Cs[c * LDC + r], ok ? Kbuf + kcol(sd, col) + row : Kbuf, ok ? 8 : 0);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    // groups 1, 2: the panels of the step's 32-column halves (zero outside)
+#pragma unroll
+    for (int q = 0; q < CHOL_STEP / TILE; ++q) {
+        if (q >= nq) break;
+        const int kc = TILE * q;
+        const int kn = min(TILE, nb - kc);
+        const double *P = Kbuf + kidx(sd, k + kc, k + kc);    // panel of columns k+kc..: entry (k+kc+i, k+kc+j) at P[i + j*ld]
+        const long long ld = kld(sd, k + kc);
+        for (int idx = threadIdx.x; idx < 32 * 64; idx += 256) {
+            const int r = idx % 64, kk = idx / 64;
+            const bool oka = kk < kn && i0 + r < N, okb = kk < kn && j0 + r < N;
+            cp_async8(&Pa[q][kk][r], oka ? P + (i0 + r - k - kc) + kk * ld : Kbuf, oka ? 8 : 0);
+            cp_async8(&Pb[q][kk][r], okb ? P + (j0 + r - k - kc) + kk * ld : Kbuf, okb ? 8 : 0);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     double acc[CHOL_STEP / TILE][4][2][2];
 #pragma unroll
     for (int q = 0; q < CHOL_STEP / TILE; ++q)
@@ -320,46 +358,38 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
             for (int b = 0; b < 2; ++b) acc[q][a][b][0] = acc[q][a][b][1] = 0.0;
 #pragma unroll
     for (int q = 0; q < CHOL_STEP / TILE; ++q) {
-        const int kc = TILE * q;
-        if (kc >= nb) break;
-        const int kn = min(TILE, nb - kc);
-        const double *P = Kbuf + kidx(sd, k + kc, k + kc);    // panel of columns k+kc..: entry (k+kc+i, k+kc+j) at P[i + j*ld]
-        const long long ld = kld(sd, k + kc);
+        if (q >= nq) break;
+        // panel q (and everything committed before it) has landed
+        if (q + 1 < nq) asm volatile("cp.async.wait_group 1;" ::: "memory");
+        else asm volatile("cp.async.wait_group 0;" ::: "memory");
         __syncthreads();
-        for (int idx = threadIdx.x; idx < 32 * 64; idx += 256) {
-            const int r = idx % 64, kk = idx / 64;
-            const bool ok = kk < kn;
-            Pa[kk][r] = (ok && i0 + r < N) ? P[(i0 + r - k - kc) + kk * ld] : 0.0;
-            Pb[kk][r] = (ok && j0 + r < N) ? P[(j0 + r - k - kc) + kk * ld] : 0.0;
-        }
-        __syncthreads();
+        const int kn = min(TILE, nb - TILE * q);
         const int kgs = (kn + 3) >> 2;
         for (int kg = 0; kg < kgs; ++kg) {
             const int kr = 4 * kg + t4;
             double av[4], bv[2];
 #pragma unroll
-            for (int a = 0; a < 4; ++a) av[a] = Pa[kr][wr + 8 * a + g];
+            for (int a = 0; a < 4; ++a) av[a] = Pa[q][kr][wr + 8 * a + g];
 #pragma unroll
-            for (int b = 0; b < 2; ++b) bv[b] = Pb[kr][wc + 8 * b + g];
+            for (int b = 0; b < 2; ++b) bv[b] = Pb[q][kr][wc + 8 * b + g];
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
                 for (int b = 0; b < 2; ++b) dmma_syrk(acc[q][a][b][0], acc[q][a][b][1], av[a], bv[b]);
         }
     }
-    const int nq = (nb + TILE - 1) / TILE;
 #pragma unroll
     for (int b = 0; b < 2; ++b)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            const int col = j0 + wc + 8 * b + 2 * t4 + h;
+            const int cl = wc + 8 * b + 2 * t4 + h, col = j0 + cl;
             if (col >= N) continue;
             double *C = Kbuf + kcol(sd, col);
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
-                const int row = i0 + wr + 8 * a + g;
+                const int rl = wr + 8 * a + g, row = i0 + rl;
                 if (row >= N || row < col) continue;
-                double c = C[row];
+                double c = Cs[cl * LDC + rl];
 #pragma unroll
                 for (int q = 0; q < CHOL_STEP / TILE; ++q)
                     if (q < nq) c -= acc[q][a][b][h];
