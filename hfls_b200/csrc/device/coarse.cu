@@ -50,21 +50,33 @@ struct CopyDesc {
     double alpha;
 };
 
-// 64x64 tile per CTA, k in chunks of 16, 4x4 outputs per thread.
+// 64x64 tile per CTA, k in chunks of 16 staged in shared memory; the
+// products on the FP64 tensor path (mma.sync m8n8k4 .f64): warp w owns rows
+// 32 (w / 4) .. +31 and columns 16 (w % 4) .. +15 of the tile as 4 x 2 tiles
+// of 8 x 8 (row stride 68 doubles: conflict-free fragment loads).
 // grid: (tiles of the largest problem, problems)
+__device__ __forceinline__ void dmma_gemm(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 __global__ void __launch_bounds__(256) k_gemm_batched(const GemmDesc *__restrict__ desc) {
-    __shared__ double As[16][65];
-    __shared__ double Bs[16][65];
+    constexpr int LD = 68;
+    __shared__ double As[16][LD];
+    __shared__ double Bs[16][LD];
     const GemmDesc g = desc[blockIdx.y];
     const int tm = (g.m + 63) / 64, tn = (g.n + 63) / 64;
     if ((int)blockIdx.x >= tm * tn) return;
     const int i0 = 64 * (blockIdx.x % tm), j0 = 64 * (blockIdx.x / tm);
-    const int t = threadIdx.x, tx = t % 16, ty = t / 16;
-    double acc[4][4];
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int gq = lane >> 2, t4 = lane & 3;
+    const int wr = 32 * (warp >> 2), wc = 16 * (warp & 3);
+    double acc[4][2][2];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+        for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
     for (int p0 = 0; p0 < g.k; p0 += 16) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -85,31 +97,34 @@ __global__ void __launch_bounds__(256) k_gemm_batched(const GemmDesc *__restrict
         }
         __syncthreads();
 #pragma unroll
-        for (int p = 0; p < 16; ++p) {
-            double av[4], bv[4];
+        for (int kg = 0; kg < 4; ++kg) {
+            const int kr = 4 * kg + t4;
+            double av[4], bv[2];
 #pragma unroll
-            for (int a = 0; a < 4; ++a) av[a] = As[p][tx + 16 * a];
+            for (int a = 0; a < 4; ++a) av[a] = As[kr][wr + 8 * a + gq];
 #pragma unroll
-            for (int b = 0; b < 4; ++b) bv[b] = Bs[p][ty + 16 * b];
+            for (int b = 0; b < 2; ++b) bv[b] = Bs[kr][wc + 8 * b + gq];
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+                for (int b = 0; b < 2; ++b) dmma_gemm(acc[a][b][0], acc[a][b][1], av[a], bv[b]);
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        const int j = j0 + ty + 16 * b;
-        if (j >= g.n) continue;
+    for (int b = 0; b < 2; ++b)
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int i = i0 + tx + 16 * a;
-            if (i >= g.m) continue;
-            double *c = g.C + i + (size_t)j * g.ldc;
-            *c = g.alpha * acc[a][b] + (g.beta != 0.0 ? g.beta * *c : 0.0);
+        for (int h = 0; h < 2; ++h) {
+            const int j = j0 + wc + 8 * b + 2 * t4 + h;
+            if (j >= g.n) continue;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const int i = i0 + wr + 8 * a + gq;
+                if (i >= g.m) continue;
+                double *c = g.C + i + (size_t)j * g.ldc;
+                *c = g.alpha * acc[a][b][h] + (g.beta != 0.0 ? g.beta * *c : 0.0);
+            }
         }
-    }
 }
 
 // Cluster Fc = sum_d Bc_d F_d Bc_d^T (Cluster.cpp:190-198) assembled in place
