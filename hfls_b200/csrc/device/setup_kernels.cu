@@ -650,11 +650,48 @@ namespace htf {
 // given.  The next 32x32 block of L and of X is loaded into registers while
 // the current one is multiplied out of shared memory.
 // ---------------------------------------------------------------------------
+// acc(32 x 32) += A Xs on the FP64 tensor path (mma.sync m8n8k4): A = Ls
+// (TR = false) or Ls^T (TR = true); warp w owns the 8-row tile w / 2 and the
+// 8-column tiles 2 (w % 2), 2 (w % 2) + 1 (d[ct][h]: row 8 (w / 2) + lane / 4,
+// column 8 (2 (w % 2) + ct) + 2 (lane % 4) + h).  Row stride 36 doubles: the
+// fragment loads are conflict-free.
+template <bool TR>
+__device__ __forceinline__ void trsm_block_mma(const double (*Ls)[36], const double (*Xs)[36], int w, int lane,
+                                               double (&d)[2][2]) {
+    const int g = lane >> 2, t4 = lane & 3, rt = w >> 1, ct0 = 2 * (w & 1);
+#pragma unroll
+    for (int kg = 0; kg < 8; ++kg) {
+        const int kr = 4 * kg + t4;
+        const double a = TR ? Ls[kr][8 * rt + g] : Ls[8 * rt + g][kr];
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) {
+            const double b = Xs[kr][8 * (ct0 + ct) + g];
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                         : "+d"(d[ct][0]), "+d"(d[ct][1])
+                         : "d"(a), "d"(b));
+        }
+    }
+}
+
+// the block products' fragments into acc[q] = row lane, column 4 w + q (T: 32 x 36 scratch)
+__device__ __forceinline__ void trsm_gather(double (*T)[36], const double (&d)[2][2], int w, int lane,
+                                            double (&acc)[4]) {
+    const int g = lane >> 2, t4 = lane & 3, rt = w >> 1, ct0 = 2 * (w & 1);
+#pragma unroll
+    for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) T[8 * rt + g][8 * (ct0 + ct) + 2 * t4 + h] = d[ct][h];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = T[lane][4 * w + q];
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict__ subs,
                                                         const double *__restrict__ Kbuf, double *__restrict__ v,
                                                         long long ldv, int nrhs, const int *__restrict__ ncols) {
-    __shared__ double Ls[32][33];
-    __shared__ double Xs[32][33];
+    __shared__ double Ls[32][36];
+    __shared__ double Xs[32][36];
     __shared__ double rinv[32];
     const SubDev &sd = subs[blockIdx.x];
     const long long ld = ldv > 0 ? ldv : sd.N;
@@ -667,6 +704,7 @@ __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict
     for (int b = 0; b < nblk; ++b) {
         const int kb = 32 * b, nrow = min(32, N - kb);
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        double d[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
         double lr[4], xr[4];
         // chunk cb: L rows kb.., columns 32cb.. (all < kb <= N); X rows 32cb..
         auto load = [&](int cb) {
@@ -686,14 +724,10 @@ __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict
             }
             __syncthreads();
             if (cb + 1 < b) load(cb + 1);
-#pragma unroll 8
-            for (int c = 0; c < 32; ++c) {
-                const double l = Ls[lane][c];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q] += l * Xs[c][4 * w + q];
-            }
+            trsm_block_mma<false>(Ls, Xs, w, lane, d);
             __syncthreads();
         }
+        if (b > 0) trsm_gather(Xs, d, w, lane, acc);
         // diagonal block: forward substitution, one shuffle per row
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -730,8 +764,8 @@ __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict
 __global__ void __launch_bounds__(256) k_trsm_bwd_multi(const SubDev *__restrict__ subs,
                                                         const double *__restrict__ Kbuf, double *__restrict__ v,
                                                         long long ldv, int nrhs, const int *__restrict__ ncols) {
-    __shared__ double Ls[32][33];
-    __shared__ double Xs[32][33];
+    __shared__ double Ls[32][36];
+    __shared__ double Xs[32][36];
     __shared__ double rinv[32];
     const SubDev &sd = subs[blockIdx.x];
     const long long ld = ldv > 0 ? ldv : sd.N;
@@ -744,6 +778,7 @@ __global__ void __launch_bounds__(256) k_trsm_bwd_multi(const SubDev *__restrict
     for (int b = nblk - 1; b >= 0; --b) {
         const int kb = 32 * b, nrow = min(32, N - kb);
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        double d[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
         double lr[4], xr[4];
         // chunk cb > b: rows c = 32cb + lane of L's columns kb.. (L^T), X rows c
         auto load = [&](int cb) {
@@ -764,14 +799,10 @@ __global__ void __launch_bounds__(256) k_trsm_bwd_multi(const SubDev *__restrict
             }
             __syncthreads();
             if (cb + 1 < nblk) load(cb + 1);
-#pragma unroll 8
-            for (int c = 0; c < 32; ++c) {
-                const double l = Ls[c][lane];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q] += l * Xs[c][4 * w + q];
-            }
+            trsm_block_mma<true>(Ls, Xs, w, lane, d);
             __syncthreads();
         }
+        if (b + 1 < nblk) trsm_gather(Xs, d, w, lane, acc);
         // diagonal block: Ls[p][r] = L[kb + p][kb + r], r <= p; back substitution with L^T
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
