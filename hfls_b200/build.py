@@ -23,7 +23,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 CU_SOURCES = ["device/setup_kernels.cu", "device/pcpg_kernels.cu", "device/engine.cu", "device/noalloc.cu",
               "device/tc_gemm.cu", "device/pcpg_multi.cu", "device/engine_batch.cu", "device/coarse.cu",
-              "device/autotune.cu", "device/kernel_fix.cu"]
+              "device/autotune.cu", "device/kernel_fix.cu", "device/frontend.cu"]
 CPP_SOURCES = ["host/mesh.cpp", "host/problem.cpp", "host/vtk.cpp", "host/dump.cpp", "capi.cpp", "server.cpp",
                "cxx/surface.cpp"]
 HEADERS = ["device/device.cuh", "device/engine.hpp", "host/problem.hpp"]

@@ -194,31 +194,12 @@ bool bc_rank_full(const std::vector<double> &A, int rows, int cols) {
 }
 }  // namespace
 
-int build_problem(Problem &p, std::string &err, bool on_device) {
+// l2g, interface groups, Bf rows and weights, b sets and Bf CSR on the host
+// (the inspection entry points; frontend_on_device restates it on the GPU);
+// node_ptr / node_subs: the sorted subdomains of every node
+static int frontend_host(Problem &p, std::vector<int> &node_ptr, std::vector<int> &node_subs, std::string &err) {
     Mesh &m = p.mesh;
-    const int ns = m.n_sub(), ne = m.n_elems();
-    if (ns < 1 || ne < 1) { err = "empty mesh"; return HTF_EINVAL; }
-    for (int e = 0; e < ne; ++e)
-        if (m.elem_sub[e] < 0 || m.elem_sub[e] >= ns) { err = "elem_sub out of range"; return HTF_EINVAL; }
-    for (int v : m.elems)
-        if (v < 0 || v >= m.n_nodes) { err = "element node id out of range"; return HTF_EINVAL; }
-    p.sub.assign(ns, Subdomain());
-    int ncl = 0;
-    for (int d = 0; d < ns; ++d) {
-        if (m.sub_cluster[d] < 0) { err = "negative cluster id"; return HTF_EINVAL; }
-        ncl = std::max(ncl, m.sub_cluster[d] + 1);
-    }
-    p.clu.assign(ncl, Cluster());
-    for (int d = 0; d < ns; ++d) {
-        Subdomain &s = p.sub[d];
-        s.id = d;
-        s.cluster = m.sub_cluster[d];
-        s.cl_index = int(p.clu[s.cluster].subs.size());
-        p.clu[s.cluster].subs.push_back(d);
-    }
-    for (int c = 0; c < ncl; ++c)
-        if (p.clu[c].subs.empty()) { err = "cluster without subdomains"; return HTF_EINVAL; }
-    for (int e = 0; e < ne; ++e) p.sub[m.elem_sub[e]].elems.push_back(e);
+    const int ns = m.n_sub();
     // l2g (Data.cpp:111-144)
     for (int d = 0; d < ns; ++d)
         if (p.sub[d].elems.empty()) { err = "subdomain without elements"; return HTF_EINVAL; }
@@ -249,19 +230,31 @@ int build_problem(Problem &p, std::string &err, bool on_device) {
         if (j - i >= 2) {
             int gi = int(grp_ptr.size());
             grp_ptr.push_back(int(grp.size()));
+    node_ptr.assign(size_t(m.n_nodes) + 1, 0);
+    node_subs.clear();
+    for (const auto &x : ds)
+        if (x.first % 3 == 0) ++node_ptr[x.first / 3 + 1];
+    for (int v = 0; v < m.n_nodes; ++v) node_ptr[v + 1] += node_ptr[v];
+    for (const auto &x : ds)
+        if (x.first % 3 == 0) node_subs.push_back(x.second);
             for (size_t k = i; k < j; ++k) grp.push_back(ds[k].second);
             for (size_t k = i; k < j; ++k) iface[ds[k].second].emplace_back(ds[i].first, gi);
         }
         i = j;
     }
     grp_ptr.push_back(int(grp.size()));
-    std::vector<char> is_dir(3 * size_t(m.n_nodes), 0), is_corner(3 * size_t(m.n_nodes), 0);
+    node_ptr.assign(size_t(m.n_nodes) + 1, 0);
+    node_subs.clear();
+    for (const auto &x : ds)
+        if (x.first % 3 == 0) ++node_ptr[x.first / 3 + 1];
+    for (int v = 0; v < m.n_nodes; ++v) node_ptr[v + 1] += node_ptr[v];
+    for (const auto &x : ds)
+        if (x.first % 3 == 0) node_subs.push_back(x.second);
+    std::vector<char> is_dir(3 * size_t(m.n_nodes), 0);
     for (int g : m.dirichlet) {
         if (g < 0 || g >= 3 * m.n_nodes) { err = "Dirichlet DOF out of range"; return HTF_EINVAL; }
         is_dir[g] = 1;
     }
-    for (int g : m.corner)
-        if (g >= 0 && g < 3 * m.n_nodes) is_corner[g] = 1;
     auto local_of = [&](int d, int g) {
         const std::vector<int> &l = p.sub[d].l2g;
         return int(std::lower_bound(l.begin(), l.end(), g) - l.begin());
@@ -357,6 +350,51 @@ int build_problem(Problem &p, std::string &err, bool on_device) {
         }
         if (few >= 0) { err = "subdomain with fewer than 6 interface/Dirichlet DOFs"; return HTF_EINVAL; }
     }
+    return HTF_OK;
+}
+
+int build_problem(Problem &p, std::string &err, bool on_device) {
+    Mesh &m = p.mesh;
+    const int ns = m.n_sub(), ne = m.n_elems();
+    if (ns < 1 || ne < 1) { err = "empty mesh"; return HTF_EINVAL; }
+    for (int e = 0; e < ne; ++e)
+        if (m.elem_sub[e] < 0 || m.elem_sub[e] >= ns) { err = "elem_sub out of range"; return HTF_EINVAL; }
+    for (int v : m.elems)
+        if (v < 0 || v >= m.n_nodes) { err = "element node id out of range"; return HTF_EINVAL; }
+    p.sub.assign(ns, Subdomain());
+    int ncl = 0;
+    for (int d = 0; d < ns; ++d) {
+        if (m.sub_cluster[d] < 0) { err = "negative cluster id"; return HTF_EINVAL; }
+        ncl = std::max(ncl, m.sub_cluster[d] + 1);
+    }
+    p.clu.assign(ncl, Cluster());
+    for (int d = 0; d < ns; ++d) {
+        Subdomain &s = p.sub[d];
+        s.id = d;
+        s.cluster = m.sub_cluster[d];
+        s.cl_index = int(p.clu[s.cluster].subs.size());
+        p.clu[s.cluster].subs.push_back(d);
+    }
+    for (int c = 0; c < ncl; ++c)
+        if (p.clu[c].subs.empty()) { err = "cluster without subdomains"; return HTF_EINVAL; }
+    for (int e = 0; e < ne; ++e) p.sub[m.elem_sub[e]].elems.push_back(e);
+    for (int d = 0; d < ns; ++d)
+        if (p.sub[d].elems.empty()) { err = "subdomain without elements"; return HTF_EINVAL; }
+    // l2g, Bf rows, b sets: on the device for a set-up (frontend.cu), on the
+    // host for the inspection entry points, for Dirichlet lists with repeated
+    // DOFs and without a device (the set-up then fails at its first device
+    // step), bit for bit the same
+    std::vector<int> node_ptr, node_subs;
+    int frc = on_device ? frontend_on_device(p, node_ptr, node_subs, err) : HTF_ESTATE;
+    if (frc == HTF_ESTATE || frc == HTF_ENODEV) frc = frontend_host(p, node_ptr, node_subs, err);
+    if (frc) return frc;
+    std::vector<char> is_corner(3 * size_t(m.n_nodes), 0);
+    for (int g : m.corner)
+        if (g >= 0 && g < 3 * m.n_nodes) is_corner[g] = 1;
+    auto local_of = [&](int d, int g) {
+        const std::vector<int> &l = p.sub[d].l2g;
+        return int(std::lower_bound(l.begin(), l.end(), g) - l.begin());
+    };
     // kernels and fix DOFs: on the device for a set-up (kernel_fix.cu), on the
     // host for the layout inspection entry points, bit for bit the same
     if (on_device) {
@@ -379,12 +417,12 @@ int build_problem(Problem &p, std::string &err, bool on_device) {
         std::sort(s.fix.begin(), s.fix.end());
     }
     }
-    // neighbour lists (subdomains sharing at least one DOF)
+    // neighbour lists (subdomains sharing at least one node)
     std::vector<std::vector<int>> neigh(ns);
-    for (size_t gi = 0; gi + 1 < grp_ptr.size(); ++gi)
-        for (int a = grp_ptr[gi]; a < grp_ptr[gi + 1]; ++a)
-            for (int b = grp_ptr[gi]; b < grp_ptr[gi + 1]; ++b)
-                if (a != b) neigh[grp[a]].push_back(grp[b]);
+    for (int v = 0; v < m.n_nodes; ++v)
+        for (int a = node_ptr[v]; a < node_ptr[v + 1]; ++a)
+            for (int b = node_ptr[v]; b < node_ptr[v + 1]; ++b)
+                if (a != b) neigh[node_subs[a]].push_back(node_subs[b]);
     for (auto &v : neigh) {
         std::sort(v.begin(), v.end());
         v.erase(std::unique(v.begin(), v.end()), v.end());
@@ -395,11 +433,11 @@ int build_problem(Problem &p, std::string &err, bool on_device) {
         int cnt = 0;
         if (p.opt.typeBc == "cor") {             // Cluster.cpp:846-903 with full rank
             for (int d : cl.subs)
-                for (auto &it : iface[d]) {
-                    int g = it.first;
-                    if (!is_corner[g]) continue;
-                    for (int k = grp_ptr[it.second]; k < grp_ptr[it.second + 1]; ++k) {
-                        int nb = grp[k];
+                for (int g : p.sub[d].l2g) {          // the shared DOFs of d, ascending
+                    const int v = g / 3;
+                    if (node_ptr[v + 1] - node_ptr[v] < 2 || !is_corner[g]) continue;
+                    for (int k = node_ptr[v]; k < node_ptr[v + 1]; ++k) {
+                        int nb = node_subs[k];
                         if (nb > d && m.sub_cluster[nb] == ci) {
                             Subdomain &a = p.sub[d], &b = p.sub[nb];
                             a.bc_row.push_back(cnt); a.bc_col.push_back(local_of(d, g)); a.bc_val.push_back(1.0);

