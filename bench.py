@@ -447,7 +447,7 @@ def run_serving(hb, local, n_req, fp64_requests=None):
     budget = 0.85 * free
     stream = serve_stream(hb, n_req)
     loads = [hb.traction(spec, seed=fseed, n_rhs=k) for (_, spec, k, fseed, _) in stream]
-    opts = dict(OPTS, device=str(local), precision="mixed", batch="16", max_iter="3000")
+    opts = dict(OPTS, device=str(local), precision="mixed", batch="16", max_iter="12000")
     srv = hb.Server(opts, hbm_budget_bytes=budget, max_live=8)
     tickets = []
     t0 = time.perf_counter()
