@@ -421,6 +421,43 @@ __global__ void k_snapshot(const int *__restrict__ dlist, const SubDev *__restri
     }
 }
 
+// acc(32 x 32) += A Xs on the FP64 tensor path (mma.sync m8n8k4): A = Ls
+// (TR = false) or Ls^T (TR = true); warp w owns the 8-row tile w / 2 and the
+// 8-column tiles 2 (w % 2), 2 (w % 2) + 1 (d[ct][h]: row 8 (w / 2) + lane / 4,
+// column 8 (2 (w % 2) + ct) + 2 (lane % 4) + h).  Row stride 36 doubles: the
+// fragment loads are conflict-free.
+template <bool TR>
+__device__ __forceinline__ void trsm_block_mma(const double (*Ls)[36], const double (*Xs)[36], int w, int lane,
+                                               double (&d)[2][2]) {
+    const int g = lane >> 2, t4 = lane & 3, rt = w >> 1, ct0 = 2 * (w & 1);
+#pragma unroll
+    for (int kg = 0; kg < 8; ++kg) {
+        const int kr = 4 * kg + t4;
+        const double a = TR ? Ls[kr][8 * rt + g] : Ls[8 * rt + g][kr];
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) {
+            const double b = Xs[kr][8 * (ct0 + ct) + g];
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                         : "+d"(d[ct][0]), "+d"(d[ct][1])
+                         : "d"(a), "d"(b));
+        }
+    }
+}
+
+// the block products' fragments into acc[q] = row lane, column 4 w + q (T: 32 x 36 scratch)
+__device__ __forceinline__ void trsm_gather(double (*T)[36], const double (&d)[2][2], int w, int lane,
+                                            double (&acc)[4]) {
+    const int g = lane >> 2, t4 = lane & 3, rt = w >> 1, ct0 = 2 * (w & 1);
+#pragma unroll
+    for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) T[8 * rt + g][8 * (ct0 + ct) + 2 * t4 + h] = d[ct][h];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = T[lane][4 * w + q];
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // X = L_bb^{-1}: block row i of X, all block columns j <= i
 // ---------------------------------------------------------------------------
@@ -428,19 +465,19 @@ __global__ void __launch_bounds__(256) k_trtri_step(int i, const int *__restrict
                                                     const SubDev *__restrict__ subs,
                                                     const double *__restrict__ Kbuf,
                                                     double *__restrict__ Xbuf) {
-    __shared__ double La[32][33];
-    __shared__ double Xb[32][33];
-    __shared__ double T[32][33];
+    __shared__ double La[32][36];
+    __shared__ double Xb[32][36];
+    __shared__ double T[32][36];
     const SubDev &sd = subs[dlist[blockIdx.x]];
     const int j = blockIdx.y;
     if (i >= sd.nt || j > i) return;
     const int N = sd.N, nbp = sd.nbp, base = sd.nr;
     double *X = Xbuf + sd.X_off;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int r = tid % 32, c0 = (tid / 32) * 4;
-    double acc[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc[q] = (i == j && r == c0 + q) ? 1.0 : 0.0;
+    (void)N;
+    // sum_kb L_i,kb X_kb,j on the FP64 tensor path, then T = I - sum (block j = i) or -sum
+    double d[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
     for (int kb = j; kb < i; ++kb) {
         for (int idx = tid; idx < 1024; idx += 256) {
             const int rr = idx % 32, cc = idx / 32;
@@ -448,16 +485,13 @@ __global__ void __launch_bounds__(256) k_trtri_step(int i, const int *__restrict
             Xb[rr][cc] = X[(32 * kb + rr) + (size_t)(32 * j + cc) * nbp];
         }
         __syncthreads();
-#pragma unroll 8
-        for (int q = 0; q < 32; ++q) {
-            const double l = La[r][q];
-#pragma unroll
-            for (int cc = 0; cc < 4; ++cc) acc[cc] -= l * Xb[q][c0 + cc];
-        }
+        trsm_block_mma<false>(La, Xb, w, lane, d);
         __syncthreads();
     }
+    double acc[4];
+    trsm_gather(T, d, w, lane, acc);
 #pragma unroll
-    for (int cc = 0; cc < 4; ++cc) T[r][c0 + cc] = acc[cc];
+    for (int cc = 0; cc < 4; ++cc) T[r][c0 + cc] = ((i == j && r == c0 + cc) ? 1.0 : 0.0) - acc[cc];
     for (int idx = tid; idx < 1024; idx += 256) {
         const int rr = idx % 32, cc = idx / 32;
         La[rr][cc] = (cc <= rr) ? Kbuf[kidx(sd, base + 32 * i + rr, base + 32 * i + cc)] : 0.0;
@@ -483,8 +517,8 @@ __global__ void __launch_bounds__(256) k_lauum_tiles(const int *__restrict__ dli
                                                      const SubDev *__restrict__ subs,
                                                      const double *__restrict__ Xbuf,
                                                      double *__restrict__ Fbuf) {
-    __shared__ double A[32][33];
-    __shared__ double B[32][33];
+    __shared__ double A[32][36];
+    __shared__ double B[32][36];
     const SubDev &sd = subs[dlist[blockIdx.x]];
     const int tile = blockIdx.y;
     if (tile >= sd.nt * (sd.nt + 1) / 2) return;
@@ -494,8 +528,9 @@ __global__ void __launch_bounds__(256) k_lauum_tiles(const int *__restrict__ dli
     const int J = tile - I * (I + 1) / 2;
     const double *X = Xbuf + sd.X_off;
     const int nbp = sd.nbp;
-    const int tid = threadIdx.x, r = tid % 32, c0 = (tid / 32) * 4;
-    double acc[4] = {0, 0, 0, 0};
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    // sum_kb X_kb,I^T X_kb,J on the FP64 tensor path (A = X_kb,I read transposed)
+    double d[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
     for (int kb = I; kb < sd.nt; ++kb) {
         for (int idx = tid; idx < 1024; idx += 256) {
             const int q = idx % 32, cc = idx / 32;
@@ -503,17 +538,15 @@ __global__ void __launch_bounds__(256) k_lauum_tiles(const int *__restrict__ dli
             B[q][cc] = X[(32 * kb + q) + (size_t)(32 * J + cc) * nbp];
         }
         __syncthreads();
-#pragma unroll 8
-        for (int q = 0; q < 32; ++q) {
-            const double a = A[q][r];
-#pragma unroll
-            for (int cc = 0; cc < 4; ++cc) acc[cc] += a * B[q][c0 + cc];
-        }
+        trsm_block_mma<true>(A, B, w, lane, d);
         __syncthreads();
     }
     double *T = Fbuf + (sd.T_off + tile) * TILE_ELEMS;
+    const int g = lane >> 2, t4 = lane & 3, rt = w >> 1, ct0 = 2 * (w & 1);
 #pragma unroll
-    for (int cc = 0; cc < 4; ++cc) T[r * TILE + c0 + cc] = acc[cc];
+    for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) T[(8 * rt + g) * TILE + 8 * (ct0 + ct) + 2 * t4 + h] = d[ct][h];
 }
 
 // ---------------------------------------------------------------------------
@@ -650,43 +683,6 @@ namespace htf {
 // given.  The next 32x32 block of L and of X is loaded into registers while
 // the current one is multiplied out of shared memory.
 // ---------------------------------------------------------------------------
-// acc(32 x 32) += A Xs on the FP64 tensor path (mma.sync m8n8k4): A = Ls
-// (TR = false) or Ls^T (TR = true); warp w owns the 8-row tile w / 2 and the
-// 8-column tiles 2 (w % 2), 2 (w % 2) + 1 (d[ct][h]: row 8 (w / 2) + lane / 4,
-// column 8 (2 (w % 2) + ct) + 2 (lane % 4) + h).  Row stride 36 doubles: the
-// fragment loads are conflict-free.
-template <bool TR>
-__device__ __forceinline__ void trsm_block_mma(const double (*Ls)[36], const double (*Xs)[36], int w, int lane,
-                                               double (&d)[2][2]) {
-    const int g = lane >> 2, t4 = lane & 3, rt = w >> 1, ct0 = 2 * (w & 1);
-#pragma unroll
-    for (int kg = 0; kg < 8; ++kg) {
-        const int kr = 4 * kg + t4;
-        const double a = TR ? Ls[kr][8 * rt + g] : Ls[8 * rt + g][kr];
-#pragma unroll
-        for (int ct = 0; ct < 2; ++ct) {
-            const double b = Xs[kr][8 * (ct0 + ct) + g];
-            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                         : "+d"(d[ct][0]), "+d"(d[ct][1])
-                         : "d"(a), "d"(b));
-        }
-    }
-}
-
-// the block products' fragments into acc[q] = row lane, column 4 w + q (T: 32 x 36 scratch)
-__device__ __forceinline__ void trsm_gather(double (*T)[36], const double (&d)[2][2], int w, int lane,
-                                            double (&acc)[4]) {
-    const int g = lane >> 2, t4 = lane & 3, rt = w >> 1, ct0 = 2 * (w & 1);
-#pragma unroll
-    for (int ct = 0; ct < 2; ++ct)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) T[8 * rt + g][8 * (ct0 + ct) + 2 * t4 + h] = d[ct][h];
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc[q] = T[lane][4 * w + q];
-    __syncthreads();
-}
-
 __global__ void __launch_bounds__(256) k_trsm_fwd_multi(const SubDev *__restrict__ subs,
                                                         const double *__restrict__ Kbuf, double *__restrict__ v,
                                                         long long ldv, int nrhs, const int *__restrict__ ncols) {
