@@ -638,6 +638,7 @@ def main():
                        ["problem_build", "device_context", "layout_upload", "assembly_factor_FS", "load_maps",
                         "cluster_coarse", "outer_coarse", "symv_tuning_fp32_slabs"], prof.setup_phase_ms)},
                    "kernel_detection_ms": round(prof.kernel_detection_ms, 1),
+                   "frontend_ms": round(prof.frontend_ms, 1),
                    "symv_unit_tiles": list(prof.symv_unit_tiles), "symv_tuned": int(prof.symv_tuned),
                    "l2": "inputs larger than L2 (F_i and S_i tiles: %.2f GB per PCPG iteration)"
                          % ((prof.symv_F_bytes + prof.symv_S_bytes) / 1e9),

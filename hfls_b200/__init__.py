@@ -53,7 +53,7 @@ class ProfileInfo(ctypes.Structure):
                 ("batch_iteration_ms", ctypes.c_double), ("kernels_per_batch_iteration", ctypes.c_int),
                 ("setup_phase_ms", ctypes.c_double * 8), ("symv_unit_tiles", ctypes.c_int * 5),
                 ("symv_tuned", ctypes.c_int), ("device_bytes", ctypes.c_double),
-                ("kernel_detection_ms", ctypes.c_double)]
+                ("kernel_detection_ms", ctypes.c_double), ("frontend_ms", ctypes.c_double)]
 
 
 class RequestInfo(ctypes.Structure):

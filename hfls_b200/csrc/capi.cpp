@@ -132,6 +132,7 @@ int htf_setup(htf_ctx *ctx) {
     ctx->eng->phase_ms[0] =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() - ctx->p.context_ms;
     ctx->eng->kernel_detection_ms = ctx->p.kernel_ms;
+    ctx->eng->frontend_ms = ctx->p.frontend_ms;
     rc = ctx->eng->setup(ctx->p, ctx->err);
     if (rc) return rc;
     ctx->eng->phase_ms[1] += ctx->p.context_ms;

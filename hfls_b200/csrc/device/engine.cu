@@ -1117,6 +1117,7 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
     info->symv_tuned = tuned_ ? 1 : 0;
     info->device_bytes = double(device_bytes());
     info->kernel_detection_ms = kernel_detection_ms;
+    info->frontend_ms = frontend_ms;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));

@@ -76,6 +76,7 @@ public:
     bool symv_tuned() const { return tuned_; }
     double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // see htf_profile_info::setup_phase_ms
     double kernel_detection_ms = 0.0;                 // part of phase 0 run on the device
+    double frontend_ms = 0.0;                         // part of phase 0 run on the device
     int status_sub = -1;
 
 private:

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <string>
 #include <vector>
@@ -385,13 +386,19 @@ int frontend_on_device(Problem &p, std::vector<int> &node_ptr, std::vector<int> 
         if (dpos[g] >= 0) return HTF_ESTATE;            // repeated DOF: the host front-end builds this mesh
         dpos[g] = int(i);
     }
+    const auto t0 = std::chrono::steady_clock::now();     // runtime initialisation and context creation
     cudaGetLastError();
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
         cudaGetLastError();
         return HTF_ENODEV;                               // the host front-end runs (and the set-up fails later)
     }
-    if (cudaSetDevice(p.opt.device) != cudaSuccess) { err = "front-end: cudaSetDevice failed"; return HTF_ECUDA; }
+    if (cudaSetDevice(p.opt.device) != cudaSuccess || cudaFree(nullptr) != cudaSuccess) {
+        err = "front-end: cudaSetDevice failed";
+        return HTF_ECUDA;
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    p.context_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
     if (cudaFuncSetAttribute(k_sort_segments, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(FE_SORT_CAP * sizeof(ull))) != cudaSuccess) {
         err = "front-end: shared memory opt-in failed";
@@ -542,6 +549,7 @@ int frontend_on_device(Problem &p, std::vector<int> &node_ptr, std::vector<int> 
         }
     }
     if (few >= 0) { err = "subdomain with fewer than 6 interface/Dirichlet DOFs"; return HTF_EINVAL; }
+    p.frontend_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
     return HTF_OK;
 }
 

@@ -385,6 +385,7 @@ int build_problem(Problem &p, std::string &err, bool on_device) {
     // DOFs and without a device (the set-up then fails at its first device
     // step), bit for bit the same
     std::vector<int> node_ptr, node_subs;
+    p.context_ms = p.frontend_ms = p.kernel_ms = 0.0;
     int frc = on_device ? frontend_on_device(p, node_ptr, node_subs, err) : HTF_ESTATE;
     if (frc == HTF_ESTATE || frc == HTF_ENODEV) frc = frontend_host(p, node_ptr, node_subs, err);
     if (frc) return frc;
@@ -400,7 +401,7 @@ int build_problem(Problem &p, std::string &err, bool on_device) {
     if (on_device) {
         double t[2] = {0.0, 0.0};
         const int rc = kernels_fix_on_device(m, p.sub, p.opt.device, err, t);
-        p.context_ms = t[0];
+        p.context_ms += t[0];
         p.kernel_ms = t[1];
         if (rc) return rc;
     } else {

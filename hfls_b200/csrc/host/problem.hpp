@@ -112,6 +112,7 @@ struct Problem {
     std::vector<double> f_nodal;            // 3*n_nodes*nrhs (optional)
     double context_ms = 0.0;                // host wall of the device context creation (set-up only)
     double kernel_ms = 0.0;                 // host wall of the device kernel detection (set-up only)
+    double frontend_ms = 0.0;               // host wall of the device front-end (set-up only)
 };
 
 // Data::buildMappingStruct + Cluster::create_cluster_constraints +

@@ -194,6 +194,8 @@ typedef struct htf_profile_info {
     double kernel_detection_ms;         /* host wall of the kernel bases and fix
                                            DOFs computed on the device (part of
                                            setup phase 0)                           */
+    double frontend_ms;                 /* host wall of the l2g / Bf rows / b sets
+                                           built on the device (part of phase 0)    */
 } htf_profile_info;
 int htf_profile(htf_ctx *ctx, int reps, htf_profile_info *info);
 
