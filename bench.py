@@ -492,16 +492,20 @@ def run_serving(hb, local, n_req, fp64_requests=None):
         s.close()
         service.append(time.perf_counter() - t)
         err = max(err, max(float(np.linalg.norm(u[j] - u64[j]) / np.linalg.norm(u64[j])) for j in range(k)))
-    # the served displacements against tight FP64 solves (eps 1e-11) of the three
+    # the served displacements against tight FP64 solves (eps 1e-10) of the three
     # smallest served requests: the mixed form's bound is 1e-7 against a converged u
     tight_err, tight_req = 0.0, []
     for (i, u, *_) in sorted(ok, key=lambda x: int(np.prod(stream[x[0]][4])))[:3]:      # c s e: elements^(1/3)
         spec, k = stream[i][1], stream[i][2]
-        s = hb.Solver(dict(OPTS, device=str(local), eps_iter="1e-11", max_iter="20000"))
-        s.set_mesh(hb.generate_mesh(spec))
-        s.setup()
-        ut, _ = s.solve(loads[i])
-        s.close()
+        s = hb.Solver(dict(OPTS, device=str(local), eps_iter="1e-10", max_iter="20000"))
+        try:
+            s.set_mesh(hb.generate_mesh(spec))
+            s.setup()
+            ut, _ = s.solve(loads[i])
+        except hb.HTFError:
+            continue
+        finally:
+            s.close()
         tight_req.append(i)
         tight_err = max(tight_err, max(float(np.linalg.norm(u[j] - ut[j]) / np.linalg.norm(ut[j])) for j in range(k)))
     fin, lat64 = 0.0, []
@@ -525,7 +529,7 @@ def run_serving(hb, local, n_req, fp64_requests=None):
         "u_rel_err_max_vs_fp64": err,
         "u_rel_err_vs_fp64_note": "both stop at eps 1e-8 (the served form at 1e-8 x mixed_eps_factor 0.1): the "
                                   "difference includes the FP64 solve's own distance from convergence",
-        "u_rel_err_max_vs_tight_fp64": tight_err,
+        "u_rel_err_max_vs_tight_fp64": tight_err if tight_req else None,
         "tight_fp64_requests": tight_req,
         "sizes": [dict(c=x[4][0], s=x[4][1], e=x[4][2], load_cases=x[2]) for x in stream],
         "per_request": [dict(request=x[0], **x[5]) for x in ok],
