@@ -50,7 +50,8 @@ struct CopyDesc {
     double alpha;
 };
 
-// 64x64 tile per CTA, k in chunks of 16 staged in shared memory; the
+// 64x64 tile per CTA, k in chunks of 16 staged in shared memory (the next
+// chunk register-prefetched while the current one multiplies); the
 // products on the FP64 tensor path (mma.sync m8n8k4 .f64): warp w owns rows
 // 32 (w / 4) .. +31 and columns 16 (w % 4) .. +15 of the tile as 4 x 2 tiles
 // of 8 x 8 (row stride 68 doubles: conflict-free fragment loads).
@@ -77,7 +78,9 @@ __global__ void __launch_bounds__(256) k_gemm_batched(const GemmDesc *__restrict
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
-    for (int p0 = 0; p0 < g.k; p0 += 16) {
+    // the next k chunk is loaded into registers while the current one multiplies
+    double ra[4], rb[4];
+    auto load = [&](int p0) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int e = t + 256 * q;                       // 0..1023
@@ -85,17 +88,29 @@ __global__ void __launch_bounds__(256) k_gemm_batched(const GemmDesc *__restrict
             int i, p;
             if (!g.ta) { i = e % 64; p = e / 64; } else { p = e % 16; i = e / 16; }
             const int gi = i0 + i, gp = p0 + p;
-            double va = 0.0;
-            if (gi < g.m && gp < g.k) va = g.ta ? g.A[gp + (size_t)gi * g.lda] : g.A[gi + (size_t)gp * g.lda];
-            As[p][i] = va;
+            ra[q] = (gi < g.m && gp < g.k) ? (g.ta ? g.A[gp + (size_t)gi * g.lda] : g.A[gi + (size_t)gp * g.lda])
+                                           : 0.0;
             int j, pb;
             if (!g.tb) { pb = e % 16; j = e / 16; } else { j = e % 64; pb = e / 64; }
             const int gj = j0 + j, gpb = p0 + pb;
-            double vb = 0.0;
-            if (gj < g.n && gpb < g.k) vb = g.tb ? g.B[gj + (size_t)gpb * g.ldb] : g.B[gpb + (size_t)gj * g.ldb];
-            Bs[pb][j] = vb;
+            rb[q] = (gj < g.n && gpb < g.k) ? (g.tb ? g.B[gj + (size_t)gpb * g.ldb] : g.B[gpb + (size_t)gj * g.ldb])
+                                            : 0.0;
+        }
+    };
+    if (g.k > 0) load(0);
+    for (int p0 = 0; p0 < g.k; p0 += 16) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = t + 256 * q;
+            int i, p;
+            if (!g.ta) { i = e % 64; p = e / 64; } else { p = e % 16; i = e / 16; }
+            As[p][i] = ra[q];
+            int j, pb;
+            if (!g.tb) { pb = e % 16; j = e / 16; } else { j = e % 64; pb = e / 64; }
+            Bs[pb][j] = rb[q];
         }
         __syncthreads();
+        if (p0 + 16 < g.k) load(p0 + 16);
 #pragma unroll
         for (int kg = 0; kg < 4; ++kg) {
             const int kr = 4 * kg + t4;
