@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(128) k_trsm_panel(const StepDesc *__restrict__
 // values per 16 FMAs per thread and was bound by shared-memory loads).  A
 // row stride of 68 doubles keeps both fragment loads free of bank
 // conflicts.  All loads are cp.async into shared memory, issued at the start
-// in three groups (the C block, panel 0, panel 1), so panel 1 and C land
+// in three groups (panel 0, panel 1, the C block), so panel 1 and C land
 // while panel 0 multiplies.  grid: the step's trailing tiles (flattened);
 // dynamic shared memory SYRK_SMEM.
 __device__ __forceinline__ void dmma_syrk(double &d0, double &d1, double a, double b) {
@@ -325,15 +325,7 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
     const int g = lane >> 2, t4 = lane & 3;
     const int wr = 32 * (warp >> 2), wc = 16 * (warp & 3);
     const int nq = (nb + TILE - 1) / TILE;
-    // group 0: the lower part of the C block (rows >= columns, inside the matrix)
-    for (int idx = threadIdx.x; idx < 64 * 64; idx += 256) {
-        const int r = idx % 64, c = idx / 64;
-        const int row = i0 + r, col = j0 + c;
-        const bool ok = row < N && col < N && row >= col;
-        cp_async8(&Cs[c * LDC + r], ok ? Kbuf + kcol(sd, col) + row : Kbuf, ok ? 8 : 0);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    // groups 1, 2: the panels of the step's 32-column halves (zero outside)
+    // groups 0, 1: the panels of the step's 32-column halves (zero outside)
 #pragma unroll
     for (int q = 0; q < CHOL_STEP / TILE; ++q) {
         if (q >= nq) break;
@@ -349,6 +341,15 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     }
+    // last group: the lower part of the C block (rows >= columns, inside the
+    // matrix), needed only after the products
+    for (int idx = threadIdx.x; idx < 64 * 64; idx += 256) {
+        const int r = idx % 64, c = idx / 64;
+        const int row = i0 + r, col = j0 + c;
+        const bool ok = row < N && col < N && row >= col;
+        cp_async8(&Cs[c * LDC + r], ok ? Kbuf + kcol(sd, col) + row : Kbuf, ok ? 8 : 0);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
     double acc[CHOL_STEP / TILE][4][2][2];
 #pragma unroll
     for (int q = 0; q < CHOL_STEP / TILE; ++q)
@@ -359,9 +360,10 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
 #pragma unroll
     for (int q = 0; q < CHOL_STEP / TILE; ++q) {
         if (q >= nq) break;
-        // panel q (and everything committed before it) has landed
-        if (q + 1 < nq) asm volatile("cp.async.wait_group 1;" ::: "memory");
-        else asm volatile("cp.async.wait_group 0;" ::: "memory");
+        // panel q (and everything committed before it) has landed; the later
+        // panel and the C block may still be in flight
+        if (q + 1 < nq) asm volatile("cp.async.wait_group 2;" ::: "memory");
+        else asm volatile("cp.async.wait_group 1;" ::: "memory");
         __syncthreads();
         const int kn = min(TILE, nb - TILE * q);
         const int kgs = (kn + 3) >> 2;
@@ -378,6 +380,8 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
                 for (int b = 0; b < 2; ++b) dmma_syrk(acc[q][a][b][0], acc[q][a][b][1], av[a], bv[b]);
         }
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");    // the C block
+    __syncthreads();
 #pragma unroll
     for (int b = 0; b < 2; ++b)
 #pragma unroll
