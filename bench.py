@@ -552,6 +552,8 @@ def main():
                     help="only the serving measurement (its own JSON line); the plain FP64 comparison runs on the "
                          "first --serve-fp64 served requests")
     ap.add_argument("--serve-fp64", type=int, default=None)
+    ap.add_argument("--setup-only", action="store_true",
+                    help="set up the headline mesh once, print its set-up phases and exit (for launch lists)")
     ap.add_argument("--workload", default="full", choices=["full"] + sorted(REDUCED),
                     help="reduced meshes of the same constructions, for ncu captures only: uneven-small is one "
                          "cluster of the uneven cube; small / mid are one / two clusters of 2x4x4 cube subdomains "
@@ -563,6 +565,22 @@ def main():
 
     rank, world, local, dist = dist_setup(args.gpus)
     import hfls_b200 as hb
+    if args.setup_only:
+        s = hb.Solver(dict(OPTS, device=str(local)))
+        s.set_mesh(hb.generate_mesh(uneven_spec(hb)))
+        t = time.perf_counter()
+        s.setup()
+        wall = time.perf_counter() - t
+        prof = s.profile(reps=1)
+        s.close()
+        if rank == 0:
+            print(json.dumps({"workload": UNEVEN_WORKLOAD, "setup_s": wall,
+                              "setup_phase_ms": [round(x, 1) for x in prof.setup_phase_ms],
+                              "frontend_ms": round(prof.frontend_ms, 1),
+                              "kernel_detection_ms": round(prof.kernel_detection_ms, 1)}))
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
     if args.serve_only:
         out = run_serving(hb, local, args.serve_requests, args.serve_fp64)
         if rank == 0:
