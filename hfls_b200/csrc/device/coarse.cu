@@ -25,8 +25,8 @@
 namespace htf {
 
 __global__ void k_potrf_diag(const StepDesc *, const SubDev *, double *, int *);
-__global__ void k_trsm_panel(const StepDesc *, int, const SubDev *, double *);
-__global__ void k_syrk_update(const StepDesc *, int, const SubDev *, double *);
+__global__ void k_trsm_panel(const StepDesc *, int, const SubDev *, double *, const int *);
+__global__ void k_syrk_update(const StepDesc *, int, const SubDev *, double *, const int *);
 __global__ void k_trsm_fwd_multi(const SubDev *, const double *, double *, long long, int, const int *);
 __global__ void k_trsm_bwd_multi(const SubDev *, const double *, double *, long long, int, const int *);
 __global__ void k_build_Fc(const SubDev *, const double *, const int *, const int *, const double *,
@@ -254,15 +254,25 @@ static cudaError_t chol_batched(const std::vector<SubDev> &hm, const SubDev *dm,
     if (flat.empty()) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(k_syrk_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM);
     if (e != cudaSuccess) return e;
+    std::vector<int> hints;
+    std::vector<size_t> htri, hrb;
+    for (size_t st = 0; st < steps.size(); ++st) {
+        htri.push_back(hints.size());
+        step_hints(steps[st], ntri[st], true, hints);
+        hrb.push_back(hints.size());
+        step_hints(steps[st], nrb[st], false, hints);
+    }
     StepDesc *d = tmp.get<StepDesc>(flat.size(), e);
+    int *dh = tmp.get<int>(hints.size(), e);
     if (e != cudaSuccess) return e;
     e = cudaMemcpyAsync(d, flat.data(), flat.size() * sizeof(StepDesc), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dh, hints.data(), hints.size() * sizeof(int), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return e;
     for (size_t st = 0; st < steps.size(); ++st) {
         const int cnt = int(steps[st].size());
         k_potrf_diag<<<cnt, CHOL_STEP, 0, s>>>(d + off[st], dm, buf, status);
-        if (nrb[st] > 0) k_trsm_panel<<<nrb[st], 128, 0, s>>>(d + off[st], cnt, dm, buf);
-        if (ntri[st] > 0) k_syrk_update<<<ntri[st], 256, SYRK_SMEM, s>>>(d + off[st], cnt, dm, buf);
+        if (nrb[st] > 0) k_trsm_panel<<<nrb[st], 128, 0, s>>>(d + off[st], cnt, dm, buf, dh + hrb[st]);
+        if (ntri[st] > 0) k_syrk_update<<<ntri[st], 256, SYRK_SMEM, s>>>(d + off[st], cnt, dm, buf, dh + htri[st]);
     }
     return cudaGetLastError();
 }

@@ -18,6 +18,7 @@
 //   * b-space vectors (x_b, y_b) are concatenated with per-subdomain offsets
 //     xb_off (multiples of 32).
 #pragma once
+#include <vector>
 #include <cstdint>
 
 namespace htf {
@@ -180,11 +181,33 @@ struct StepDesc {
     int rb0;
 };
 
+// CTAs of a step's flattened grid per entry hint
+constexpr int STEP_HINT = 256;
+
+// hints of one step's grid of `total` CTAs: out gets, for every range of
+// STEP_HINT CTAs, the entry of its first CTA, then the last entry (so the
+// entry of CTA b lies between hint[b / STEP_HINT] and hint[b / STEP_HINT + 1])
+inline void step_hints(const std::vector<StepDesc> &v, int total, bool tri, std::vector<int> &out) {
+    const int nh = (total + STEP_HINT - 1) / STEP_HINT;
+    int e = 0;
+    for (int h = 0; h < nh; ++h) {
+        const int b = h * STEP_HINT;
+        while (e + 1 < int(v.size()) && (tri ? v[e + 1].tri0 : v[e + 1].rb0) <= b) ++e;
+        out.push_back(e);
+    }
+    out.push_back(int(v.size()) - 1);
+}
+
 #ifdef __CUDACC__
-// entry of a step whose flattened range holds block b (the last one starting at or before b)
+// entry of a step whose flattened range holds block b (the last one starting at
+// or before b); hint (step_hints) narrows the search to the entries of b's range
 template <typename F>
-__device__ __forceinline__ int step_entry(const StepDesc *st, int cnt, int b, F start) {
+__device__ __forceinline__ int step_entry(const StepDesc *st, int cnt, int b, F start, const int *hint) {
     int lo = 0, hi = cnt - 1;
+    if (hint) {
+        lo = hint[b / STEP_HINT];
+        hi = hint[b / STEP_HINT + 1];
+    }
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (start(st[mid]) <= b) lo = mid;

@@ -18,8 +18,8 @@ __global__ void k_assemble(const int *, int, const double *, const int *, const 
                            const double *, const SubDev *, double *, double *, double, double, double);
 __global__ void k_regularize(SubDev *, int, double *);
 __global__ void k_potrf_diag(const StepDesc *, const SubDev *, double *, int *);
-__global__ void k_trsm_panel(const StepDesc *, int, const SubDev *, double *);
-__global__ void k_syrk_update(const StepDesc *, int, const SubDev *, double *);
+__global__ void k_trsm_panel(const StepDesc *, int, const SubDev *, double *, const int *);
+__global__ void k_syrk_update(const StepDesc *, int, const SubDev *, double *, const int *);
 __global__ void k_snapshot(const int *, const SubDev *, const double *, double *);
 __global__ void k_trtri_step(int, const int *, const SubDev *, const double *, double *);
 __global__ void k_lauum_tiles(const int *, const SubDev *, const double *, double *);
@@ -598,10 +598,21 @@ int Engine::factorize(Problem &p, std::string &err) {
     for (auto &v : snap_after) { snap_off.push_back(snap_flat.size()); snap_flat.insert(snap_flat.end(), v.begin(), v.end()); }
     size_t snap_first_off = snap_flat.size();
     snap_flat.insert(snap_flat.end(), snap_first.begin(), snap_first.end());
+    // entry hints of every step's SYRK and panel-solve grids
+    std::vector<int> hints;
+    std::vector<size_t> htri, hrb;
+    for (size_t s = 0; s < steps.size(); ++s) {
+        htri.push_back(hints.size());
+        step_hints(steps[s], ntri[s], true, hints);
+        hrb.push_back(hints.size());
+        step_hints(steps[s], nrb[s], false, hints);
+    }
     StepDesc *d_steps = alloc<StepDesc>(flat.size(), err, rc);
     int *d_snap = alloc<int>(std::max<size_t>(snap_flat.size(), 1), err, rc);
+    int *d_hints = alloc<int>(hints.size(), err, rc);
     if (rc) return rc;
     CK(cudaMemcpyAsync(d_steps, flat.data(), flat.size() * sizeof(StepDesc), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_hints, hints.data(), hints.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
     if (!snap_flat.empty())
         CK(cudaMemcpyAsync(d_snap, snap_flat.data(), snap_flat.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
     if (dirichlet && !snap_first.empty()) {
@@ -613,8 +624,9 @@ int Engine::factorize(Problem &p, std::string &err) {
         const int cnt = int(steps[s].size());
         const StepDesc *ds = d_steps + soff[s];
         k_potrf_diag<<<cnt, CHOL_STEP, 0, s_>>>(ds, d_subs_, d_K_, d_status_);
-        if (nrb[s] > 0) k_trsm_panel<<<nrb[s], 128, 0, s_>>>(ds, cnt, d_subs_, d_K_);
-        if (ntri[s] > 0) k_syrk_update<<<ntri[s], 256, SYRK_SMEM, s_>>>(ds, cnt, d_subs_, d_K_);
+        if (nrb[s] > 0) k_trsm_panel<<<nrb[s], 128, 0, s_>>>(ds, cnt, d_subs_, d_K_, d_hints + hrb[s]);
+        if (ntri[s] > 0)
+            k_syrk_update<<<ntri[s], 256, SYRK_SMEM, s_>>>(ds, cnt, d_subs_, d_K_, d_hints + htri[s]);
         if (dirichlet && !snap_after[s].empty())
             k_snapshot<<<dim3(int(snap_after[s].size()), max_tiles), 256, 0, s_>>>(d_snap + snap_off[s], d_subs_, d_K_, d_S_);
         CK(cudaGetLastError());

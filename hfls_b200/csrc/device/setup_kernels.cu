@@ -219,9 +219,10 @@ __global__ void __launch_bounds__(CHOL_STEP) k_potrf_diag(const StepDesc *__rest
 // rows below the diagonal block: x = x L_kk^{-T}, one row per thread
 // grid: the step's row blocks of 128 (flattened over its entries)
 __global__ void __launch_bounds__(128) k_trsm_panel(const StepDesc *__restrict__ st, int cnt,
-                                                    const SubDev *__restrict__ subs, double *__restrict__ Kbuf) {
+                                                    const SubDev *__restrict__ subs, double *__restrict__ Kbuf,
+                                                    const int *__restrict__ hint) {
     __shared__ double L[CHOL_STEP][CHOL_STEP + 1];
-    const int e = step_entry(st, cnt, int(blockIdx.x), [](const StepDesc &x) { return x.rb0; });
+    const int e = step_entry(st, cnt, int(blockIdx.x), [](const StepDesc &x) { return x.rb0; }, hint);
     const StepDesc s = st[e];
     const int rb = int(blockIdx.x) - s.rb0;
     const SubDev &sd = subs[s.d];
@@ -301,13 +302,13 @@ __device__ __forceinline__ void cp_async8(double *dst, const double *src, int sr
 
 __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict__ st, int cnt,
                                                      const SubDev *__restrict__ subs,
-                                                     double *__restrict__ Kbuf) {
+                                                     double *__restrict__ Kbuf, const int *__restrict__ hint) {
     constexpr int LDP = 68, LDC = 65;
     extern __shared__ double syrk_sm[];
     double(*Pa)[32][LDP] = reinterpret_cast<double(*)[32][LDP]>(syrk_sm);                 // [2][32][LDP]
     double(*Pb)[32][LDP] = reinterpret_cast<double(*)[32][LDP]>(syrk_sm + 2 * 32 * LDP);  // [2][32][LDP]
     double *Cs = syrk_sm + 4 * 32 * LDP;                                                    // [64 cols][LDC]
-    const int e = step_entry(st, cnt, int(blockIdx.x), [](const StepDesc &x) { return x.tri0; });
+    const int e = step_entry(st, cnt, int(blockIdx.x), [](const StepDesc &x) { return x.tri0; }, hint);
     const StepDesc s = st[e];
     const SubDev &sd = subs[s.d];
     const int N = sd.N, k = s.k, nb = s.nb;
