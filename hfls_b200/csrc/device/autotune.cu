@@ -141,10 +141,13 @@ void write_file(const std::string &path) {
 
 // Units of the given schedule (host side): sets u0 / u1 of every subdomain.
 void Engine::build_units(const std::vector<int> &tiles, std::vector<SymvUnit> &units, long long &yoff,
-                         int &smem) {
+                         int &smem, std::vector<int> &rbptr, std::vector<int> &rbunit) {
     units.clear();
+    rbptr.assign(1, 0);
+    rbunit.clear();
     yoff = 0;
     int max_rows = 0;
+    std::vector<std::vector<int>> cover;
     for (int d = 0; d < nsub_; ++d) {
         SubDev &h = hs_[d];
         h.u0 = int(units.size());
@@ -154,6 +157,22 @@ void Engine::build_units(const std::vector<int> &tiles, std::vector<SymvUnit> &u
             max_rows = std::max(max_rows, rows);
         });
         h.u1 = int(units.size());
+        // the units covering each 32-row block, in unit order (the order of the partial sums)
+        cover.assign(h.nt, std::vector<int>());
+        for (int k = h.u0; k < h.u1; ++k) {
+            const SymvUnit &u = units[k];
+            const int seg = u.kind == 2 ? u.rows - TILE : u.rows;
+            for (int R = u.row0 / TILE; R < (u.row0 + seg + TILE - 1) / TILE && R < h.nt; ++R) cover[R].push_back(k);
+            if (u.kind == 2) {
+                const int R = u.rowI / TILE;
+                if (R < h.nt && (cover[R].empty() || cover[R].back() != k)) cover[R].push_back(k);
+            }
+        }
+        h.rb_off = int(rbptr.size()) - 1;
+        for (int R = 0; R < h.nt; ++R) {
+            rbunit.insert(rbunit.end(), cover[R].begin(), cover[R].end());
+            rbptr.push_back(int(rbunit.size()));
+        }
     }
     for (int d = 0; d < nsub_; ++d) units.push_back(SymvUnit{d, 1, 0, 0, 0, 0, 0, 0, 0});   // V^T x units
     smem = SYMV_ROW_DOUBLES * max_rows * int(sizeof(double));
@@ -170,8 +189,10 @@ int Engine::apply_schedule(const std::vector<int> &tiles, bool subs_on_device, s
         CKE(cudaMemcpyAsync(hs_.data(), d_subs_, nsub_ * sizeof(SubDev), cudaMemcpyDeviceToHost, s_));
         CKE(cudaStreamSynchronize(s_));
     }
-    build_units(tiles, units, yoff, smem);
-    if ((long long)units.size() > units_cap_ || yoff > ypart_cap_ || smem > symv_smem_cap_) {
+    std::vector<int> rbptr, rbunit;
+    build_units(tiles, units, yoff, smem, rbptr, rbunit);
+    if ((long long)units.size() > units_cap_ || yoff > ypart_cap_ || smem > symv_smem_cap_ ||
+        (long long)rbptr.size() > rbptr_cap_ || (long long)rbunit.size() > rbunit_cap_) {
         err = "SYMV schedule exceeds its buffers";
         return HTF_EINVAL;
     }
@@ -179,6 +200,10 @@ int Engine::apply_schedule(const std::vector<int> &tiles, bool subs_on_device, s
     symv_smem_ = smem;
     schedule_ = tiles;
     CKE(cudaMemcpyAsync(d_units_, units.data(), units.size() * sizeof(SymvUnit), cudaMemcpyHostToDevice, s_));
+    CKE(cudaMemcpyAsync(d_rbptr_, rbptr.data(), rbptr.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+    if (!rbunit.empty())
+        CKE(cudaMemcpyAsync(d_rbunit_, rbunit.data(), rbunit.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+    // (pageable copies: the host vectors may go out of scope once the calls return)
     if (subs_on_device)
         CKE(cudaMemcpyAsync(d_subs_, hs_.data(), nsub_ * sizeof(SubDev), cudaMemcpyHostToDevice, s_));
     return HTF_OK;
@@ -216,8 +241,15 @@ int Engine::alloc_units(std::string &err) {
     units_cap_ = ucap;
     ypart_cap_ = ycap;
     symv_smem_cap_ = scap;
+    // row-block lists: a unit covers at most rows / 32 + 1 blocks (its window and its tile row)
+    long long ntsum = 0;
+    for (auto &h : hs_) ntsum += h.nt;
+    rbptr_cap_ = ntsum + 1;
+    rbunit_cap_ = ycap / TILE + 2 * ucap;
     d_units_ = alloc<SymvUnit>(ucap, err, rc);
     d_ypart_ = alloc<double>(ycap, err, rc);
+    d_rbptr_ = alloc<int>(rbptr_cap_, err, rc);
+    d_rbunit_ = alloc<int>(rbunit_cap_, err, rc);
     if (rc) return rc;
     if (scap > 48 * 1024) {
         CKE(cudaFuncSetAttribute(k_symv_units<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, scap));

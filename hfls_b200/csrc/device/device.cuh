@@ -65,6 +65,7 @@ struct SubDev {
     int bce_off;                          // Bc entries (CSR by compressed Bc row): ptr offset
     long long R_off;                      // R in permuted local order, N x 6 (padded rows 0)
     int u0, u1;                           // SYMV work units of this subdomain [u0, u1)
+    int rb_off;                           // its nt + 1 pointers into the units covering each 32-row block
     int fix[6];                           // fix DOFs (positions in permuted order)
     double fix_diag[6];                   // original diagonal at the fix DOFs
 };

@@ -34,7 +34,7 @@ __global__ void k_gather_b(int, const int *, const int *, const double *, const 
 template <typename T>
 __global__ void k_symv_units(const SymvUnit *, const SubDev *, const T *, const double *, const double *, double *,
                              double *, const PcpgState *);
-__global__ void k_reduce_correct(const SubDev *, const SymvUnit *, const double *, const ClusterDev *,
+__global__ void k_reduce_correct(const SubDev *, const SymvUnit *, const int *, const int *, const double *, const ClusterDev *,
                                  const double *, const int *, const double *, double *, const PcpgState *);
 __global__ void k_lbt_x(const int2 *, const SubDev *, const double *, const double *, double *, const PcpgState *);
 __global__ void k_lb_t(const int2 *, const SubDev *, const double *, const double *, const double *, double *,
@@ -44,6 +44,9 @@ __global__ void k_msym_rows(const int2 *, const ClusterDev *, const double *, co
                             const PcpgState *);
 __global__ void k_msym_reduce(const int2 *, const ClusterDev *, const double *, const double *, double *,
                               const PcpgState *);
+__global__ void k_gf_coef(int, const int *, const double *, const double *, double *, double *, const PcpgState *);
+__global__ void k_gf_apply(int, int, const double *, const int *, const double *, const double *, double *,
+                           const double *, double *, const PcpgState *);
 __global__ void k_gf_apply_fused(int, int, const int *, const double *, const double *, const int *,
                                  const double *, const double *, double *, double *, double *, const double *,
                                  double *, const PcpgState *);
@@ -805,6 +808,12 @@ int Engine::setup(Problem &p, std::string &err) {
         if (!rc)
             rc = check(cudaFuncSetAttribute(k_gf_apply_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                        "cudaFuncSetAttribute(k_gf_apply_fused)", err);
+        if (!rc)
+            rc = check(cudaFuncSetAttribute(k_gf_coef, cudaFuncAttributeMaxDynamicSharedMemorySize, smem / 2),
+                       "cudaFuncSetAttribute(k_gf_coef)", err);
+        if (!rc)
+            rc = check(cudaFuncSetAttribute(k_gf_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, smem / 2),
+                       "cudaFuncSetAttribute(k_gf_apply)", err);
     }
     lap(2);
     if (!rc) rc = factorize(p, err);
@@ -879,7 +888,7 @@ void Engine::op_F(const double *w, double *Fw, const double *dotv, double *parti
     k_symv_units<double><<<nunits_ + nsub_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, st);
     k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, st);
     coarse_apply(d_gc_, d_s_, st);
-    k_reduce_correct<<<dim3(nsub_, cdiv(max_nbp_, 256)), 256, 0, s_>>>(d_subs_, d_units_, d_ypart_, d_cl_, d_V_, d_bcr_,
+    k_reduce_correct<<<dim3(nsub_, cdiv(max_nbp_, 256)), 256, 0, s_>>>(d_subs_, d_units_, d_rbptr_, d_rbunit_, d_ypart_, d_cl_, d_V_, d_bcr_,
                                                                        d_s_, d_yb_, st);
     k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, nullptr, Fw, dotv, partial, st);
 }
@@ -893,7 +902,7 @@ void Engine::op_M(const double *x, double *z, PcpgState *st) {
         return;
     }
     k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_, st);
-    k_reduce_correct<<<dim3(nsub_, cdiv(max_nbp_, 256)), 256, 0, s_>>>(d_subs_, d_units_, d_ypart_, d_cl_, d_V_, d_bcr_,
+    k_reduce_correct<<<dim3(nsub_, cdiv(max_nbp_, 256)), 256, 0, s_>>>(d_subs_, d_units_, d_rbptr_, d_rbunit_, d_ypart_, d_cl_, d_V_, d_bcr_,
                                                                        nullptr, d_yb_, st);
     k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, d_weight_, z, nullptr, nullptr, st);
 }
@@ -901,9 +910,12 @@ void Engine::op_M(const double *x, double *z, PcpgState *st) {
 void Engine::op_P(const double *x, double *Px, double *alpha_out, const double *dotv, double *partial,
                   PcpgState *st) {
     k_gft_partial<<<nchunks_, 256, 0, s_>>>(d_chunk_cl_, d_chunk_beg_, d_chunk_end_, d_crow_, d_cval_, x, d_gpart_, st);
-    k_gf_apply_fused<<<npart_, 256, 12 * ncl_ * sizeof(double), s_>>>(nlam_, ncl_, d_cl_chunk_ptr_, d_gpart_, d_invGtG_,
-                                                                        d_gcl_, d_gval_, x, d_a_, alpha_out, Px, dotv,
-                                                                        partial, st);
+    // the coarse coefficient once, then the rows (k_gf_apply_fused, which
+    // recomputes it in every CTA, stays for the allocation-free entry point)
+    k_gf_coef<<<1, 256, 6 * ncl_ * sizeof(double), s_>>>(ncl_, d_cl_chunk_ptr_, d_gpart_, d_invGtG_, d_a_, alpha_out,
+                                                          st);
+    k_gf_apply<<<npart_, 256, 6 * ncl_ * sizeof(double), s_>>>(nlam_, ncl_, d_a_, d_gcl_, d_gval_, x, Px, dotv,
+                                                                partial, st);
 }
 
 void Engine::iteration(PcpgState *st) {

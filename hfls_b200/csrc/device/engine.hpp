@@ -100,7 +100,8 @@ private:
     int check(cudaError_t e, const char *what, std::string &err, const char *file = nullptr, int line = 0);
     int upload_layout(Problem &p, std::string &err);
     // SYMV work-unit schedules (autotune.cu)
-    void build_units(const std::vector<int> &tiles, std::vector<SymvUnit> &units, long long &yoff, int &smem);
+    void build_units(const std::vector<int> &tiles, std::vector<SymvUnit> &units, long long &yoff, int &smem,
+                     std::vector<int> &rbptr, std::vector<int> &rbunit);
     int apply_schedule(const std::vector<int> &tiles, bool subs_on_device, std::string &err);
     int alloc_units(std::string &err);
     std::string schedule_key() const;
@@ -159,6 +160,8 @@ private:
     int kernels_per_iter_ = 0;
     long long launches_ = 0;                   // kernels launched by the current solve call
     SymvUnit *d_units_ = nullptr;              // SYMV work units (+ one V^T x unit per subdomain)
+    int *d_rbptr_ = nullptr, *d_rbunit_ = nullptr;   // per 32-row block of every subdomain: the units covering it
+    long long rbptr_cap_ = 0, rbunit_cap_ = 0;
     double *d_ypart_ = nullptr;                // partial y sums of the units (scratch)
     int nunits_ = 0, max_nbp_ = 0;
     long long units_cap_ = 0, ypart_cap_ = 0;    // unit buffers, sized for every candidate schedule

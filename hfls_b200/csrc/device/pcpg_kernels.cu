@@ -144,9 +144,11 @@ template __global__ void k_symv_units<double>(const SymvUnit *, const SubDev *, 
 template __global__ void k_symv_units<float>(const SymvUnit *, const SubDev *, const float *, const double *,
                                              const double *, double *, double *, const PcpgState *);
 
-// y_b = sum of the unit partials (in unit order) [- V_d s_d when s != null];
+// y_b = sum of the unit partials (in unit order: only the units covering the
+// row's 32-row block, listed per block) [- V_d s_d when s != null];
 // grid (subdomain, chunk of 256 b rows)
 __global__ void k_reduce_correct(const SubDev *__restrict__ subs, const SymvUnit *__restrict__ units,
+                                 const int *__restrict__ rbptr, const int *__restrict__ rbunit,
                                  const double *__restrict__ ypart, const ClusterDev *__restrict__ cl,
                                  const double *__restrict__ Vbuf, const int *__restrict__ bcrows,
                                  const double *__restrict__ s, double *__restrict__ yb,
@@ -166,8 +168,9 @@ __global__ void k_reduce_correct(const SubDev *__restrict__ subs, const SymvUnit
     }
     if (blockIdx.y * blockDim.x >= sd.nbp || i >= sd.nbp) return;
     double a = 0.0;
-    for (int k = sd.u0; k < sd.u1; ++k) {
-        const SymvUnit &u = units[k];
+    const int R = i / TILE;                  // the units covering this row's block, in unit order
+    for (int q = rbptr[sd.rb_off + R]; q < rbptr[sd.rb_off + R + 1]; ++q) {
+        const SymvUnit &u = units[rbunit[q]];
         const int seg = u.kind == 2 ? u.rows - TILE : u.rows;
         if (i >= u.row0 && i < u.row0 + seg) a += ypart[u.y_off + (i - u.row0)];
         if (u.kind == 2 && i >= u.rowI && i < u.rowI + TILE) a += ypart[u.y_off + seg + (i - u.rowI)];
@@ -335,6 +338,68 @@ __global__ void k_gf_apply_fused(int nlam, int ncl, const int *__restrict__ cl_c
             if (alpha_out) alpha_out[q] = -s;
         }
     }
+    __syncthreads();
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    double prod = 0.0;
+    if (r < nlam) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int c = gcl[2 * r + k];
+            if (c < 0) continue;
+            const double *g = gval + 6 * (size_t)(2 * r + k);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) v += g[q] * a[6 * c + q];
+        }
+        const double pv = x[r] - v;
+        Px[r] = pv;
+        if (dotv) prod = pv * dotv[r];
+    }
+    if (!partial) return;
+    red[threadIdx.x] = prod;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+// a = invGtG * (chunk partials summed per cluster), once (one CTA): the
+// coefficient that k_gf_apply_fused recomputes in every CTA, with the same sums
+// in the same order; a_out gets a, alpha_out (if given) -a.
+__global__ void k_gf_coef(int ncl, const int *__restrict__ cl_chunk_ptr, const double *__restrict__ gpart,
+                          const double *__restrict__ invGtG, double *__restrict__ a_out,
+                          double *__restrict__ alpha_out, const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    extern __shared__ double sh[];
+    double *gt = sh;                 // 6*ncl
+    const int m = 6 * ncl;
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+        const int c = q / 6, i = q % 6;
+        double s = 0.0;
+        for (int ch = cl_chunk_ptr[c]; ch < cl_chunk_ptr[c + 1]; ++ch) s += gpart[6 * (size_t)ch + i];
+        gt[q] = s;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+        double s = 0.0;
+        for (int p = 0; p < m; ++p) s += invGtG[q + (size_t)p * m] * gt[p];
+        a_out[q] = s;
+        if (alpha_out) alpha_out[q] = -s;
+    }
+}
+
+// Px = x - Gf a for the coefficient a of k_gf_coef (and the partials of Px.dotv)
+__global__ void k_gf_apply(int nlam, int ncl, const double *__restrict__ acoef, const int *__restrict__ gcl,
+                           const double *__restrict__ gval, const double *__restrict__ x, double *__restrict__ Px,
+                           const double *__restrict__ dotv, double *__restrict__ partial,
+                           const PcpgState *__restrict__ st) {
+    if (st && st->done) return;
+    extern __shared__ double sh[];
+    double *a = sh;                  // 6*ncl
+    __shared__ double red[256];
+    for (int q = threadIdx.x; q < 6 * ncl; q += blockDim.x) a[q] = acoef[q];
     __syncthreads();
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     double prod = 0.0;
