@@ -40,7 +40,6 @@ __global__ void k_symv_units(const SymvUnit *, const SubDev *, const T *, const 
 
 namespace {
 
-constexpr int SYMV_ROW_DOUBLES = 5;            // shared doubles per window row: x + 4 warp partials
 constexpr long long SYMV_TUNE_MIN_TILES = 1LL << 17;   // 1 GiB of FP64 tiles
 const int CANDIDATES[] = {8, 12, 16, 24, 32, 48, 64, 96};
 
@@ -302,7 +301,7 @@ int Engine::autotune_symv(std::string &err) {
         int rc = apply_schedule(t, true, err);
         if (rc) return rc;
         auto launch = [&] {
-            k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_,
+            k_symv_units<double><<<nunits_, SYMV_WARPS * 32, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_,
                                                                   d_t_, nullptr);
         };
         launch();

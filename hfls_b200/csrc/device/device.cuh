@@ -140,6 +140,8 @@ struct SymvUnit {
 constexpr int SYMV_BUCKETS = 5;
 constexpr int SYMV_BUCKET_NT[SYMV_BUCKETS] = {8, 16, 32, 64, 1 << 30};
 constexpr int SYMV_DEFAULT_TILES = 48;
+constexpr int SYMV_WARPS = 4;                 // warps of a SYMV work-unit CTA
+constexpr int SYMV_ROW_DOUBLES = 1 + SYMV_WARPS;   // shared doubles per window row: x + the warps' partials
 
 // One CTA of the tensor-core multi-RHS product: 128-row block m of
 // subdomain d.  The symmetric A_d is stored as its lower triangle at 128-row

@@ -885,7 +885,7 @@ int Engine::setup(Problem &p, std::string &err) {
 // ---------------------------------------------------------------------------
 void Engine::op_F(const double *w, double *Fw, const double *dotv, double *partial, PcpgState *st) {
     k_gather_b<<<cdiv(nslots_, 256), 256, 0, s_>>>(nslots_, d_slot_ptr_, d_slot_ent_, w, nullptr, d_xb_, st);
-    k_symv_units<double><<<nunits_ + nsub_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, st);
+    k_symv_units<double><<<nunits_ + nsub_, SYMV_WARPS * 32, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, st);
     k_gc<<<cdiv(ngc_total_, 256), 256, 0, s_>>>(ngc_total_, d_gptr_, d_gidx_, d_t_, d_gc_, st);
     coarse_apply(d_gc_, d_s_, st);
     k_reduce_correct<<<dim3(nsub_, cdiv(max_nbp_, 256)), 256, 0, s_>>>(d_subs_, d_units_, d_rbptr_, d_rbunit_, d_ypart_, d_cl_, d_V_, d_bcr_,
@@ -901,7 +901,7 @@ void Engine::op_M(const double *x, double *z, PcpgState *st) {
         k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, d_weight_, z, nullptr, nullptr, st);
         return;
     }
-    k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_, st);
+    k_symv_units<double><<<nunits_, SYMV_WARPS * 32, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_, st);
     k_reduce_correct<<<dim3(nsub_, cdiv(max_nbp_, 256)), 256, 0, s_>>>(d_subs_, d_units_, d_rbptr_, d_rbunit_, d_ypart_, d_cl_, d_V_, d_bcr_,
                                                                        nullptr, d_yb_, st);
     k_rows<<<npart_, 256, 0, s_>>>(nlam_, d_rslot_, d_rsign_, d_yb_, d_weight_, z, nullptr, nullptr, st);
@@ -1160,7 +1160,7 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
     double tri = 0.0, vec = 0.0;
     for (auto &h : hs_) { tri += sz * double(h.nb) * (h.nb + 1) / 2; vec += 16.0 * h.nb; }
     info->symv_F_ms = timeit([&] {
-        k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
+        k_symv_units<double><<<nunits_, SYMV_WARPS * 32, symv_smem_, s_>>>(d_units_, d_subs_, d_F_, d_V_, d_xb_, d_ypart_, d_t_, nullptr);
     });
     info->symv_F_bytes = tri + vec;
     if (implicit_) {              // the two passes over L_bb (its triangle read twice)
@@ -1171,7 +1171,7 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
         info->symv_S_bytes = 2.0 * tri + 2.0 * vec;
     } else {
         info->symv_S_ms = timeit([&] {
-            k_symv_units<double><<<nunits_, 128, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_,
+            k_symv_units<double><<<nunits_, SYMV_WARPS * 32, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_,
                                                                    nullptr);
         });
         info->symv_S_bytes = tri + vec;

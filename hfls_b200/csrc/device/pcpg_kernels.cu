@@ -61,7 +61,6 @@ __device__ __forceinline__ void reduce_scatter32(double (&p)[32], int lane) {
     }
 }
 
-constexpr int SYMV_WARPS = 4;
 
 
 // SYMV over work units (kinds 0 and 2) and V^T x (kind 1) in one launch; the
