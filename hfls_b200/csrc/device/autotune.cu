@@ -6,8 +6,10 @@
 // 32-row tile rows nt).  Small units give more CTAs per SM (less shared
 // memory for the unit's row window) and more partial sums to reduce; large
 // units the reverse.  The tuner times the F launch on the problem's own tiles
-// for each candidate unit size, bucket by bucket (coordinate descent from the
-// default), keeps the fastest schedule per (device, problem class) for the
+// for each candidate unit size, first the same size in every bucket (the
+// largest window of the launch sets every CTA's shared memory), then bucket
+// by bucket (coordinate descent from the best uniform schedule), keeps the
+// fastest schedule per (device, problem class) for the
 // life of the process, and reads / extends an optional JSON file of tuned
 // schedules:
 //   {"schedules": [{"key": "<device>|<class>", "tiles": [t0, t1, t2, t3, t4]}, ...]}
@@ -314,9 +316,19 @@ int Engine::autotune_symv(std::string &err) {
         ms = f / 3.0;
         return HTF_OK;
     };
+    // the launch's shared memory (and so its CTAs per SM) follows the largest
+    // window of any bucket, which one-bucket steps cannot lower: uniform
+    // schedules first, then coordinate descent per bucket from the best one
     std::vector<int> best(SYMV_BUCKETS, SYMV_DEFAULT_TILES);
     double best_ms = 0.0;
     int rc = time_of(best, best_ms);
+    for (int c : CANDIDATES) {
+        if (rc || c == SYMV_DEFAULT_TILES) continue;
+        std::vector<int> t(SYMV_BUCKETS, c);
+        double ms = 0.0;
+        if ((rc = time_of(t, ms))) break;
+        if (ms < best_ms) { best_ms = ms; best = t; }
+    }
     for (int b = 0; !rc && b < SYMV_BUCKETS; ++b) {
         if (!present[b]) continue;
         for (int c : CANDIDATES) {
