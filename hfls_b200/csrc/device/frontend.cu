@@ -431,6 +431,7 @@ int frontend_on_device(Problem &p, std::vector<int> &node_ptr, std::vector<int> 
     k_fe_node_unique<<<blocks_for(nn, 256), 256>>>(nn, off, bucket, nptr);
     ull nU = 0;
     if ((e = scan(nptr, nn + 1, nU, mem)) != cudaSuccess) return fail();
+    if (nU > 0x7fffffffull) { err = "front-end: too many (node, subdomain) pairs"; return HTF_EINVAL; }
     // 2. the nodes of every subdomain, sorted
     step = "subdomain nodes";
     int *nsub = mem.get<int>(nU, e);
