@@ -52,7 +52,12 @@
 namespace htf {
 
 constexpr int TC_SLAB_A = 128 * 32;          // floats per A slab (16 KB)
-constexpr unsigned TC_WAIT_LIMIT = 1u << 26;  // bounded spin on mbarriers
+// bounded waits on mbarriers: TC_WAIT_LIMIT tries of up to TC_WAIT_HINT_NS
+// each (a waiting thread is suspended until the phase completes or the hint
+// runs out, so waiting warps leave the issue slots to the working ones);
+// at most ~10 s in all before the wait reports a time-out
+constexpr unsigned TC_WAIT_LIMIT = 1u << 20;
+constexpr unsigned TC_WAIT_HINT_NS = 10000;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -72,10 +77,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
     for (unsigned it = 0; it < TC_WAIT_LIMIT; ++it) {
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}"
             : "=r"(done)
-            : "r"(smem_u32(bar)), "r"(parity)
+            : "r"(smem_u32(bar)), "r"(parity), "r"(TC_WAIT_HINT_NS)
             : "memory");
         if (done) return true;
     }
