@@ -545,6 +545,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision multi-load-case measurement")
+    ap.add_argument("--mixed-only", action="store_true",
+                    help="only the mixed-precision measurement on the 512-subdomain cube (for launch lists)")
     ap.add_argument("--no-cube", action="store_true", help="skip the 512-subdomain cube measurement")
     ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS,
                     help="requests of the seeded serving stream to serve (0 skips the serving measurement)")
@@ -565,6 +567,13 @@ def main():
 
     rank, world, local, dist = dist_setup(args.gpus)
     import hfls_b200 as hb
+    if args.mixed_only:
+        out = run_mixed(hb, local, dist, None)
+        if rank == 0:
+            print(json.dumps({"mixed": out}))
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
     if args.setup_only:
         s = hb.Solver(dict(OPTS, device=str(local)))
         s.set_mesh(hb.generate_mesh(uneven_spec(hb)))
