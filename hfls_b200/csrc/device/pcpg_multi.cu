@@ -271,7 +271,7 @@ __device__ __forceinline__ double row_value(int r, int K, int j, const int *__re
 // outputs in registers (rows rg + RG i, cases jg + JG c: conflict-free
 // shared-memory reads), summed over the columns in order.
 template <int K>
-__global__ void __launch_bounds__(256) k_correct_multi(const SubDev *__restrict__ subs,
+__global__ void __launch_bounds__(256, 2) k_correct_multi(const SubDev *__restrict__ subs,
                                                        const ClusterDev *__restrict__ cl,
                                                        const double *__restrict__ V, const int *__restrict__ bcr,
                                                        const double *__restrict__ s, double *__restrict__ yb) {
@@ -299,14 +299,36 @@ __global__ void __launch_bounds__(256) k_correct_multi(const SubDev *__restrict_
     for (int i = 0; i < RPT; ++i)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[i][c] = 0.0;
+    // the next V chunk is loaded into registers while the current one multiplies
+    constexpr int VPT = QC * 128 / 256;               // V values per thread and chunk
+    double vr[VPT];
+    auto fetch = [&](int q0) {
+#pragma unroll
+        for (int u = 0; u < VPT; ++u) {
+            const int o = threadIdx.x + 256 * u, q = o >> 7, r = o & 127;
+            vr[u] = (q0 + q < nc && r < rend) ? Vd[(size_t)(q0 + q) * sd.nbp + r] : 0.0;
+        }
+    };
+    fetch(0);
+    // this thread's y entries, read now so their latency overlaps the products
+    double yv[RPT][4];
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        const int row = rg + RG * i;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            yv[i][c] = row < rend ? yb[((size_t)sd.xb_off + r0 + row) * K + jg + JG * c] : 0.0;
+    }
     for (int q0 = 0; q0 < nc; q0 += QC) {
         const int qn = min(QC, nc - q0);
         __syncthreads();                              // s_d staged, the previous chunk consumed
-        for (int o = threadIdx.x; o < qn * 128; o += blockDim.x) {
-            const int q = o >> 7, r = o & 127;
-            vs[q][r] = r < rend ? Vd[(size_t)(q0 + q) * sd.nbp + r] : 0.0;
+#pragma unroll
+        for (int u = 0; u < VPT; ++u) {
+            const int o = threadIdx.x + 256 * u;
+            vs[o >> 7][o & 127] = vr[u];
         }
         __syncthreads();
+        if (q0 + QC < nc) fetch(q0 + QC);
         for (int q = 0; q < qn; ++q) {
             const double *sq = ss + (q0 + q) * K + jg;
             double sv[4];
@@ -326,7 +348,7 @@ __global__ void __launch_bounds__(256) k_correct_multi(const SubDev *__restrict_
         if (row < rend) {
             double *y = yb + ((size_t)sd.xb_off + r0 + row) * K + jg;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) y[JG * c] -= acc[i][c];
+            for (int c = 0; c < 4; ++c) y[JG * c] = yv[i][c] - acc[i][c];
         }
     }
 }
