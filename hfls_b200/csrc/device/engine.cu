@@ -331,11 +331,16 @@ int Engine::upload_layout(Problem &p, std::string &err) {
         std::vector<int> bcrows(std::max(bcr, 1)), bptr(std::max(bce, 1));
         std::vector<int> bpos;
         std::vector<double> bval;
-        for (int d = 0; d < nsub_; ++d) {
+#pragma omp parallel for schedule(dynamic, 16)
+        for (int d = 0; d < nsub_; ++d) {              // disjoint ranges of R per subdomain
             const Subdomain &s = p.sub[d];
             const SubDev &h = hs_[d];
             for (int j = 0; j < 6; ++j)
                 for (int l = 0; l < s.n; ++l) R[h.R_off + (size_t)j * h.N + s.perm[l]] = s.R[l + (size_t)j * s.n];
+        }
+        for (int d = 0; d < nsub_; ++d) {
+            const Subdomain &s = p.sub[d];
+            const SubDev &h = hs_[d];
             for (int q = 0; q < h.c; ++q) bcrows[h.bcr_off + q] = s.bc_rows[q];
             // entries grouped by compressed row
             std::vector<std::vector<std::pair<int, double>>> rows(h.c);
@@ -678,6 +683,7 @@ int Engine::outer_coarse(Problem &p, std::string &err) {
     const int m = 6 * ncl_;
     std::vector<int> gcl(2 * (size_t)nlam_, -1);
     std::vector<double> gval(12 * (size_t)nlam_, 0.0);
+#pragma omp parallel for schedule(static, 4096)
     for (int r = 0; r < nlam_; ++r) {
         for (int k = 0; k < 2; ++k) {
             int d = p.rows[r].sub[k];
@@ -706,16 +712,30 @@ int Engine::outer_coarse(Problem &p, std::string &err) {
             crow[c].push_back(r);
             for (int q = 0; q < 6; ++q) cval[c].push_back(gval[6 * (2 * (size_t)r + k) + q]);
         }
-    for (int r = 0; r < nlam_; ++r)
-        for (int k1 = 0; k1 < 2; ++k1)
-            for (int k2 = 0; k2 < 2; ++k2) {
-                int c1 = gcl[2 * r + k1], c2 = gcl[2 * r + k2];
-                if (c1 < 0 || c2 < 0) continue;
-                for (int a = 0; a < 6; ++a)
-                    for (int b = 0; b < 6; ++b)
-                        GtG[(6 * c1 + a) + size_t(6 * c2 + b) * m] +=
-                            gval[6 * (2 * (size_t)r + k1) + a] * gval[6 * (2 * (size_t)r + k2) + b];
-            }
+    // Gf^T Gf: partial sums over a fixed number of row chunks (independent of
+    // the thread count), added in chunk order; small problems keep one chunk
+    const int nch = (nlam_ >= (1 << 16) && m <= 512) ? 32 : 1;
+    std::vector<std::vector<double>> gpartial(nch);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int ch = 0; ch < nch; ++ch) {
+        std::vector<double> &P = gpartial[ch];
+        P.assign(size_t(m) * m, 0.0);
+        const int r0 = int((long long)nlam_ * ch / nch), r1 = int((long long)nlam_ * (ch + 1) / nch);
+        for (int r = r0; r < r1; ++r)
+            for (int k1 = 0; k1 < 2; ++k1)
+                for (int k2 = 0; k2 < 2; ++k2) {
+                    int c1 = gcl[2 * r + k1], c2 = gcl[2 * r + k2];
+                    if (c1 < 0 || c2 < 0) continue;
+                    for (int a = 0; a < 6; ++a)
+                        for (int b = 0; b < 6; ++b)
+                            P[(6 * c1 + a) + size_t(6 * c2 + b) * m] +=
+                                gval[6 * (2 * (size_t)r + k1) + a] * gval[6 * (2 * (size_t)r + k2) + b];
+                }
+    }
+    if (nch == 1) GtG.swap(gpartial[0]);
+    else
+        for (int ch = 0; ch < nch; ++ch)
+            for (size_t i = 0; i < GtG.size(); ++i) GtG[i] += gpartial[ch][i];
     if (opt_.print_matrices >= 2) {               // for htf_dump
         gtg_ = GtG;
         gcl_ = gcl;
