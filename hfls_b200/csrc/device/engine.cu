@@ -3,6 +3,7 @@
 //   pcpg    Cluster::pcpg + printVTK reconstruction (Cluster.cpp:1363-1458, 1648-1678)
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -241,6 +242,11 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     const long long XWAVE = 1LL << 29;           // 4 GiB
     xwave_.assign(1, 0);
     xwave_max_ = 0;
+    // factor waves of at most FCAP doubles of panels (a subdomain larger than that is a wave of its own)
+    const long long FCAP = opt_.factor_wave_gb > 0.0 ? std::max(1LL, (long long)(opt_.factor_wave_gb * 1e9 / 8.0))
+                                                     : LLONG_MAX;
+    fwave_.assign(1, 0);
+    long long kwave_max = 0;
     int xb = 0, nf = 0, t_off = 0, bcr = 0, bce = 0;
     for (int d = 0; d < nsub_; ++d) {
         const Subdomain &s = p.sub[d];
@@ -249,12 +255,20 @@ int Engine::upload_layout(Problem &p, std::string &err) {
         h.nt = (s.nb + TILE - 1) / TILE;
         h.nbp = h.nt * TILE;
         h.N = h.nr + h.nbp;
-        h.K_off = K_off; K_off += kpanel_doubles(h.nr, h.nbp);
+        const long long kp = kpanel_doubles(h.nr, h.nbp);
+        const bool new_fwave = K_off > 0 && K_off + kp > FCAP;
+        if (new_fwave) {
+            fwave_.push_back(d);
+            K_off = 0;
+        }
+        h.K_off = K_off; K_off += kp;
+        kwave_max = std::max(kwave_max, K_off);
         h.K_bset = kpanel_interior(h.nr, h.N);
         h.T_off = T_off; T_off += (long long)h.nt * (h.nt + 1) / 2;
-        // L_bb^{-1} scratch of the F_i set-up, in waves of subdomains of at most XWAVE doubles
+        // L_bb^{-1} scratch of the F_i set-up, in waves of subdomains of at most XWAVE doubles that
+        // never cross a factor wave
         const long long xs = (long long)h.nbp * h.nbp;
-        if (X_off > 0 && X_off + xs > XWAVE) {
+        if (X_off > 0 && (new_fwave || X_off + xs > XWAVE)) {
             xwave_.push_back(d);
             X_off = 0;
         }
@@ -278,6 +292,12 @@ int Engine::upload_layout(Problem &p, std::string &err) {
         for (int q = 0; q < 6; ++q) { h.fix[q] = s.perm[s.fix[q]]; h.fix_diag[q] = 0.0; }
     }
     xwave_.push_back(nsub_);
+    fwave_.push_back(nsub_);
+    waves_ = fwave_.size() > 2;
+    if (waves_ && (!opt_.mixed || opt_.preconditioner == "Dirichlet_implicit" || opt_.print_matrices >= 2)) {
+        err = "factor_wave_gb needs precision=mixed, an explicit preconditioner and print_matrices < 2";
+        return HTF_EINVAL;
+    }
     nslots_ = xb;
     nfull_ = nf;
     ntiles_ = T_off;
@@ -306,8 +326,8 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     d_subs_ = alloc<SubDev>(nsub_, err, rc);
     d_cl_ = alloc<ClusterDev>(ncl_, err, rc);
     d_all_subs_ = alloc<int>(nsub_, err, rc);
-    d_K_ = alloc<double>(K_off, err, rc);
-    kpanel_total_ = K_off;
+    d_K_ = alloc<double>(kwave_max, err, rc);
+    kpanel_total_ = kwave_max;
     d_F_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);
     implicit_ = opt_.preconditioner == "Dirichlet_implicit";
     if (!implicit_) d_S_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);   // implicit: S applied through L_bb
@@ -518,142 +538,116 @@ int Engine::factorize(Problem &p, std::string &err) {
         ncol = std::max(ncol, c + 1);
         for (int a = 0; a < 8; ++a) mask[m.elems[8 * (size_t)e + a]] |= 1u << c;
     }
-    std::vector<int> order(ne), cptr(ncol + 1, 0);
-    for (int e = 0; e < ne; ++e) cptr[col[e] + 1]++;
-    for (int c = 0; c < ncol; ++c) cptr[c + 1] += cptr[c];
+    // elements grouped by factor wave, then colour (with one wave: colour order)
+    const int nfw = int(fwave_.size()) - 1;
+    std::vector<int> wave_of(nsub_);
+    for (int w = 0; w < nfw; ++w)
+        for (int d = fwave_[w]; d < fwave_[w + 1]; ++d) wave_of[d] = w;
+    std::vector<int> order(ne);
+    ecptr_.assign((size_t)nfw * ncol + 1, 0);
+    for (int e = 0; e < ne; ++e) ecptr_[(size_t)wave_of[m.elem_sub[e]] * ncol + col[e] + 1]++;
+    for (size_t i = 0; i + 1 < ecptr_.size(); ++i) ecptr_[i + 1] += ecptr_[i];
     {
-        std::vector<int> pos(cptr.begin(), cptr.end() - 1);
-        for (int e = 0; e < ne; ++e) order[pos[col[e]]++] = e;
+        std::vector<int> pos(ecptr_.begin(), ecptr_.end() - 1);
+        for (int e = 0; e < ne; ++e) order[pos[(size_t)wave_of[m.elem_sub[e]] * ncol + col[e]]++] = e;
     }
-    double *d_ec = alloc<double>(ec.size(), err, rc);
-    int *d_ep = alloc<int>(ep.size(), err, rc);
-    int *d_es = alloc<int>(ne, err, rc);
-    int *d_order = alloc<int>(ne, err, rc);
-    double *d_E = alloc<double>(nsub_, err, rc);
-    double *d_nu = alloc<double>(nsub_, err, rc);
+    ncol_ = ncol;
+    d_ec_ = alloc<double>(ec.size(), err, rc);
+    d_ep_ = alloc<int>(ep.size(), err, rc);
+    d_es_ = alloc<int>(ne, err, rc);
+    d_order_ = alloc<int>(ne, err, rc);
+    d_E_ = alloc<double>(nsub_, err, rc);
+    d_nu_ = alloc<double>(nsub_, err, rc);
     if (rc) return rc;
-    CK(cudaMemcpyAsync(d_ec, ec.data(), ec.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
-    CK(cudaMemcpyAsync(d_ep, ep.data(), ep.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
-    CK(cudaMemcpyAsync(d_es, m.elem_sub.data(), ne * sizeof(int), cudaMemcpyHostToDevice, s_));
-    CK(cudaMemcpyAsync(d_order, order.data(), ne * sizeof(int), cudaMemcpyHostToDevice, s_));
-    CK(cudaMemcpyAsync(d_E, m.sub_E.data(), nsub_ * sizeof(double), cudaMemcpyHostToDevice, s_));
-    CK(cudaMemcpyAsync(d_nu, m.sub_nu.data(), nsub_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_ec_, ec.data(), ec.size() * sizeof(double), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_ep_, ep.data(), ep.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_es_, m.elem_sub.data(), ne * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_order_, order.data(), ne * sizeof(int), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_E_, m.sub_E.data(), nsub_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+    CK(cudaMemcpyAsync(d_nu_, m.sub_nu.data(), nsub_ * sizeof(double), cudaMemcpyHostToDevice, s_));
     CK(cudaMemcpyAsync(d_subs_, hs_.data(), nsub_ * sizeof(SubDev), cudaMemcpyHostToDevice, s_));
     CK(set_gauss_points(s_));
-    long long Ktot = 0;
-    for (auto &h : hs_) Ktot += kpanel_doubles(h.nr, h.nbp);
-    CK(cudaMemsetAsync(d_K_, 0, Ktot * sizeof(double), s_));
+    for (int c = 0; c < 3; ++c) bf_[c] = m.body_force[c];
     CK(cudaMemsetAsync(d_f_, 0, (size_t)nfull_ * p.nrhs * sizeof(double), s_));
-    for (int c = 0; c < ncol; ++c) {
-        int cnt = cptr[c + 1] - cptr[c];
-        if (cnt == 0) continue;
-        k_assemble<<<cnt, 64, 0, s_>>>(d_order + cptr[c], cnt, d_ec, d_es, d_ep, d_E, d_nu, d_subs_, d_K_, d_f_,
-                                       m.body_force[0], m.body_force[1], m.body_force[2]);
-    }
-    CK(cudaGetLastError());
-    k_regularize<<<nsub_, 128, 0, s_>>>(d_subs_, nsub_, d_K_);
-    CK(cudaGetLastError());
-    if (opt_.print_matrices >= 2) {               // K_reg panels before the factorisation, for htf_dump
-        dumpK_.assign(size_t(kpanel_total_), 0.0);
-        CK(cudaMemcpyAsync(dumpK_.data(), d_K_, dumpK_.size() * sizeof(double), cudaMemcpyDeviceToHost, s_));
-        CK(cudaStreamSynchronize(s_));
-    }
     // explicit Dirichlet: snapshot S_reg - D_fix as tiles; implicit: nothing (L_bb stays in the factor)
     const bool dirichlet = opt_.preconditioner == "Dirichlet_explicit";
-    int max_nt = 0, max_tiles = 0;
-    for (auto &h : hs_) { max_nt = std::max(max_nt, h.nt); max_tiles = std::max(max_tiles, h.nt * (h.nt + 1) / 2); }
     const bool lumped = opt_.preconditioner == "lumped";
+    max_tiles_ = 0;
+    for (auto &h : hs_) max_tiles_ = std::max(max_tiles_, h.nt * (h.nt + 1) / 2);
     if ((dirichlet || lumped) && !d_S_) {
         err = "preconditioner blocks were not allocated";
         return HTF_EINVAL;
     }
-    if (lumped) {              // lumped: K_bb before any elimination
-        k_snapshot<<<dim3(nsub_, max_tiles), 256, 0, s_>>>(d_all_subs_, d_subs_, d_K_, d_S_);
-        CK(cudaGetLastError());
-    }
-    // step tables
-    std::vector<std::vector<StepDesc>> steps;
-    std::vector<std::vector<int>> snap_after;      // subdomains whose interior ends after step s
-    std::vector<int> snap_first;                   // nr == 0
-    for (int d = 0; d < nsub_; ++d) {
-        const SubDev &h = hs_[d];
-        std::vector<std::pair<int, int>> blocks;      // steps never cross from the interior into the b set
-        for (int k = 0; k < h.nr; k += CHOL_STEP) blocks.push_back({k, std::min(CHOL_STEP, h.nr - k)});
-        int interior_steps = int(blocks.size());
-        for (int k = h.nr; k < h.N; k += CHOL_STEP) blocks.push_back({k, std::min(CHOL_STEP, h.N - k)});
-        if (steps.size() < blocks.size()) { steps.resize(blocks.size()); snap_after.resize(blocks.size()); }
-        for (size_t s = 0; s < blocks.size(); ++s) steps[s].push_back({d, blocks[s].first, blocks[s].second, 0, 0});
-        if (interior_steps == 0) snap_first.push_back(d);
-        else snap_after[interior_steps - 1].push_back(d);
-    }
-    std::vector<StepDesc> flat;
-    std::vector<size_t> soff;
-    std::vector<int> ntri, nrb;                    // flattened grid sizes per step
-    for (auto &v : steps) {
-        int tri = 0, rb = 0;
-        for (auto &x : v) {
-            const int rows = hs_[x.d].N - x.k - x.nb, nbr = (rows + 63) / 64;
-            x.tri0 = tri; tri += nbr * (nbr + 1) / 2;
-            x.rb0 = rb; rb += (rows + 127) / 128;
+    // step tables of every wave
+    fw_.assign(nfw, FactorWave());
+    for (int w = 0; w < nfw; ++w) {
+        FactorWave &W = fw_[w];
+        W.a = fwave_[w];
+        W.b = fwave_[w + 1];
+        W.eoff = (size_t)w * ncol;
+        std::vector<std::vector<StepDesc>> steps;
+        std::vector<std::vector<int>> snap_after;      // subdomains whose interior ends after step s
+        std::vector<int> snap_first;                   // nr == 0
+        for (int d = W.a; d < W.b; ++d) {
+            const SubDev &h = hs_[d];
+            W.kdoubles += kpanel_doubles(h.nr, h.nbp);
+            std::vector<std::pair<int, int>> blocks;      // steps never cross from the interior into the b set
+            for (int k = 0; k < h.nr; k += CHOL_STEP) blocks.push_back({k, std::min(CHOL_STEP, h.nr - k)});
+            int interior_steps = int(blocks.size());
+            for (int k = h.nr; k < h.N; k += CHOL_STEP) blocks.push_back({k, std::min(CHOL_STEP, h.N - k)});
+            if (steps.size() < blocks.size()) { steps.resize(blocks.size()); snap_after.resize(blocks.size()); }
+            for (size_t s = 0; s < blocks.size(); ++s) steps[s].push_back({d, blocks[s].first, blocks[s].second, 0, 0});
+            if (interior_steps == 0) snap_first.push_back(d);
+            else snap_after[interior_steps - 1].push_back(d);
         }
-        ntri.push_back(tri);
-        nrb.push_back(rb);
-        soff.push_back(flat.size());
-        flat.insert(flat.end(), v.begin(), v.end());
-    }
-    std::vector<int> snap_flat;
-    std::vector<size_t> snap_off;
-    for (auto &v : snap_after) { snap_off.push_back(snap_flat.size()); snap_flat.insert(snap_flat.end(), v.begin(), v.end()); }
-    size_t snap_first_off = snap_flat.size();
-    snap_flat.insert(snap_flat.end(), snap_first.begin(), snap_first.end());
-    // entry hints of every step's SYRK and panel-solve grids
-    std::vector<int> hints;
-    std::vector<size_t> htri, hrb;
-    for (size_t s = 0; s < steps.size(); ++s) {
-        htri.push_back(hints.size());
-        step_hints(steps[s], ntri[s], true, hints);
-        hrb.push_back(hints.size());
-        step_hints(steps[s], nrb[s], false, hints);
-    }
-    StepDesc *d_steps = alloc<StepDesc>(flat.size(), err, rc);
-    int *d_snap = alloc<int>(std::max<size_t>(snap_flat.size(), 1), err, rc);
-    int *d_hints = alloc<int>(hints.size(), err, rc);
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(d_steps, flat.data(), flat.size() * sizeof(StepDesc), cudaMemcpyHostToDevice, s_));
-    CK(cudaMemcpyAsync(d_hints, hints.data(), hints.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
-    if (!snap_flat.empty())
-        CK(cudaMemcpyAsync(d_snap, snap_flat.data(), snap_flat.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
-    if (dirichlet && !snap_first.empty()) {
-        k_snapshot<<<dim3(int(snap_first.size()), max_tiles), 256, 0, s_>>>(d_snap + snap_first_off, d_subs_, d_K_, d_S_);
-        CK(cudaGetLastError());
+        std::vector<StepDesc> flat;
+        for (auto &v : steps) {
+            int tri = 0, rb = 0;
+            for (auto &x : v) {
+                const int rows = hs_[x.d].N - x.k - x.nb, nbr = (rows + 63) / 64;
+                x.tri0 = tri; tri += nbr * (nbr + 1) / 2;
+                x.rb0 = rb; rb += (rows + 127) / 128;
+            }
+            W.cnt.push_back(int(v.size()));
+            W.ntri.push_back(tri);
+            W.nrb.push_back(rb);
+            W.soff.push_back(flat.size());
+            flat.insert(flat.end(), v.begin(), v.end());
+        }
+        std::vector<int> snap_flat;
+        for (auto &v : snap_after) {
+            W.snap_off.push_back(snap_flat.size());
+            W.nsnap.push_back(int(v.size()));
+            snap_flat.insert(snap_flat.end(), v.begin(), v.end());
+        }
+        W.snap_first_off = snap_flat.size();
+        W.nsnap_first = int(snap_first.size());
+        snap_flat.insert(snap_flat.end(), snap_first.begin(), snap_first.end());
+        // entry hints of every step's SYRK and panel-solve grids
+        std::vector<int> hints;
+        for (size_t s = 0; s < steps.size(); ++s) {
+            W.htri.push_back(hints.size());
+            step_hints(steps[s], W.ntri[s], true, hints);
+            W.hrb.push_back(hints.size());
+            step_hints(steps[s], W.nrb[s], false, hints);
+        }
+        W.steps = alloc<StepDesc>(std::max<size_t>(flat.size(), 1), err, rc);
+        W.snap = alloc<int>(std::max<size_t>(snap_flat.size(), 1), err, rc);
+        W.hints = alloc<int>(std::max<size_t>(hints.size(), 1), err, rc);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(W.steps, flat.data(), flat.size() * sizeof(StepDesc), cudaMemcpyHostToDevice, s_));
+        if (!hints.empty())
+            CK(cudaMemcpyAsync(W.hints, hints.data(), hints.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+        if (!snap_flat.empty())
+            CK(cudaMemcpyAsync(W.snap, snap_flat.data(), snap_flat.size() * sizeof(int), cudaMemcpyHostToDevice, s_));
+        // the host copies of flat, hints and snap_flat must outlive the asynchronous copies
+        CK(cudaStreamSynchronize(s_));
     }
     CK(cudaFuncSetAttribute(k_syrk_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SYRK_SMEM));
-    for (size_t s = 0; s < steps.size(); ++s) {
-        const int cnt = int(steps[s].size());
-        const StepDesc *ds = d_steps + soff[s];
-        k_potrf_diag<<<cnt, CHOL_STEP, 0, s_>>>(ds, d_subs_, d_K_, d_status_);
-        if (nrb[s] > 0) k_trsm_panel<<<nrb[s], 128, 0, s_>>>(ds, cnt, d_subs_, d_K_, d_hints + hrb[s]);
-        if (ntri[s] > 0)
-            k_syrk_update<<<ntri[s], 256, SYRK_SMEM, s_>>>(ds, cnt, d_subs_, d_K_, d_hints + htri[s]);
-        if (dirichlet && !snap_after[s].empty())
-            k_snapshot<<<dim3(int(snap_after[s].size()), max_tiles), 256, 0, s_>>>(d_snap + snap_off[s], d_subs_, d_K_, d_S_);
-        CK(cudaGetLastError());
-    }
-    // X = L_bb^{-1}, F = X^T X, in waves of subdomains sharing one scratch buffer
     {
         double *X = nullptr;
         CK(cudaMalloc(&X, std::max<long long>(xwave_max_, 1) * sizeof(double)));
-        for (size_t w = 0; w + 1 < xwave_.size(); ++w) {
-            const int a = xwave_[w], b = xwave_[w + 1];
-            int wnt = 0, wtiles = 0;
-            for (int d = a; d < b; ++d) {
-                wnt = std::max(wnt, hs_[d].nt);
-                wtiles = std::max(wtiles, hs_[d].nt * (hs_[d].nt + 1) / 2);
-            }
-            for (int i = 0; i < wnt; ++i)
-                k_trtri_step<<<dim3(b - a, i + 1), 256, 0, s_>>>(i, d_all_subs_ + a, d_subs_, d_K_, X);
-            k_lauum_tiles<<<dim3(b - a, wtiles), 256, 0, s_>>>(d_all_subs_ + a, d_subs_, X, d_F_);
-        }
+        for (int w = 0; w < nfw; ++w) factor_wave(w, true, X);
         const cudaError_t le = cudaGetLastError();
         const cudaError_t se = cudaStreamSynchronize(s_);
         cudaFree(X);
@@ -674,7 +668,61 @@ int Engine::factorize(Problem &p, std::string &err) {
                   std::to_string(status[d] - 1) + ")";
             return HTF_ENOTSPD;
         }
+    if (!waves_) {                  // resident factors: the element data is not needed again
+        for (void *q : {(void *)d_ec_, (void *)d_ep_, (void *)d_es_, (void *)d_order_, (void *)d_E_, (void *)d_nu_})
+            release(q);
+        d_ec_ = d_E_ = d_nu_ = nullptr;
+        d_ep_ = d_es_ = d_order_ = nullptr;
+    }
     return HTF_OK;
+}
+
+void Engine::factor_wave(int w, bool build, double *X) {
+    const FactorWave &W = fw_[w];
+    const bool dirichlet = opt_.preconditioner == "Dirichlet_explicit";
+    const bool lumped = opt_.preconditioner == "lumped";
+    const int nw = W.b - W.a;
+    cudaMemsetAsync(d_K_, 0, W.kdoubles * sizeof(double), s_);
+    for (int c = 0; c < ncol_; ++c) {
+        const int e0 = ecptr_[W.eoff + c], cnt = ecptr_[W.eoff + c + 1] - e0;
+        if (cnt == 0) continue;
+        k_assemble<<<cnt, 64, 0, s_>>>(d_order_ + e0, cnt, d_ec_, d_es_, d_ep_, d_E_, d_nu_, d_subs_, d_K_,
+                                       build ? d_f_ : nullptr, bf_[0], bf_[1], bf_[2]);
+    }
+    k_regularize<<<nw, 128, 0, s_>>>(d_subs_ + W.a, nw, d_K_);
+    if (build && opt_.print_matrices >= 2) {      // K_reg panels before the factorisation, for htf_dump (one wave)
+        dumpK_.assign(size_t(kpanel_total_), 0.0);
+        cudaMemcpyAsync(dumpK_.data(), d_K_, dumpK_.size() * sizeof(double), cudaMemcpyDeviceToHost, s_);
+        cudaStreamSynchronize(s_);
+    }
+    if (build && lumped)            // lumped: K_bb before any elimination
+        k_snapshot<<<dim3(nw, max_tiles_), 256, 0, s_>>>(d_all_subs_ + W.a, d_subs_, d_K_, d_S_);
+    if (build && dirichlet && W.nsnap_first > 0)
+        k_snapshot<<<dim3(W.nsnap_first, max_tiles_), 256, 0, s_>>>(W.snap + W.snap_first_off, d_subs_, d_K_, d_S_);
+    for (size_t s = 0; s < W.soff.size(); ++s) {
+        const int cnt = W.cnt[s];
+        const StepDesc *ds = W.steps + W.soff[s];
+        k_potrf_diag<<<cnt, CHOL_STEP, 0, s_>>>(ds, d_subs_, d_K_, d_status_);
+        if (W.nrb[s] > 0) k_trsm_panel<<<W.nrb[s], 128, 0, s_>>>(ds, cnt, d_subs_, d_K_, W.hints + W.hrb[s]);
+        if (W.ntri[s] > 0)
+            k_syrk_update<<<W.ntri[s], 256, SYRK_SMEM, s_>>>(ds, cnt, d_subs_, d_K_, W.hints + W.htri[s]);
+        if (build && dirichlet && W.nsnap[s] > 0)
+            k_snapshot<<<dim3(W.nsnap[s], max_tiles_), 256, 0, s_>>>(W.snap + W.snap_off[s], d_subs_, d_K_, d_S_);
+    }
+    if (!build) return;
+    // X = L_bb^{-1}, F = X^T X, in the L_bb^{-1} waves of this factor wave, sharing one scratch buffer
+    for (size_t x = 0; x + 1 < xwave_.size(); ++x) {
+        const int a = xwave_[x], b = xwave_[x + 1];
+        if (a < W.a || b > W.b) continue;
+        int wnt = 0, wtiles = 0;
+        for (int d = a; d < b; ++d) {
+            wnt = std::max(wnt, hs_[d].nt);
+            wtiles = std::max(wtiles, hs_[d].nt * (hs_[d].nt + 1) / 2);
+        }
+        for (int i = 0; i < wnt; ++i)
+            k_trtri_step<<<dim3(b - a, i + 1), 256, 0, s_>>>(i, d_all_subs_ + a, d_subs_, d_K_, X);
+        k_lauum_tiles<<<dim3(b - a, wtiles), 256, 0, s_>>>(d_all_subs_ + a, d_subs_, X, d_F_);
+    }
 }
 
 // Gf = Bf Rf, Rf_d = R_d H_d (Cluster.cpp:1332-1352); (Gf^T Gf)^{-1} (1227-1273)

@@ -134,6 +134,31 @@ private:
     double *d_K_ = nullptr, *d_F_ = nullptr, *d_S_ = nullptr;
     std::vector<int> xwave_;             // subdomain boundaries of the L_bb^{-1} scratch waves
     long long xwave_max_ = 0;            // doubles of the largest wave
+    // factor waves: consecutive subdomains whose panels share d_K_ (one wave
+    // over all subdomains unless opt_.factor_wave_gb > 0); each is a union of
+    // L_bb^{-1} waves, and K_off of a subdomain counts from its wave's start
+    struct FactorWave {
+        int a = 0, b = 0;                        // subdomains [a, b)
+        long long kdoubles = 0;                  // its panels
+        size_t eoff = 0;                         // its first (wave, colour) entry of ecptr_
+        StepDesc *steps = nullptr;               // Cholesky step tables of its subdomains
+        int *snap = nullptr, *hints = nullptr;
+        std::vector<size_t> soff, htri, hrb, snap_off;
+        std::vector<int> cnt, ntri, nrb, nsnap;
+        size_t snap_first_off = 0;
+        int nsnap_first = 0;
+    };
+    std::vector<int> fwave_;             // subdomain boundaries of the factor waves
+    std::vector<FactorWave> fw_;
+    std::vector<int> ecptr_;             // element ranges of d_order_ per (wave, colour)
+    int ncol_ = 0, max_tiles_ = 0;
+    bool waves_ = false;                 // factors dropped between uses (more than one wave)
+    double *d_ec_ = nullptr, *d_E_ = nullptr, *d_nu_ = nullptr;   // element data for re-assembly
+    int *d_ep_ = nullptr, *d_es_ = nullptr, *d_order_ = nullptr;
+    double bf_[3] = {0.0, 0.0, 0.0};
+    // assemble, regularise and factorise wave w; with build also the preconditioner
+    // snapshots, the body-force load and F_i (X: L_bb^{-1} scratch)
+    void factor_wave(int w, bool build, double *X);
     double *d_V_ = nullptr, *d_R_ = nullptr, *d_M_ = nullptr, *d_H_ = nullptr;
     double *d_MT_ = nullptr, *d_mP_ = nullptr, *d_mD_ = nullptr;   // packed symmetric M, its partial sums
     int2 *d_mt_ = nullptr;                     // (cluster, tile row) pairs of M

@@ -567,8 +567,18 @@ int Engine::batch_finish(htf_stats *stats, double &ms, std::string &err) {
 }
 
 void Engine::trsm_multi(double *v, int nrhs) {
-    k_trsm_fwd_multi<<<nsub_, 256, 0, s_>>>(d_subs_, d_K_, v, nfull_, nrhs, nullptr);
-    k_trsm_bwd_multi<<<nsub_, 256, 0, s_>>>(d_subs_, d_K_, v, nfull_, nrhs, nullptr);
+    if (!waves_) {
+        k_trsm_fwd_multi<<<nsub_, 256, 0, s_>>>(d_subs_, d_K_, v, nfull_, nrhs, nullptr);
+        k_trsm_bwd_multi<<<nsub_, 256, 0, s_>>>(d_subs_, d_K_, v, nfull_, nrhs, nullptr);
+        return;
+    }
+    // the factor panels were dropped: assemble and factorise each wave again, then solve its subdomains
+    for (size_t w = 0; w < fw_.size(); ++w) {
+        factor_wave(int(w), false, nullptr);
+        const int a = fw_[w].a, nw = fw_[w].b - fw_[w].a;
+        k_trsm_fwd_multi<<<nw, 256, 0, s_>>>(d_subs_ + a, d_K_, v, nfull_, nrhs, nullptr);
+        k_trsm_bwd_multi<<<nw, 256, 0, s_>>>(d_subs_ + a, d_K_, v, nfull_, nrhs, nullptr);
+    }
 }
 
 int Engine::batch_graph(std::string &err) {

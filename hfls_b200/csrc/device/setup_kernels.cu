@@ -117,7 +117,7 @@ __global__ void k_assemble(const int *__restrict__ elist, int count, const doubl
         }
         Kbuf[kidx(sd, pI, pJ)] += v;
     }
-    if (t < 24) {
+    if (fbuf && t < 24) {             // no fbuf: a re-assembly of the factor alone
         const int i = t >> 3, a = t & 7;
         const double bf = (i == 0) ? bfx : (i == 1) ? bfy : bfz;
         double v = 0.0;

@@ -70,22 +70,6 @@ int mesh_sizes(const htf_mesh_spec &s, int *nn, int *ne, int *ns, int *nc, int *
     return HTF_OK;
 }
 
-double factor_panel_bytes(const htf_mesh_spec &s) {
-    Axes ax;
-    std::string err;
-    if (make_axes(s, ax, err)) return 0.0;
-    // per subdomain n = 3 (w_x+1)(w_y+1)(w_z+1) DOFs; its lower-triangular
-    // column-panel factor holds at least n^2/2 + 16 n doubles
-    double sq[3] = {0.0, 0.0, 0.0}, lin[3] = {0.0, 0.0, 0.0};
-    for (int a = 0; a < 3; ++a)
-        for (int k = 0; k < ax.NS[a]; ++k) {
-            const double w = ax.bound[a][k + 1] - ax.bound[a][k] + 1;
-            sq[a] += w * w;
-            lin[a] += w;
-        }
-    return 8.0 * (0.5 * 9.0 * sq[0] * sq[1] * sq[2] + 16.0 * 3.0 * lin[0] * lin[1] * lin[2]);
-}
-
 int generate_mesh(const htf_mesh_spec &s, Mesh &m, std::string &err) {
     Axes ax;
     int rc = make_axes(s, ax, err);
@@ -236,6 +220,10 @@ int parse_options(const char *s, Options &o, std::string &err) {
         else if (k == "verbose") o.verbose = std::atoi(v.c_str());
         else if (k == "autotune") o.autotune = std::atoi(v.c_str());
         else if (k == "tune_file") o.tune_file = v;
+        else if (k == "factor_wave_gb") {
+            o.factor_wave_gb = std::atof(v.c_str());
+            if (!(o.factor_wave_gb >= 0.0)) { err = "factor_wave_gb must be >= 0"; return HTF_EINVAL; }
+        }
         else if (k == "batch") {
             o.batch = std::atoi(v.c_str());
             if (o.batch != 16 && o.batch != 32) { err = "batch must be 16 or 32"; return HTF_EINVAL; }

@@ -34,7 +34,6 @@ int generate_mesh(const htf_mesh_spec &s, Mesh &m, std::string &err);
 // sum over subdomains of 8 (n_d^2/2 + 16 n_d) (n_d = 3 x nodes of subdomain
 // d): the column-panel factors alone, a lower bound of the device footprint
 // of a spec's problem
-double factor_panel_bytes(const htf_mesh_spec &s);
 int mesh_sizes(const htf_mesh_spec &s, int *nn, int *ne, int *ns, int *nc, int *nd, int *ncr,
                std::string &err);
 int mesh_traction(const htf_mesh_spec &s, uint64_t seed, int n_rhs, double scale, double *f,
@@ -63,6 +62,10 @@ struct Options {
                                                       // problem class) for problems of >= 1 GiB of FP64 tiles;
                                                       // 2 = every problem; 0 = fixed default schedule
     std::string tune_file;                            // JSON file of tuned schedules, read and extended
+    double factor_wave_gb = 0.0;                      // > 0: the factor panels of at most this many GB of
+                                                      // subdomains are held at a time; set-up and every later
+                                                      // K_reg solve assemble and factorise them again, wave
+                                                      // by wave (batched mixed form, explicit preconditioners)
 };
 int parse_options(const char *s, Options &o, std::string &err);
 

@@ -4,7 +4,10 @@
 // A setup thread admits them in order while the estimated device footprint
 // of factors, F_i / S_i and vectors fits the HBM budget and a slot is free,
 // and runs their setup on each request's own stream, overlapping the
-// iterations of the requests already running.  A run thread advances every
+// iterations of the requests already running.  A request whose factor panels
+// do not fit beside the rest holds them a wave of subdomains at a time and
+// has them assembled and factorised again for its start solve and its
+// reconstruction.  A run thread advances every
 // live request one batched mixed-precision PCPG iteration at a time: the
 // FP64 phases of the requests run side by side, each on its own stream forked
 // from and joined back to the server stream, around ONE tensor-core launch
@@ -75,7 +78,7 @@ private:
     void setup_loop();
     void run_loop();
     int prepare(Request &r, std::string &err);
-    size_t estimate(const Problem &p, int nrhs) const;
+    size_t estimate(const Problem &p, int nrhs, double wave_gb) const;
     int rebuild_graph(std::string &err);
     void finish(Request *r, int rc, const std::string &msg);
     void release_graph();
@@ -169,9 +172,7 @@ int Server::submit(const htf_mesh_spec &spec, int nrhs, const double *f, double 
             r->spec.widths[a] = r->widths[a].data();
         }
     r->nrhs = nrhs;
-    // the factor panels alone exceed the budget: fail at once, before any host work
-    const double lower = factor_panel_bytes(r->spec);
-    if (f && lower <= budget_) r->f.assign(f, f + (size_t)3 * nn * nrhs);
+    if (f) r->f.assign(f, f + (size_t)3 * nn * nrhs);
     r->u_out = u;
     r->info.status = HTF_REQ_QUEUED;
     r->info.n_rhs = nrhs;
@@ -180,17 +181,6 @@ int Server::submit(const htf_mesh_spec &spec, int nrhs, const double *f, double 
     r->id = next_id_++;
     r->info.t_submit_ms = now_ms();
     *ticket = r->id;
-    if (lower > budget_) {
-        r->info.bytes_estimate = lower;
-        r->info.rc = HTF_ENOMEM;
-        r->info.status = HTF_REQ_FAILED;
-        r->info.t_done_ms = r->info.t_submit_ms;
-        r->err = "request needs more than " + std::to_string(size_t(lower) >> 20) +
-                 " MiB for its factor panels, more than the server budget";
-        all_[r->id] = std::move(r);
-        cv_.notify_all();
-        return HTF_OK;
-    }
     ++outstanding_;
     queue_.push_back(r.get());
     all_[r->id] = std::move(r);
@@ -222,19 +212,31 @@ int Server::wait(long long ticket, double timeout_ms, htf_request_info *out) {
     return r->info.status == HTF_REQ_DONE ? HTF_OK : r->info.rc;
 }
 
-// device bytes of a request after setup, from the host-side problem (dense
-// K_i, F_i / S_i tiles, setup scratch, V, R, FP32 slabs, coarse M, vectors),
-// with a margin
-size_t Server::estimate(const Problem &p, int nrhs) const {
+// device bytes of a request after setup, from the host-side problem (factor
+// panels of all subdomains, or of the largest factor wave when wave_gb > 0,
+// F_i / S_i tiles, setup scratch, V, R, FP32 slabs, coarse M, vectors), with
+// a margin
+size_t Server::estimate(const Problem &p, int nrhs, double wave_gb) const {
     const double K = opt_.batch;
     double b = 0.0, nslots = 0.0, nfull = 0.0, xs = 0.0;
+    // panels held at once: all, or the largest wave of the engine's partition
+    const double cap = wave_gb > 0.0 ? std::max(1.0, wave_gb * 1e9 / 8.0) : 1e300;
+    double panels = 0.0, wave = 0.0;
+    for (const Subdomain &s : p.sub) {
+        const double nbp = 32.0 * ((s.nb + 31) / 32);
+        const double kp = double(kpanel_doubles(s.n - s.nb, int(nbp)));
+        if (wave > 0.0 && wave + kp > cap) wave = 0.0;
+        wave += kp;
+        panels = std::max(panels, wave);
+    }
+    b += 8.0 * panels;
+    if (wave_gb > 0.0) b += 296.0 * p.mesh.n_elems();     // element data kept for the re-assembly
     for (const Subdomain &s : p.sub) {
         const double nbp = 32.0 * ((s.nb + 31) / 32), N = (s.n - s.nb) + nbp, nt = nbp / 32;
         const double mb = std::ceil(nbp / 128.0), nks = nbp / 32;
         double stored = 0.0;                              // FP32 slabs: lower triangle of 128-row blocks
         for (int m = 0; m < int(mb); ++m) stored += std::min(4.0 * (m + 1), nks);
-        b += 8.0 * (double(kpanel_doubles(s.n - s.nb, int(nbp))) + nt * (nt + 1) * 1024.0 +
-                    nbp * (s.c() + 6) + 6 * N + 2 * nbp);
+        b += 8.0 * (nt * (nt + 1) * 1024.0 + nbp * (s.c() + 6) + 6 * N + 2 * nbp);
         xs += nbp * nbp;
         b += 2.0 * stored * 4096.0 * 4.0;
         nslots += nbp;
@@ -261,12 +263,23 @@ int Server::prepare(Request &r, std::string &err) {
     p.nrhs = r.nrhs;
     if (!r.f.empty()) p.f_nodal = r.f;
     if ((rc = build_problem(p, err, true))) return rc;
-    const size_t est = estimate(p, r.nrhs);
+    // factor panels that do not fit beside the rest are held a wave at a time
+    // and factorised again for each later K_reg solve (set-up start solve and
+    // reconstruction): a wave of half the room left by everything else, at most 16 GB
+    double wave_gb = opt_.factor_wave_gb;
+    size_t est = estimate(p, r.nrhs, wave_gb);
+    if (wave_gb <= 0.0 && double(est) > budget_) {
+        const double rest = double(estimate(p, r.nrhs, 1e-9));
+        wave_gb = std::min(16.0, std::max(1e-3, 0.5 * (budget_ - rest) / 1e9));
+        est = estimate(p, r.nrhs, wave_gb);
+    }
+    p.opt.factor_wave_gb = wave_gb;
     {
         std::unique_lock<std::mutex> lk(mu_);
         r.info.bytes_estimate = double(est);
         if (double(est) > budget_) {
-            err = "request needs about " + std::to_string(est >> 20) + " MiB, more than the server budget";
+            err = "request needs about " + std::to_string(est >> 20) +
+                  " MiB with its factor panels held a wave at a time, more than the server budget";
             return HTF_ENOMEM;
         }
         // admission: waits for memory and a slot (live requests always finish)

@@ -101,7 +101,11 @@ int htf_write_vtk(const char *path, int n_nodes, const double *coords, int n_ele
  * sizes per subdomain-size bucket at set-up, once per process and problem
  * class: 1 for problems of at least 1 GiB of FP64 tiles, 2 for every
  * problem, 0 never), tune_file = <path of a JSON file of tuned schedules,
- * read and extended>, verbose = 0 | 1.                                     */
+ * read and extended>, factor_wave_gb = <GB> (0: every factor panel stays
+ * resident; > 0: the panels of at most that many GB of subdomains are held
+ * at a time and are assembled and factorised again, wave by wave, for each
+ * later K_reg solve — the batched mixed form with an explicit
+ * preconditioner only), verbose = 0 | 1.                                   */
 typedef struct htf_ctx htf_ctx;
 
 int htf_create(const char *options, htf_ctx **ctx);

@@ -186,3 +186,12 @@ def test_header_and_library_from_plain_c(tmp_path):
     assert (int(nn), int(ne), int(ns)) == (125, 64, 8)
     assert "before htf_set_mesh" in msg
     assert (tmp_path / "box.vtk").read_text().startswith("# vtk DataFile Version 3.0\n")
+
+
+def test_factor_wave_option_is_checked():
+    """factor_wave_gb (factor panels held a wave of subdomains at a time) is
+    parsed at htf_create: a negative size is refused with HTF_EINVAL."""
+    with pytest.raises(hb.HTFError) as e:
+        hb.Solver({"factor_wave_gb": "-1"})
+    assert e.value.code == hb.HTF_EINVAL
+    hb.Solver({"factor_wave_gb": "2.5", "precision": "mixed"}).close()

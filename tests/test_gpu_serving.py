@@ -136,3 +136,60 @@ def test_largest_request_of_a_mix_against_tight_fp64():
     s.close()
     for k in range(4):
         assert rel(u[k], u64[k]) < 1e-7, k
+
+
+# 8 subdomains of 6^3 hex8: factor panels of ~4.3 MB each, the larger part of
+# the request's device footprint
+WAVE_SPEC = dict(clusters=(1, 1, 1), subs=(2, 2, 2), elems=(6, 6, 6), jitter=0.1, seed=21,
+                 material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e3, nu=0.3)
+
+
+def test_factor_waves_same_as_resident_factors():
+    """factor_wave_gb = 6 MB holds one subdomain's panels at a time: the set-up
+    factorises wave by wave and the start solve and the reconstruction
+    assemble and factorise every wave again.  Each subdomain's arithmetic is
+    the one of the resident-factor solve, so iterations and displacements
+    agree (to rounding, 1e-13)."""
+    spec = hb.mesh_spec(**WAVE_SPEC)
+    f = hb.traction(spec, seed=31, n_rhs=3)
+    out = []
+    for extra in ({}, {"factor_wave_gb": "0.006"}):
+        s = hb.Solver(dict(OPTS, precision="mixed", **extra))
+        s.set_mesh(hb.generate_mesh(spec))
+        s.setup()
+        out.append(s.solve(f))
+        s.close()
+    (u0, st0), (u1, st1) = out
+    assert list(st1.iterations[:3]) == list(st0.iterations[:3])
+    assert rel(u1, u0) < 1e-13
+
+
+def test_server_holds_factor_panels_in_waves_when_they_do_not_fit():
+    """Factor waves in the server.  Forced (factor_wave_gb = 20 MB, one
+    subdomain of 8^3 hex8 per wave): smaller estimate and device bytes, the
+    displacements of the resident-factor run.  Chosen by admission: a budget
+    just above the forced run's estimate, below the resident-factor estimate,
+    admits the request with its panels held a wave at a time."""
+    spec = hb.mesh_spec(**dict(WAVE_SPEC, elems=(8, 8, 8)))
+    f = hb.traction(spec, seed=31, n_rhs=2)
+    one = hb.Server(OPTS)
+    u0, info0 = one.wait(one.submit(spec, f))
+    one.close()
+    forced = hb.Server(dict(OPTS, factor_wave_gb="0.02"))
+    u1, info1 = forced.wait(forced.submit(spec, f))
+    forced.close()
+    assert info1.bytes < info0.bytes and info1.bytes_estimate < info0.bytes_estimate
+    assert info1.iterations_max == info0.iterations_max
+    assert rel(u1, u0) < 1e-13
+    budget = 1.05 * info1.bytes_estimate
+    assert budget < info0.bytes_estimate
+    srv = hb.Server(OPTS, hbm_budget_bytes=budget)
+    u2, info2 = srv.wait(srv.submit(spec, f))
+    srv.close()
+    assert info2.rc == 0 and info2.status == hb.HTF_REQ_DONE
+    assert info2.bytes_estimate <= budget
+    assert info2.iterations_max == info0.iterations_max
+    assert rel(u2, u0) < 1e-13
+    print("resident / forced waves / admitted in waves: estimate MB %.1f %.1f %.1f, device MB %.1f %.1f %.1f" % (
+        info0.bytes_estimate / 1e6, info1.bytes_estimate / 1e6, info2.bytes_estimate / 1e6,
+        info0.bytes / 1e6, info1.bytes / 1e6, info2.bytes / 1e6))
