@@ -21,7 +21,8 @@ __global__ void k_regularize(SubDev *, int, double *);
 __global__ void k_potrf_diag(const StepDesc *, const SubDev *, double *, int *);
 __global__ void k_trsm_panel(const StepDesc *, int, const SubDev *, double *, const int *);
 __global__ void k_syrk_update(const StepDesc *, int, const SubDev *, double *, const int *);
-__global__ void k_snapshot(const int *, const SubDev *, const double *, double *);
+__global__ void k_snapshot(const int *, const SubDev *, const double *, double *, long long);
+__global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *, long long);
 __global__ void k_trtri_step(int, const int *, const SubDev *, const double *, double *);
 __global__ void k_lauum_tiles(const int *, const SubDev *, const double *, double *);
 __global__ void k_build_V(const SubDev *, const double *, const int *, const int *, const double *,
@@ -298,6 +299,21 @@ int Engine::upload_layout(Problem &p, std::string &err) {
         err = "factor_wave_gb needs precision=mixed, an explicit preconditioner and print_matrices < 2";
         return HTF_EINVAL;
     }
+    s_lean_ = !opt_.S_fp64;
+    if (s_lean_ && (!opt_.mixed || opt_.preconditioner == "Dirichlet_implicit")) {
+        err = "S_fp64=0 needs precision=mixed and an explicit preconditioner";
+        return HTF_EINVAL;
+    }
+    // S tiles of the largest factor wave (S_fp64=0) or of all subdomains
+    long long s_tiles = T_off;
+    if (s_lean_) {
+        s_tiles = 0;
+        for (size_t w = 0; w + 1 < fwave_.size(); ++w) {
+            const int a = fwave_[w], b = fwave_[w + 1];
+            const SubDev &hl = hs_[b - 1];
+            s_tiles = std::max(s_tiles, hl.T_off + (long long)hl.nt * (hl.nt + 1) / 2 - hs_[a].T_off);
+        }
+    }
     nslots_ = xb;
     nfull_ = nf;
     ntiles_ = T_off;
@@ -330,7 +346,7 @@ int Engine::upload_layout(Problem &p, std::string &err) {
     kpanel_total_ = kwave_max;
     d_F_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);
     implicit_ = opt_.preconditioner == "Dirichlet_implicit";
-    if (!implicit_) d_S_ = alloc<double>(ntiles_ * TILE_ELEMS, err, rc);   // implicit: S applied through L_bb
+    if (!implicit_) d_S_ = alloc<double>(s_tiles * TILE_ELEMS, err, rc);   // implicit: S applied through L_bb
     d_V_ = alloc<double>(V_off, err, rc);
     d_R_ = alloc<double>(R_off, err, rc);
     d_M_ = alloc<double>(M_off, err, rc);
@@ -585,6 +601,10 @@ int Engine::factorize(Problem &p, std::string &err) {
         W.a = fwave_[w];
         W.b = fwave_[w + 1];
         W.eoff = (size_t)w * ncol;
+        if (!sub_blk0_.empty()) {
+            W.blk0 = sub_blk0_[W.a];
+            W.blk1 = sub_blk0_[W.b];
+        }
         std::vector<std::vector<StepDesc>> steps;
         std::vector<std::vector<int>> snap_after;      // subdomains whose interior ends after step s
         std::vector<int> snap_first;                   // nr == 0
@@ -682,6 +702,8 @@ void Engine::factor_wave(int w, bool build, double *X) {
     const bool dirichlet = opt_.preconditioner == "Dirichlet_explicit";
     const bool lumped = opt_.preconditioner == "lumped";
     const int nw = W.b - W.a;
+    // S tiles: all resident (from tile 0), or this wave's only, made into FP32 slabs below
+    const long long st0 = s_lean_ ? hs_[W.a].T_off : 0;
     cudaMemsetAsync(d_K_, 0, W.kdoubles * sizeof(double), s_);
     for (int c = 0; c < ncol_; ++c) {
         const int e0 = ecptr_[W.eoff + c], cnt = ecptr_[W.eoff + c + 1] - e0;
@@ -696,9 +718,10 @@ void Engine::factor_wave(int w, bool build, double *X) {
         cudaStreamSynchronize(s_);
     }
     if (build && lumped)            // lumped: K_bb before any elimination
-        k_snapshot<<<dim3(nw, max_tiles_), 256, 0, s_>>>(d_all_subs_ + W.a, d_subs_, d_K_, d_S_);
+        k_snapshot<<<dim3(nw, max_tiles_), 256, 0, s_>>>(d_all_subs_ + W.a, d_subs_, d_K_, d_S_, st0);
     if (build && dirichlet && W.nsnap_first > 0)
-        k_snapshot<<<dim3(W.nsnap_first, max_tiles_), 256, 0, s_>>>(W.snap + W.snap_first_off, d_subs_, d_K_, d_S_);
+        k_snapshot<<<dim3(W.nsnap_first, max_tiles_), 256, 0, s_>>>(W.snap + W.snap_first_off, d_subs_, d_K_, d_S_,
+                                                                    st0);
     for (size_t s = 0; s < W.soff.size(); ++s) {
         const int cnt = W.cnt[s];
         const StepDesc *ds = W.steps + W.soff[s];
@@ -707,9 +730,13 @@ void Engine::factor_wave(int w, bool build, double *X) {
         if (W.ntri[s] > 0)
             k_syrk_update<<<W.ntri[s], 256, SYRK_SMEM, s_>>>(ds, cnt, d_subs_, d_K_, W.hints + W.htri[s]);
         if (build && dirichlet && W.nsnap[s] > 0)
-            k_snapshot<<<dim3(W.nsnap[s], max_tiles_), 256, 0, s_>>>(W.snap + W.snap_off[s], d_subs_, d_K_, d_S_);
+            k_snapshot<<<dim3(W.nsnap[s], max_tiles_), 256, 0, s_>>>(W.snap + W.snap_off[s], d_subs_, d_K_, d_S_,
+                                                                     st0);
     }
     if (!build) return;
+    if (s_lean_ && (dirichlet || lumped) && W.blk1 > W.blk0)
+        k_make_slabs<<<dim3(W.blk1 - W.blk0, maxks_), 256, 0, s_>>>(static_cast<const GemmBlock *>(d_blocks_) + W.blk0,
+                                                                   d_subs_, d_S_, d_AS_, st0);
     // X = L_bb^{-1}, F = X^T X, in the L_bb^{-1} waves of this factor wave, sharing one scratch buffer
     for (size_t x = 0; x + 1 < xwave_.size(); ++x) {
         const int a = xwave_[x], b = xwave_[x + 1];
@@ -884,6 +911,7 @@ int Engine::setup(Problem &p, std::string &err) {
                        "cudaFuncSetAttribute(k_gf_apply)", err);
     }
     lap(2);
+    if (!rc && s_lean_) rc = plan_slabs(opt_.batch, err);   // S_i goes into its slabs wave by wave
     if (!rc) rc = factorize(p, err);
     lap(3);
     if (!rc) {                    // body-force load, load ownership and the displacement gather map
@@ -928,6 +956,11 @@ int Engine::setup(Problem &p, std::string &err) {
         // FP64 tiles stay resident for the FP64 residuals
         mixed_ = true;
         rc = setup_batch(opt_.batch, err);
+        if (!rc && s_lean_) {         // the FP64 S tiles of the last wave are not needed again
+            rc = check(cudaStreamSynchronize(s_), "sync", err);
+            release(d_S_);
+            d_S_ = nullptr;
+        }
     }
     if (!rc) rc = check(cudaEventRecord(e1, s_), "cudaEventRecord", err);
     if (!rc) rc = check(cudaEventSynchronize(e1), "cudaEventSynchronize", err);
@@ -1237,7 +1270,7 @@ int Engine::profile(int reps, htf_profile_info *info, std::string &err) {
             k_lb_t<<<nlblk_, 128, 0, s_>>>(d_lblk_, d_subs_, d_K_, d_tb_, d_xb_, d_yb_, nullptr);
         });
         info->symv_S_bytes = 2.0 * tri + 2.0 * vec;
-    } else {
+    } else if (d_S_) {
         info->symv_S_ms = timeit([&] {
             k_symv_units<double><<<nunits_, SYMV_WARPS * 32, symv_smem_, s_>>>(d_units_, d_subs_, d_S_, d_V_, d_xb_, d_ypart_, d_t_,
                                                                    nullptr);

@@ -47,6 +47,7 @@ public:
     int history(int rhs, double *out, int cap, std::string &err) const;
     // batched mixed-precision form (engine_batch.cu)
     int setup_batch(int K, std::string &err);
+    int plan_slabs(int K, std::string &err);       // tensor-core blocks and FP32 slab buffers
     int solve_batch(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err);
     int apply_batch(int op, const double *x, double *y, int nrhs, std::string &err);
     bool batch_ready() const { return bK_ > 0; }
@@ -141,6 +142,7 @@ private:
         int a = 0, b = 0;                        // subdomains [a, b)
         long long kdoubles = 0;                  // its panels
         size_t eoff = 0;                         // its first (wave, colour) entry of ecptr_
+        int blk0 = 0, blk1 = 0;                  // its tensor-core blocks (FP32 slab layout)
         StepDesc *steps = nullptr;               // Cholesky step tables of its subdomains
         int *snap = nullptr, *hints = nullptr;
         std::vector<size_t> soff, htri, hrb, snap_off;
@@ -153,6 +155,9 @@ private:
     std::vector<int> ecptr_;             // element ranges of d_order_ per (wave, colour)
     int ncol_ = 0, max_tiles_ = 0;
     bool waves_ = false;                 // factors dropped between uses (more than one wave)
+    bool s_lean_ = false;                // S_i only as FP32 slabs: d_S_ holds one wave's FP64 tiles during set-up
+    int maxks_ = 0;                      // largest nbp / 32
+    std::vector<int> sub_blk0_;          // first tensor-core block of each subdomain (nsub + 1)
     double *d_ec_ = nullptr, *d_E_ = nullptr, *d_nu_ = nullptr;   // element data for re-assembly
     int *d_ep_ = nullptr, *d_es_ = nullptr, *d_order_ = nullptr;
     double bf_[3] = {0.0, 0.0, 0.0};

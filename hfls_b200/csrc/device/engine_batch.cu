@@ -27,7 +27,7 @@ namespace htf {
 
 template <int K>
 __global__ void k_tc_gemm(const GemmBlock *, const TcSet *, int, int *);
-__global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *);
+__global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *, long long);
 __global__ void k_gather_multi(int, int, const int *, const int *, const double *, const double *, double *, float *,
                                float *);
 template <int K, int QN>
@@ -84,24 +84,20 @@ static inline int cdivb(long long a, long long b) { return int((a + b - 1) / b);
         if (_rc) return _rc;                                       \
     } while (0)
 
-int Engine::setup_batch(int K, std::string &err) {
+// tensor-core blocks and FP32 slab buffers (once; before the factorisation
+// when S_i is made into slabs wave by wave)
+int Engine::plan_slabs(int K, std::string &err) {
+    if (d_blocks_) return HTF_OK;
     if (K != 16 && K != 32) { err = "batch width must be 16 or 32"; return HTF_EINVAL; }
-    if (implicit_) {
-        err = "precision=mixed needs the explicit preconditioner blocks (Dirichlet_explicit or lumped)";
-        return HTF_EINVAL;
-    }
     int rc = HTF_OK;
-    for (auto &h : hs_)
-        if ((h.c + 6) * K > 2048) {
-            err = "too many Bc rows for the batched form";
-            return HTF_EINVAL;
-        }
     // tensor-core blocks and FP32 slabs: the lower triangle at 128-row block
     // granularity (block m stores its slabs kk < min(4 (m + 1), ks), so the
     // block's first slab is 2 m (m + 1) slabs after the subdomain's first)
     std::vector<GemmBlock> blocks;
     long long aoff = 0;
+    sub_blk0_.assign(nsub_ + 1, 0);
     for (int d = 0; d < nsub_; ++d) {
+        sub_blk0_[d] = int(blocks.size());
         const SubDev &h = hs_[d];
         const int mb = (h.nbp + 127) / 128, ks = h.nbp / 32;
         long long stored = 0;
@@ -115,29 +111,48 @@ int Engine::setup_batch(int K, std::string &err) {
         }
         aoff += stored * 4096;
     }
+    sub_blk0_[nsub_] = int(blocks.size());
     nblocks_ = int(blocks.size());
     d_blocks_ = alloc<GemmBlock>(blocks.size(), err, rc);
     d_AF_ = alloc<float>(aoff, err, rc);               // FP32 slabs, split into TF32 parts in the kernel
     d_AS_ = alloc<float>(aoff, err, rc);
-    d_Xs_ = alloc<float>(2 * (size_t)nslots_ * K, err, rc);
     aoff_ = aoff;
+    hblocks_ = blocks;
+    maxks_ = 0;
+    for (auto &h : hs_) maxks_ = std::max(maxks_, h.nbp / 32);
+    if (rc) return rc;
+    CKB(cudaMemcpyAsync(d_blocks_, blocks.data(), blocks.size() * sizeof(GemmBlock), cudaMemcpyHostToDevice, s_));
+    CKB(cudaStreamSynchronize(s_));
+    return HTF_OK;
+}
+
+int Engine::setup_batch(int K, std::string &err) {
+    if (K != 16 && K != 32) { err = "batch width must be 16 or 32"; return HTF_EINVAL; }
+    if (implicit_) {
+        err = "precision=mixed needs the explicit preconditioner blocks (Dirichlet_explicit or lumped)";
+        return HTF_EINVAL;
+    }
+    int rc = HTF_OK;
+    for (auto &h : hs_)
+        if ((h.c + 6) * K > 2048) {
+            err = "too many Bc rows for the batched form";
+            return HTF_EINVAL;
+        }
+    if ((rc = plan_slabs(K, err))) return rc;
+    d_Xs_ = alloc<float>(2 * (size_t)nslots_ * K, err, rc);
     d_slot_sub_ = alloc<int>(nslots_, err, rc);
     d_tcerr_ = alloc<int>(1, err, rc);
     d_tcset_ = alloc<TcSet>(1, err, rc);
-    hblocks_ = blocks;
     if (rc) return rc;
     std::vector<int> ss(nslots_);
     for (int d = 0; d < nsub_; ++d)
         for (int i = 0; i < hs_[d].nbp; ++i) ss[hs_[d].xb_off + i] = d;
-    CKB(cudaMemcpyAsync(d_blocks_, blocks.data(), blocks.size() * sizeof(GemmBlock), cudaMemcpyHostToDevice, s_));
     CKB(cudaMemcpyAsync(d_slot_sub_, ss.data(), nslots_ * sizeof(int), cudaMemcpyHostToDevice, s_));
     CKB(cudaMemsetAsync(d_Xs_, 0, 2 * (size_t)nslots_ * K * sizeof(float), s_));
     CKB(cudaMemsetAsync(d_tcerr_, 0, sizeof(int), s_));
-    int maxks = 0;
-    for (auto &h : hs_) maxks = std::max(maxks, h.nbp / 32);
     const GemmBlock *db = static_cast<const GemmBlock *>(d_blocks_);
-    k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_F_, d_AF_);
-    k_make_slabs<<<dim3(nblocks_, maxks), 256, 0, s_>>>(db, d_subs_, d_S_, d_AS_);
+    k_make_slabs<<<dim3(nblocks_, maxks_), 256, 0, s_>>>(db, d_subs_, d_F_, d_AF_, 0);
+    if (!s_lean_) k_make_slabs<<<dim3(nblocks_, maxks_), 256, 0, s_>>>(db, d_subs_, d_S_, d_AS_, 0);
     CKB(cudaGetLastError());
     // TC_STAGES stages of A (16 KB), X_hi, X_lo (k x 128 B each) + alignment slack (A_lo lives in TMEM)
     tc_smem_ = tc_smem_bytes(K);
@@ -386,10 +401,14 @@ int Engine::fp64_residual_batch(const std::vector<int> &sel, const std::vector<i
     k_axpby<<<cdivb(nk, 256), 256, 0, s_>>>(int(nk), -1.0, b_d_, 1.0, b_tmp_);
     op_P_batch(b_tmp_, b_Pg_, b_alpha2_, nullptr, nullptr);
     // z = M P g, P z, g'Pz
-    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, b_Pg_, d_weight_, b_xb_,
-                                                 nullptr, nullptr);
-    symv(d_S_, nullptr);
-    k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, d_weight_, b_z_, nullptr, nullptr);
+    if (d_S_) {
+        k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, b_Pg_, d_weight_, b_xb_,
+                                                     nullptr, nullptr);
+        symv(d_S_, nullptr);
+        k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, d_weight_, b_z_, nullptr, nullptr);
+    } else {
+        op_M_batch(b_Pg_, b_z_);      // S_i only as FP32 slabs: the tensor-core product
+    }
     op_P_batch(b_z_, b_Pz_, nullptr, b_tmp_, b_part_);
     k_colsum<<<K, 256, 0, s_>>>(b_part_, bnpart_, K, b_gPz_);
     // the selected columns back into the recurrence

@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(256) k_syrk_update(const StepDesc *__restrict_
 
 // Copy the trailing nbp x nbp block into packed tiles, minus the fix diagonal.
 __global__ void k_snapshot(const int *__restrict__ dlist, const SubDev *__restrict__ subs,
-                           const double *__restrict__ Kbuf, double *__restrict__ Sbuf) {
+                           const double *__restrict__ Kbuf, double *__restrict__ Sbuf, long long t0) {
     const SubDev &sd = subs[dlist[blockIdx.x]];
     const int tile = blockIdx.y;
     if (tile >= sd.nt * (sd.nt + 1) / 2) return;
@@ -413,7 +413,7 @@ __global__ void k_snapshot(const int *__restrict__ dlist, const SubDev *__restri
     while ((I + 1) * (I + 2) / 2 <= tile) ++I;
     while (I * (I + 1) / 2 > tile) --I;
     const int J = tile - I * (I + 1) / 2;
-    double *T = Sbuf + (sd.T_off + tile) * TILE_ELEMS;
+    double *T = Sbuf + (sd.T_off - t0 + tile) * TILE_ELEMS;     // Sbuf holds the tiles from t0 on
     for (int idx = threadIdx.x; idx < TILE_ELEMS; idx += blockDim.x) {
         const int r = idx / TILE, c = idx % TILE;
         int gr = sd.nr + TILE * I + r, gc = sd.nr + TILE * J + c;

@@ -416,9 +416,10 @@ template __global__ void k_tc_gemm<32>(const GemmBlock *, const TcSet *, int, in
 // FP32 slabs of the lower triangle (at 128-row block granularity) of a packed
 // symmetric FP64 tile matrix: slab (m, kk), kk < kd, of subdomain d holds
 // rows [128m, 128m+128) x columns [32kk, 32kk+32) of the symmetric block,
-// swizzled for SWIZZLE_128B K-major.  grid (block, kk).
+// swizzled for SWIZZLE_128B K-major.  tiles holds the packed tiles from tile
+// t0 on.  grid (block, kk).
 __global__ void k_make_slabs(const GemmBlock *__restrict__ blocks, const SubDev *__restrict__ subs,
-                             const double *__restrict__ tiles, float *__restrict__ A) {
+                             const double *__restrict__ tiles, float *__restrict__ A, long long t0) {
     const GemmBlock g = blocks[blockIdx.x];
     const int kk = blockIdx.y;
     if (kk >= g.kd) return;
@@ -432,7 +433,7 @@ __global__ void k_make_slabs(const GemmBlock *__restrict__ blocks, const SubDev 
             int i = gr, j = gc;
             if (i < j) { int t = i; i = j; j = t; }
             const int I = i / TILE, J = j / TILE;
-            const double *T = tiles + (sd.T_off + (long long)I * (I + 1) / 2 + J) * TILE_ELEMS;
+            const double *T = tiles + (sd.T_off - t0 + (long long)I * (I + 1) / 2 + J) * TILE_ELEMS;
             v = (float)T[(i % TILE) * TILE + (j % TILE)];
         }
         const uint32_t b = uint32_t(r * 128 + c * 4);

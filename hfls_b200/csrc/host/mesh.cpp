@@ -220,7 +220,10 @@ int parse_options(const char *s, Options &o, std::string &err) {
         else if (k == "verbose") o.verbose = std::atoi(v.c_str());
         else if (k == "autotune") o.autotune = std::atoi(v.c_str());
         else if (k == "tune_file") o.tune_file = v;
-        else if (k == "factor_wave_gb") {
+        else if (k == "S_fp64") {
+            if (v != "0" && v != "1") { err = "S_fp64 must be 0 or 1"; return HTF_EINVAL; }
+            o.S_fp64 = (v == "1");
+        } else if (k == "factor_wave_gb") {
             o.factor_wave_gb = std::atof(v.c_str());
             if (!(o.factor_wave_gb >= 0.0)) { err = "factor_wave_gb must be >= 0"; return HTF_EINVAL; }
         }

@@ -66,6 +66,9 @@ struct Options {
                                                       // subdomains are held at a time; set-up and every later
                                                       // K_reg solve assemble and factorise them again, wave
                                                       // by wave (batched mixed form, explicit preconditioners)
+    bool S_fp64 = true;                               // false: S_i is kept only as the FP32 slabs of the tensor-
+                                                      // core product, which the FP64 residual replacements apply
+                                                      // too (batched mixed form, explicit preconditioners)
 };
 int parse_options(const char *s, Options &o, std::string &err);
 

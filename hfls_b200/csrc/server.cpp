@@ -78,7 +78,7 @@ private:
     void setup_loop();
     void run_loop();
     int prepare(Request &r, std::string &err);
-    size_t estimate(const Problem &p, int nrhs, double wave_gb) const;
+    size_t estimate(const Problem &p, int nrhs, double wave_gb, bool s_fp64) const;
     int rebuild_graph(std::string &err);
     void finish(Request *r, int rc, const std::string &msg);
     void release_graph();
@@ -212,31 +212,35 @@ int Server::wait(long long ticket, double timeout_ms, htf_request_info *out) {
     return r->info.status == HTF_REQ_DONE ? HTF_OK : r->info.rc;
 }
 
-// device bytes of a request after setup, from the host-side problem (factor
-// panels of all subdomains, or of the largest factor wave when wave_gb > 0,
-// F_i / S_i tiles, setup scratch, V, R, FP32 slabs, coarse M, vectors), with
-// a margin
-size_t Server::estimate(const Problem &p, int nrhs, double wave_gb) const {
+// device bytes of a request during and after setup, from the host-side
+// problem (factor panels of all subdomains, or of the largest factor wave when
+// wave_gb > 0; F_i tiles; S_i tiles of all subdomains, or of the largest wave
+// without s_fp64; setup scratch, V, R, FP32 slabs, coarse M, vectors), with a
+// margin
+size_t Server::estimate(const Problem &p, int nrhs, double wave_gb, bool s_fp64) const {
     const double K = opt_.batch;
     double b = 0.0, nslots = 0.0, nfull = 0.0, xs = 0.0;
-    // panels held at once: all, or the largest wave of the engine's partition
+    // panels (and S tiles) held at once: all, or the largest wave of the engine's partition
     const double cap = wave_gb > 0.0 ? std::max(1.0, wave_gb * 1e9 / 8.0) : 1e300;
-    double panels = 0.0, wave = 0.0;
+    double panels = 0.0, wave = 0.0, stiles = 0.0, swave = 0.0;
     for (const Subdomain &s : p.sub) {
-        const double nbp = 32.0 * ((s.nb + 31) / 32);
+        const double nbp = 32.0 * ((s.nb + 31) / 32), nt = nbp / 32;
         const double kp = double(kpanel_doubles(s.n - s.nb, int(nbp)));
-        if (wave > 0.0 && wave + kp > cap) wave = 0.0;
+        if (wave > 0.0 && wave + kp > cap) wave = swave = 0.0;
         wave += kp;
+        swave += nt * (nt + 1) / 2 * 1024.0;
         panels = std::max(panels, wave);
+        stiles = std::max(stiles, swave);
     }
     b += 8.0 * panels;
+    if (!s_fp64) b += 8.0 * stiles;
     if (wave_gb > 0.0) b += 296.0 * p.mesh.n_elems();     // element data kept for the re-assembly
     for (const Subdomain &s : p.sub) {
         const double nbp = 32.0 * ((s.nb + 31) / 32), N = (s.n - s.nb) + nbp, nt = nbp / 32;
         const double mb = std::ceil(nbp / 128.0), nks = nbp / 32;
         double stored = 0.0;                              // FP32 slabs: lower triangle of 128-row blocks
         for (int m = 0; m < int(mb); ++m) stored += std::min(4.0 * (m + 1), nks);
-        b += 8.0 * (nt * (nt + 1) * 1024.0 + nbp * (s.c() + 6) + 6 * N + 2 * nbp);
+        b += 8.0 * ((s_fp64 ? 2.0 : 1.0) * nt * (nt + 1) / 2 * 1024.0 + nbp * (s.c() + 6) + 6 * N + 2 * nbp);
         xs += nbp * nbp;
         b += 2.0 * stored * 4096.0 * 4.0;
         nslots += nbp;
@@ -265,21 +269,31 @@ int Server::prepare(Request &r, std::string &err) {
     if ((rc = build_problem(p, err, true))) return rc;
     // factor panels that do not fit beside the rest are held a wave at a time
     // and factorised again for each later K_reg solve (set-up start solve and
-    // reconstruction): a wave of half the room left by everything else, at most 16 GB
+    // reconstruction): a wave of half the room left by everything else, at most
+    // 16 GB; if that is not enough, S_i is kept only as its FP32 slabs too
     double wave_gb = opt_.factor_wave_gb;
-    size_t est = estimate(p, r.nrhs, wave_gb);
-    if (wave_gb <= 0.0 && double(est) > budget_) {
-        const double rest = double(estimate(p, r.nrhs, 1e-9));
+    bool s_fp64 = opt_.S_fp64;
+    size_t est = estimate(p, r.nrhs, wave_gb, s_fp64);
+    auto waves = [&] {
+        if (opt_.factor_wave_gb > 0.0) return;
+        const double rest = double(estimate(p, r.nrhs, 1e-9, s_fp64));
         wave_gb = std::min(16.0, std::max(1e-3, 0.5 * (budget_ - rest) / 1e9));
-        est = estimate(p, r.nrhs, wave_gb);
+        est = estimate(p, r.nrhs, wave_gb, s_fp64);
+    };
+    if (double(est) > budget_) waves();
+    if (double(est) > budget_ && s_fp64) {
+        s_fp64 = false;
+        est = estimate(p, r.nrhs, wave_gb, s_fp64);
+        if (double(est) > budget_) waves();
     }
     p.opt.factor_wave_gb = wave_gb;
+    p.opt.S_fp64 = s_fp64;
     {
         std::unique_lock<std::mutex> lk(mu_);
         r.info.bytes_estimate = double(est);
         if (double(est) > budget_) {
             err = "request needs about " + std::to_string(est >> 20) +
-                  " MiB with its factor panels held a wave at a time, more than the server budget";
+                  " MiB with its factor panels held a wave at a time and S_i in FP32 only, more than the server budget";
             return HTF_ENOMEM;
         }
         // admission: waits for memory and a slot (live requests always finish)

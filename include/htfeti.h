@@ -105,7 +105,11 @@ int htf_write_vtk(const char *path, int n_nodes, const double *coords, int n_ele
  * resident; > 0: the panels of at most that many GB of subdomains are held
  * at a time and are assembled and factorised again, wave by wave, for each
  * later K_reg solve — the batched mixed form with an explicit
- * preconditioner only), verbose = 0 | 1.                                   */
+ * preconditioner only), S_fp64 = 1 | 0 (0: S_i is kept only as the FP32
+ * slabs of the tensor-core product, which the FP64 residual replacements
+ * apply too — batched mixed form, explicit preconditioner), verbose = 0 | 1.
+ * The server picks factor_wave_gb and S_fp64 per request when its footprint
+ * does not fit the budget otherwise.                                       */
 typedef struct htf_ctx htf_ctx;
 
 int htf_create(const char *options, htf_ctx **ctx);

@@ -193,3 +193,24 @@ def test_server_holds_factor_panels_in_waves_when_they_do_not_fit():
     print("resident / forced waves / admitted in waves: estimate MB %.1f %.1f %.1f, device MB %.1f %.1f %.1f" % (
         info0.bytes_estimate / 1e6, info1.bytes_estimate / 1e6, info2.bytes_estimate / 1e6,
         info0.bytes / 1e6, info1.bytes / 1e6, info2.bytes / 1e6))
+
+
+def test_s_kept_as_fp32_slabs_only():
+    """S_fp64=0 with factor waves: S_i is snapshotted into one wave's FP64
+    scratch, made into its FP32 slabs and dropped; the FP64 residual
+    replacements apply it through the tensor-core product too.  The
+    displacements stay within the mixed form's 1e-7 of the resident run, the
+    iteration counts within a few check intervals."""
+    spec = hb.mesh_spec(**WAVE_SPEC)
+    f = hb.traction(spec, seed=31, n_rhs=3)
+    out = []
+    for extra in ({}, {"factor_wave_gb": "0.006", "S_fp64": "0"}):
+        s = hb.Solver(dict(OPTS, precision="mixed", **extra))
+        s.set_mesh(hb.generate_mesh(spec))
+        s.setup()
+        out.append(s.solve(f))
+        s.close()
+    (u0, st0), (u1, st1) = out
+    for k in range(3):
+        assert abs(int(st1.iterations[k]) - int(st0.iterations[k])) <= 16 + 0.02 * st0.iterations[k], k
+        assert rel(u1[k], u0[k]) < 1e-7, k
