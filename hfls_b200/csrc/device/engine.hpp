@@ -25,8 +25,24 @@ struct BatchRun {
     std::vector<PcpgState> st;
     std::vector<double> last;      // g'Pz at the last FP64 residual
     std::vector<double> rel;       // last FP64 sqrt(g'Pz)/norm0
-    std::vector<int> conv;         // 0 running, 1 converged, 2 max_iter
+    std::vector<double> best;      // smallest FP64 rel seen at a residual replacement
+    std::vector<int> best_it;      // iteration at which best was set
+    std::vector<int> stall;        // residual replacements since best was set
+    std::vector<int> conv;         // 0 running, 1 converged, 2 max_iter, 3 stagnated
 };
+
+// A load case of the batched mixed form is stopped as stagnated (HTF_ENOCONV)
+// when MIXED_STALL_LIMIT FP64 residual replacements, over at least
+// MIXED_STALL_ITERATIONS iterations, have passed without its FP64 residual
+// falling below half of its smallest value so far.  A replacement follows a
+// 100x drop of the recursive g'Pz or a recursion that says converged; while
+// the form converges the FP64 residual follows the recursive one down, so a
+// run of replacements without progress means the FP32 operator cannot carry
+// the FP64 residual any lower (its rounding times the problem's conditioning
+// is above eps), and the iterations left to max_iter would only add FP64
+// replacements.
+constexpr int MIXED_STALL_LIMIT = 10;
+constexpr int MIXED_STALL_ITERATIONS = 500;
 
 struct DevBuf {
     void *p = nullptr;

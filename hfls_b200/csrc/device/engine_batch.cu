@@ -466,6 +466,9 @@ int Engine::batch_begin(int r0, int kc, std::string &err) {
     r.st.assign(K, PcpgState{});
     r.last.assign(K, 0.0);
     r.rel.assign(K, 0.0);
+    r.best.assign(K, 0.0);
+    r.best_it.assign(K, 0);
+    r.stall.assign(K, 0);
     r.conv.assign(K, 0);
     CKB(cudaMemsetAsync(b_lam_, 0, (size_t)nlam_ * K * sizeof(double), s_));
     CKB(cudaMemsetAsync(b_d_, 0, (size_t)nlam_ * K * sizeof(double), s_));
@@ -523,6 +526,17 @@ int Engine::batch_check(bool &all_done, std::string &err) {
         }
     }
     if (changed && (rc = fp64_residual_batch(sel, reset, err))) return rc;
+    for (int j = 0; j < K; ++j) {
+        if (!sel[j] || r.conv[j]) continue;
+        if (r.best[j] == 0.0 || r.rel[j] < 0.5 * r.best[j]) {
+            r.best[j] = r.rel[j];
+            r.best_it[j] = r.st[j].it;
+            r.stall[j] = 0;
+        } else if (++r.stall[j] >= MIXED_STALL_LIMIT && r.st[j].it - r.best_it[j] >= MIXED_STALL_ITERATIONS) {
+            r.conv[j] = 3;
+            r.st[j].done = 1;          // the iterations leave it alone from here on
+        }
+    }
     if (changed) CKB(cudaMemcpyAsync(b_st_, r.st.data(), K * sizeof(PcpgState), cudaMemcpyHostToDevice, s_));
     all_done = true;
     for (int j = 0; j < K; ++j) all_done &= r.conv[j] != 0;
@@ -582,6 +596,18 @@ int Engine::batch_finish(htf_stats *stats, double &ms, std::string &err) {
     CKB(cudaGetLastError());
     for (int j = 0; j < r.kc; ++j)
         if (r.conv[j] == 2) { err = "PCPG did not converge within max_iter"; return HTF_ENOCONV; }
+    for (int j = 0; j < r.kc; ++j)
+        if (r.conv[j] == 3) {
+            char msg[256];
+            std::snprintf(msg, sizeof msg,
+                          "PCPG stagnated: load case %d stayed at a relative FP64 residual of %.3e (target %.1e) "
+                          "from iteration %d to %d (%d residual replacements); the mixed form cannot reach "
+                          "eps_iter on this problem",
+                          r.r0 + j, r.best[j], opt_.eps_iter * opt_.mixed_eps_factor, r.best_it[j], r.st[j].it,
+                          r.stall[j]);
+            err = msg;
+            return HTF_ENOCONV;
+        }
     return HTF_OK;
 }
 

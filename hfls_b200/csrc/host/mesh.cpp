@@ -223,6 +223,9 @@ int parse_options(const char *s, Options &o, std::string &err) {
         else if (k == "S_fp64") {
             if (v != "0" && v != "1") { err = "S_fp64 must be 0 or 1"; return HTF_EINVAL; }
             o.S_fp64 = (v == "1");
+        } else if (k == "admit_oversize") {
+            if (v != "0" && v != "1") { err = "admit_oversize must be 0 or 1"; return HTF_EINVAL; }
+            o.admit_oversize = (v == "1");
         } else if (k == "factor_wave_gb") {
             o.factor_wave_gb = std::atof(v.c_str());
             if (!(o.factor_wave_gb >= 0.0)) { err = "factor_wave_gb must be >= 0"; return HTF_EINVAL; }

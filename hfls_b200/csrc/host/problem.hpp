@@ -69,6 +69,9 @@ struct Options {
     bool S_fp64 = true;                               // false: S_i is kept only as the FP32 slabs of the tensor-
                                                       // core product, which the FP64 residual replacements apply
                                                       // too (batched mixed form, explicit preconditioners)
+    bool admit_oversize = false;                      // server: a request that does not fit the budget alone is
+                                                      // admitted with factor waves (and S_fp64 = 0 if needed)
+                                                      // instead of being refused with HTF_ENOMEM
 };
 int parse_options(const char *s, Options &o, std::string &err);
 

@@ -4,10 +4,10 @@
 // A setup thread admits them in order while the estimated device footprint
 // of factors, F_i / S_i and vectors fits the HBM budget and a slot is free,
 // and runs their setup on each request's own stream, overlapping the
-// iterations of the requests already running.  A request whose factor panels
-// do not fit beside the rest holds them a wave of subdomains at a time and
-// has them assembled and factorised again for its start solve and its
-// reconstruction.  A run thread advances every
+// iterations of the requests already running.  With admit_oversize, a
+// request whose factor panels do not fit beside the rest holds them a wave of
+// subdomains at a time and has them assembled and factorised again for its
+// start solve and its reconstruction.  A run thread advances every
 // live request one batched mixed-precision PCPG iteration at a time: the
 // FP64 phases of the requests run side by side, each on its own stream forked
 // from and joined back to the server stream, around ONE tensor-core launch
@@ -267,10 +267,11 @@ int Server::prepare(Request &r, std::string &err) {
     p.nrhs = r.nrhs;
     if (!r.f.empty()) p.f_nodal = r.f;
     if ((rc = build_problem(p, err, true))) return rc;
-    // factor panels that do not fit beside the rest are held a wave at a time
-    // and factorised again for each later K_reg solve (set-up start solve and
-    // reconstruction): a wave of half the room left by everything else, at most
-    // 16 GB; if that is not enough, S_i is kept only as its FP32 slabs too
+    // with admit_oversize, factor panels that do not fit beside the rest are
+    // held a wave at a time and factorised again for each later K_reg solve
+    // (set-up start solve and reconstruction): a wave of half the room left by
+    // everything else, at most 16 GB; if that is not enough, S_i is kept only
+    // as its FP32 slabs too
     double wave_gb = opt_.factor_wave_gb;
     bool s_fp64 = opt_.S_fp64;
     size_t est = estimate(p, r.nrhs, wave_gb, s_fp64);
@@ -280,11 +281,14 @@ int Server::prepare(Request &r, std::string &err) {
         wave_gb = std::min(16.0, std::max(1e-3, 0.5 * (budget_ - rest) / 1e9));
         est = estimate(p, r.nrhs, wave_gb, s_fp64);
     };
-    if (double(est) > budget_) waves();
-    if (double(est) > budget_ && s_fp64) {
-        s_fp64 = false;
-        est = estimate(p, r.nrhs, wave_gb, s_fp64);
+    const size_t resident = est;
+    if (opt_.admit_oversize) {
         if (double(est) > budget_) waves();
+        if (double(est) > budget_ && s_fp64) {
+            s_fp64 = false;
+            est = estimate(p, r.nrhs, wave_gb, s_fp64);
+            if (double(est) > budget_) waves();
+        }
     }
     p.opt.factor_wave_gb = wave_gb;
     p.opt.S_fp64 = s_fp64;
@@ -292,8 +296,13 @@ int Server::prepare(Request &r, std::string &err) {
         std::unique_lock<std::mutex> lk(mu_);
         r.info.bytes_estimate = double(est);
         if (double(est) > budget_) {
-            err = "request needs about " + std::to_string(est >> 20) +
-                  " MiB with its factor panels held a wave at a time and S_i in FP32 only, more than the server budget";
+            err = opt_.admit_oversize
+                      ? "request needs about " + std::to_string(est >> 20) +
+                            " MiB with its factor panels held a wave at a time and S_i in FP32 only, more than the "
+                            "server budget"
+                      : "request needs about " + std::to_string(resident >> 20) +
+                            " MiB, more than the server budget (admit_oversize=1 admits it with its factor panels "
+                            "held a wave at a time)";
             return HTF_ENOMEM;
         }
         // admission: waits for memory and a slot (live requests always finish)

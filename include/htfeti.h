@@ -107,9 +107,13 @@ int htf_write_vtk(const char *path, int n_nodes, const double *coords, int n_ele
  * later K_reg solve — the batched mixed form with an explicit
  * preconditioner only), S_fp64 = 1 | 0 (0: S_i is kept only as the FP32
  * slabs of the tensor-core product, which the FP64 residual replacements
- * apply too — batched mixed form, explicit preconditioner), verbose = 0 | 1.
- * The server picks factor_wave_gb and S_fp64 per request when its footprint
- * does not fit the budget otherwise.                                       */
+ * apply too — batched mixed form, explicit preconditioner), verbose = 0 | 1,
+ * admit_oversize = 0 | 1 (server only; 1: a request whose footprint does not
+ * fit the budget alone is admitted with factor_wave_gb and, if still needed,
+ * S_fp64 = 0 picked for it, instead of failing with HTF_ENOMEM).
+ * The batched mixed form stops a load case whose FP64 residual has not halved
+ * over ten residual replacements and at least 500 iterations with
+ * HTF_ENOCONV ("stagnated"): its FP32 products cannot reach eps_iter.     */
 typedef struct htf_ctx htf_ctx;
 
 int htf_create(const char *options, htf_ctx **ctx);

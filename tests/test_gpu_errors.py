@@ -67,6 +67,26 @@ def test_max_iter_gives_enoconv(precision):
     solve_next_problem()
 
 
+def test_unreachable_eps_stops_the_mixed_form_as_stagnated():
+    """eps_iter = 1e-15 is below what an FP32 operator can carry the FP64
+    residual to: the batched mixed form stops with HTF_ENOCONV once ten FP64
+    residual replacements over at least 500 iterations have passed without
+    the FP64 residual halving, long before max_iter."""
+    m = hb.generate_mesh(hb.mesh_spec(**SPEC))
+    s = hb.Solver(dict(OPTS, eps_iter="1e-15", max_iter="20000", precision="mixed", batch="16"))
+    s.set_mesh(m)
+    s.setup()
+    with pytest.raises(hb.HTFError) as e:
+        s.pcpg()
+    assert e.value.code == hb.HTF_ENOCONV
+    msg = str(e.value)
+    assert "stagnated" in msg, msg
+    it = int(msg.split(" to ")[1].split()[0])
+    assert it < 5000, msg
+    s.close()
+    solve_next_problem()
+
+
 def test_floating_body_gives_singular_gftgf():
     m = hb.generate_mesh(hb.mesh_spec(**SPEC))
     free = hb.Mesh(m.coords, m.elems, m.elem_sub, m.sub_cluster, m.sub_E, m.sub_nu,

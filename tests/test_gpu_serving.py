@@ -169,7 +169,8 @@ def test_server_holds_factor_panels_in_waves_when_they_do_not_fit():
     subdomain of 8^3 hex8 per wave): smaller estimate and device bytes, the
     displacements of the resident-factor run.  Chosen by admission: a budget
     just above the forced run's estimate, below the resident-factor estimate,
-    admits the request with its panels held a wave at a time."""
+    refuses the request (HTF_ENOMEM) by default and, with admit_oversize=1,
+    admits it with its panels held a wave at a time."""
     spec = hb.mesh_spec(**dict(WAVE_SPEC, elems=(8, 8, 8)))
     f = hb.traction(spec, seed=31, n_rhs=2)
     one = hb.Server(OPTS)
@@ -183,7 +184,12 @@ def test_server_holds_factor_panels_in_waves_when_they_do_not_fit():
     assert rel(u1, u0) < 1e-13
     budget = 1.05 * info1.bytes_estimate
     assert budget < info0.bytes_estimate
-    srv = hb.Server(OPTS, hbm_budget_bytes=budget)
+    refuse = hb.Server(OPTS, hbm_budget_bytes=budget)
+    with pytest.raises(hb.HTFError) as e:
+        refuse.wait(refuse.submit(spec, f))
+    refuse.close()
+    assert e.value.code == hb.HTF_ENOMEM
+    srv = hb.Server(dict(OPTS, admit_oversize="1"), hbm_budget_bytes=budget)
     u2, info2 = srv.wait(srv.submit(spec, f))
     srv.close()
     assert info2.rc == 0 and info2.status == hb.HTF_REQ_DONE
