@@ -195,3 +195,17 @@ def test_factor_wave_option_is_checked():
         hb.Solver({"factor_wave_gb": "-1"})
     assert e.value.code == hb.HTF_EINVAL
     hb.Solver({"factor_wave_gb": "2.5", "precision": "mixed"}).close()
+
+
+def test_oversize_admission_option_is_checked():
+    """admit_oversize (the server admits a request that does not fit its
+    budget alone with factor waves) is 0 or 1; anything else is refused with
+    HTF_EINVAL by the option parser, before the server touches a device."""
+    for bad in ("2", "yes", ""):
+        with pytest.raises(hb.HTFError) as e:
+            hb.Server({"admit_oversize": bad})
+        assert e.value.code == hb.HTF_EINVAL
+        with pytest.raises(hb.HTFError) as e:
+            hb.Solver({"admit_oversize": bad})
+        assert e.value.code == hb.HTF_EINVAL
+    hb.Solver({"admit_oversize": "1", "precision": "mixed"}).close()
