@@ -62,7 +62,8 @@ SMALL_WORKLOAD = ("the reference's CPU configuration: 2x2x2 subdomains x 5^3 hex
                   "Bc of kernel type, Dirichlet preconditioner, eps 1e-8")
 MIXED_RHS = 32
 MIXED_WORKLOAD = ("cube512 mesh, body force (0,0,-1) + 32 seeded N(0,1) tractions on x=1, solved as one batch of 32: "
-                  "F_i/S_i FP32 slabs, 3xTF32 tcgen05 products, FP64 coarse/projector/residual replacement, eps 1e-8")
+                  "F_i/S_i as scaled FP16 hi+lo slabs, tcgen05 kind::f16 products (A_hi X_hi + A_hi X_lo + A_lo X_hi), "
+                  "FP64 coarse/projector/residual replacement, eps 1e-8")
 SERVE_REQUESTS = 12          # requests of the seeded stream that one bench run serves
 SERVE_RATE = 1.0             # Poisson arrivals per second
 SERVE_WORKLOAD = ("seeded Poisson stream (rate %.1f/s): cube meshes of c^3 clusters, (c s)^3 subdomains of e^3 hex8, "
@@ -414,7 +415,7 @@ def run_mixed(hb, local, dist, reduced=None):
         "fp64_iterations": its64, "oracle_iterations_fp64": its_oracle,
         "u_rel_err_max": max(err), "fp64_u_rel_err_max": max(err64), "u_err_against": against,
         "batch_iteration_ms": prof.batch_iteration_ms,
-        "tc_F": {"kernel": "k_tc_gemm<32> (F_i FP32 slabs x 32 load cases)", "ms": prof.tc_F_ms,
+        "tc_F": {"kernel": "k_tc_gemm<32> (F_i FP16-pair slabs x 32 load cases)", "ms": prof.tc_F_ms,
                  "bytes": prof.tc_F_bytes, "gbs": tc_gbs, "frac": tc_gbs / peak, "peak_kind": peak_kind},
     }
 

@@ -24,16 +24,17 @@
 namespace htf {
 
 #ifdef __CUDACC__
-// FP32 -> TF32 (10 explicit mantissa bits), round to nearest, ties away from
-// zero; the low 13 bits of the result are zero
-__device__ __forceinline__ float tf32_rna(float a) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(a));
-    return __uint_as_float(r);
+// Power-of-two scale exponent of a tensor-core operand: values of magnitude
+// up to m * mult (m given as FP32 bits) times 2^E stay below 2^14, a quarter
+// of the FP16 range, so the hi + lo FP16 pair of a scaled value keeps 22
+// significant bits.  m * mult = f 2^e, f in [0.5, 1): E = 14 - e; 0 for zero.
+__device__ __forceinline__ int tc_scale_exp(unsigned m_bits, float mult) {
+    const float m = __uint_as_float(m_bits) * mult;
+    if (!(m > 0.f)) return 0;
+    int e;
+    frexpf(m, &e);
+    return 14 - e;
 }
-// the TF32 value a tensor-core product uses for an FP32 operand (low 13
-// mantissa bits dropped)
-__device__ __forceinline__ float tf32_trunc(float a) { return __uint_as_float(__float_as_uint(a) & 0xFFFFE000u); }
 #endif
 
 constexpr int TILE = 32;                  // packed tile edge
@@ -41,9 +42,8 @@ constexpr int CHOL_STEP = 64;             // columns per batched Cholesky step (
 // dynamic shared memory of k_syrk_update: two 32-column panels of 64 rows for
 // each operand (row stride 68) and the 64 x 64 C block (column stride 65)
 constexpr int SYRK_SMEM = (4 * 32 * 68 + 64 * 65) * 8;
-constexpr int TC_STAGES = 4;              // pipeline stages of the tensor-core product (2 CTAs per SM)
-constexpr int TC_LO = 4;                  // A_lo buffers (in TMEM) of the tensor-core product
-constexpr int TC_THREADS = 320;           // threads of the tensor-core product: producer, MMA, 8 splitting warps
+constexpr int TC_STAGES = 5;              // pipeline stages of the tensor-core product (2 CTAs per SM)
+constexpr int TC_THREADS = 320;           // threads of the tensor-core product: producer, MMA, 8 epilogue warps
 constexpr int TILE_ELEMS = TILE * TILE;
 
 struct SubDev {
@@ -165,10 +165,12 @@ struct GemmBlock {
 
 // Operands of the tensor-core products of one problem.
 struct TcSet {
-    const float *AF, *AS;                 // FP32 slabs of F_i and S_i
-    const float *Xs;                      // X_hi slabs; X_lo slabs at Xs + xlo
-    long long xlo;
+    const float *AF, *AS;                 // FP16-pair slabs of F_i and S_i (4 bytes per entry)
+    const float *Xs;                      // FP16-pair X slabs (k x 32 words per 32 b-space slots)
     double *yb;                           // b-space output, RHS-interleaved
+    const unsigned *amaxF, *amaxS;        // largest |F_i|, |S_i| per subdomain (FP32 bits): scale of A
+    const unsigned *xmax;                 // largest |w_j| of the gathered batch vector (FP32 bits)
+    float xbound;                         // |x_b| <= xbound * max|w_j|: scale of X
 };
 
 // One step of the batched Cholesky for one subdomain: columns [k, k + nb),

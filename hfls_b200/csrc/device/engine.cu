@@ -22,7 +22,9 @@ __global__ void k_potrf_diag(const StepDesc *, const SubDev *, double *, int *);
 __global__ void k_trsm_panel(const StepDesc *, int, const SubDev *, double *, const int *);
 __global__ void k_syrk_update(const StepDesc *, int, const SubDev *, double *, const int *);
 __global__ void k_snapshot(const int *, const SubDev *, const double *, double *, long long);
-__global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *, long long);
+__global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *, long long,
+                             const unsigned *);
+__global__ void k_slab_amax(const GemmBlock *, const SubDev *, const double *, long long, unsigned *);
 __global__ void k_trtri_step(int, const int *, const SubDev *, const double *, double *);
 __global__ void k_lauum_tiles(const int *, const SubDev *, const double *, double *);
 __global__ void k_build_V(const SubDev *, const double *, const int *, const int *, const double *,
@@ -702,7 +704,7 @@ void Engine::factor_wave(int w, bool build, double *X) {
     const bool dirichlet = opt_.preconditioner == "Dirichlet_explicit";
     const bool lumped = opt_.preconditioner == "lumped";
     const int nw = W.b - W.a;
-    // S tiles: all resident (from tile 0), or this wave's only, made into FP32 slabs below
+    // S tiles: all resident (from tile 0), or this wave's only, made into tensor-core slabs below
     const long long st0 = s_lean_ ? hs_[W.a].T_off : 0;
     cudaMemsetAsync(d_K_, 0, W.kdoubles * sizeof(double), s_);
     for (int c = 0; c < ncol_; ++c) {
@@ -734,9 +736,11 @@ void Engine::factor_wave(int w, bool build, double *X) {
                                                                      st0);
     }
     if (!build) return;
-    if (s_lean_ && (dirichlet || lumped) && W.blk1 > W.blk0)
-        k_make_slabs<<<dim3(W.blk1 - W.blk0, maxks_), 256, 0, s_>>>(static_cast<const GemmBlock *>(d_blocks_) + W.blk0,
-                                                                   d_subs_, d_S_, d_AS_, st0);
+    if (s_lean_ && (dirichlet || lumped) && W.blk1 > W.blk0) {
+        const GemmBlock *wb = static_cast<const GemmBlock *>(d_blocks_) + W.blk0;
+        k_slab_amax<<<dim3(W.blk1 - W.blk0, maxks_), 256, 0, s_>>>(wb, d_subs_, d_S_, st0, d_amaxS_);
+        k_make_slabs<<<dim3(W.blk1 - W.blk0, maxks_), 256, 0, s_>>>(wb, d_subs_, d_S_, d_AS_, st0, d_amaxS_);
+    }
     // X = L_bb^{-1}, F = X^T X, in the L_bb^{-1} waves of this factor wave, sharing one scratch buffer
     for (size_t x = 0; x + 1 < xwave_.size(); ++x) {
         const int a = xwave_[x], b = xwave_[x + 1];
@@ -952,7 +956,7 @@ int Engine::setup(Problem &p, std::string &err) {
     lap(6);
     if (!rc) rc = autotune_symv(err);             // SYMV work-unit schedule of this problem class
     if (!rc && opt_.mixed) {
-        // FP32 slabs for the tensor-core products of the batched form; the
+        // FP16-pair slabs for the tensor-core products of the batched form; the
         // FP64 tiles stay resident for the FP64 residuals
         mixed_ = true;
         rc = setup_batch(opt_.batch, err);

@@ -63,7 +63,7 @@ public:
     int history(int rhs, double *out, int cap, std::string &err) const;
     // batched mixed-precision form (engine_batch.cu)
     int setup_batch(int K, std::string &err);
-    int plan_slabs(int K, std::string &err);       // tensor-core blocks and FP32 slab buffers
+    int plan_slabs(int K, std::string &err);       // tensor-core blocks and slab buffers
     int solve_batch(Problem &p, int nrhs, const double *f_nodal, double *u, htf_stats *stats, std::string &err);
     int apply_batch(int op, const double *x, double *y, int nrhs, std::string &err);
     bool batch_ready() const { return bK_ > 0; }
@@ -107,6 +107,7 @@ private:
     void coarse_batch();
     void f_post(double *Fw, const double *dotv, double *partial);
     void m_pre(const double *x);
+    void gather_x(const double *w, const double *weight, double *xb);   // x_b and the X slabs
     void m_post(double *z);
     int fp64_residual_batch(const std::vector<int> &sel, const std::vector<int> &reset, std::string &err);
     void profile_batch_gather(const double *w);
@@ -158,7 +159,7 @@ private:
         int a = 0, b = 0;                        // subdomains [a, b)
         long long kdoubles = 0;                  // its panels
         size_t eoff = 0;                         // its first (wave, colour) entry of ecptr_
-        int blk0 = 0, blk1 = 0;                  // its tensor-core blocks (FP32 slab layout)
+        int blk0 = 0, blk1 = 0;                  // its tensor-core blocks (tensor-core slab layout)
         StepDesc *steps = nullptr;               // Cholesky step tables of its subdomains
         int *snap = nullptr, *hints = nullptr;
         std::vector<size_t> soff, htri, hrb, snap_off;
@@ -171,7 +172,7 @@ private:
     std::vector<int> ecptr_;             // element ranges of d_order_ per (wave, colour)
     int ncol_ = 0, max_tiles_ = 0;
     bool waves_ = false;                 // factors dropped between uses (more than one wave)
-    bool s_lean_ = false;                // S_i only as FP32 slabs: d_S_ holds one wave's FP64 tiles during set-up
+    bool s_lean_ = false;                // S_i only as tensor-core slabs: d_S_ holds one wave's FP64 tiles during set-up
     int maxks_ = 0;                      // largest nbp / 32
     std::vector<int> sub_blk0_;          // first tensor-core block of each subdomain (nsub + 1)
     double *d_ec_ = nullptr, *d_E_ = nullptr, *d_nu_ = nullptr;   // element data for re-assembly
@@ -217,6 +218,9 @@ private:
     // batched mixed-precision form
     int bK_ = 0, nblocks_ = 0, bnpart_ = 0, bnpartP_ = 0;
     float *d_AF_ = nullptr, *d_AS_ = nullptr, *d_Xs_ = nullptr;
+    unsigned *d_amaxF_ = nullptr, *d_amaxS_ = nullptr;   // scales of the FP16-pair slabs (largest |A| per subdomain)
+    unsigned *d_xmax_ = nullptr;                         // scale of the X slabs (largest |w_j| per column)
+    float xbound_ = 1.f;                                 // |x_b| <= xbound_ max|w_j|
     void *d_blocks_ = nullptr;
     TcSet *d_tcset_ = nullptr;
     std::vector<GemmBlock> hblocks_;
@@ -237,7 +241,7 @@ private:
     cudaGraphExec_t bgraph_ = nullptr;
     int bkernels_per_iter_ = 0;
     int tc_smem_ = 0, vt_nch_ = 1, vt_qn_ = 64;
-    long long aoff_ = 0;                       // floats per FP32 slab array
+    long long aoff_ = 0;                       // 4-byte words per slab array
     // vectors
     double *d_f_ = nullptr, *d_full_ = nullptr, *d_full2_ = nullptr;
     double *d_lam_ = nullptr, *d_g_ = nullptr, *d_w_ = nullptr, *d_Fw_ = nullptr, *d_Pg_ = nullptr,

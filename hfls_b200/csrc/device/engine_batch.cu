@@ -1,8 +1,9 @@
 // Batched mixed-precision PCPG (K load cases at once).
 //
-// F_i and S_i are applied as full FP32 matrices on the tensor cores
-// (tc_gemm.cu, 3xTF32 products, FP32 accumulation in TMEM); gather, coarse
-// problem, projector and recurrences stay FP64.  Each load case follows
+// F_i and S_i are applied on the tensor cores as scaled FP16 hi + lo pairs
+// (tc_gemm.cu: three FP16 products per K step, FP32 accumulation in TMEM,
+// 22 significant bits per operand); gather, coarse problem, projector and
+// recurrences stay FP64.  Each load case follows
 // Cluster::pcpg (Cluster.cpp:1363-1458) with reliable updates: its residual
 // is replaced by the FP64 one g = F lambda - d (FP64 F_i, one load case at a
 // time) whenever its recursive g'Pz has dropped 100x or it looks converged,
@@ -27,9 +28,12 @@ namespace htf {
 
 template <int K>
 __global__ void k_tc_gemm(const GemmBlock *, const TcSet *, int, int *);
-__global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *, long long);
+__global__ void k_make_slabs(const GemmBlock *, const SubDev *, const double *, float *, long long,
+                             const unsigned *);
+__global__ void k_slab_amax(const GemmBlock *, const SubDev *, const double *, long long, unsigned *);
+__global__ void k_colmax(int, int, const double *, unsigned *);
 __global__ void k_gather_multi(int, int, const int *, const int *, const double *, const double *, double *, float *,
-                               float *);
+                               const unsigned *, float);
 template <int K, int QN>
 __global__ void k_vt_multi(int, const SubDev *, const double *, const double *, double *);
 __global__ void k_gc_multi(int, int, int, const int *, const int *, const double *, double *);
@@ -84,13 +88,13 @@ static inline int cdivb(long long a, long long b) { return int((a + b - 1) / b);
         if (_rc) return _rc;                                       \
     } while (0)
 
-// tensor-core blocks and FP32 slab buffers (once; before the factorisation
+// tensor-core blocks and slab buffers (once; before the factorisation
 // when S_i is made into slabs wave by wave)
 int Engine::plan_slabs(int K, std::string &err) {
     if (d_blocks_) return HTF_OK;
     if (K != 16 && K != 32) { err = "batch width must be 16 or 32"; return HTF_EINVAL; }
     int rc = HTF_OK;
-    // tensor-core blocks and FP32 slabs: the lower triangle at 128-row block
+    // tensor-core blocks and slabs: the lower triangle at 128-row block
     // granularity (block m stores its slabs kk < min(4 (m + 1), ks), so the
     // block's first slab is 2 m (m + 1) slabs after the subdomain's first)
     std::vector<GemmBlock> blocks;
@@ -114,14 +118,18 @@ int Engine::plan_slabs(int K, std::string &err) {
     sub_blk0_[nsub_] = int(blocks.size());
     nblocks_ = int(blocks.size());
     d_blocks_ = alloc<GemmBlock>(blocks.size(), err, rc);
-    d_AF_ = alloc<float>(aoff, err, rc);               // FP32 slabs, split into TF32 parts in the kernel
+    d_AF_ = alloc<float>(aoff, err, rc);               // FP16-pair slabs (4 bytes per entry)
     d_AS_ = alloc<float>(aoff, err, rc);
+    d_amaxF_ = alloc<unsigned>(nsub_, err, rc);        // largest |F_i|, |S_i| per subdomain: the slabs' scales
+    d_amaxS_ = alloc<unsigned>(nsub_, err, rc);
     aoff_ = aoff;
     hblocks_ = blocks;
     maxks_ = 0;
     for (auto &h : hs_) maxks_ = std::max(maxks_, h.nbp / 32);
     if (rc) return rc;
     CKB(cudaMemcpyAsync(d_blocks_, blocks.data(), blocks.size() * sizeof(GemmBlock), cudaMemcpyHostToDevice, s_));
+    CKB(cudaMemsetAsync(d_amaxF_, 0, nsub_ * sizeof(unsigned), s_));
+    CKB(cudaMemsetAsync(d_amaxS_, 0, nsub_ * sizeof(unsigned), s_));
     CKB(cudaStreamSynchronize(s_));
     return HTF_OK;
 }
@@ -139,7 +147,8 @@ int Engine::setup_batch(int K, std::string &err) {
             return HTF_EINVAL;
         }
     if ((rc = plan_slabs(K, err))) return rc;
-    d_Xs_ = alloc<float>(2 * (size_t)nslots_ * K, err, rc);
+    d_Xs_ = alloc<float>((size_t)nslots_ * K, err, rc);
+    d_xmax_ = alloc<unsigned>(K, err, rc);
     d_slot_sub_ = alloc<int>(nslots_, err, rc);
     d_tcerr_ = alloc<int>(1, err, rc);
     d_tcset_ = alloc<TcSet>(1, err, rc);
@@ -148,13 +157,29 @@ int Engine::setup_batch(int K, std::string &err) {
     for (int d = 0; d < nsub_; ++d)
         for (int i = 0; i < hs_[d].nbp; ++i) ss[hs_[d].xb_off + i] = d;
     CKB(cudaMemcpyAsync(d_slot_sub_, ss.data(), nslots_ * sizeof(int), cudaMemcpyHostToDevice, s_));
-    CKB(cudaMemsetAsync(d_Xs_, 0, 2 * (size_t)nslots_ * K * sizeof(float), s_));
+    CKB(cudaMemsetAsync(d_Xs_, 0, (size_t)nslots_ * K * sizeof(float), s_));
     CKB(cudaMemsetAsync(d_tcerr_, 0, sizeof(int), s_));
+    {
+        // |x_b| <= (entries of a slot) x (largest weight) x max|w|: the bound behind X's scale
+        std::vector<int> sp(nslots_ + 1);
+        std::vector<double> wt(nlam_);
+        CKB(cudaMemcpy(sp.data(), d_slot_ptr_, sp.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        CKB(cudaMemcpy(wt.data(), d_weight_, wt.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        int nent = 1;
+        for (int i = 0; i < nslots_; ++i) nent = std::max(nent, sp[i + 1] - sp[i]);
+        double wmax = 1.0;
+        for (double x : wt) wmax = std::max(wmax, std::fabs(x));
+        xbound_ = float(nent * wmax);
+    }
     const GemmBlock *db = static_cast<const GemmBlock *>(d_blocks_);
-    k_make_slabs<<<dim3(nblocks_, maxks_), 256, 0, s_>>>(db, d_subs_, d_F_, d_AF_, 0);
-    if (!s_lean_) k_make_slabs<<<dim3(nblocks_, maxks_), 256, 0, s_>>>(db, d_subs_, d_S_, d_AS_, 0);
+    k_slab_amax<<<dim3(nblocks_, maxks_), 256, 0, s_>>>(db, d_subs_, d_F_, 0, d_amaxF_);
+    k_make_slabs<<<dim3(nblocks_, maxks_), 256, 0, s_>>>(db, d_subs_, d_F_, d_AF_, 0, d_amaxF_);
+    if (!s_lean_) {
+        k_slab_amax<<<dim3(nblocks_, maxks_), 256, 0, s_>>>(db, d_subs_, d_S_, 0, d_amaxS_);
+        k_make_slabs<<<dim3(nblocks_, maxks_), 256, 0, s_>>>(db, d_subs_, d_S_, d_AS_, 0, d_amaxS_);
+    }
     CKB(cudaGetLastError());
-    // TC_STAGES stages of A (16 KB), X_hi, X_lo (k x 128 B each) + alignment slack (A_lo lives in TMEM)
+    // TC_STAGES stages of A (16 KB) and X (k x 128 B) + alignment slack
     tc_smem_ = tc_smem_bytes(K);
     if (K == 16)
         CKB(cudaFuncSetAttribute(k_tc_gemm<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_));
@@ -210,15 +235,21 @@ int Engine::setup_batch(int K, std::string &err) {
 // the coarse correction of the F product runs after it (k_correct_multi in
 // f_post), so the product's epilogue gets no coarse solution
 TcSet Engine::tc_set() const {
-    return TcSet{d_AF_, d_AS_, d_Xs_, (long long)nslots_ * bK_, b_yb_};
+    return TcSet{d_AF_, d_AS_, d_Xs_, b_yb_, d_amaxF_, d_amaxS_, d_xmax_, xbound_};
+}
+
+// x_b = Bf^T w (weighted when weight != nullptr; into xb when xb != nullptr)
+// and the X slabs of the tensor-core product, scaled from w's column maxima
+void Engine::gather_x(const double *w, const double *weight, double *xb) {
+    const int K = bK_;
+    cudaMemsetAsync(d_xmax_, 0, K * sizeof(unsigned), s_);
+    k_colmax<<<std::min(cdivb((long long)nlam_ * K, 256), 1184), 256, 0, s_>>>(nlam_, K, w, d_xmax_);
+    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, w, weight, xb, d_Xs_, d_xmax_,
+                                                 xbound_);
 }
 
 // X slabs of a batch vector (for timing the tensor-core product alone)
-void Engine::profile_batch_gather(const double *w) {
-    const long long xlo = (long long)nslots_ * bK_;
-    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, bK_, d_slot_ptr_, d_slot_ent_, w, nullptr, b_xb_, d_Xs_,
-                                                 d_Xs_ + xlo);
-}
+void Engine::profile_batch_gather(const double *w) { gather_x(w, nullptr, b_xb_); }
 
 // one tensor-core launch over the given blocks / operand sets (which: 0 = F,
 // 1 = S; the coarse correction of F follows in k_correct_multi)
@@ -230,7 +261,7 @@ int tc_launch(int K, const GemmBlock *blocks, int nblocks, const TcSet *sets, in
     return 0;
 }
 
-int tc_smem_bytes(int K) { return 1024 + TC_STAGES * (128 * 32 + 2 * K * 32) * 4; }
+int tc_smem_bytes(int K) { return 1024 + TC_STAGES * (128 * 32 + K * 32) * 4; }
 
 void Engine::tc_apply(int which) {
     tc_launch(bK_, static_cast<const GemmBlock *>(d_blocks_), nblocks_, d_tcset_, which, tc_smem_, d_tcerr_, s_);
@@ -239,10 +270,7 @@ void Engine::tc_apply(int which) {
 // F w = Bf [F_d x_b - V_d M_c V_d^T x_b]: the coarse solve before the
 // tensor-core product, whose epilogue applies the correction
 void Engine::f_pre(const double *w) {
-    const int K = bK_;
-    const long long xlo = (long long)nslots_ * K;
-    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, w, nullptr, b_xb_, d_Xs_,
-                                                 d_Xs_ + xlo);
+    gather_x(w, nullptr, b_xb_);
     coarse_batch();
 }
 
@@ -274,13 +302,8 @@ void Engine::f_post(double *Fw, const double *dotv, double *partial) {
     k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, bK_, d_rslot_, d_rsign_, b_yb_, nullptr, Fw, dotv, partial);
 }
 
-// the preconditioner must stay a fixed linear operator for the PCPG
-// recurrences, so it uses the same 3xTF32 products as F
-void Engine::m_pre(const double *x) {
-    const long long xlo = (long long)nslots_ * bK_;
-    k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, bK_, d_slot_ptr_, d_slot_ent_, x, d_weight_, nullptr, d_Xs_,
-                                                 d_Xs_ + xlo);
-}
+// the preconditioner uses the same FP16-pair products as F
+void Engine::m_pre(const double *x) { gather_x(x, d_weight_, nullptr); }
 
 void Engine::m_post(double *z) {
     k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, bK_, d_rslot_, d_rsign_, b_yb_, d_weight_, z, nullptr, nullptr);
@@ -394,7 +417,7 @@ int Engine::fp64_residual_batch(const std::vector<int> &sel, const std::vector<i
     };
     // g = F lambda - d
     k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, b_lam_, nullptr, b_xb_, nullptr,
-                                                 nullptr);
+                                                 nullptr, 0.f);
     coarse_batch();
     symv(d_F_, b_s_);
     k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, nullptr, b_tmp_, nullptr, nullptr);
@@ -403,11 +426,11 @@ int Engine::fp64_residual_batch(const std::vector<int> &sel, const std::vector<i
     // z = M P g, P z, g'Pz
     if (d_S_) {
         k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, b_Pg_, d_weight_, b_xb_,
-                                                     nullptr, nullptr);
+                                                     nullptr, nullptr, 0.f);
         symv(d_S_, nullptr);
         k_rows_multi<<<bnpart_, 256, 0, s_>>>(nlam_, K, d_rslot_, d_rsign_, b_yb_, d_weight_, b_z_, nullptr, nullptr);
     } else {
-        op_M_batch(b_Pg_, b_z_);      // S_i only as FP32 slabs: the tensor-core product
+        op_M_batch(b_Pg_, b_z_);      // S_i only as tensor-core slabs: the tensor-core product
     }
     op_P_batch(b_z_, b_Pz_, nullptr, b_tmp_, b_part_);
     k_colsum<<<K, 256, 0, s_>>>(b_part_, bnpart_, K, b_gPz_);

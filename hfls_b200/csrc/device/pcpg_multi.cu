@@ -3,6 +3,7 @@
 // case follows Cluster::pcpg (Cluster.cpp:1363-1458) independently; the
 // matrices are read once per iteration for all K.  Reductions are
 // fixed-order (deterministic).
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -20,15 +21,19 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
 }
 
 // x_b = Bf^T w (optionally weighted; x_b itself only when xb != nullptr) for
-// all K columns; also writes the X
-// slabs of the tensor-core product (TF32 part and TF32 remainder) in the
-// SWIZZLE_128B K-major layout.  One CTA per 32 consecutive slots (one K slab
-// of one subdomain: b offsets and padded sizes are multiples of 32); the
-// values go through shared memory so both outputs are written coalesced.
+// all K columns; also writes the X slabs of the tensor-core product: every
+// column scaled by 2^EX_j (EX_j from the column's largest |w| times the bound
+// xbound >= |x_b| / max|w|) as FP16 hi + lo, the hi plane (K rows x 64 B)
+// then the lo plane, SWIZZLE_64B K-major.  One CTA per 32 consecutive slots
+// (one K slab of one subdomain: b offsets and padded sizes are multiples of
+// 32); the values go through shared memory so both outputs are written
+// coalesced.
 __global__ void k_gather_multi(int nslots, int K, const int *__restrict__ ptr, const int *__restrict__ ent,
                                const double *__restrict__ w, const double *__restrict__ weight,
-                               double *__restrict__ xb, float *__restrict__ Xs, float *__restrict__ Xlo) {
+                               double *__restrict__ xb, float *__restrict__ Xs, const unsigned *__restrict__ xmax,
+                               float xbound) {
     __shared__ double vs[32 * 33];
+    __shared__ int ex[32];
     const int i0 = blockIdx.x * 32;
     for (int o = threadIdx.x; o < 32 * K; o += blockDim.x) {
         const int il = o / K, j = o % K, i = i0 + il;
@@ -45,17 +50,19 @@ __global__ void k_gather_multi(int nslots, int K, const int *__restrict__ ptr, c
         vs[il * 33 + j] = v;
     }
     if (!Xs) return;
+    if (threadIdx.x < K) ex[threadIdx.x] = tc_scale_exp(xmax[threadIdx.x], xbound);
     __syncthreads();
-    // slab row j (load case) holds the 32 slots of this chunk, 128 bytes
+    // row j (load case) of each plane holds the 32 slots of this chunk, 64 bytes
+    __half *hi = reinterpret_cast<__half *>(Xs + (size_t)i0 * K);
+    __half *lo = hi + 32 * K;
     for (int o = threadIdx.x; o < 32 * K; o += blockDim.x) {
         const int j = o / 32, c = o % 32;
-        const double v = vs[c * 33 + j];
-        const uint32_t b = uint32_t(j * 128 + c * 4);
-        const uint32_t bs = b ^ (((b >> 7) & 7u) << 4);
-        const size_t at = (size_t)i0 * K + bs / 4;
-        const float hi = tf32_rna((float)v);
-        Xs[at] = hi;
-        if (Xlo) Xlo[at] = tf32_rna((float)(v - (double)hi));   // 3xTF32 remainder
+        const double v = ldexp(vs[c * 33 + j], ex[j]);
+        const __half vh = __double2half(v);
+        const uint32_t b = uint32_t(j * 64 + c * 2);
+        const uint32_t bs = b ^ (((b >> 7) & 3u) << 4);
+        hi[bs / 2] = vh;
+        lo[bs / 2] = __double2half(v - (double)__half2float(vh));
     }
 }
 

@@ -66,7 +66,7 @@ struct Options {
                                                       // subdomains are held at a time; set-up and every later
                                                       // K_reg solve assemble and factorise them again, wave
                                                       // by wave (batched mixed form, explicit preconditioners)
-    bool S_fp64 = true;                               // false: S_i is kept only as the FP32 slabs of the tensor-
+    bool S_fp64 = true;                               // false: S_i is kept only as the 4-byte slabs of the tensor-
                                                       // core product, which the FP64 residual replacements apply
                                                       // too (batched mixed form, explicit preconditioners)
     bool admit_oversize = false;                      // server: a request that does not fit the budget alone is

@@ -215,7 +215,7 @@ int Server::wait(long long ticket, double timeout_ms, htf_request_info *out) {
 // device bytes of a request during and after setup, from the host-side
 // problem (factor panels of all subdomains, or of the largest factor wave when
 // wave_gb > 0; F_i tiles; S_i tiles of all subdomains, or of the largest wave
-// without s_fp64; setup scratch, V, R, FP32 slabs, coarse M, vectors), with a
+// without s_fp64; setup scratch, V, R, tensor-core slabs, coarse M, vectors), with a
 // margin
 size_t Server::estimate(const Problem &p, int nrhs, double wave_gb, bool s_fp64) const {
     const double K = opt_.batch;
@@ -238,7 +238,7 @@ size_t Server::estimate(const Problem &p, int nrhs, double wave_gb, bool s_fp64)
     for (const Subdomain &s : p.sub) {
         const double nbp = 32.0 * ((s.nb + 31) / 32), N = (s.n - s.nb) + nbp, nt = nbp / 32;
         const double mb = std::ceil(nbp / 128.0), nks = nbp / 32;
-        double stored = 0.0;                              // FP32 slabs: lower triangle of 128-row blocks
+        double stored = 0.0;                              // tensor-core slabs: lower triangle of 128-row blocks
         for (int m = 0; m < int(mb); ++m) stored += std::min(4.0 * (m + 1), nks);
         b += 8.0 * ((s_fp64 ? 2.0 : 1.0) * nt * (nt + 1) / 2 * 1024.0 + nbp * (s.c() + 6) + 6 * N + 2 * nbp);
         xs += nbp * nbp;
@@ -271,7 +271,7 @@ int Server::prepare(Request &r, std::string &err) {
     // held a wave at a time and factorised again for each later K_reg solve
     // (set-up start solve and reconstruction): a wave of half the room left by
     // everything else, at most 16 GB; if that is not enough, S_i is kept only
-    // as its FP32 slabs too
+    // as its tensor-core slabs too
     double wave_gb = opt_.factor_wave_gb;
     bool s_fp64 = opt_.S_fp64;
     size_t est = estimate(p, r.nrhs, wave_gb, s_fp64);
@@ -298,7 +298,7 @@ int Server::prepare(Request &r, std::string &err) {
         if (double(est) > budget_) {
             err = opt_.admit_oversize
                       ? "request needs about " + std::to_string(est >> 20) +
-                            " MiB with its factor panels held a wave at a time and S_i in FP32 only, more than the "
+                            " MiB with its factor panels held a wave at a time and S_i in the tensor-core slabs only, more than the "
                             "server budget"
                       : "request needs about " + std::to_string(resident >> 20) +
                             " MiB, more than the server budget (admit_oversize=1 admits it with its factor panels "

@@ -105,7 +105,7 @@ int htf_write_vtk(const char *path, int n_nodes, const double *coords, int n_ele
  * resident; > 0: the panels of at most that many GB of subdomains are held
  * at a time and are assembled and factorised again, wave by wave, for each
  * later K_reg solve — the batched mixed form with an explicit
- * preconditioner only), S_fp64 = 1 | 0 (0: S_i is kept only as the FP32
+ * preconditioner only), S_fp64 = 1 | 0 (0: S_i is kept only as the 4-byte
  * slabs of the tensor-core product, which the FP64 residual replacements
  * apply too — batched mixed form, explicit preconditioner), verbose = 0 | 1,
  * admit_oversize = 0 | 1 (server only; 1: a request whose footprint does not
@@ -188,14 +188,14 @@ typedef struct htf_profile_info {
     /* batched mixed-precision form (precision=mixed after a solve; else 0)  */
     int batch_width;                    /* load cases per batch                     */
     double tc_F_ms, tc_F_bytes;         /* Y_b = F_i X_b for the whole batch on the
-                                           tensor cores: FP32 slabs + X + Y bytes   */
+                                           tensor cores: 4-byte slabs + X + Y bytes   */
     double batch_iteration_ms;          /* one captured batched PCPG iteration      */
     int kernels_per_batch_iteration;
     /* host wall time of the phases of htf_setup (ms): 0 problem build (maps,
      * Bf/Bc, kernels, fix DOFs), 1 device context and stream, 2 layout upload
      * and allocation, 3 assembly + factorisation + F_i/S_i, 4 load and
      * displacement maps, 5 cluster coarse problems, 6 outer coarse problem,
-     * 7 SYMV schedule tuning and FP32 slabs of the batched form              */
+     * 7 SYMV schedule tuning and tensor-core slabs of the batched form              */
     double setup_phase_ms[8];
     /* SYMV schedule in use: work-unit tiles for subdomains with at most
      * 8, 16, 32, 64 and more tile rows; tuned = 1 when it came from the

@@ -1,10 +1,11 @@
-"""Batched mixed-precision form on the GPU: F_i / S_i stored in FP32 and
-applied on the tensor cores (tcgen05, 3xTF32 products, FP32 accumulation in
-TMEM) for a batch of load cases; coarse problems, projector, residual
-replacement and displacements in FP64.
+"""Batched mixed-precision form on the GPU: F_i / S_i stored as scaled FP16
+hi + lo pairs (4 bytes per entry, 22 significant bits) and applied on the
+tensor cores (tcgen05 kind::f16, three products per K step, FP32
+accumulation in TMEM) for a batch of load cases; coarse problems, projector,
+residual replacement and displacements in FP64.
 
 Tolerances: the tensor-core F apply against the FP64 oracle 1e-5 relative
-(FP32 storage, about 1e-6 after the coarse-correction cancellation), the
+(FP32-level storage, about 1e-6 after the coarse-correction cancellation), the
 preconditioner 1e-6, the batched FP64 projector 1e-12; the displacements of
 the mixed solve against the FP64 oracle 1e-7 relative (the bound for the
 mixed form)."""

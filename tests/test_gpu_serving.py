@@ -203,7 +203,7 @@ def test_server_holds_factor_panels_in_waves_when_they_do_not_fit():
 
 def test_s_kept_as_fp32_slabs_only():
     """S_fp64=0 with factor waves: S_i is snapshotted into one wave's FP64
-    scratch, made into its FP32 slabs and dropped; the FP64 residual
+    scratch, made into its tensor-core slabs and dropped; the FP64 residual
     replacements apply it through the tensor-core product too.  The
     displacements stay within the mixed form's 1e-7 of the resident run, the
     iteration counts within a few check intervals."""

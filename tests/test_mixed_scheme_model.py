@@ -69,3 +69,64 @@ def test_three_products_reach_fp32_level_accuracy():
     one = rel(model_product(F, X, 1), exact)
     assert storage < three < 5e-7                           # FP32-level accuracy
     assert 1e-4 < one and one > 100 * three                 # a single TF32 product is far worse
+
+
+def pow2_exponent(m, mult=1.0):
+    """The exponent E that scales values of magnitude <= m * mult to at most
+    2^14 (a quarter of the FP16 range): m * mult = f 2^e, f in [0.5, 1),
+    E = 14 - e; 0 for an all-zero operand."""
+    m = float(m) * mult
+    if not m > 0.0:
+        return 0
+    _, e = np.frexp(m)
+    return 14 - int(e)
+
+
+def f16_pair(v):
+    """v (FP64, already scaled) as FP16 hi + FP16 lo, both rounded to nearest."""
+    hi = v.astype(np.float16)
+    lo = (v - hi.astype(np.float64)).astype(np.float16)
+    return hi, lo
+
+
+def model_product_f16(F, X, nent=1.0):
+    """The FP16-pair form of the product: F scaled by one power of two per
+    matrix, every column of X by one power of two from its maximum times the
+    bound nent, each split into FP16 hi + lo planes (4 bytes per entry, like
+    FP32), products A_hi X_hi + A_hi X_lo + A_lo X_hi (exact in FP32) summed in
+    FP32 per 32-column slab, slabs summed and unscaled in FP64."""
+    ea = pow2_exponent(np.abs(F).max())
+    ex = np.array([pow2_exponent(np.abs(X[:, j]).max(), nent) for j in range(X.shape[1])])
+    A_hi, A_lo = f16_pair(np.ldexp(F, ea))
+    X_hi, X_lo = f16_pair(np.ldexp(X, ex[None, :]))
+    A_hi, A_lo, X_hi, X_lo = (a.astype(np.float32) for a in (A_hi, A_lo, X_hi, X_lo))
+    Y = np.zeros((F.shape[0], X.shape[1]))
+    for k0 in range(0, F.shape[1], 32):
+        s = slice(k0, k0 + 32)
+        acc = A_hi[:, s] @ X_hi[s] + A_hi[:, s] @ X_lo[s] + A_lo[:, s] @ X_hi[s]
+        Y += acc.astype(np.float64)
+    return np.ldexp(Y, -(ea + ex)[None, :])
+
+
+def test_pow2_exponent_keeps_fp16_in_range():
+    for m in (1e-300, 3e-9, 0.7, 1.0, 2.0 ** 14, 6e12):
+        e = pow2_exponent(m, 8.0)
+        assert 2.0 ** 13 <= np.ldexp(m * 8.0, e) < 2.0 ** 14
+    assert pow2_exponent(0.0) == 0
+
+
+def test_fp16_pairs_reach_the_accuracy_of_three_tf32_products():
+    """Same operands as the 3xTF32 model: the FP16-pair form with power-of-two
+    scales is at FP32 level too, also when the columns of X span many orders of
+    magnitude and the scale is taken from a bound 8x above their maximum."""
+    F = _local_schur_like(256, 1)
+    X = np.random.default_rng(2).normal(size=(256, 32))
+    X[:, 1] *= np.logspace(-10, 0, 256)
+    X[:, 2] *= 1e-200
+    exact = F @ X
+    three = rel(model_product(F, X, 3), exact)
+    pair = rel(model_product_f16(F, X, nent=8.0), exact)
+    assert pair < 5e-7 and pair < 2 * three
+    got = model_product_f16(F, X, nent=8.0)
+    for j in (1, 2):                        # max norms: the 1e-200 column's 2-norm underflows
+        assert np.abs(got[:, j] - exact[:, j]).max() < 5e-7 * np.abs(exact[:, j]).max()
