@@ -1,14 +1,19 @@
-"""A numpy model of the mixed form's tensor-core product, Y = F X with F
-stored in FP32: X split into TF32 parts X_hi + X_lo, F's FP32 value used as
-A_hi (a TF32 operand's low 13 bits do not enter the product) plus the
-rounded remainder A_lo, the products A_hi X_hi + A_hi X_lo + A_lo X_hi summed
-in FP32 per 32-column slab of F and the slabs summed in FP64.
+"""Numpy models of the mixed form's tensor-core product Y = F X, the
+products A_hi X_hi + A_hi X_lo + A_lo X_hi summed in FP32 per 32-column slab
+of F and the slabs summed in FP64, for two operand formats of 4 bytes per
+entry:
 
-What it pins: the scheme's error is at FP32 level (a few 1e-7 relative:
+* scaled FP16 pairs (the kernel's form): F and every column of X scaled by a
+  power of two below 2^14, each split into FP16 hi + lo;
+* 3xTF32 (the form it replaced): F stored in FP32, whose value serves as A_hi
+  (a TF32 operand's low 13 bits do not enter the product) plus the rounded
+  remainder A_lo, X split into TF32 parts X_hi + X_lo.
+
+What it pins: both schemes' error is at FP32 level (a few 1e-7 relative:
 the dropped A_lo X_lo term, about 2^-22, FP32 accumulation inside a slab and
-FP32 storage of F), while a single TF32 product is ~5e-4 — the level at
-which the GPU operator tests fail when the remainder terms are missing —
-which is why the kernel issues three."""
+the 4-byte storage of F), while a single TF32 product is ~5e-4 — the level
+at which the GPU operator tests fail when the remainder terms are missing —
+which is why the kernel issues three products."""
 import numpy as np
 
 
