@@ -201,7 +201,7 @@ def test_server_holds_factor_panels_in_waves_when_they_do_not_fit():
         info0.bytes / 1e6, info1.bytes / 1e6, info2.bytes / 1e6))
 
 
-def test_s_kept_as_fp32_slabs_only():
+def test_s_kept_as_tensor_core_slabs_only():
     """S_fp64=0 with factor waves: S_i is snapshotted into one wave's FP64
     scratch, made into its tensor-core slabs and dropped; the FP64 residual
     replacements apply it through the tensor-core product too.  The
