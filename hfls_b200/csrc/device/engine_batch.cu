@@ -243,7 +243,7 @@ TcSet Engine::tc_set() const {
 void Engine::gather_x(const double *w, const double *weight, double *xb) {
     const int K = bK_;
     cudaMemsetAsync(d_xmax_, 0, K * sizeof(unsigned), s_);
-    k_colmax<<<std::min(cdivb((long long)nlam_ * K, 256), 1184), 256, 0, s_>>>(nlam_, K, w, d_xmax_);
+    k_colmax<<<std::max(1, std::min(cdivb((long long)nlam_ * K, 256), 1184)), 256, 0, s_>>>(nlam_, K, w, d_xmax_);
     k_gather_multi<<<nslots_ / 32, 256, 0, s_>>>(nslots_, K, d_slot_ptr_, d_slot_ent_, w, weight, xb, d_Xs_, d_xmax_,
                                                  xbound_);
 }
