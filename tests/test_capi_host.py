@@ -209,3 +209,43 @@ def test_oversize_admission_option_is_checked():
             hb.Solver({"admit_oversize": bad})
         assert e.value.code == hb.HTF_EINVAL
     hb.Solver({"admit_oversize": "1", "precision": "mixed"}).close()
+
+
+def _random_case(seed):
+    """A seeded small mesh: 1-2 clusters and 1-3 subdomains per axis, uneven
+    slab widths of 1-3 elements, either boundary condition, either Bc type."""
+    rng = np.random.default_rng(seed)
+    clusters = tuple(int(x) for x in rng.integers(1, 3, size=3))
+    subs = tuple(int(x) for x in rng.integers(1, 4, size=3))
+    if np.prod(clusters) * np.prod(subs) < 2:
+        subs = (2,) + subs[1:]
+    widths = [rng.integers(1, 4, size=clusters[a] * subs[a]) for a in range(3)]
+    bc = int(rng.integers(0, 2))
+    typeBc = ("cor", "ker")[int(rng.integers(0, 2))]
+    return dict(clusters=clusters, subs=subs, elems=(2, 2, 2), widths=widths, bc=bc,
+                jitter=float(rng.choice([0.0, 0.1]))), typeBc
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_meshes_layout_and_fix_dofs_match_oracle(seed):
+    """Bf rows, signs, weights and fix DOFs of the host front-end are the
+    oracle's, entry for entry, on twelve seeded meshes of uneven slab widths
+    (corner and kernel Bc, clamped face and rollers)."""
+    case, typeBc = _random_case(seed)
+    spec = hb.mesh_spec(material=hb.HTF_MAT_LOGUNIFORM, E=1.0, E_hi=1e4, seed=seed, **case)
+    m = hb.generate_mesh(spec)
+    s = hb.Solver({"typeBc": typeBc})
+    s.set_mesh(m)
+    rs, rd, sg, w = s.dual_layout()
+    h = HTFETI(_oracle_mesh(m), Options(typeBc=typeBc, fix_rule="boundary", kerGc="analytic"))
+    assert len(w) == h.n_lam
+    assert np.array_equal(w, h.weight)
+    want = np.full((h.n_lam, 2), -1)
+    for r, row in enumerate(h.bf_rows):
+        for k, (d, gdof, sign) in enumerate(row):
+            assert (rd[r, k], sg[r, k]) == (gdof, sign)
+            want[r, k] = d
+    assert np.array_equal(rs, want)
+    fix = s.fix_dofs()
+    for d in range(m.n_sub):
+        assert np.array_equal(fix[d], h.l2g[d][h.fix[d]])
