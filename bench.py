@@ -538,6 +538,19 @@ def run_serving(hb, local, n_req, fp64_requests=None):
     }
 
 
+def soft(fn, *args, dist=None):
+    """Run one of the measurements beside the headline; on one process an
+    exception there is reported in its field instead of losing the headline
+    line.  Under several ranks it propagates, so that no rank leaves the
+    others waiting in a collective that it skips."""
+    if dist is not None:
+        return fn(*args)
+    try:
+        return fn(*args)
+    except Exception as e:          # noqa: BLE001  (any failure of a side measurement)
+        return {"error": f"{type(e).__name__}: {e}"[:400]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -643,18 +656,18 @@ def main():
     n_lambda = st.n_lambda
     s.close()
     full = args.workload == "full"
-    cube = None if (args.no_cube or not full) else run_cube(hb, local, dist, min(args.steps, 5))
-    mixed = None if args.no_mixed else run_mixed(hb, local, dist, None if full else REDUCED.get(
-        args.workload if args.workload in ("small", "mid") else "mid"))
+    cube = None if (args.no_cube or not full) else soft(run_cube, hb, local, dist, min(args.steps, 5), dist=dist)
+    mixed = None if args.no_mixed else soft(run_mixed, hb, local, dist, None if full else REDUCED.get(
+        args.workload if args.workload in ("small", "mid") else "mid"), dist=dist)
     serving = None
     if args.serve_requests > 0 and full:
         barrier(dist)
-        serving = run_serving(hb, local, args.serve_requests)
+        serving = soft(run_serving, hb, local, args.serve_requests, dist=dist)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return 0
-    cpu = None if args.no_cpu_baseline else cpu_baseline_small(hb, local)
+    cpu = None if args.no_cpu_baseline else soft(cpu_baseline_small, hb, local)
     peak, peak_kind = peaks()
     achieved = prof.symv_F_bytes / (prof.symv_F_ms * 1e-3) / 1e9
     ndof = 3 * mesh.n_nodes

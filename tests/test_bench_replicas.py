@@ -72,3 +72,16 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
     class A:
         warmup, steps = 3, 1
     assert bench.run_reference(A()) == 0 and not called
+
+
+def test_a_failing_side_measurement_keeps_the_line():
+    sys.path.insert(0, ROOT)
+    import bench
+
+    def boom(x):
+        raise RuntimeError("no device %d" % x)
+
+    assert bench.soft(lambda a, b: a + b, 2, 3) == 5
+    assert bench.soft(boom, 7) == {"error": "RuntimeError: no device 7"}
+    with pytest.raises(RuntimeError):
+        bench.soft(boom, 7, dist=object())          # several ranks: the failure propagates
